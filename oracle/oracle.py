@@ -1,0 +1,223 @@
+"""ctypes bindings for the CPU oracle (liboracle.so) -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and the benchmark's CPU-baseline leg may
+import this module; it is the checker, never the product path.  Arrays are numpy
+int64 in the [poly][limb][N] layout described in ckks_oracle.h.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_lib = None
+
+
+def build() -> None:
+    """Compile liboracle.so with the committed Makefile (gcc only)."""
+    import subprocess
+
+    subprocess.run(["make", "-s", "-C", _HERE, "liboracle.so"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(_LIB_PATH)
+        L = _lib
+        L.oracle_mont_mult.restype = ctypes.c_int64
+        L.oracle_mont_mult.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_uint64, ctypes.c_uint64]
+        L.oracle_mont_exit.restype = ctypes.c_int64
+        L.oracle_mont_exit.argtypes = [ctypes.c_int64, ctypes.c_uint64, ctypes.c_uint64]
+        L.oracle_calculate_k.restype = ctypes.c_uint64
+        L.oracle_calculate_k.argtypes = [ctypes.c_uint64]
+        L.oracle_find_root.restype = ctypes.c_int64
+        L.oracle_find_root.argtypes = [ctypes.c_int64, ctypes.c_int]
+        for name in ("oracle_ntt_limb", "oracle_intt_limb"):
+            f = getattr(L, name)
+            f.restype = None
+            f.argtypes = [_i64p, _i64p, _i64p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
+        L.oracle_ctx_new.restype = ctypes.c_void_p
+        L.oracle_ctx_new.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _u64p]
+        L.oracle_ctx_free.restype = None
+        L.oracle_ctx_free.argtypes = [ctypes.c_void_p]
+        L.oracle_ctx_tables.restype = None
+        L.oracle_ctx_tables.argtypes = [ctypes.c_void_p, _u64p, _i64p, _i64p, _i64p, _i64p]
+        L.oracle_chain_count.restype = ctypes.c_int
+        L.oracle_chain_count.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.oracle_partition_count.restype = ctypes.c_int
+        L.oracle_partition_count.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        for name in ("oracle_to_ntt", "oracle_to_intt"):
+            f = getattr(L, name)
+            f.restype = None
+            f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _i64p, _i64p]
+        L.oracle_tensor.restype = None
+        L.oracle_tensor.argtypes = [ctypes.c_void_p, ctypes.c_int, _i64p, _i64p, _i64p]
+        L.oracle_relinearize.restype = None
+        L.oracle_relinearize.argtypes = [ctypes.c_void_p, ctypes.c_int, _i64p, ctypes.c_int, _i64p, _i64p]
+        L.oracle_key_switch.restype = None
+        L.oracle_key_switch.argtypes = [ctypes.c_void_p, ctypes.c_int, _i64p, ctypes.c_int, _i64p, _i64p]
+        L.oracle_rescale.restype = None
+        L.oracle_rescale.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _i64p, _i64p]
+        L.oracle_mult_relin_rescale.restype = None
+        L.oracle_mult_relin_rescale.argtypes = [ctypes.c_void_p, ctypes.c_int, _i64p, _i64p,
+                                                ctypes.c_int, _i64p, _i64p]
+        L.oracle_permutation_and_sign.restype = None
+        L.oracle_permutation_and_sign.argtypes = [_i32p, _i32p, ctypes.c_int, ctypes.c_int]
+        L.oracle_ntt_permutation.restype = None
+        L.oracle_ntt_permutation.argtypes = [_i32p, ctypes.c_int, ctypes.c_int]
+    return _lib
+
+
+def _p(a: np.ndarray, t=_i64p):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(t)
+
+
+def mont_mult(a: int, b: int, q: int, k: int) -> int:
+    return lib().oracle_mont_mult(a, b, q, k)
+
+
+def mont_exit(a: int, q: int, k: int) -> int:
+    return lib().oracle_mont_exit(a, q, k)
+
+
+def calculate_k(q: int) -> int:
+    return lib().oracle_calculate_k(q)
+
+
+def find_root(q: int, n: int) -> int:
+    return lib().oracle_find_root(q, n)
+
+
+def ntt_limb(x, root, q, k):
+    x = np.ascontiguousarray(x, dtype=np.int64)
+    root = np.ascontiguousarray(root, dtype=np.int64)
+    y = np.empty_like(x)
+    n = x.shape[0]
+    lib().oracle_ntt_limb(_p(x), _p(y), _p(root), q, k, n, n.bit_length() - 1)
+    return y
+
+
+def intt_limb(x, root_inverse, q, k):
+    x = np.ascontiguousarray(x, dtype=np.int64)
+    root_inverse = np.ascontiguousarray(root_inverse, dtype=np.int64)
+    y = np.empty_like(x)
+    n = x.shape[0]
+    lib().oracle_intt_limb(_p(x), _p(y), _p(root_inverse), q, k, n, n.bit_length() - 1)
+    return y
+
+
+def permutation_and_sign(n: int, delta: int):
+    perm = np.empty(n, dtype=np.int32)
+    sign = np.empty(n, dtype=np.int32)
+    lib().oracle_permutation_and_sign(_p(perm, _i32p), _p(sign, _i32p), n, delta)
+    return perm, sign
+
+
+def ntt_permutation(n: int, delta: int):
+    perm = np.empty(n, dtype=np.int32)
+    lib().oracle_ntt_permutation(_p(perm, _i32p), n, delta)
+    return perm
+
+
+class Context:
+    """The oracle's view of one prime chain (all primes, specials last)."""
+
+    def __init__(self, log_n: int, q, special_prime_count: int):
+        self.log_n = log_n
+        self.n = 1 << log_n
+        self.q = np.ascontiguousarray(np.asarray(q, dtype=np.uint64))
+        self.prime_count = len(self.q)
+        self.special_prime_count = special_prime_count
+        self.chain_count = self.prime_count - special_prime_count
+        self._ctx = lib().oracle_ctx_new(log_n, self.prime_count, special_prime_count,
+                                         _p(self.q, _u64p))
+
+    def __del__(self):
+        if getattr(self, "_ctx", None) and _lib is not None:
+            _lib.oracle_ctx_free(self._ctx)
+            self._ctx = None
+
+    def tables(self):
+        P, n = self.prime_count, self.n
+        k = np.empty(P, dtype=np.uint64)
+        r2 = np.empty(P, dtype=np.int64)
+        ninv = np.empty(P, dtype=np.int64)
+        root = np.empty((P, n - 1), dtype=np.int64)
+        rinv = np.empty((P, n - 1), dtype=np.int64)
+        lib().oracle_ctx_tables(self._ctx, _p(k, _u64p), _p(r2), _p(ninv), _p(root), _p(rinv))
+        return dict(k=k, r_squared=r2, n_inverse=ninv, root=root, root_inverse=rinv)
+
+    def chains(self, moduli_id: int) -> int:
+        return self.chain_count - moduli_id
+
+    def partition_count(self, moduli_id: int) -> int:
+        return lib().oracle_partition_count(self._ctx, moduli_id)
+
+    def to_ntt(self, moduli_id, x):
+        x = np.ascontiguousarray(x, dtype=np.int64)
+        y = np.empty_like(x)
+        polys = x.shape[0] if x.ndim == 3 else 1
+        chains = x.shape[-2]
+        lib().oracle_to_ntt(self._ctx, moduli_id, chains, polys, _p(x), _p(y))
+        return y
+
+    def to_intt(self, moduli_id, x):
+        x = np.ascontiguousarray(x, dtype=np.int64)
+        y = np.empty_like(x)
+        polys = x.shape[0] if x.ndim == 3 else 1
+        chains = x.shape[-2]
+        lib().oracle_to_intt(self._ctx, moduli_id, chains, polys, _p(x), _p(y))
+        return y
+
+    def tensor(self, moduli_id, a, b):
+        a = np.ascontiguousarray(a, dtype=np.int64)
+        b = np.ascontiguousarray(b, dtype=np.int64)
+        L = self.chains(moduli_id)
+        out = np.empty((3, L, self.n), dtype=np.int64)
+        lib().oracle_tensor(self._ctx, moduli_id, _p(a), _p(b), _p(out))
+        return out
+
+    def relinearize(self, moduli_id, ct, key_moduli_id, key):
+        ct = np.ascontiguousarray(ct, dtype=np.int64)
+        key = np.ascontiguousarray(key, dtype=np.int64)
+        L = self.chains(moduli_id)
+        out = np.empty((2, L, self.n), dtype=np.int64)
+        lib().oracle_relinearize(self._ctx, moduli_id, _p(ct), key_moduli_id, _p(key), _p(out))
+        return out
+
+    def key_switch(self, moduli_id, x, key_moduli_id, key):
+        x = np.ascontiguousarray(x, dtype=np.int64)
+        key = np.ascontiguousarray(key, dtype=np.int64)
+        L = self.chains(moduli_id)
+        out = np.empty((2, L, self.n), dtype=np.int64)
+        lib().oracle_key_switch(self._ctx, moduli_id, _p(x), key_moduli_id, _p(key), _p(out))
+        return out
+
+    def rescale(self, moduli_id, x):
+        x = np.ascontiguousarray(x, dtype=np.int64)
+        polys = x.shape[0]
+        L = self.chains(moduli_id)
+        y = np.empty((polys, L - 1, self.n), dtype=np.int64)
+        lib().oracle_rescale(self._ctx, moduli_id, polys, _p(x), _p(y))
+        return y
+
+    def mult_relin_rescale(self, moduli_id, a, b, key_moduli_id, key):
+        a = np.ascontiguousarray(a, dtype=np.int64)
+        b = np.ascontiguousarray(b, dtype=np.int64)
+        key = np.ascontiguousarray(key, dtype=np.int64)
+        L = self.chains(moduli_id)
+        out = np.empty((2, L - 2, self.n), dtype=np.int64)
+        lib().oracle_mult_relin_rescale(self._ctx, moduli_id, _p(a), _p(b), key_moduli_id,
+                                        _p(key), _p(out))
+        return out

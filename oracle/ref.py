@@ -1,0 +1,257 @@
+"""ctypes bindings for the compiled reference (oracle/_ref/libdesilo_ref.so).
+
+TEST INFRASTRUCTURE ONLY.  The library is the reference's own C++ sources built
+by ``make -C oracle ref`` together with ref_harness.cpp.  It is optional: callers
+use :func:`available` and skip when it is absent.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_ref", "libdesilo_ref.so")
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_lib = None
+
+# SchemePreset values (engine/scheme_preset.h)
+CKKS_40_60_DEFAULT = 1
+CKKS_54_60_BOOTSTRAP = 2
+CKKS_40_60_DEFAULT_ENGINE_TEST = 3
+CKKS_54_60_BOOTSTRAP_ENGINE_TEST = 4
+
+
+def available() -> bool:
+    return os.path.exists(_LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = ctypes.CDLL(_LIB_PATH)
+        L = _lib
+        vp, ci, cd = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        sig = {
+            "ref_cached_primes": (ci, [ci, ci, _u64p, ci]),
+            "ref_engine_new": (vp, [ci, ci, ci, ci, ci, ci]),
+            "ref_engine_free": (None, [vp]),
+            "ref_engine_seed": (None, [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint8)]),
+            "ref_engine_info": (None, [vp, ctypes.POINTER(ci)]),
+            "ref_moduli_id": (ci, [vp, ci]),
+            "ref_chain_count": (ci, [vp, ci, ci]),
+            "ref_partition_count": (ci, [vp, ci, ci]),
+            "ref_tables": (ci, [vp, _u64p, _u64p, _i64p, _i64p, _i64p, _i64p]),
+            "ref_key_switch_tables": (None, [vp, _i64p, _i64p, _i64p]),
+            "ref_text_new": (vp, [vp, ci, ci, ci, ci, ctypes.c_longdouble, _i64p]),
+            "ref_key_new": (vp, [vp, ci, ci, ci, _i64p]),
+            "ref_handle_free": (None, [vp]),
+            "ref_handle_info": (ctypes.c_longdouble, [vp, ctypes.POINTER(ci)]),
+            "ref_handle_dump": (None, [vp, vp, _i64p]),
+            "ref_create_secret_key": (vp, [vp, ci]),
+            "ref_create_secret_key_from": (vp, [vp, _i64p, ci]),
+            "ref_create_public_key": (vp, [vp, vp, ci]),
+            "ref_create_relinearization_key": (vp, [vp, vp, ci]),
+            "ref_create_fixed_rotation_key": (vp, [vp, vp, ci, ci]),
+            "ref_create_conjugation_key": (vp, [vp, vp, ci]),
+            "ref_core_to_ntt": (vp, [vp, vp]),
+            "ref_core_to_intt": (vp, [vp, vp]),
+            "ref_core_tensor": (vp, [vp, vp, vp]),
+            "ref_core_relinearize": (vp, [vp, vp, vp]),
+            "ref_core_rescale": (vp, [vp, vp]),
+            "ref_core_switch_key": (vp, [vp, vp, vp]),
+            "ref_engine_multiply": (vp, [vp, vp, vp, vp]),
+            "ref_engine_relinearize": (vp, [vp, vp, vp]),
+            "ref_engine_rescale": (vp, [vp, vp]),
+            "ref_engine_rotate": (vp, [vp, vp, vp]),
+            "ref_engine_conjugate": (vp, [vp, vp, vp]),
+            "ref_engine_encode": (vp, [vp, ctypes.POINTER(cd), ctypes.POINTER(cd), ci, ci]),
+            "ref_engine_decode": (ci, [vp, vp, ctypes.POINTER(cd), ctypes.POINTER(cd)]),
+            "ref_engine_encrypt": (vp, [vp, vp, vp]),
+            "ref_engine_decrypt": (vp, [vp, vp, vp]),
+            "ref_bench_mult_relin_rescale": (cd, [ci, ci, ci, ci, ci, ci, ctypes.POINTER(cd)]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+    return _lib
+
+
+def cached_primes(kind: int, n: int):
+    out = np.zeros(256, dtype=np.uint64)
+    cnt = lib().ref_cached_primes(kind, n, out.ctypes.data_as(_u64p), 256)
+    return out[:cnt].copy()
+
+
+class Handle:
+    """A reference object (key, ciphertext, plaintext) owned by the harness."""
+
+    def __init__(self, engine: "Engine", ptr):
+        if not ptr:
+            raise RuntimeError("reference call failed")
+        self.engine = engine
+        self.ptr = ptr
+
+    def __del__(self):
+        if getattr(self, "ptr", None) and _lib is not None:
+            _lib.ref_handle_free(self.ptr)
+            self.ptr = None
+
+    def info(self):
+        info = (ctypes.c_int * 6)()
+        scale = lib().ref_handle_info(self.ptr, info)
+        kind, flag, moduli_id, level, polys, chains = list(info)
+        return dict(kind=kind, flag=flag, moduli_id=moduli_id, level=level, polys=polys,
+                    chains=chains, scale=scale)
+
+    def limbs(self) -> np.ndarray:
+        i = self.info()
+        out = np.empty((i["polys"], i["chains"], self.engine.n), dtype=np.int64)
+        lib().ref_handle_dump(self.engine.ptr, self.ptr, out.ctypes.data_as(_i64p))
+        return out
+
+
+class Engine:
+    def __init__(self, log_n=14, special_prime_count=1, max_level=-1,
+                 preset=CKKS_40_60_DEFAULT, log_slot=-1, threads=1):
+        self.ptr = lib().ref_engine_new(log_n, log_slot, special_prime_count, max_level, preset,
+                                        threads)
+        if not self.ptr:
+            raise ValueError("reference rejected the config")
+        info = (ctypes.c_int * 10)()
+        lib().ref_engine_info(self.ptr, info)
+        (self.n, self.chain_count, self.prime_count, self.full_level, self.max_level,
+         self.max_ks_level, self.slot_count, self.special_prime_count, self.scale_bits,
+         self.one_more_level) = list(info)
+
+    def __del__(self):
+        if getattr(self, "ptr", None) and _lib is not None:
+            _lib.ref_engine_free(self.ptr)
+            self.ptr = None
+
+    def seed(self, seed8, nonce2):
+        s = (ctypes.c_uint32 * 8)(*seed8)
+        n = (ctypes.c_uint8 * 2)(*nonce2)
+        lib().ref_engine_seed(self.ptr, s, n)
+
+    def moduli_id(self, level):
+        return lib().ref_moduli_id(self.ptr, level)
+
+    def chains(self, moduli_id, include_special=False):
+        return lib().ref_chain_count(self.ptr, moduli_id, int(include_special))
+
+    def partition_count(self, moduli_id, key_moduli_id):
+        return lib().ref_partition_count(self.ptr, moduli_id, key_moduli_id)
+
+    def tables(self):
+        P, n = self.prime_count, self.n
+        q = np.empty(P, dtype=np.uint64)
+        k = np.empty(P, dtype=np.uint64)
+        r2 = np.empty(P, dtype=np.int64)
+        ninv = np.empty(P, dtype=np.int64)
+        root = np.empty((P, n - 1), dtype=np.int64)
+        rinv = np.empty((P, n - 1), dtype=np.int64)
+        lib().ref_tables(self.ptr, q.ctypes.data_as(_u64p), k.ctypes.data_as(_u64p),
+                         r2.ctypes.data_as(_i64p), ninv.ctypes.data_as(_i64p),
+                         root.ctypes.data_as(_i64p), rinv.ctypes.data_as(_i64p))
+        return dict(q=q, k=k, r_squared=r2, n_inverse=ninv, root=root, root_inverse=rinv)
+
+    def text(self, limbs, moduli_id, flag=0, kind=4, scale=1.0):
+        limbs = np.ascontiguousarray(limbs, dtype=np.int64)
+        return Handle(self, lib().ref_text_new(self.ptr, kind, flag, moduli_id, limbs.shape[0],
+                                               scale, limbs.ctypes.data_as(_i64p)))
+
+    def relin_key(self, limbs, moduli_id):
+        limbs = np.ascontiguousarray(limbs, dtype=np.int64)
+        return Handle(self, lib().ref_key_new(self.ptr, 3, moduli_id, limbs.shape[0],
+                                              limbs.ctypes.data_as(_i64p)))
+
+    def switching_key(self, limbs, moduli_id):
+        limbs = np.ascontiguousarray(limbs, dtype=np.int64)
+        return Handle(self, lib().ref_key_new(self.ptr, 8, moduli_id, limbs.shape[0],
+                                              limbs.ctypes.data_as(_i64p)))
+
+    def _h(self, ptr):
+        return Handle(self, ptr)
+
+    # keys
+    def create_secret_key(self, level=-1):
+        return self._h(lib().ref_create_secret_key(self.ptr, level))
+
+    def create_public_key(self, sk, level=-1):
+        return self._h(lib().ref_create_public_key(self.ptr, sk.ptr, level))
+
+    def create_relinearization_key(self, sk, level=-1):
+        return self._h(lib().ref_create_relinearization_key(self.ptr, sk.ptr, level))
+
+    def create_fixed_rotation_key(self, sk, delta, level=-1):
+        return self._h(lib().ref_create_fixed_rotation_key(self.ptr, sk.ptr, delta, level))
+
+    def create_conjugation_key(self, sk, level=-1):
+        return self._h(lib().ref_create_conjugation_key(self.ptr, sk.ptr, level))
+
+    # core ops
+    def core_to_ntt(self, h):
+        return self._h(lib().ref_core_to_ntt(self.ptr, h.ptr))
+
+    def core_to_intt(self, h):
+        return self._h(lib().ref_core_to_intt(self.ptr, h.ptr))
+
+    def core_tensor(self, a, b):
+        return self._h(lib().ref_core_tensor(self.ptr, a.ptr, b.ptr))
+
+    def core_relinearize(self, ct, rk):
+        return self._h(lib().ref_core_relinearize(self.ptr, ct.ptr, rk.ptr))
+
+    def core_rescale(self, ct):
+        return self._h(lib().ref_core_rescale(self.ptr, ct.ptr))
+
+    def core_switch_key(self, ct, ksk):
+        return self._h(lib().ref_core_switch_key(self.ptr, ct.ptr, ksk.ptr))
+
+    # engine ops
+    def multiply(self, a, b, rk=None):
+        return self._h(lib().ref_engine_multiply(self.ptr, a.ptr, b.ptr, rk.ptr if rk else None))
+
+    def relinearize(self, a, rk):
+        return self._h(lib().ref_engine_relinearize(self.ptr, a.ptr, rk.ptr))
+
+    def rescale(self, a):
+        return self._h(lib().ref_engine_rescale(self.ptr, a.ptr))
+
+    def rotate(self, a, fixed_key):
+        return self._h(lib().ref_engine_rotate(self.ptr, a.ptr, fixed_key.ptr))
+
+    def conjugate(self, a, ck):
+        return self._h(lib().ref_engine_conjugate(self.ptr, a.ptr, ck.ptr))
+
+    def encode(self, values, level=-1):
+        values = np.asarray(values, dtype=np.complex128)
+        re = np.ascontiguousarray(values.real)
+        im = np.ascontiguousarray(values.imag)
+        cd = ctypes.POINTER(ctypes.c_double)
+        return self._h(lib().ref_engine_encode(self.ptr, re.ctypes.data_as(cd),
+                                               im.ctypes.data_as(cd), len(values), level))
+
+    def decode(self, pt):
+        re = np.empty(self.slot_count)
+        im = np.empty(self.slot_count)
+        cd = ctypes.POINTER(ctypes.c_double)
+        cnt = lib().ref_engine_decode(self.ptr, pt.ptr, re.ctypes.data_as(cd), im.ctypes.data_as(cd))
+        return (re + 1j * im)[:cnt]
+
+    def encrypt(self, pt, key):
+        return self._h(lib().ref_engine_encrypt(self.ptr, pt.ptr, key.ptr))
+
+    def decrypt(self, ct, sk):
+        return self._h(lib().ref_engine_decrypt(self.ptr, ct.ptr, sk.ptr))
+
+
+def bench_mult_relin_rescale(log_n, special_prime_count, level, threads, warmup, steps):
+    times = (ctypes.c_double * max(steps, 1))()
+    med = lib().ref_bench_mult_relin_rescale(log_n, special_prime_count, level, threads, warmup,
+                                             steps, times)
+    return med, list(times)[:steps]
