@@ -1,0 +1,397 @@
+"""Benchmark: CKKS HMult + relinearize + rescale throughput on B200.
+
+Workload (one "step"): B independent pairs of fresh ciphertexts at N = 2^16 with 10
+special primes, both at the maximum key-switching level (28 limbs), each pair going
+through the reference's engine.multiply(a, b, relinearization_key) followed by
+engine.rescale(.)  -- lazy rescale of both inputs to 27 limbs, NTT, tensor,
+relinearize (hybrid key switching with dnum = 3 partitions [7, 10, 10]) and the
+final rescale to 26 limbs.  Inputs are seeded uniform residues with a seeded random
+relinearization key (operation time does not depend on the values).
+
+  value : ciphertexts/s with inputs resident in HBM, device time (CUDA events on
+          the engine's stream) over exactly K steps, max over ranks.
+  e2e   : the same through the C ABI with pinned host buffers: every step uploads
+          its inputs, runs the op and downloads the result.
+  roofline : the dominant kernel family of the timed region, its algorithmic
+          bytes per launch over its event-timed duration, against the measured
+          HBM copy bandwidth (MEASURED_PEAKS.json).
+  cpu_baseline : the reference's own CPU implementation (oracle/_ref, all host
+          threads) on a bounded sample of the same operation.
+
+Multi-GPU: replicas -- every rank runs the same per-GPU workload on its own GPU
+with no data exchange ("scaling": "weak"); torch.distributed is used only for the
+barrier and the max-over-ranks timing reduction.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B]
+       python bench.py --impl reference ...
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+sys.path.insert(0, os.path.join(HERE, "tests", "golden"))
+
+LOG_N = 16
+SPECIAL = 10
+METRIC = "HMult+relin+rescale ct/s at N=2^16 (K=10, dnum=3, 28-limb inputs)"
+WORKLOAD = ("engine.multiply(ct_a, ct_b, relinearization_key) + engine.rescale, "
+            "N=2^16, 10 special primes, inputs at level 26 (28 limbs), dnum=3")
+
+
+# ----------------------------------------------------------------- helpers --
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def aggregate(elapsed_ms: float, units: float, world: int, backend: str | None):
+    """Max elapsed and summed units over ranks (identity on one process)."""
+    if world <= 1 or backend is None:
+        return elapsed_ms, units
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if backend == "nccl" else "cpu"
+    t = torch.tensor([elapsed_ms], dtype=torch.float64, device=dev)
+    u = torch.tensor([units], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(u.item())
+
+
+def measured_peaks():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._thread = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([c.strip() for c in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._thread = threading.Thread(target=self._run, daemon=True)
+        self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread:
+            self._thread.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for name, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def kernel_bytes(L: int, E: int, dnum: int, n: int) -> dict:
+    """Algorithmic HBM bytes per timed launch of each kernel family at the
+    relinearize level (L limbs, E = L + K extended limbs): each limb operand read or
+    written once, twiddle tables excluded."""
+    limb = 8 * n
+    return {
+        "rescale": (2 * (L + 1) + 2 * L) * limb,          # 2 polys, L+1 -> L limbs
+        "to_ntt": 2 * 4 * L * limb,                         # 4 polys in and out
+        "tensor_to_intt": (4 * L + 3 * L) * limb,           # 4 NTT polys in, 3 out
+        "mixed_radix": 2 * L * limb,                        # digits of poly 2
+        "mod_up_ntt": (L + dnum * E) * limb,                # digits in, extended out
+        "key_inner_product": (3 * dnum * E + 2 * E) * limb, # ext + 2 key polys, 2 out
+        "mod_down_intt": 2 * 2 * E * limb,                  # 2 polys in and out
+        "mod_down_epilogue": (2 * E + 2 * L + 2 * (L - 1)) * limb,
+    }
+
+
+# ------------------------------------------------------------- reference arm --
+
+def run_reference(args, rank: int):
+    """The reference's own CPU implementation of the path (oracle/_ref), all host
+    threads; each step is one HMult+relin+rescale on the same config."""
+    if rank != 0:
+        return 0
+    from oracle import ref
+
+    threads = os.cpu_count() or 1
+    line = {"impl": "reference", "metric": METRIC, "unit": "ct/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic (seeded uniform complex slots, fresh keys)",
+            "config": {"workload": WORKLOAD, "threads": threads}}
+    if not ref.available():
+        from oracle import oracle
+        import numpy as np
+        from inputs import case_inputs
+
+        # The compiled reference is absent: time the C restatement (single thread).
+        from fhe_b200 import _lib
+        import ctypes
+
+        cfg = _lib.FheConfig(LOG_N, -1, SPECIAL, -1, 1)
+        info = _lib.FheEngineInfo()
+        qbuf = (ctypes.c_uint64 * 64)()
+        _lib.check(_lib.load().fhe_parameters_query(ctypes.byref(cfg), ctypes.byref(info), qbuf, 64))
+        q = np.array(qbuf[: info.prime_count], dtype=np.uint64)
+        ctx = oracle.Context(LOG_N, q, SPECIAL)
+        mid = info.chain_count - 2 - info.max_key_switching_level
+        a, b, _, key = case_inputs(5, q, 1 << LOG_N, mid, SPECIAL)
+        times = []
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            ctx.mult_relin_rescale(mid, a, b, mid, key)
+            if i >= args.warmup:
+                times.append((time.perf_counter() - t0) * 1e3)
+        kind, cores = "port", 1
+    else:
+        _, times = ref.bench_mult_relin_rescale(LOG_N, SPECIAL, -1, threads, args.warmup, args.steps)
+        kind, cores = "reference", threads
+    ms = sum(times) / len(times)
+    value = 1000.0 / ms
+    line.update({"value": value, "ms_per_step": ms,
+                 "cpu_baseline": {"value": value, "unit": "ct/s", "cores": cores, "kind": kind,
+                                  "sample": f"{args.steps} ops after {args.warmup} warm-up"},
+                 "e2e": {"value": value, "unit": "ct/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0}})
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline_sample():
+    """Bounded CPU sample for the headline line (rank 0, one GPU only)."""
+    try:
+        from oracle import ref
+
+        if ref.available():
+            threads = os.cpu_count() or 1
+            _, times = ref.bench_mult_relin_rescale(LOG_N, SPECIAL, -1, threads, 1, 3)
+            ms = sum(times) / len(times)
+            return {"value": 1000.0 / ms, "unit": "ct/s", "cores": threads, "kind": "reference",
+                    "sample": "3 HMult+relin+rescale ops (after 1 warm-up) through the reference "
+                              "CKKSEngine with CPU_PARALLEL, keygen excluded"}
+    except Exception as exc:  # the baseline must not sink the GPU line
+        return {"value": None, "unit": "ct/s", "cores": 0, "kind": "reference",
+                "sample": f"failed: {exc}"}
+    return {"value": None, "unit": "ct/s", "cores": 0, "kind": "port",
+            "sample": "reference library not built on this host"}
+
+
+# -------------------------------------------------------------------- main --
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=16, help="ciphertext pairs per step")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    rank, world, local = dist_env()
+
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import numpy as np
+    import torch
+
+    backend = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        backend = "nccl"
+    else:
+        torch.cuda.set_device(0)
+
+    from fhe_b200 import Engine, NTT_FORM, INCLUDE_SPECIAL, RELINEARIZATION_KEY
+    from inputs import uniform_limbs
+
+    eng = Engine(log_coeff_count=LOG_N, special_prime_count=SPECIAL)
+    stream = torch.cuda.current_stream()
+    eng.set_stream(stream.cuda_stream)
+    n = eng.coeff_count
+    level = eng.max_key_switching_level
+    mid = eng.moduli_id(level)
+    L0 = eng.chains(mid)                      # 28 input limbs
+    L = L0 - 1                                # 27 limbs after the lazy rescale
+    E = L + SPECIAL
+    dnum = (L + SPECIAL - 1) // SPECIAL
+    q_in = eng.moduli[mid:mid + L0]
+    rng = np.random.default_rng(1234 + rank)
+    key = uniform_limbs(rng, eng.moduli[mid:], 2 * eng.partition_count(mid), n)
+    rk = eng.upload(key, mid, NTT_FORM | INCLUDE_SPECIAL, RELINEARIZATION_KEY)
+    B = args.batch
+    # B distinct input pairs (B * 58.7 MB of inputs, larger than the 126 MB L2 for B >= 3)
+    pairs = []
+    for _ in range(B):
+        a = eng.upload(uniform_limbs(rng, q_in, 2, n), mid)
+        b = eng.upload(uniform_limbs(rng, q_in, 2, n), mid)
+        pairs.append((a, b))
+
+    def step():
+        outs = [eng.multiply_relinearize_rescale(a, b, rk) for a, b in pairs]
+        for o in outs:
+            o.free()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if backend:
+        torch.distributed.barrier()
+    eng.profile_reset()
+    eng.set_profiling(True)
+    launches0 = Engine.kernel_launch_count()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        stop.record(stream)
+        torch.cuda.synchronize()
+    launches = Engine.kernel_launch_count() - launches0
+    eng.set_profiling(False)
+    prof = eng.profile()
+    elapsed = start.elapsed_time(stop)
+    if backend:
+        torch.distributed.barrier()
+    elapsed_max, units = aggregate(elapsed, float(B * args.steps), world, backend)
+    value = units / (elapsed_max / 1e3)
+
+    # ---- roofline of the dominant kernel family (event-timed in the region above)
+    bytes_per = kernel_bytes(L, E, dnum, n)
+    dominant = max(prof, key=lambda k: prof[k][1]) if prof else None
+    peak, peak_kind = measured_peaks()
+    roofline = None
+    if dominant:
+        cnt, ms = prof[dominant]
+        avg_ms = ms / cnt
+        achieved = bytes_per.get(dominant, 0) / (avg_ms / 1e3) / 1e9
+        traffic = None
+        tpath = os.path.join(HERE, "profiles", "traffic.json")
+        if os.path.exists(tpath):
+            traffic = json.load(open(tpath)).get(dominant)
+        roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
+                    "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                    "peak_source": peak_kind, "avg_launch_ms": avg_ms,
+                    "algorithmic_bytes_per_launch": bytes_per.get(dominant),
+                    "share_of_timed_region": ms / elapsed,
+                    "kernel_ms_per_step": {k: v[1] / args.steps for k, v in prof.items()}}
+
+    # ---- end to end through the C ABI with pinned host buffers
+    in_words = 2 * L0 * n
+    out_words = 2 * (L - 1) * n
+    pin_in = torch.empty((B, 2, in_words), dtype=torch.int64, pin_memory=True)
+    pin_out = torch.empty((B, out_words), dtype=torch.int64, pin_memory=True)
+    for i in range(B):
+        pin_in[i, 0].copy_(torch.from_numpy(uniform_limbs(rng, q_in, 2, n).reshape(-1)))
+        pin_in[i, 1].copy_(torch.from_numpy(uniform_limbs(rng, q_in, 2, n).reshape(-1)))
+
+    def e2e_step():
+        outs = []
+        for i in range(B):
+            a = eng.upload_from_pointer(pin_in[i, 0].data_ptr(), mid, 2)
+            b = eng.upload_from_pointer(pin_in[i, 1].data_ptr(), mid, 2)
+            o = eng.multiply_relinearize_rescale(a, b, rk)
+            eng.download_to_pointer(o, pin_out[i].data_ptr(), wait=False)
+            outs.append((a, b, o))
+        eng.synchronize()
+        for t in outs:
+            for d in t:
+                d.free()
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if backend:
+        torch.distributed.barrier()
+    e_steps = max(1, min(args.steps, 5))
+    s2, t2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s2.record(stream)
+    for _ in range(e_steps):
+        e2e_step()
+    t2.record(stream)
+    torch.cuda.synchronize()
+    e_elapsed, e_units = aggregate(s2.elapsed_time(t2), float(B * e_steps), world, backend)
+    e2e_value = e_units / (e_elapsed / 1e3)
+
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline_sample()
+        line = {
+            "metric": METRIC, "value": value, "unit": "ct/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": elapsed_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic (seeded uniform residues, random relinearization key)",
+            "config": {"workload": WORKLOAD, "pairs_per_step": B, "log_n": LOG_N,
+                       "special_prime_count": SPECIAL, "input_limbs": L0,
+                       "relinearize_limbs": L, "dnum": dnum, "parallelism": f"replicas{world}",
+                       "l2": f"inputs larger than L2 ({B} pairs x {2 * 2 * L0 * n * 8 / 1e6:.1f} MB)"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "ct/s",
+                    "h2d_bytes_per_step": B * 2 * in_words * 8,
+                    "d2h_bytes_per_step": B * out_words * 8},
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    del pairs, rk
+    eng.close()
+    if backend:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,121 @@
+"""Loader and ctypes signatures of the engine's C ABI (include/fhe_b200.h).
+
+The shared library is built in-tree by ``python -m fhe_b200.build``.  There is no
+fallback: if it is missing, importing the engine raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfhe_b200.so")
+
+FHE_OK = 0
+STATUS_NAMES = {
+    -1: "FHE_ERR_INVALID_ARGUMENT",
+    -2: "FHE_ERR_RUNTIME",
+    -3: "FHE_ERR_CUDA",
+    -4: "FHE_ERR_OUT_OF_MEMORY",
+    -5: "FHE_ERR_NULL_HANDLE",
+    -6: "FHE_ERR_UNSUPPORTED",
+}
+
+# Every symbol include/fhe_b200.h declares, with (restype, argtypes).
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_pp = ctypes.POINTER(ctypes.c_void_p)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+
+
+class FheConfig(ctypes.Structure):
+    _fields_ = [("log_coeff_count", ctypes.c_int), ("log_slot_count", ctypes.c_int),
+                ("special_prime_count", ctypes.c_int), ("max_level", ctypes.c_int),
+                ("scheme_preset", ctypes.c_int)]
+
+
+class FheEngineInfo(ctypes.Structure):
+    _fields_ = [("coeff_count", ctypes.c_int), ("slot_count", ctypes.c_int),
+                ("chain_count", ctypes.c_int), ("prime_count", ctypes.c_int),
+                ("special_prime_count", ctypes.c_int), ("full_level", ctypes.c_int),
+                ("max_level", ctypes.c_int), ("max_key_switching_level", ctypes.c_int),
+                ("scale_bit_length", ctypes.c_int)]
+
+
+class FheDataInfo(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("flag", ctypes.c_int), ("moduli_id", ctypes.c_int),
+                ("level", ctypes.c_int), ("polys", ctypes.c_int), ("chains", ctypes.c_int),
+                ("delta", ctypes.c_int), ("ckks_scale", ctypes.c_longdouble)]
+
+
+SIGNATURES = {
+    "fhe_last_error": (ctypes.c_char_p, []),
+    "fhe_config_default": (None, [ctypes.POINTER(FheConfig)]),
+    "fhe_engine_set_profiling": (_i, [_vp, _i]),
+    "fhe_engine_profile_report": (_i, [_vp, ctypes.c_char_p, _i]),
+    "fhe_engine_profile_reset": (_i, [_vp]),
+    "fhe_kernel_launch_count": (ctypes.c_ulonglong, []),
+    "fhe_parameters_query":(_i, [ctypes.POINTER(FheConfig), ctypes.POINTER(FheEngineInfo),
+                                  ctypes.POINTER(ctypes.c_uint64), _i]),
+    "fhe_parameters_tables": (_i, [ctypes.POINTER(FheConfig), ctypes.POINTER(ctypes.c_uint64),
+                                   _i64p, _i64p, _i64p, _i64p]),
+    "fhe_engine_create": (_i, [ctypes.POINTER(FheConfig), _pp]),
+    "fhe_engine_destroy": (_i, [_vp]),
+    "fhe_engine_info_get": (_i, [_vp, ctypes.POINTER(FheEngineInfo)]),
+    "fhe_engine_moduli": (_i, [_vp, ctypes.POINTER(ctypes.c_uint64), _i]),
+    "fhe_engine_moduli_id": (_i, [_vp, _i, ctypes.POINTER(ctypes.c_int)]),
+    "fhe_engine_synchronize": (_i, [_vp]),
+    "fhe_engine_set_stream": (_i, [_vp, _vp]),
+    "fhe_data_upload": (_i, [_vp, _i, _i, _i, _i, ctypes.c_longdouble, _i64p, _pp]),
+    "fhe_data_download": (_i, [_vp, _i64p]),
+    "fhe_data_download_async": (_i, [_vp, _i64p]),
+    "fhe_data_info_get": (_i, [_vp, ctypes.POINTER(FheDataInfo)]),
+    "fhe_data_set_delta": (_i, [_vp, _i]),
+    "fhe_data_device_pointer": (_i, [_vp, ctypes.POINTER(_i64p)]),
+    "fhe_data_destroy": (_i, [_vp]),
+    "fhe_multiply": (_i, [_vp, _vp, _vp, _pp]),
+    "fhe_multiply_relinearize": (_i, [_vp, _vp, _vp, _vp, _pp]),
+    "fhe_relinearize": (_i, [_vp, _vp, _vp, _pp]),
+    "fhe_rescale": (_i, [_vp, _vp, _pp]),
+    "fhe_multiply_relinearize_rescale": (_i, [_vp, _vp, _vp, _vp, _pp]),
+    "fhe_to_ntt": (_i, [_vp, _vp, _pp]),
+    "fhe_to_intt": (_i, [_vp, _vp, _pp]),
+    "fhe_ntt_limbs": (_i, [_vp, _i64p, _i, _i, _i, ctypes.c_longlong, _i]),
+}
+
+_lib = None
+
+
+def load():
+    """Load libfhe_b200.so and bind every C-ABI symbol (raises if missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing; build it with `python -m fhe_b200.build`")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class FheError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+        self.message = message
+
+
+def check(status: int) -> None:
+    if status != FHE_OK:
+        msg = load().fhe_last_error().decode()
+        if status == -1:
+            raise FheInvalidArgument(status, msg)
+        raise FheError(status, msg)
+
+
+class FheInvalidArgument(FheError, ValueError):
+    pass

@@ -1,0 +1,345 @@
+// C ABI of the B200 CKKS engine (include/fhe_b200.h): handle wrappers, status
+// codes and the thread-local last-error message.  No function lets a C++
+// exception or a CUDA error escape.
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/fhe_b200.h"
+#include "engine.hpp"
+
+using fhe_b200::Data;
+using fhe_b200::Engine;
+
+struct fhe_engine {
+  Engine *impl;
+};
+
+struct fhe_data {
+  Data *impl;
+};
+
+namespace fhe_b200 {
+namespace {
+thread_local std::string g_last_error;
+}
+void set_last_error(const std::string &message) { g_last_error = message; }
+}  // namespace fhe_b200
+
+namespace {
+
+template <class F>
+int guarded(F &&f) {
+  try {
+    f();
+    fhe_b200::set_last_error("");
+    return FHE_OK;
+  } catch (const std::invalid_argument &e) {
+    fhe_b200::set_last_error(e.what());
+    return FHE_ERR_INVALID_ARGUMENT;
+  } catch (const std::out_of_range &e) {
+    fhe_b200::set_last_error(e.what());
+    return FHE_ERR_INVALID_ARGUMENT;
+  } catch (const fhe_b200::CudaError &e) {
+    fhe_b200::set_last_error(e.what());
+    return FHE_ERR_CUDA;
+  } catch (const std::bad_alloc &) {
+    fhe_b200::set_last_error("out of device or host memory");
+    return FHE_ERR_OUT_OF_MEMORY;
+  } catch (const std::runtime_error &e) {
+    fhe_b200::set_last_error(e.what());
+    return FHE_ERR_RUNTIME;
+  } catch (...) {
+    fhe_b200::set_last_error("unknown error");
+    return FHE_ERR_RUNTIME;
+  }
+}
+
+#define REQUIRE_HANDLE(h)                                  \
+  do {                                                     \
+    if (!(h) || !(h)->impl) {                              \
+      fhe_b200::set_last_error("null handle: " #h);        \
+      return FHE_ERR_NULL_HANDLE;                          \
+    }                                                      \
+  } while (0)
+
+#define REQUIRE_OUT(p)                                     \
+  do {                                                     \
+    if (!(p)) {                                            \
+      fhe_b200::set_last_error("null output pointer: " #p); \
+      return FHE_ERR_NULL_HANDLE;                          \
+    }                                                      \
+  } while (0)
+
+// The object behind a handle, checked to be alive and owned by `engine`
+// (is_compatible, engine_require.cpp:15-22).
+const Data &live(const fhe_engine *engine, const fhe_data *d) {
+  if (!d->impl->engine) throw std::runtime_error("the engine of the input object was destroyed.");
+  if (engine && d->impl->engine != engine->impl)
+    throw std::runtime_error("the input object is not compatible with this engine.");
+  return *d->impl;
+}
+
+fhe_data *wrap(std::unique_ptr<Data> d) {
+  auto h = new fhe_data;
+  h->impl = d.release();
+  return h;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *fhe_last_error(void) { return fhe_b200::g_last_error.c_str(); }
+
+void fhe_config_default(fhe_config *config) {
+  if (!config) return;
+  config->log_coeff_count = 14;
+  config->log_slot_count = -1;
+  config->special_prime_count = 1;
+  config->max_level = -1;
+  config->scheme_preset = FHE_PRESET_CKKS_40_60_DEFAULT;
+}
+
+static fhe_b200::Config to_config(const fhe_config *config) {
+  fhe_b200::Config c;
+  c.log_coeff_count = config->log_coeff_count;
+  c.log_slot_count = config->log_slot_count;
+  c.special_prime_count = config->special_prime_count;
+  c.max_level = config->max_level;
+  c.preset = static_cast<fhe_b200::SchemePreset>(config->scheme_preset);
+  return c;
+}
+
+static void fill_info(const fhe_b200::Parameters &p, fhe_engine_info *info) {
+  info->coeff_count = p.n;
+  info->slot_count = p.slot_count;
+  info->chain_count = p.chain_count;
+  info->prime_count = p.prime_count;
+  info->special_prime_count = p.special_prime_count;
+  info->full_level = p.full_level;
+  info->max_level = p.max_level();
+  info->max_key_switching_level = p.max_key_switching_level();
+  info->scale_bit_length = p.preset.scale_bits;
+}
+
+int fhe_parameters_query(const fhe_config *config, fhe_engine_info *info, uint64_t *moduli,
+                         int capacity) {
+  REQUIRE_OUT(config);
+  return guarded([&] {
+    fhe_b200::Parameters p(to_config(config));
+    if (info) fill_info(p, info);
+    if (moduli)
+      for (int i = 0; i < capacity && i < p.prime_count; i++) moduli[i] = p.q[i];
+  });
+}
+
+int fhe_parameters_tables(const fhe_config *config, uint64_t *k, int64_t *r_squared,
+                          int64_t *n_inverse, int64_t *root, int64_t *root_inverse) {
+  REQUIRE_OUT(config);
+  return guarded([&] {
+    fhe_b200::Parameters p(to_config(config));
+    if (k) std::memcpy(k, p.k.data(), sizeof(uint64_t) * p.k.size());
+    if (r_squared) std::memcpy(r_squared, p.r_squared.data(), sizeof(int64_t) * p.r_squared.size());
+    if (n_inverse) std::memcpy(n_inverse, p.n_inverse.data(), sizeof(int64_t) * p.n_inverse.size());
+    if (root) std::memcpy(root, p.root.data(), sizeof(int64_t) * p.root.size());
+    if (root_inverse)
+      std::memcpy(root_inverse, p.root_inverse.data(), sizeof(int64_t) * p.root_inverse.size());
+  });
+}
+
+int fhe_engine_create(const fhe_config *config, fhe_engine **engine) {
+  REQUIRE_OUT(config);
+  REQUIRE_OUT(engine);
+  *engine = nullptr;
+  return guarded([&] {
+    auto e = new Engine(to_config(config));
+    *engine = new fhe_engine{e};
+  });
+}
+
+int fhe_engine_destroy(fhe_engine *engine) {
+  if (!engine) return FHE_OK;
+  int rc = guarded([&] { delete engine->impl; });
+  delete engine;
+  return rc;
+}
+
+int fhe_engine_info_get(const fhe_engine *engine, fhe_engine_info *info) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_OUT(info);
+  return guarded([&] {
+    fill_info(engine->impl->params, info);
+  });
+}
+
+int fhe_engine_moduli(const fhe_engine *engine, uint64_t *moduli, int capacity) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_OUT(moduli);
+  return guarded([&] {
+    const auto &q = engine->impl->params.q;
+    for (int i = 0; i < capacity && i < static_cast<int>(q.size()); i++) moduli[i] = q[i];
+  });
+}
+
+int fhe_engine_moduli_id(const fhe_engine *engine, int level, int *moduli_id) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_OUT(moduli_id);
+  return guarded([&] { *moduli_id = engine->impl->params.moduli_id(level); });
+}
+
+int fhe_engine_synchronize(fhe_engine *engine) {
+  REQUIRE_HANDLE(engine);
+  return guarded([&] { engine->impl->synchronize(); });
+}
+
+int fhe_engine_set_stream(fhe_engine *engine, void *cuda_stream) {
+  REQUIRE_HANDLE(engine);
+  return guarded([&] { engine->impl->set_stream(static_cast<cudaStream_t>(cuda_stream)); });
+}
+
+int fhe_engine_set_profiling(fhe_engine *engine, int enable) {
+  REQUIRE_HANDLE(engine);
+  return guarded([&] { engine->impl->set_profiling(enable != 0); });
+}
+
+int fhe_engine_profile_report(fhe_engine *engine, char *buffer, int capacity) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_OUT(buffer);
+  return guarded([&] {
+    const std::string r = engine->impl->profile_report();
+    if (capacity <= 0) throw std::invalid_argument("the report buffer is empty.");
+    const size_t n = std::min(r.size(), static_cast<size_t>(capacity - 1));
+    std::memcpy(buffer, r.data(), n);
+    buffer[n] = '\0';
+  });
+}
+
+int fhe_engine_profile_reset(fhe_engine *engine) {
+  REQUIRE_HANDLE(engine);
+  return guarded([&] { engine->impl->profile_reset(); });
+}
+
+unsigned long long fhe_kernel_launch_count(void) { return fhe_b200::kernel_launch_count(); }
+
+int fhe_data_upload(fhe_engine *engine, int type, int flag, int moduli_id, int polys,
+                    long double ckks_scale, const int64_t *host_limbs, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] {
+    *out = wrap(engine->impl->upload(type, flag, moduli_id, polys, ckks_scale, host_limbs));
+  });
+}
+
+int fhe_data_download(const fhe_data *data, int64_t *host_limbs) {
+  REQUIRE_HANDLE(data);
+  return guarded([&] { live(nullptr, data).engine->download(*data->impl, host_limbs); });
+}
+
+int fhe_data_download_async(const fhe_data *data, int64_t *host_limbs) {
+  REQUIRE_HANDLE(data);
+  return guarded([&] { live(nullptr, data).engine->download_async(*data->impl, host_limbs); });
+}
+
+int fhe_data_info_get(const fhe_data *data, fhe_data_info *info) {
+  REQUIRE_HANDLE(data);
+  REQUIRE_OUT(info);
+  return guarded([&] {
+    const Data &d = live(nullptr, data);
+    info->type = d.type;
+    info->flag = d.flag;
+    info->moduli_id = d.moduli_id;
+    info->level = d.level();
+    info->polys = d.polys;
+    info->chains = d.chains;
+    info->delta = d.delta;
+    info->ckks_scale = d.scale;
+  });
+}
+
+int fhe_data_set_delta(fhe_data *data, int delta) {
+  REQUIRE_HANDLE(data);
+  data->impl->delta = delta;
+  return FHE_OK;
+}
+
+int fhe_data_device_pointer(const fhe_data *data, int64_t **device_limbs) {
+  REQUIRE_HANDLE(data);
+  REQUIRE_OUT(device_limbs);
+  *device_limbs = data->impl->d;
+  return FHE_OK;
+}
+
+int fhe_data_destroy(fhe_data *data) {
+  if (!data) return FHE_OK;
+  int rc = guarded([&] { delete data->impl; });
+  delete data;
+  return rc;
+}
+
+#define UNARY_OP(name, call)                                                  \
+  int name(fhe_engine *engine, const fhe_data *x, fhe_data **out) {           \
+    REQUIRE_HANDLE(engine);                                                   \
+    REQUIRE_HANDLE(x);                                                        \
+    REQUIRE_OUT(out);                                                         \
+    *out = nullptr;                                                           \
+    return guarded([&] { *out = wrap(engine->impl->call(live(engine, x))); }); \
+  }
+
+UNARY_OP(fhe_rescale, rescale)
+UNARY_OP(fhe_to_ntt, to_ntt)
+UNARY_OP(fhe_to_intt, to_intt)
+
+int fhe_multiply(fhe_engine *engine, const fhe_data *a, const fhe_data *b, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(a);
+  REQUIRE_HANDLE(b);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] { *out = wrap(engine->impl->multiply(live(engine, a), live(engine, b))); });
+}
+
+int fhe_multiply_relinearize(fhe_engine *engine, const fhe_data *a, const fhe_data *b,
+                             const fhe_data *rk, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(a);
+  REQUIRE_HANDLE(b);
+  REQUIRE_HANDLE(rk);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded(
+      [&] { *out = wrap(engine->impl->multiply_relinearize(live(engine, a), live(engine, b), live(engine, rk))); });
+}
+
+int fhe_multiply_relinearize_rescale(fhe_engine *engine, const fhe_data *a, const fhe_data *b,
+                                     const fhe_data *rk, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(a);
+  REQUIRE_HANDLE(b);
+  REQUIRE_HANDLE(rk);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] {
+    *out = wrap(engine->impl->multiply_relinearize_rescale(live(engine, a), live(engine, b), live(engine, rk)));
+  });
+}
+
+int fhe_relinearize(fhe_engine *engine, const fhe_data *ct, const fhe_data *rk, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(ct);
+  REQUIRE_HANDLE(rk);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] { *out = wrap(engine->impl->relinearize(live(engine, ct), live(engine, rk))); });
+}
+
+int fhe_ntt_limbs(fhe_engine *engine, int64_t *device_limbs, int moduli_id, int chains, int polys,
+                  long long poly_stride, int inverse) {
+  REQUIRE_HANDLE(engine);
+  return guarded([&] {
+    engine->impl->ntt_limbs(device_limbs, moduli_id, chains, polys, poly_stride, inverse != 0);
+  });
+}
+
+}  // extern "C"

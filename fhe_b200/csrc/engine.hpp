@@ -1,0 +1,164 @@
+// The B200 CKKS engine: HBM-resident objects and the CKKS operations of the
+// reference's CKKSEngine (DESILO FHE, src/ckks/engine.h) executed by the device
+// kernels of kernels.cu / ntt.cuh.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <set>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "kernels.cuh"
+#include "params.hpp"
+
+namespace fhe_b200 {
+
+enum DataFlag : int {
+  kFlagNone = 0,
+  kFlagComplex = 1,
+  kFlagNtt = 2,
+  kFlagRescaled = 4,
+  kFlagSparse = 8,
+  kFlagSpecial = 16,
+};
+
+enum DataType : int {
+  kSecretKey = 1,
+  kPublicKey = 2,
+  kRelinearizationKey = 3,
+  kUnitCiphertext = 4,
+  kUnitPlaintext = 5,
+  kFixedRotationKey = 6,
+  kConjugationKey = 7,
+  kKeySwitchingKey = 8,
+};
+
+class CudaError : public std::runtime_error {
+ public:
+  explicit CudaError(const std::string &what) : std::runtime_error(what) {}
+};
+
+class Engine;
+
+// One HBM-resident object (key, ciphertext or plaintext).
+struct Data {
+  Engine *engine = nullptr;
+  int type = 0;
+  int flag = 0;
+  int moduli_id = 0;
+  int polys = 0;
+  int chains = 0;  // limbs per polynomial
+  int delta = 0;
+  long double scale = 1.0L;
+  int64_t *d = nullptr;
+
+  size_t words() const;
+  long long poly_stride() const;
+  int level() const;  // data.h:21-32
+  bool is_ntt() const { return flag & kFlagNtt; }
+  bool is_rescaled() const { return flag & kFlagRescaled; }
+  const char *type_name() const;
+  ~Data();
+};
+
+class Engine {
+ public:
+  explicit Engine(const Config &config);
+  ~Engine();
+  Engine(const Engine &) = delete;
+  Engine &operator=(const Engine &) = delete;
+
+  const Parameters params;
+
+  cudaStream_t stream() const { return stream_; }
+  void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
+  void synchronize();
+
+  // Device memory from the stream-ordered pool.
+  int64_t *alloc_words(size_t words);
+  void free_words(int64_t *p);
+
+  std::unique_ptr<Data> make_data(int type, int flag, int moduli_id, int polys, long double scale);
+  std::unique_ptr<Data> upload(int type, int flag, int moduli_id, int polys, long double scale,
+                               const int64_t *host);
+  void download(const Data &d, int64_t *host);
+  void download_async(const Data &d, int64_t *host);
+  std::unique_ptr<Data> clone(const Data &d);
+  void forget(Data *d);  // called by ~Data
+
+  // Engine-level operations (reference semantics, see fhe_b200.h).
+  std::unique_ptr<Data> multiply(const Data &a, const Data &b);
+  std::unique_ptr<Data> multiply_relinearize(const Data &a, const Data &b, const Data &rk);
+  std::unique_ptr<Data> multiply_relinearize_rescale(const Data &a, const Data &b, const Data &rk);
+  std::unique_ptr<Data> relinearize(const Data &ct, const Data &rk);
+  std::unique_ptr<Data> rescale(const Data &ct);
+  std::unique_ptr<Data> to_ntt(const Data &text);
+  std::unique_ptr<Data> to_intt(const Data &text);
+
+  void ntt_limbs(int64_t *limbs, int moduli_id, int chains, int polys, long long stride,
+                 bool inverse);
+
+  // Per-kernel-family device time, measured with CUDA events on the engine's
+  // stream around each launch while profiling is on.
+  void set_profiling(bool on);
+  std::string profile_report();  // "name launches total_ms" lines; synchronizes
+  void profile_reset();
+
+  const PrimeTables &tables() const { return tables_; }
+  const KeySwitchTables &key_switch_tables() const { return ks_; }
+  const DevicePartitions &partitions(int moduli_id, int key_moduli_id);
+
+ private:
+  cudaStream_t own_stream_ = nullptr;
+  cudaStream_t stream_ = nullptr;
+  std::vector<int64_t *> table_buffers_;
+  PrimeTables tables_{};
+  KeySwitchTables ks_{};
+  std::map<std::pair<int, int>, DevicePartitions> partition_cache_;
+  std::set<Data *> live_;
+
+  struct PendingTiming {
+    const char *name;
+    cudaEvent_t start;
+    cudaEvent_t stop;
+  };
+  bool profiling_ = false;
+  std::vector<PendingTiming> pending_;
+  std::vector<cudaEvent_t> event_pool_;
+  std::map<std::string, std::pair<uint64_t, double>> stats_;
+  cudaEvent_t take_event();
+  void collect_timings();
+  template <class F>
+  cudaError_t timed(const char *name, F &&launch) {
+    if (!profiling_) return launch();
+    PendingTiming p{name, take_event(), take_event()};
+    cudaEventRecord(p.start, stream_);
+    const cudaError_t e = launch();
+    cudaEventRecord(p.stop, stream_);
+    pending_.push_back(p);
+    return e;
+  }
+
+  void check(cudaError_t e, const char *what);
+  template <class T>
+  T *upload_table(const std::vector<T> &v);
+
+  // Core steps.
+  std::unique_ptr<Data> core_rescale(const Data &ct);          // coefficient form
+  std::unique_ptr<Data> prepare_for_multiply(const Data &text, int level);
+  // Key switch tail shared by relinearize variants; t3 is [3][L][N] coefficient
+  // form at moduli_id (poly 2 is switched).
+  void relinearize_tail(const int64_t *t3, int moduli_id, const Data &rk, int mode, int64_t *out);
+  void require_key_level(const std::string &fn, const Data &text, const Data &key,
+                         bool for_multiply);
+};
+
+// Thread-local last error of the C ABI.
+void set_last_error(const std::string &message);
+
+}  // namespace fhe_b200

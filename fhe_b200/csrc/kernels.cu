@@ -1,0 +1,404 @@
+// Device kernels of the B200 CKKS engine: element-wise families, rescale and the
+// hybrid key-switching pipeline (see kernels.cuh for the contract of each launcher).
+#include "kernels.cuh"
+#include "ntt.cuh"
+
+#include <atomic>
+
+namespace fhe_b200 {
+
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+}
+
+void note_launch(unsigned count) { g_launches.fetch_add(count, std::memory_order_relaxed); }
+unsigned long long kernel_launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline unsigned blocks_for(long long work) {
+  long long b = (work + kThreads - 1) / kThreads;
+  return static_cast<unsigned>(b < 1 ? 1 : b);
+}
+
+// --------------------------------------------------------------- tensor --
+
+__global__ void tensor_kernel(PrimeTables t, int n, int limbs, int prime_base, const int64_t *a,
+                              const int64_t *b, int64_t *z) {
+  const long long total = static_cast<long long>(limbs) * n;
+  const long long ps = total;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int prime = prime_base + static_cast<int>(i / n);
+    const uint64_t q = t.q[prime], k = t.k[prime];
+    const int64_t qs = static_cast<int64_t>(q), q2 = qs << 1;
+    const int64_t a0 = a[i], a1 = a[ps + i], b0 = b[i], b1 = b[ps + i];
+    z[i] = mont_mult(a0, b0, q, k);
+    z[ps + i] = guard(guard(mont_mult(a0, b1, q, k) + mont_mult(a1, b0, q, k), q2), qs);
+    z[2 * ps + i] = mont_mult(a1, b1, q, k);
+  }
+}
+
+__global__ void add_reduce_kernel(PrimeTables t, int n, int limbs, int prime_base, long long total,
+                                  const int64_t *x1, const int64_t *x2, int64_t *y) {
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int prime = prime_base + static_cast<int>((i / n) % limbs);
+    const int64_t qs = static_cast<int64_t>(t.q[prime]);
+    y[i] = guard(guard(x1[i] + x2[i], qs << 1), qs);
+  }
+}
+
+// -------------------------------------------------------------- rescale --
+
+__device__ __forceinline__ int64_t rescale_word(int64_t xj, int64_t x0, int64_t rounder,
+                                                uint64_t q, uint64_t k, int64_t constant) {
+  const int64_t qs = static_cast<int64_t>(q), q2 = qs << 1;
+  int64_t v = xj - x0;  // mont_subtract (unit.cpp:58-64)
+  v = v >= 0 ? v : v + q2;
+  v = guard(v, qs);
+  v = mont_mult(v, constant, q, k);
+  v = guard(v + rounder, q2);  // add_tiled
+  return guard(v, qs);
+}
+
+__global__ void rescale_kernel(PrimeTables t, KeySwitchTables ks, int n, int limbs, int moduli_id,
+                               const int64_t *x, long long xs, int64_t *y, long long ys) {
+  const int poly = blockIdx.y;
+  const long long per_poly = static_cast<long long>(limbs - 1) * n;
+  const int64_t q_half = static_cast<int64_t>(t.q[moduli_id] >> 1);
+  const int64_t *xp = x + poly * xs;
+  int64_t *yp = y + poly * ys;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < per_poly;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int j = static_cast<int>(i / n);
+    const int c = static_cast<int>(i - static_cast<long long>(j) * n);
+    const int prime = moduli_id + 1 + j;
+    const int64_t x0 = xp[c];
+    const int64_t rounder = x0 > q_half ? 1 : 0;  // get_rounder (unit.cpp:66-70)
+    yp[i] = rescale_word(xp[static_cast<long long>(j + 1) * n + c], x0, rounder, t.q[prime],
+                         t.k[prime], ks.rescale_scale[static_cast<long long>(moduli_id) * ks.prime_count + prime]);
+  }
+}
+
+// ---------------------------------------------------------- mixed radix --
+
+// One partition of alpha = A limbs per thread-coefficient (rns_to_mrs,
+// core_key_switch.cpp:21-56, Garner's algorithm with the reference's lazy ranges).
+template <int A>
+__global__ void mixed_radix_kernel(PrimeTables t, DevicePartitions dp, int n, int moduli_id,
+                                   const int64_t *x, int64_t *digits) {
+  const int p = blockIdx.y;
+  if (dp.size[p] != A) return;
+  const int start = dp.start[p];
+  const int coeff = blockIdx.x * blockDim.x + threadIdx.x;
+  if (coeff >= n) return;
+  int64_t y[A];
+  const int64_t first = x[static_cast<long long>(start) * n + coeff];
+#pragma unroll
+  for (int c = 0; c < A; c++) y[c] = first;
+#pragma unroll
+  for (int ci = 0; ci < A - 1; ci++) {
+    const int yo = ci + 1;
+    const int prime = moduli_id + start + yo;
+    const uint64_t q = t.q[prime], k = t.k[prime];
+    const int64_t qs = static_cast<int64_t>(q), q2 = qs << 1;
+    const int64_t xv = x[static_cast<long long>(start + yo) * n + coeff];
+    // mont_sub_enter_reduce_2q_to_q (compound.cpp:36-43)
+    y[yo] = guard(mont_mult(guard(xv + q2 - y[yo], q2), dp.inverse_r[p * 16 + ci], q, k), qs);
+#pragma unroll
+    for (int t2 = 0; t2 < A - ci - 2; t2++) {
+      const int dst = yo + 1 + t2;
+      const int prime2 = moduli_id + start + dst;
+      const uint64_t qq = t.q[prime2], kk = t.k[prime2];
+      const int64_t qqs = static_cast<int64_t>(qq), qq2 = qqs << 1;
+      // mont_enter_add_reduce_2q_to_q (compound.cpp:17-24)
+      y[dst] = guard(guard(mont_mult(y[yo], dp.product_r[(p * 16 + ci) * 16 + t2], qq, kk) + y[dst],
+                           qq2), qqs);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < A; c++) digits[static_cast<long long>(start + c) * n + coeff] = y[c];
+}
+
+// ModUp contraction of one extended limb (core_key_switch.cpp:92-106), evaluated
+// while the forward NTT loads its input.
+struct ModUpLoad {
+  DevicePartitions dp;
+  const int64_t *digits;
+  const int64_t *r_squared;
+  const uint64_t *q;
+  const uint64_t *k;
+  __device__ __forceinline__ int64_t operator()(int p, int limb, int prime, int gi, int n) const {
+    const int start = dp.start[p];
+    const int size = dp.size[p];
+    const uint64_t qq = q[prime], kk = k[prime];
+    const int64_t q2 = static_cast<int64_t>(qq << 1);
+    const int64_t *d = digits + static_cast<long long>(start) * n + gi;
+    int64_t acc = mont_mult(d[0], r_squared[prime], qq, kk);
+    const int64_t *c = dp.product_r_squared + static_cast<long long>(p) * 16 * dp.extended + limb;
+    for (int ci = 0; ci < size - 1; ci++) {
+      acc = guard(mont_mult(d[static_cast<long long>(ci + 1) * n], c[static_cast<long long>(ci) * dp.extended], qq, kk) + acc, q2);
+    }
+    return acc;
+  }
+};
+
+// ------------------------------------------------------ key inner product --
+
+__global__ void key_inner_product_kernel(PrimeTables t, DevicePartitions dp, int n, int moduli_id,
+                                         const int64_t *ext, const int64_t *key, int key_primes,
+                                         int view_offset, int64_t *acc) {
+  const int E = dp.extended;
+  const long long total = static_cast<long long>(E) * n;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int j = static_cast<int>(i / n);
+    const int prime = moduli_id + j;
+    const uint64_t q = t.q[prime], k = t.k[prime];
+    const int64_t qs = static_cast<int64_t>(q), q2 = qs << 1;
+    int64_t x0 = 0, x1 = 0;
+    for (int p = 0; p < dp.count; p++) {
+      const int64_t e = ext[static_cast<long long>(p) * total + i];
+      const int kidx = dp.key_index[p];
+      const long long k0 = (static_cast<long long>(2 * kidx) * key_primes + view_offset) * n + i;
+      const long long k1 = (static_cast<long long>(2 * kidx + 1) * key_primes + view_offset) * n + i;
+      const int64_t a0 = mont_mult(e, key[k0], q, k);
+      const int64_t a1 = mont_mult(e, key[k1], q, k);
+      if (p == 0) {
+        x0 = a0;
+        x1 = a1;
+      } else {  // mont_mult_add then reduce_2q_to_q
+        x0 = guard(guard(a0 + x0, q2), qs);
+        x1 = guard(guard(a1 + x1, q2), qs);
+      }
+    }
+    acc[i] = x0;
+    acc[total + i] = x1;
+  }
+}
+
+// ------------------------------------------------------ mod down epilogue --
+
+// Sequential exact division by the K special primes, last first
+// (core_key_switch.cpp:123-160, mont_sub_enter compound.cpp:45-52 with its
+// [0, 2p) outputs carried into the next division), then make_unsigned and the
+// caller's combination (see launch_mod_down_epilogue).
+template <int K>
+__global__ void mod_down_epilogue_kernel(PrimeTables t, KeySwitchTables ks, int n, int moduli_id,
+                                         int limbs, const int64_t *acc, const int64_t *base,
+                                         int mode, int64_t *out) {
+  const int poly = blockIdx.y;
+  const int coeff = blockIdx.x * blockDim.x + threadIdx.x;
+  if (coeff >= n) return;
+  const int L = limbs;
+  const int E = L + K;
+  const int P = ks.prime_count;
+  const int64_t *x = acc + static_cast<long long>(poly) * E * n + coeff;
+
+  int64_t sp[K];
+  int64_t d[K];
+#pragma unroll
+  for (int i = 0; i < K; i++) sp[i] = x[static_cast<long long>(L + i) * n];
+#pragma unroll
+  for (int s = 0; s < K; s++) {
+    const int idx = K - 1 - s;
+    d[s] = sp[idx];
+#pragma unroll
+    for (int i = 0; i < idx; i++) {
+      const int prime = moduli_id + L + i;
+      const uint64_t q = t.q[prime], kk = t.k[prime];
+      const int64_t q2 = static_cast<int64_t>(q << 1);
+      sp[i] = mont_mult(guard(sp[i] + q2 - d[s], q2), ks.p_inverse_mult_r[s * P + prime], q, kk);
+    }
+  }
+
+  auto divide = [&](int j) -> int64_t {
+    const int prime = moduli_id + j;
+    const uint64_t q = t.q[prime], kk = t.k[prime];
+    const int64_t qs = static_cast<int64_t>(q), q2 = qs << 1;
+    int64_t v = x[static_cast<long long>(j) * n];
+#pragma unroll
+    for (int s = 0; s < K; s++)
+      v = mont_mult(guard(v + q2 - d[s], q2), ks.p_inverse_mult_r[s * P + prime], q, kk);
+    return v < 0 ? v + qs : guard(v, qs);  // make_unsigned_reduce_2q_to_q
+  };
+
+  const long long in_stride = static_cast<long long>(L) * n;
+  if (mode == 0) {
+    int64_t *o = out + poly * in_stride + coeff;
+    for (int j = 0; j < L; j++) o[static_cast<long long>(j) * n] = divide(j);
+    return;
+  }
+  const int64_t *b = base + poly * in_stride + coeff;
+  auto combined = [&](int j) -> int64_t {
+    const int64_t qs = static_cast<int64_t>(t.q[moduli_id + j]);
+    return guard(guard(b[static_cast<long long>(j) * n] + divide(j), qs << 1), qs);
+  };
+  if (mode == 1) {
+    int64_t *o = out + poly * in_stride + coeff;
+    for (int j = 0; j < L; j++) o[static_cast<long long>(j) * n] = combined(j);
+    return;
+  }
+  // mode 2: rescale of the relinearized polynomial (core_rescale.cpp:5-25).
+  const long long out_stride = static_cast<long long>(L - 1) * n;
+  int64_t *o = out + poly * out_stride + coeff;
+  const int64_t y0 = combined(0);
+  const int64_t rounder = y0 > static_cast<int64_t>(t.q[moduli_id] >> 1) ? 1 : 0;
+  for (int j = 1; j < L; j++) {
+    const int prime = moduli_id + j;
+    o[static_cast<long long>(j - 1) * n] =
+        rescale_word(combined(j), y0, rounder, t.q[prime], t.k[prime],
+                     ks.rescale_scale[static_cast<long long>(moduli_id) * P + prime]);
+  }
+}
+
+struct TensorLoad {
+  const int64_t *a;
+  const int64_t *b;
+  long long poly_stride;  // limbs * n
+  const uint64_t *q;
+  const uint64_t *k;
+  __device__ __forceinline__ int64_t operator()(int poly, int limb, int prime, int gi, int n) const {
+    const long long i = static_cast<long long>(limb) * n + gi;
+    const uint64_t qq = q[prime], kk = k[prime];
+    if (poly == 0) return mont_mult(a[i], b[i], qq, kk);
+    if (poly == 2) return mont_mult(a[poly_stride + i], b[poly_stride + i], qq, kk);
+    const int64_t qs = static_cast<int64_t>(qq);
+    return guard(guard(mont_mult(a[i], b[poly_stride + i], qq, kk) +
+                           mont_mult(a[poly_stride + i], b[i], qq, kk),
+                       qs << 1),
+                 qs);
+  }
+};
+
+}  // namespace
+
+// ============================================================ launchers ==
+
+cudaError_t launch_tensor(const PrimeTables &t, int n, int limbs, int prime_base, const int64_t *a,
+                          const int64_t *b, int64_t *z, cudaStream_t s) {
+  note_launch();
+  tensor_kernel<<<blocks_for(static_cast<long long>(limbs) * n), kThreads, 0, s>>>(t, n, limbs,
+                                                                                  prime_base, a, b, z);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_add_reduce(const PrimeTables &t, int n, int polys, int limbs, int prime_base,
+                              const int64_t *x1, const int64_t *x2, int64_t *y, cudaStream_t s) {
+  const long long total = static_cast<long long>(polys) * limbs * n;
+  note_launch();
+  add_reduce_kernel<<<blocks_for(total), kThreads, 0, s>>>(t, n, limbs, prime_base, total, x1, x2, y);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rescale(const PrimeTables &t, const KeySwitchTables &ks, int n, int polys,
+                           int limbs, int moduli_id, const int64_t *x, long long xs, int64_t *y,
+                           long long ys, cudaStream_t s) {
+  const dim3 grid(blocks_for(static_cast<long long>(limbs - 1) * n), polys);
+  note_launch();
+  rescale_kernel<<<grid, kThreads, 0, s>>>(t, ks, n, limbs, moduli_id, x, xs, y, ys);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mixed_radix(const PrimeTables &t, const DevicePartitions &dp, int n,
+                               int moduli_id, const int64_t *x, int64_t *digits, cudaStream_t s) {
+  const dim3 grid(blocks_for(n), dp.count);
+  // One launch per distinct partition size; blocks of other sizes exit at once.
+  for (int size = 1; size <= 16; size++) {
+    if (!(dp.size_mask & (1u << size))) continue;
+    switch (size) {
+#define FHE_MRS_CASE(A) \
+  case A: note_launch(); mixed_radix_kernel<A><<<grid, kThreads, 0, s>>>(t, dp, n, moduli_id, x, digits); break;
+      FHE_MRS_CASE(1) FHE_MRS_CASE(2) FHE_MRS_CASE(3) FHE_MRS_CASE(4) FHE_MRS_CASE(5)
+      FHE_MRS_CASE(6) FHE_MRS_CASE(7) FHE_MRS_CASE(8) FHE_MRS_CASE(9) FHE_MRS_CASE(10)
+      FHE_MRS_CASE(11) FHE_MRS_CASE(12) FHE_MRS_CASE(13) FHE_MRS_CASE(14) FHE_MRS_CASE(15)
+      FHE_MRS_CASE(16)
+#undef FHE_MRS_CASE
+      default: return cudaErrorInvalidValue;
+    }
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mod_up_ntt(const PrimeTables &t, const DevicePartitions &dp, int log_n,
+                              int moduli_id, const int64_t *digits, int64_t *ext, cudaStream_t s) {
+  const int n = 1 << log_n;
+  const long long stride = static_cast<long long>(dp.extended) * n;
+  ModUpLoad ld{dp, digits, t.r_squared, t.q, t.k};
+  PlainStore st{ext, stride};
+  return forward_ntt(log_n, dp.count, dp.extended, moduli_id, t, ld, st, ext, stride, s);
+}
+
+cudaError_t launch_key_inner_product(const PrimeTables &t, const DevicePartitions &dp, int n,
+                                     int moduli_id, const int64_t *ext, const int64_t *key,
+                                     int key_primes, int view_offset, int64_t *acc, cudaStream_t s) {
+  note_launch();
+  key_inner_product_kernel<<<blocks_for(static_cast<long long>(dp.extended) * n), kThreads, 0, s>>>(
+      t, dp, n, moduli_id, ext, key, key_primes, view_offset, acc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mod_down_intt(const PrimeTables &t, int log_n, int moduli_id, int extended,
+                                 int64_t *acc, cudaStream_t s) {
+  const long long stride = static_cast<long long>(extended) << log_n;
+  PlainLoad ld{acc, stride};
+  EnterExitStore<true> st{acc, stride, t.n_inverse, t.q, t.k};
+  return inverse_ntt(log_n, 2, extended, moduli_id, t, ld, st, acc, stride, s);
+}
+
+cudaError_t launch_mod_down_epilogue(const PrimeTables &t, const KeySwitchTables &ks, int n,
+                                     int moduli_id, int limbs, const int64_t *acc,
+                                     const int64_t *base, int mode, int64_t *out, cudaStream_t s) {
+  const dim3 grid(blocks_for(n), 2);
+  switch (ks.special_count) {
+#define FHE_MD_CASE(K)                                                                      \
+  case K:                                                                                   \
+    note_launch();                                                                          \
+    mod_down_epilogue_kernel<K><<<grid, kThreads, 0, s>>>(t, ks, n, moduli_id, limbs, acc, base, \
+                                                          mode, out);                       \
+    break;
+    FHE_MD_CASE(1) FHE_MD_CASE(2) FHE_MD_CASE(3) FHE_MD_CASE(4) FHE_MD_CASE(5) FHE_MD_CASE(6)
+    FHE_MD_CASE(7) FHE_MD_CASE(8) FHE_MD_CASE(9) FHE_MD_CASE(10) FHE_MD_CASE(11) FHE_MD_CASE(12)
+    FHE_MD_CASE(13) FHE_MD_CASE(14) FHE_MD_CASE(15) FHE_MD_CASE(16)
+#undef FHE_MD_CASE
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_to_ntt(const PrimeTables &t, int log_n, int polys, int limbs, int prime_base,
+                          const int64_t *x, long long x_stride, int64_t *y, long long y_stride,
+                          cudaStream_t s) {
+  EnterLoad ld{x, x_stride, t.r_squared, t.q, t.k};
+  PlainStore st{y, y_stride};
+  return forward_ntt(log_n, polys, limbs, prime_base, t, ld, st, y, y_stride, s);
+}
+
+cudaError_t launch_to_intt(const PrimeTables &t, int log_n, int polys, int limbs, int prime_base,
+                           const int64_t *x, long long x_stride, int64_t *y, long long y_stride,
+                           cudaStream_t s) {
+  PlainLoad ld{x, x_stride};
+  EnterExitStore<false> st{y, y_stride, t.n_inverse, t.q, t.k};
+  return inverse_ntt(log_n, polys, limbs, prime_base, t, ld, st, y, y_stride, s);
+}
+
+cudaError_t launch_ntt_plain(const PrimeTables &t, int log_n, int polys, int limbs, int prime_base,
+                             int64_t *x, long long stride, bool inverse, cudaStream_t s) {
+  PlainLoad ld{x, stride};
+  PlainStore st{x, stride};
+  if (inverse) return inverse_ntt(log_n, polys, limbs, prime_base, t, ld, st, x, stride, s);
+  return forward_ntt(log_n, polys, limbs, prime_base, t, ld, st, x, stride, s);
+}
+
+cudaError_t launch_tensor_to_intt(const PrimeTables &t, int log_n, int limbs, int prime_base,
+                                  const int64_t *a, const int64_t *b, int64_t *y, cudaStream_t s) {
+  const long long stride = static_cast<long long>(limbs) << log_n;
+  TensorLoad ld{a, b, stride, t.q, t.k};
+  EnterExitStore<false> st{y, stride, t.n_inverse, t.q, t.k};
+  return inverse_ntt(log_n, 3, limbs, prime_base, t, ld, st, y, stride, s);
+}
+
+}  // namespace fhe_b200

@@ -1,0 +1,112 @@
+// Launchers of the engine's device kernels (element-wise families, hybrid key
+// switching, rescale).  All pointers are device pointers; objects are laid out
+// [poly][limb][N] int64 and limb j of an object at moduli id m is modulo prime m + j.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "modarith.cuh"
+
+namespace fhe_b200 {
+
+// Constants of the partitions of one (ciphertext moduli id, key moduli id) pair,
+// resident on the device.  Host side: Parameters::partition_constants.
+struct DevicePartitions {
+  int count = 0;          // dnum
+  int max_size = 0;       // max alpha
+  unsigned size_mask = 0; // bit a set when some partition has alpha == a
+  int extended = 0;       // prime_count(moduli_id): limbs of an extended polynomial
+  int max_key_index = 0;  // largest partition_index (host copy)
+  int *start = nullptr;   // [count]
+  int *size = nullptr;    // [count]
+  int *key_index = nullptr;           // [count] partition_index
+  int64_t *inverse_r = nullptr;       // [count][16]
+  int64_t *product_r = nullptr;       // [count][16][16]
+  int64_t *product_r_squared = nullptr;  // [count][16][extended]
+};
+
+// Process-wide count of kernel launches made by this library.
+void note_launch(unsigned count = 1);
+unsigned long long kernel_launch_count();
+
+struct KeySwitchTables {
+  const int64_t *p_inverse_mult_r;  // [K][P] (entry for prime i at [s*P + i])
+  const int64_t *rescale_scale;     // [P][P] (entry for from,to at [from*P + to])
+  int prime_count;
+  int special_count;
+};
+
+// z = tensor of two NTT-form ciphertexts (core.cpp:284-314): z0 = a0 b0,
+// z1 = a0 b1 + a1 b0 (reduced to [0,q)), z2 = a1 b1.
+cudaError_t launch_tensor(const PrimeTables &t, int n, int limbs, int prime_base,
+                          const int64_t *a, const int64_t *b, int64_t *z, cudaStream_t s);
+
+// y = guard(guard(x1 + x2, 2q), q) over polys x limbs (mont_add_reduce_2q_to_q).
+cudaError_t launch_add_reduce(const PrimeTables &t, int n, int polys, int limbs, int prime_base,
+                              const int64_t *x1, const int64_t *x2, int64_t *y, cudaStream_t s);
+
+// rescale_once_ (core_rescale.cpp:5-25): x [polys][L][N] at moduli id m -> y
+// [polys][L-1][N] at m+1.
+cudaError_t launch_rescale(const PrimeTables &t, const KeySwitchTables &ks, int n, int polys,
+                           int limbs, int moduli_id, const int64_t *x, long long x_poly_stride,
+                           int64_t *y, long long y_poly_stride, cudaStream_t s);
+
+// Full relinearize / key switch pipeline pieces ------------------------------
+
+// rns_to_mrs for every partition (core_key_switch.cpp:21-56): x is the
+// coefficient-form polynomial at moduli_id (L limbs); digits [L][N] hold partition
+// p's alpha digits at limbs [start_p, start_p + alpha_p).
+cudaError_t launch_mixed_radix(const PrimeTables &t, const DevicePartitions &dp, int n,
+                               int moduli_id, const int64_t *x, int64_t *digits, cudaStream_t s);
+
+// ModUp + NTT of every partition (core_key_switch.cpp:92-108): ext [count][E][N].
+cudaError_t launch_mod_up_ntt(const PrimeTables &t, const DevicePartitions &dp, int log_n,
+                              int moduli_id, const int64_t *digits, int64_t *ext,
+                              cudaStream_t s);
+
+// Key inner product (core_key_switch.cpp:320-349): acc[2][E][N] = sum over
+// partitions of ext_p * (key_{2i}, key_{2i+1}), reference reduction pattern.
+// key is [2*dnum_key][key_primes][N]; view_offset = moduli_id - key_moduli_id.
+cudaError_t launch_key_inner_product(const PrimeTables &t, const DevicePartitions &dp, int n,
+                                     int moduli_id, const int64_t *ext, const int64_t *key,
+                                     int key_primes, int view_offset, int64_t *acc,
+                                     cudaStream_t s);
+
+// Inverse NTT of both accumulators, then to_intt_ scaling and reduce_2q_to_q
+// (mod_down, core_key_switch.cpp:110-121), in place.
+cudaError_t launch_mod_down_intt(const PrimeTables &t, int log_n, int moduli_id, int extended,
+                                 int64_t *acc, cudaStream_t s);
+
+// Epilogue of a key switch on (acc0, acc1) = INTT'd extended accumulators:
+// the sequential division by the special primes (core_key_switch.cpp:123-160),
+// then
+//   mode 0: out[p] = ks[p]                                  (key switcher)
+//   mode 1: out[p] = add_reduce(base[p], ks[p])             (relinearize)
+//   mode 2: as mode 1, then rescale (drops limb 0)          (relinearize+rescale)
+// base is [2][L][N] (coefficient form); out is [2][L or L-1][N].
+cudaError_t launch_mod_down_epilogue(const PrimeTables &t, const KeySwitchTables &ks, int n,
+                                     int moduli_id, int limbs, const int64_t *acc,
+                                     const int64_t *base, int mode, int64_t *out,
+                                     cudaStream_t s);
+
+// Forward NTT with Montgomery enter (to_ntt_) of polys x limbs, in place or not.
+cudaError_t launch_to_ntt(const PrimeTables &t, int log_n, int polys, int limbs, int prime_base,
+                          const int64_t *x, long long x_stride, int64_t *y, long long y_stride,
+                          cudaStream_t s);
+// Inverse NTT with N^-1 enter-exit (to_intt_).
+cudaError_t launch_to_intt(const PrimeTables &t, int log_n, int polys, int limbs, int prime_base,
+                           const int64_t *x, long long x_stride, int64_t *y, long long y_stride,
+                           cudaStream_t s);
+// Plain transforms (operation/ntt.cpp ntt/intt on each limb), in place.
+cudaError_t launch_ntt_plain(const PrimeTables &t, int log_n, int polys, int limbs,
+                             int prime_base, int64_t *x, long long stride, bool inverse,
+                             cudaStream_t s);
+// Inverse NTT (to_intt_) of the tensor of two NTT-form 2-poly ciphertexts a, b
+// without materialising the tensor: y [3][L][N] coefficient form.
+cudaError_t launch_tensor_to_intt(const PrimeTables &t, int log_n, int limbs, int prime_base,
+                                  const int64_t *a, const int64_t *b, int64_t *y,
+                                  cudaStream_t s);
+
+}  // namespace fhe_b200

@@ -1,0 +1,296 @@
+// Batched negacyclic NTT / inverse NTT for the B200 CKKS engine.
+//
+// The transform of one limb (N = 2^log_n words) is split into passes.  A pass
+// performs S consecutive radix-2 stages on independent sub-transforms of 2^S words
+// each: "strided" passes take one word out of every T = 2^(log_n - S) (the early
+// forward stages / late inverse stages), "contiguous" passes take 2^S adjacent
+// words.  A CTA stages a tile of sub-transforms in shared memory; inside a tile the
+// stages are done three at a time in registers (radix-8 rounds), so shared memory
+// is touched once per three stages.  The first round of a pass reads global memory
+// through a Loader and the last round writes through a Storer, which is where the
+// element-wise work before and after a transform (Montgomery enter, N^-1 scaling,
+// ModUp digit contraction, key products ...) is fused.
+//
+// Each butterfly is exactly the reference's (operation/ntt.cpp:46-134 forward,
+// Cooley-Tukey with the bit-reversed psi table; 177-272 inverse, Gentleman-Sande
+// with the "backward paint" table), so the output words are bit-identical whatever
+// the pass split.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "modarith.cuh"
+
+namespace fhe_b200 {
+
+void note_launch(unsigned count);
+
+struct NttPass {
+  int log_n;
+  int stride_log;  // log2(T); 0 for contiguous passes
+  int first;       // forward: first global stage; inverse: first distance exponent
+  int columns;     // sub-transforms per CTA tile
+  int polys;       // batch: polys x limbs, grid.y = limbs * polys (poly fastest)
+  int limbs;
+  int prime_base;  // prime index of limb 0
+};
+
+// Reads word gi of (poly, limb) from a [poly][limb][N] buffer.
+struct PlainLoad {
+  const int64_t *src;
+  long long poly_stride;
+  __device__ __forceinline__ int64_t operator()(int poly, int limb, int, int gi, int n) const {
+    return src[poly * poly_stride + (long long)limb * n + gi];
+  }
+};
+
+struct PlainStore {
+  int64_t *dst;
+  long long poly_stride;
+  __device__ __forceinline__ void operator()(int poly, int limb, int, int gi, int n, int64_t v) const {
+    dst[poly * poly_stride + (long long)limb * n + gi] = v;
+  }
+};
+
+// mont_enter by a per-prime constant on the way in: to_ntt_ (core_ntt.cpp:91-100).
+struct EnterLoad {
+  const int64_t *src;
+  long long poly_stride;
+  const int64_t *constant;  // indexed by prime
+  const uint64_t *q;
+  const uint64_t *k;
+  __device__ __forceinline__ int64_t operator()(int poly, int limb, int prime, int gi, int n) const {
+    const int64_t x = src[poly * poly_stride + (long long)limb * n + gi];
+    return mont_mult(x, constant[prime], q[prime], k[prime]);
+  }
+};
+
+// mont_enter_exit by N^-1*R on the way out: to_intt_ (core_ntt.cpp:131-148),
+// optionally followed by reduce_2q_to_q (mod_down, core_key_switch.cpp:121).
+template <bool REDUCE>
+struct EnterExitStore {
+  int64_t *dst;
+  long long poly_stride;
+  const int64_t *n_inverse;
+  const uint64_t *q;
+  const uint64_t *k;
+  __device__ __forceinline__ void operator()(int poly, int limb, int prime, int gi, int n, int64_t v) const {
+    const uint64_t qq = q[prime], kk = k[prime];
+    int64_t y = mont_exit(mont_mult(v, n_inverse[prime], qq, kk), qq, kk);
+    if (REDUCE) y = guard(y, static_cast<int64_t>(qq));
+    dst[poly * poly_stride + (long long)limb * n + gi] = y;
+  }
+};
+
+template <int S, bool INVERSE, class Loader, class Storer>
+__global__ void __launch_bounds__(256)
+    ntt_pass_kernel(NttPass a, PrimeTables t, Loader load, Storer store) {
+  constexpr int M = 1 << S;
+  constexpr int PM = M + 1;  // padded sub-transform pitch in shared memory
+  constexpr int R = (S + 2) / 3;
+  extern __shared__ int64_t tile_smem[];
+
+  const int pl = blockIdx.y;
+  const int poly = pl % a.polys;
+  const int limb = pl / a.polys;
+  const int prime = a.prime_base + limb;
+  const uint64_t q = t.q[prime];
+  const uint64_t k = t.k[prime];
+  const int64_t q2 = static_cast<int64_t>(q << 1);
+  const int n = 1 << a.log_n;
+  const int64_t *tw = (INVERSE ? t.root_inverse : t.root) + static_cast<size_t>(prime) * (n - 1);
+  const int T = 1 << a.stride_log;
+  const bool strided = T > 1;
+  const int C = a.columns;
+  const int u0 = blockIdx.x * C;
+
+#pragma unroll
+  for (int round = 0; round < R; round++) {
+    constexpr int kLastR = S - 3 * (R - 1);
+    const int r = (round < R - 1) ? 3 : kLastR;
+    const int E = 1 << r;
+    const int first_local = 3 * round;
+    const int dlog = INVERSE ? first_local : (S - first_local - r);
+    const int D = 1 << dlog;
+    const int groups_per_col = M >> r;
+    const int total = C * groups_per_col;
+    for (int gid = threadIdx.x; gid < total; gid += blockDim.x) {
+      int c, g;
+      if (strided) {
+        c = gid % C;
+        g = gid / C;
+      } else {
+        c = gid / groups_per_col;
+        g = gid - c * groups_per_col;
+      }
+      const int base = ((g >> dlog) << (dlog + r)) | (g & (D - 1));
+      const int u = u0 + c;
+      const int gbase = (u >> a.stride_log) * (M << a.stride_log) + (u & (T - 1));
+      int64_t x[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        if (e < E) {
+          const int i = base + e * D;
+          if (round == 0) {
+            x[e] = load(poly, limb, prime, gbase + i * T, n);
+          } else {
+            x[e] = tile_smem[c * PM + i];
+          }
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        if (j < r) {
+          if (!INVERSE) {
+            const int s = a.first + first_local + j;
+            const int half = E >> (j + 1);
+#pragma unroll
+            for (int e = 0; e < 8; e++) {
+              if (e < E && (e & half) == 0) {
+                const int gi = gbase + (base + e * D) * T;
+                const int64_t w = __ldg(&tw[(1 << s) - 1 + (gi >> (a.log_n - s))]);
+                const int64_t uu = x[e];
+                const int64_t p = mont_mult(w, x[e + half], q, k);
+                x[e] = guard(uu + p, q2);
+                x[e + half] = guard(uu + q2 - p, q2);
+              }
+            }
+          } else {
+            const int dg = a.first + first_local + j;
+            const int half = 1 << j;
+#pragma unroll
+            for (int e = 0; e < 8; e++) {
+              if (e < E && (e & half) == 0) {
+                const int gi = gbase + (base + e * D) * T;
+                const int64_t w = __ldg(&tw[n - (n >> dg) + (gi >> (dg + 1))]);
+                const int64_t uu = x[e];
+                const int64_t vv = x[e + half];
+                x[e] = guard(uu + vv, q2);
+                x[e + half] = mont_mult(w, guard(uu + q2 - vv, q2), q, k);
+              }
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        if (e < E) {
+          const int i = base + e * D;
+          if (round == R - 1) {
+            store(poly, limb, prime, gbase + i * T, n, x[e]);
+          } else {
+            tile_smem[c * PM + i] = x[e];
+          }
+        }
+      }
+    }
+    if (round < R - 1) __syncthreads();
+  }
+}
+
+// Pass plan of a transform of 2^log_n words.
+struct NttPlan {
+  int passes;     // 1 or 2
+  int s_first;    // S of the strided (outer) pass, or log_n for a single pass
+  int s_second;   // S of the contiguous (inner) pass
+};
+
+inline NttPlan ntt_plan(int log_n) {
+  if (log_n <= 11) return {1, log_n, 0};
+  const int s2 = log_n >= 15 ? 8 : (log_n >= 13 ? 7 : 6);
+  return {2, log_n - s2, s2};
+}
+
+constexpr int kNttTileWords = 4096;
+constexpr int kNttThreads = 256;
+
+template <int S, bool INVERSE, class Loader, class Storer>
+cudaError_t launch_ntt_pass(const NttPass &a, const PrimeTables &t, const Loader &ld,
+                            const Storer &st, cudaStream_t stream) {
+  const int subs = (1 << a.log_n) >> S;
+  const dim3 grid(subs / a.columns, a.polys * a.limbs);
+  const size_t smem = sizeof(int64_t) * a.columns * ((1 << S) + 1);
+  auto kernel = ntt_pass_kernel<S, INVERSE, Loader, Storer>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+  }
+  note_launch(1);
+  kernel<<<grid, kNttThreads, smem, stream>>>(a, t, ld, st);
+  return cudaGetLastError();
+}
+
+template <bool INVERSE, class Loader, class Storer>
+cudaError_t dispatch_ntt_pass(int S, const NttPass &a, const PrimeTables &t, const Loader &ld,
+                              const Storer &st, cudaStream_t stream) {
+  switch (S) {
+    case 1: return launch_ntt_pass<1, INVERSE>(a, t, ld, st, stream);
+    case 2: return launch_ntt_pass<2, INVERSE>(a, t, ld, st, stream);
+    case 3: return launch_ntt_pass<3, INVERSE>(a, t, ld, st, stream);
+    case 4: return launch_ntt_pass<4, INVERSE>(a, t, ld, st, stream);
+    case 5: return launch_ntt_pass<5, INVERSE>(a, t, ld, st, stream);
+    case 6: return launch_ntt_pass<6, INVERSE>(a, t, ld, st, stream);
+    case 7: return launch_ntt_pass<7, INVERSE>(a, t, ld, st, stream);
+    case 8: return launch_ntt_pass<8, INVERSE>(a, t, ld, st, stream);
+    case 9: return launch_ntt_pass<9, INVERSE>(a, t, ld, st, stream);
+    case 10: return launch_ntt_pass<10, INVERSE>(a, t, ld, st, stream);
+    case 11: return launch_ntt_pass<11, INVERSE>(a, t, ld, st, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// Batched forward NTT of `polys` x `limbs` limbs.  The first pass reads through
+// `ld`, the last pass writes through `st`; intermediate data lives in `work`
+// ([poly][limb][N], stride work_stride), which may alias the final destination.
+template <class Loader, class Storer>
+cudaError_t forward_ntt(int log_n, int polys, int limbs, int prime_base, const PrimeTables &t,
+                        const Loader &ld, const Storer &st, int64_t *work, long long work_stride,
+                        cudaStream_t stream) {
+  const NttPlan plan = ntt_plan(log_n);
+  NttPass a{log_n, 0, 0, 1, polys, limbs, prime_base};
+  if (plan.passes == 1) {
+    a.stride_log = 0;
+    a.first = 0;
+    a.columns = 1;
+    return dispatch_ntt_pass<false>(plan.s_first, a, t, ld, st, stream);
+  }
+  PlainStore mid_store{work, work_stride};
+  PlainLoad mid_load{work, work_stride};
+  a.stride_log = plan.s_second;
+  a.first = 0;
+  a.columns = (1 << plan.s_first) >= 512 ? 8 : 16;
+  cudaError_t e = dispatch_ntt_pass<false>(plan.s_first, a, t, ld, mid_store, stream);
+  if (e != cudaSuccess) return e;
+  a.stride_log = 0;
+  a.first = plan.s_first;
+  a.columns = kNttTileWords >> plan.s_second;
+  return dispatch_ntt_pass<false>(plan.s_second, a, t, mid_load, st, stream);
+}
+
+template <class Loader, class Storer>
+cudaError_t inverse_ntt(int log_n, int polys, int limbs, int prime_base, const PrimeTables &t,
+                        const Loader &ld, const Storer &st, int64_t *work, long long work_stride,
+                        cudaStream_t stream) {
+  const NttPlan plan = ntt_plan(log_n);
+  NttPass a{log_n, 0, 0, 1, polys, limbs, prime_base};
+  if (plan.passes == 1) {
+    a.stride_log = 0;
+    a.first = 0;
+    a.columns = 1;
+    return dispatch_ntt_pass<true>(plan.s_first, a, t, ld, st, stream);
+  }
+  PlainStore mid_store{work, work_stride};
+  PlainLoad mid_load{work, work_stride};
+  a.stride_log = 0;
+  a.first = 0;
+  a.columns = kNttTileWords >> plan.s_second;
+  cudaError_t e = dispatch_ntt_pass<true>(plan.s_second, a, t, ld, mid_store, stream);
+  if (e != cudaSuccess) return e;
+  a.stride_log = plan.s_second;
+  a.first = plan.s_second;
+  a.columns = (1 << plan.s_first) >= 512 ? 8 : 16;
+  return dispatch_ntt_pass<true>(plan.s_first, a, t, mid_load, st, stream);
+}
+
+}  // namespace fhe_b200

@@ -1,0 +1,211 @@
+"""Python host mirror of the reference engine API over the C ABI.
+
+Names and argument meaning follow DESILO FHE's CKKSEngine (src/ckks/engine.h):
+``multiply``, ``relinearize``, ``rescale``, ``ntt`` / ``intt``; objects are HBM
+resident and wrapped by :class:`Data`.  Errors raise :class:`FheError` carrying the
+reference's message text (``"<Function Name>: <reason>"``).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import FheError, check  # noqa: F401  (re-exported)
+
+# DataFlag (src/data/flag.h:7-13)
+NONE, COMPLEX, NTT_FORM, RESCALED, SPARSE, INCLUDE_SPECIAL = 0, 1, 2, 4, 8, 16
+# Object kinds (include/fhe_b200.h)
+SECRET_KEY, PUBLIC_KEY, RELINEARIZATION_KEY, UNIT_CIPHERTEXT, UNIT_PLAINTEXT = 1, 2, 3, 4, 5
+FIXED_ROTATION_KEY, CONJUGATION_KEY, KEY_SWITCHING_KEY = 6, 7, 8
+# SchemePreset (src/engine/scheme_preset.h)
+CKKS_40_60_DEFAULT, CKKS_54_60_BOOTSTRAP = 1, 2
+CKKS_40_60_DEFAULT_ENGINE_TEST, CKKS_54_60_BOOTSTRAP_ENGINE_TEST = 3, 4
+
+
+class Data:
+    """One HBM-resident object (key, ciphertext or plaintext)."""
+
+    def __init__(self, engine: "Engine", handle: ctypes.c_void_p):
+        self.engine = engine
+        self._h = handle
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self) -> dict:
+        inf = _lib.FheDataInfo()
+        check(_lib.load().fhe_data_info_get(self._h, ctypes.byref(inf)))
+        return dict(type=inf.type, flag=inf.flag, moduli_id=inf.moduli_id, level=inf.level,
+                    polys=inf.polys, chains=inf.chains, delta=inf.delta, scale=inf.ckks_scale)
+
+    @property
+    def level(self) -> int:
+        return self.info()["level"]
+
+    def download(self) -> np.ndarray:
+        i = self.info()
+        out = np.empty((i["polys"], i["chains"], self.engine.coeff_count), dtype=np.int64)
+        check(_lib.load().fhe_data_download(self._h, out.ctypes.data_as(_lib._i64p)))
+        return out
+
+    def device_pointer(self) -> int:
+        p = _lib._i64p()
+        check(_lib.load().fhe_data_device_pointer(self._h, ctypes.byref(p)))
+        return ctypes.cast(p, ctypes.c_void_p).value
+
+    def free(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.load().fhe_data_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Engine:
+    """CKKS engine on one B200 (create_ckks_engine(CKKSConfig))."""
+
+    def __init__(self, log_coeff_count: int = 14, special_prime_count: int = 1,
+                 max_level: int = -1, scheme_preset: int = CKKS_40_60_DEFAULT,
+                 log_slot_count: int = -1):
+        lib = _lib.load()
+        cfg = _lib.FheConfig(log_coeff_count, log_slot_count, special_prime_count, max_level,
+                             scheme_preset)
+        h = ctypes.c_void_p()
+        check(lib.fhe_engine_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        inf = _lib.FheEngineInfo()
+        check(lib.fhe_engine_info_get(self._h, ctypes.byref(inf)))
+        self.coeff_count = inf.coeff_count
+        self.slot_count = inf.slot_count
+        self.chain_count = inf.chain_count
+        self.prime_count = inf.prime_count
+        self.special_prime_count = inf.special_prime_count
+        self.full_level = inf.full_level
+        self.max_level = inf.max_level
+        self.max_key_switching_level = inf.max_key_switching_level
+        self.scale_bit_length = inf.scale_bit_length
+        q = (ctypes.c_uint64 * self.prime_count)()
+        check(lib.fhe_engine_moduli(self._h, q, self.prime_count))
+        self.moduli = np.array(list(q), dtype=np.uint64)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.load().fhe_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ------------------------------------------------------------- metadata --
+    def moduli_id(self, level: int) -> int:
+        out = ctypes.c_int()
+        check(_lib.load().fhe_engine_moduli_id(self._h, level, ctypes.byref(out)))
+        return out.value
+
+    def chains(self, moduli_id: int, include_special: bool = False) -> int:
+        return self.chain_count - moduli_id + (self.special_prime_count if include_special else 0)
+
+    def partition_count(self, moduli_id: int) -> int:
+        k = self.special_prime_count
+        return (self.chains(moduli_id) + k - 1) // k
+
+    def synchronize(self) -> None:
+        check(_lib.load().fhe_engine_synchronize(self._h))
+
+    def set_stream(self, cuda_stream: int | None) -> None:
+        check(_lib.load().fhe_engine_set_stream(self._h, cuda_stream or None))
+
+    # ----------------------------------------------------------- profiling --
+    def set_profiling(self, enable: bool) -> None:
+        check(_lib.load().fhe_engine_set_profiling(self._h, int(enable)))
+
+    def profile(self) -> dict:
+        """{kernel family: (launches, total device ms)} since the last reset."""
+        buf = ctypes.create_string_buffer(1 << 16)
+        check(_lib.load().fhe_engine_profile_report(self._h, buf, len(buf)))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, launches, ms = line.split()
+            out[name] = (int(launches), float(ms))
+        return out
+
+    def profile_reset(self) -> None:
+        check(_lib.load().fhe_engine_profile_reset(self._h))
+
+    @staticmethod
+    def kernel_launch_count() -> int:
+        return int(_lib.load().fhe_kernel_launch_count())
+
+    # -------------------------------------------------------------- objects --
+    def upload(self, limbs, moduli_id: int, flag: int = NONE, kind: int = UNIT_CIPHERTEXT,
+               scale: float = 1.0) -> Data:
+        limbs = np.ascontiguousarray(limbs, dtype=np.int64)
+        polys = limbs.shape[0]
+        chains = self.chains(moduli_id, bool(flag & INCLUDE_SPECIAL))
+        if limbs.shape != (polys, chains, self.coeff_count):
+            raise ValueError(f"limbs must have shape ({polys}, {chains}, {self.coeff_count})")
+        h = ctypes.c_void_p()
+        check(_lib.load().fhe_data_upload(self._h, kind, flag, moduli_id, polys, scale,
+                                          limbs.ctypes.data_as(_lib._i64p), ctypes.byref(h)))
+        return Data(self, h)
+
+    def upload_from_pointer(self, host_ptr: int, moduli_id: int, polys: int, flag: int = NONE,
+                            kind: int = UNIT_CIPHERTEXT, scale: float = 1.0) -> Data:
+        """Upload limbs [polys][chains][N] from a raw host address (e.g. pinned memory)."""
+        h = ctypes.c_void_p()
+        check(_lib.load().fhe_data_upload(self._h, kind, flag, moduli_id, polys, scale,
+                                          ctypes.cast(host_ptr, _lib._i64p), ctypes.byref(h)))
+        return Data(self, h)
+
+    def download_to_pointer(self, data: Data, host_ptr: int, wait: bool = True) -> None:
+        fn = _lib.load().fhe_data_download if wait else _lib.load().fhe_data_download_async
+        check(fn(data.handle, ctypes.cast(host_ptr, _lib._i64p)))
+
+    def upload_relinearization_key(self, limbs, moduli_id: int) -> Data:
+        return self.upload(limbs, moduli_id, NTT_FORM | INCLUDE_SPECIAL, RELINEARIZATION_KEY)
+
+    def _call(self, fn, *args) -> Data:
+        h = ctypes.c_void_p()
+        check(getattr(_lib.load(), fn)(self._h, *[a.handle for a in args], ctypes.byref(h)))
+        return Data(self, h)
+
+    # ------------------------------------------------------------ operations --
+    def multiply(self, a: Data, b: Data, relinearization_key: Data | None = None) -> Data:
+        if relinearization_key is None:
+            return self._call("fhe_multiply", a, b)
+        return self._call("fhe_multiply_relinearize", a, b, relinearization_key)
+
+    def multiply_relinearize_rescale(self, a: Data, b: Data, relinearization_key: Data) -> Data:
+        return self._call("fhe_multiply_relinearize_rescale", a, b, relinearization_key)
+
+    def relinearize(self, ct: Data, relinearization_key: Data) -> Data:
+        return self._call("fhe_relinearize", ct, relinearization_key)
+
+    def rescale(self, ct: Data) -> Data:
+        return self._call("fhe_rescale", ct)
+
+    def ntt(self, text: Data) -> Data:
+        return self._call("fhe_to_ntt", text)
+
+    def intt(self, text: Data) -> Data:
+        return self._call("fhe_to_intt", text)
+
+    def ntt_limbs(self, device_ptr: int, moduli_id: int, chains: int, polys: int,
+                  poly_stride: int, inverse: bool = False) -> None:
+        """Plain per-limb NTT/iNTT (SingleProcessor::ntt/intt) on device memory, in place."""
+        check(_lib.load().fhe_ntt_limbs(self._h, ctypes.cast(device_ptr, _lib._i64p), moduli_id,
+                                        chains, polys, poly_stride, int(inverse)))

@@ -1,0 +1,211 @@
+/*
+ * fhe_b200 -- C ABI of the B200-native CKKS engine.
+ *
+ * The drop-in boundary for the reference's CKKS hot path (DESILO FHE,
+ * open-source variant).  The reference exposes a C++ pure-virtual engine
+ * (src/engine/abstract_engine.h:12-299, implemented by CKKSEngine in
+ * src/ckks/engine.h:19-897) and no C ABI; every function below replaces one of
+ * its members, cited beside it.  Objects live in HBM behind opaque handles; limbs
+ * cross the boundary as plain int64 arrays laid out [poly][limb][N] in the
+ * reference's own representation (Montgomery domain with R = 2^62 in NTT form,
+ * bit-reversed NTT order), so keys and ciphertexts move between the reference and
+ * this engine unchanged.
+ *
+ * Conventions
+ *  - Every function returns FHE_OK (0) or a negative fhe_status; the message of
+ *    the last failure on the calling thread is fhe_last_error().  The reference
+ *    throws std::invalid_argument / std::runtime_error with
+ *    "<Function Name>: <reason>" (src/ckks/engine_require.cpp); the same text is
+ *    reported here and the exception class maps to FHE_ERR_INVALID_ARGUMENT /
+ *    FHE_ERR_RUNTIME.
+ *  - Operations return new objects owned by the caller (fhe_data_destroy), as the
+ *    reference returns new heap objects the caller deletes.
+ *  - Work is queued on the engine's CUDA stream; fhe_data_download and
+ *    fhe_engine_synchronize wait for it.  One engine per thread, or external
+ *    locking (the reference engine is not thread-safe either).
+ *  - No function aborts the process or traps the GPU.
+ */
+#ifndef FHE_B200_H
+#define FHE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum fhe_status {
+  FHE_OK = 0,
+  FHE_ERR_INVALID_ARGUMENT = -1, /* std::invalid_argument in the reference */
+  FHE_ERR_RUNTIME = -2,          /* std::runtime_error in the reference */
+  FHE_ERR_CUDA = -3,             /* a CUDA call failed */
+  FHE_ERR_OUT_OF_MEMORY = -4,
+  FHE_ERR_NULL_HANDLE = -5,
+  FHE_ERR_UNSUPPORTED = -6
+} fhe_status;
+
+/* SchemePreset, src/engine/scheme_preset.h:9-15 */
+enum {
+  FHE_PRESET_CKKS_40_60_DEFAULT = 1,
+  FHE_PRESET_CKKS_54_60_BOOTSTRAP = 2,
+  FHE_PRESET_CKKS_40_60_DEFAULT_ENGINE_TEST = 3,
+  FHE_PRESET_CKKS_54_60_BOOTSTRAP_ENGINE_TEST = 4
+};
+
+/* DataFlag bits, src/data/flag.h:7-13 */
+enum {
+  FHE_FLAG_NONE = 0,
+  FHE_FLAG_COMPLEX = 1,
+  FHE_FLAG_NTT_FORM = 2,
+  FHE_FLAG_RESCALED = 4,
+  FHE_FLAG_SPARSE = 8,
+  FHE_FLAG_INCLUDE_SPECIAL = 16
+};
+
+/* Object kinds: SecretKey, PublicKey, RelinearizationKey, UnitCiphertext,
+ * UnitPlaintext, FixedRotationKey, ConjugationKey, KeySwitchingKey
+ * (src/data/data.h:94-300). */
+enum {
+  FHE_SECRET_KEY = 1,
+  FHE_PUBLIC_KEY = 2,
+  FHE_RELINEARIZATION_KEY = 3,
+  FHE_UNIT_CIPHERTEXT = 4,
+  FHE_UNIT_PLAINTEXT = 5,
+  FHE_FIXED_ROTATION_KEY = 6,
+  FHE_CONJUGATION_KEY = 7,
+  FHE_KEY_SWITCHING_KEY = 8
+};
+
+typedef struct fhe_engine fhe_engine;
+typedef struct fhe_data fhe_data;
+
+/* CKKSConfig, src/ckks/config.h:11-34 (processor/stream/thread fields have no
+ * GPU meaning and are absent). */
+typedef struct fhe_config {
+  int log_coeff_count;     /* default 14 */
+  int log_slot_count;      /* -1: log_coeff_count - 1 */
+  int special_prime_count; /* default 1 */
+  int max_level;           /* -1: full level */
+  int scheme_preset;       /* FHE_PRESET_* */
+} fhe_config;
+
+typedef struct fhe_engine_info {
+  int coeff_count;         /* N */
+  int slot_count;
+  int chain_count;         /* non-special primes at moduli id 0 */
+  int prime_count;         /* chain_count + special_prime_count */
+  int special_prime_count;
+  int full_level;
+  int max_level;
+  int max_key_switching_level;
+  int scale_bit_length;
+} fhe_engine_info;
+
+typedef struct fhe_data_info {
+  int type;       /* FHE_SECRET_KEY ... */
+  int flag;       /* FHE_FLAG_* bits */
+  int moduli_id;  /* first prime of the object's chain */
+  int level;      /* to_level, src/data/data.h:21-32 */
+  int polys;      /* polynomial count */
+  int chains;     /* limbs per polynomial (with specials when INCLUDE_SPECIAL) */
+  int delta;      /* rotation step of a fixed rotation key, else 0 */
+  long double ckks_scale;
+} fhe_data_info;
+
+/* ---- library / engine ------------------------------------------------------ */
+
+/* Message of the last failure on this thread ("" when none). */
+const char *fhe_last_error(void);
+/* fhe_config with the reference's defaults (CKKSConfig{}). */
+void fhe_config_default(fhe_config *config);
+
+/* create_ckks_engine(CKKSConfig), src/engine/engine.cpp:17-20 (validates the
+ * config like CKKSConfig::validate, src/ckks/config.cpp:9-47). */
+int fhe_engine_create(const fhe_config *config, fhe_engine **engine);
+/* delete engine */
+int fhe_engine_destroy(fhe_engine *engine);
+/* get_coeff_count/get_slot_count/... , src/ckks/engine.h:505-515 */
+int fhe_engine_info_get(const fhe_engine *engine, fhe_engine_info *info);
+/* The full moduli chain q_0..q_{P-1} (CKKSParameters::get_moduli(0),
+ * src/ckks/parameters.cpp:219-238).  Writes min(capacity, P) values. */
+int fhe_engine_moduli(const fhe_engine *engine, uint64_t *moduli, int capacity);
+/* CKKSParameters::get_moduli_id(level), src/ckks/parameters.cpp:246-248 */
+int fhe_engine_moduli_id(const fhe_engine *engine, int level, int *moduli_id);
+/* Wait for all queued work. */
+int fhe_engine_synchronize(fhe_engine *engine);
+/* Queue subsequent work on a caller-owned cudaStream_t (NULL: the engine's own). */
+int fhe_engine_set_stream(fhe_engine *engine, void *cuda_stream);
+
+/* Diagnostics (no reference counterpart; the reference has no tracing).  While
+ * profiling is on, each kernel family launched on the engine's stream is timed with
+ * CUDA events; the report is "name launches total_ms" lines.  The launch count is
+ * the number of kernels this library has launched in the process. */
+int fhe_engine_set_profiling(fhe_engine *engine, int enable);
+int fhe_engine_profile_report(fhe_engine *engine, char *buffer, int capacity);
+int fhe_engine_profile_reset(fhe_engine *engine);
+unsigned long long fhe_kernel_launch_count(void);
+
+/* Host-only parameter queries (no GPU needed).  The moduli chain and per-prime
+ * tables a config produces: CKKSParameters (src/ckks/parameters.cpp:9-105) and
+ * CKKSPrecomputed / CKKSDerivedParameters (src/ckks/precomputed.cpp:33-217,
+ * src/ckks/derived_parameters.cpp:19-50).  `moduli` receives up to `capacity`
+ * primes; each table pointer may be NULL, and root tables hold
+ * prime_count * (N - 1) entries. */
+int fhe_parameters_query(const fhe_config *config, fhe_engine_info *info, uint64_t *moduli,
+                         int capacity);
+int fhe_parameters_tables(const fhe_config *config, uint64_t *k, int64_t *r_squared,
+                          int64_t *n_inverse, int64_t *root, int64_t *root_inverse);
+
+/* ---- objects ------------------------------------------------------------------ */
+
+/* Build an object from host limbs [polys][chains][N] (chains implied by
+ * moduli_id and FHE_FLAG_INCLUDE_SPECIAL).  Replaces constructing Data
+ * (src/data/data.cpp:9-48) around the reference's per-limb arrays. */
+int fhe_data_upload(fhe_engine *engine, int type, int flag, int moduli_id, int polys,
+                    long double ckks_scale, const int64_t *host_limbs, fhe_data **out);
+/* Copy all limbs to host memory [polys][chains][N] (waits for queued work). */
+int fhe_data_download(const fhe_data *data, int64_t *host_limbs);
+/* Queue the same copy on the engine's stream without waiting (the host buffer
+ * should be pinned; completion is observed with fhe_engine_synchronize). */
+int fhe_data_download_async(const fhe_data *data, int64_t *host_limbs);
+int fhe_data_info_get(const fhe_data *data, fhe_data_info *info);
+/* Set the rotation step carried by a fixed rotation key (FixedRotationKey::delta_). */
+int fhe_data_set_delta(fhe_data *data, int delta);
+/* Device address of the limbs (valid until fhe_data_destroy). */
+int fhe_data_device_pointer(const fhe_data *data, int64_t **device_limbs);
+int fhe_data_destroy(fhe_data *data);
+
+/* ---- CKKS operations (engine level, src/ckks/engine.h) ---------------------------- */
+
+/* CKKSEngine::multiply(UnitCiphertext*, UnitCiphertext*), engine_multiply.cpp:40-57:
+ * lazy rescale of both inputs (prepare_for_multiply, :13-28), then the tensor. */
+int fhe_multiply(fhe_engine *engine, const fhe_data *a, const fhe_data *b, fhe_data **out);
+/* CKKSEngine::multiply(ct, ct, RelinearizationKey*), engine_multiply.cpp:132-147 */
+int fhe_multiply_relinearize(fhe_engine *engine, const fhe_data *a, const fhe_data *b,
+                             const fhe_data *relinearization_key, fhe_data **out);
+/* CKKSEngine::relinearize, engine_relinearize.cpp:14-29 */
+int fhe_relinearize(fhe_engine *engine, const fhe_data *ct, const fhe_data *relinearization_key,
+                    fhe_data **out);
+/* CKKSEngine::rescale, engine_rescale.cpp:45-55 */
+int fhe_rescale(fhe_engine *engine, const fhe_data *ct, fhe_data **out);
+/* engine.multiply(a, b, rk) followed by engine.rescale(.) in one call: the same
+ * output words as the two reference calls, with the relinearized intermediate
+ * never leaving the chip. */
+int fhe_multiply_relinearize_rescale(fhe_engine *engine, const fhe_data *a, const fhe_data *b,
+                                     const fhe_data *relinearization_key, fhe_data **out);
+/* CKKSEngine::ntt / intt (engine_ntt.cpp:35-42, engine_intt.cpp) */
+int fhe_to_ntt(fhe_engine *engine, const fhe_data *text, fhe_data **out);
+int fhe_to_intt(fhe_engine *engine, const fhe_data *text, fhe_data **out);
+
+/* ---- processor-level kernels on device limbs (src/processor/single.h) --------------- */
+
+/* SingleProcessor::ntt / intt (single.cpp:420-454) on `polys` x `chains` device limbs
+ * at moduli_id, in place, [poly][chain][N] with the given poly stride (words). */
+int fhe_ntt_limbs(fhe_engine *engine, int64_t *device_limbs, int moduli_id, int chains,
+                  int polys, long long poly_stride, int inverse);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FHE_B200_H */

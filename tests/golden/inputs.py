@@ -1,0 +1,53 @@
+"""Seeded synthetic inputs shared by the fixture generator and the tests.
+
+Residues are uniform in [0, q_i) per limb from numpy's PCG64 generator, so a
+fixture only needs to store its seed and the digest of the expected output.
+"""
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+
+# (log_n, special_prime_count, scheme_preset) of the reference's tiers
+# (ckks/config.cpp:106-139, for_bootstrap :188-193).  Sand/Pebble use the
+# engine-test preset, which has the same chain as the default preset there.
+TIERS = {
+    "sand": (3, 1, 3),
+    "pebble": (4, 1, 3),
+    "iron": (13, 1, 1),
+    "bronze": (14, 1, 1),
+    "silver": (15, 2, 1),
+    "gold": (16, 4, 1),
+    "platinum": (17, 6, 1),
+    "bootstrap_gold": (16, 4, 2),
+}
+
+
+def uniform_limbs(rng: np.random.Generator, moduli, polys: int, n: int) -> np.ndarray:
+    out = np.empty((polys, len(moduli), n), dtype=np.int64)
+    for p in range(polys):
+        for j, q in enumerate(moduli):
+            out[p, j] = rng.integers(0, int(q), size=n, dtype=np.int64)
+    return out
+
+
+def digest(a: np.ndarray) -> str:
+    a = np.ascontiguousarray(a, dtype=np.int64)
+    return hashlib.sha256(a.tobytes()).hexdigest()
+
+
+def case_inputs(seed: int, moduli, n: int, moduli_id: int, special: int):
+    """Inputs of one op-parity case at `moduli_id`: two 2-poly texts, one 3-poly
+    NTT text and a relinearization key at the same moduli id."""
+    rng = np.random.default_rng(seed)
+    chain = len(moduli) - special
+    L = chain - moduli_id
+    qs = moduli[moduli_id:moduli_id + L]
+    ext = moduli[moduli_id:]
+    dnum = (L + special - 1) // special
+    a = uniform_limbs(rng, qs, 2, n)
+    b = uniform_limbs(rng, qs, 2, n)
+    ct3 = uniform_limbs(rng, qs, 3, n)
+    key = uniform_limbs(rng, ext, 2 * dnum, n)
+    return a, b, ct3, key

@@ -1,0 +1,138 @@
+"""Regenerate the golden fixtures under tests/golden/.
+
+1. ``ntt_kat.json`` and ``precomputed_kat.json``: the known-answer vectors of the
+   reference's own unit tests (test/operation/ntt.cpp and
+   test/ckks/precomputed/default.cpp), read as text.
+2. ``ref_ops.json``: outputs of the compiled reference library (oracle/_ref, built
+   by ``make -C oracle ref``) on seeded inputs (tests/golden/inputs.py): NTT /
+   iNTT, tensor, relinearize, rescale and engine multiply+relinearize+rescale,
+   stored as SHA-256 digests of the int64 limbs (full arrays for N <= 16).
+
+Needs the reference tree (default /root/reference, or $FHE_REFERENCE); the tests
+read only the committed JSON.  Usage: python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import json
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, HERE)
+
+from inputs import TIERS, case_inputs, digest  # noqa: E402
+
+REF = os.environ.get("FHE_REFERENCE", "/root/reference")
+
+
+def _tests(text: str):
+    """Split a googletest file into {name: body}."""
+    out = {}
+    for m in re.finditer(r"TEST\((\w+),\s*(\w+)\)\s*\{", text):
+        start = m.end()
+        depth, i = 1, start
+        while depth:
+            depth += {"{": 1, "}": -1}.get(text[i], 0)
+            i += 1
+        out[f"{m.group(1)}.{m.group(2)}"] = text[start:i - 1]
+    return out
+
+
+def _ints(body: str):
+    return [int(eval(v.strip())) for v in body.replace("\n", " ").split(",") if v.strip()]
+
+
+def parse_ntt_kats():
+    text = open(os.path.join(REF, "test/operation/ntt.cpp")).read()
+    kats = []
+    for name, body in _tests(text).items():
+        if not re.match(r"^NTT\.I?NTT(Inplace)?\d$", name):
+            continue  # split/unit helpers and composite tests are not single transforms
+        call = re.search(r"desilo::fhe::(ntt|intt)\((\w+),\s*(\w+),\s*(\w+)", body)
+        if not call:
+            continue
+        kind, src, dst, table = call.groups()
+        arrays = {m.group(1): _ints(m.group(2))
+                  for m in re.finditer(r"int64_t\s+(\w+)\[\d*\]\s*\{([^}]*)\}", body)}
+        scalars = {m.group(1): int(m.group(2))
+                   for m in re.finditer(r"(?:uint64_t|int64_t|int)\s+(\w+)\s*=\s*(\d+)\s*;", body)}
+        kats.append(dict(name=name, kind=kind, x=arrays[src], table=arrays[table],
+                         q=scalars["q"], k=scalars["k"], expected=arrays["expected"]))
+    return kats
+
+
+def parse_precomputed_kats():
+    text = open(os.path.join(REF, "test/ckks/precomputed/default.cpp")).read()
+    out = {}
+    for name, body in _tests(text).items():
+        tier = re.search(r'from_tier\("(\w+)"\)', body)
+        if tier:
+            tier = tier.group(1)
+        elif "for_bootstrap()" in body:
+            tier = "bootstrap_gold"
+        else:
+            continue
+        vectors = {}
+        for m in re.finditer(r"std::vector<(u?int64_t)>\s+(\w+)\s*=\s*\{(.*?)\};", body, re.S):
+            vectors[m.group(2)] = _ints(m.group(3))
+        for m in re.finditer(r"std::vector<std::vector<int64_t>>\s+(\w+)\s*=\s*\{(.*?)\};", body, re.S):
+            rows = re.findall(r"\{([^{}]*)\}", m.group(2))
+            vectors[m.group(1)] = [_ints(r) for r in rows]
+        out[name] = dict(tier=tier, vectors=vectors)
+    return out
+
+
+def reference_ops():
+    from oracle import ref
+
+    cases = []
+    plan = [("pebble", [0, 1, 5]), ("sand", [2]), ("iron", [1]), ("bronze", [1, 3]),
+            ("silver", [1]), ("gold", [5]), ("bootstrap_gold", [1])]
+    seed = 1000
+    for tier, moduli_ids in plan:
+        log_n, K, preset = TIERS[tier]
+        e = ref.Engine(log_n=log_n, special_prime_count=K, preset=preset)
+        q = e.tables()["q"]
+        n = e.n
+        for mid in moduli_ids:
+            seed += 1
+            a, b, ct3, key = case_inputs(seed, q, n, mid, K)
+            res = {}
+            x = e.text(a, mid, flag=0)
+            xn = e.core_to_ntt(x)
+            res["to_ntt"] = xn.limbs()
+            res["to_intt"] = e.core_to_intt(e.text(a, mid, flag=2)).limbs()
+            res["tensor"] = e.core_tensor(e.text(a, mid, flag=2), e.text(b, mid, flag=2)).limbs()
+            rk = e.relin_key(key, mid)
+            res["relinearize"] = e.core_relinearize(e.text(ct3, mid, flag=2), rk).limbs()
+            res["rescale"] = e.core_rescale(e.text(a, mid, flag=0)).limbs()
+            try:
+                m = e.multiply(e.text(a, mid, flag=0), e.text(b, mid, flag=0), rk)
+                res["mult_relin_rescale"] = e.rescale(m).limbs()
+            except RuntimeError:
+                pass
+            entry = dict(tier=tier, log_n=log_n, special_prime_count=K, preset=preset,
+                         moduli_id=mid, seed=seed, moduli=[int(v) for v in q],
+                         digests={k: digest(v) for k, v in res.items()})
+            if n <= 16:
+                entry["arrays"] = {k: v.tolist() for k, v in res.items()}
+            cases.append(entry)
+    return cases
+
+
+def main():
+    with open(os.path.join(HERE, "ntt_kat.json"), "w") as f:
+        json.dump(parse_ntt_kats(), f, indent=1)
+    with open(os.path.join(HERE, "precomputed_kat.json"), "w") as f:
+        json.dump(parse_precomputed_kats(), f, indent=1)
+    with open(os.path.join(HERE, "ref_ops.json"), "w") as f:
+        json.dump(reference_ops(), f, indent=1)
+
+
+if __name__ == "__main__":
+    main()
