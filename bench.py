@@ -221,6 +221,57 @@ def cpu_baseline_sample():
             "sample": "reference library not built on this host"}
 
 
+# ------------------------------------------------------------ NTT microbench --
+
+def run_ntt_microbench(args, torch, np, rank, world, local, backend, stream):
+    """Forward NTT (SingleProcessor::ntt per limb) of `batch` polynomials of 24 limbs
+    at N = 2^16 over the first 24 primes of the Gold chain, in place.  Algorithmic
+    bytes: one read and one write of every limb (twiddles excluded)."""
+    from fhe_b200 import Engine, UNIT_PLAINTEXT
+    from inputs import uniform_limbs
+
+    eng = Engine(log_coeff_count=16, special_prime_count=4)
+    eng.set_stream(stream.cuda_stream)
+    n, limbs, B = eng.coeff_count, 24, args.batch
+    rng = np.random.default_rng(5 + rank)
+    buf = eng.upload(uniform_limbs(rng, eng.moduli[:limbs], B, n), eng.chain_count - limbs,
+                     kind=UNIT_PLAINTEXT)
+    ptr = buf.device_pointer()
+    stride = limbs * n
+    for _ in range(args.warmup):
+        eng.ntt_limbs(ptr, 0, limbs, B, stride)
+    torch.cuda.synchronize()
+    if backend:
+        torch.distributed.barrier()
+    launches0 = Engine.kernel_launch_count()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            eng.ntt_limbs(ptr, 0, limbs, B, stride)
+        stop.record(stream)
+        torch.cuda.synchronize()
+    elapsed = start.elapsed_time(stop)
+    launches = Engine.kernel_launch_count() - launches0
+    elapsed_max, units = aggregate(elapsed, float(B * args.steps), world, backend)
+    bytes_per_step = 2 * B * limbs * n * 8
+    gbs = bytes_per_step * args.steps * world / (elapsed_max / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "forward NTT polys/s (24 limbs, N=2^16)", "value": units / (elapsed_max / 1e3),
+            "unit": "polys/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": elapsed_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic uniform residues",
+            "config": {"workload": "ntt 24 limbs x batch", "batch": B},
+            "roofline": {"bound": "hbm", "achieved": gbs / world, "peak": peak, "unit": "GB/s",
+                         "frac": gbs / world / peak, "traffic": None, "peak_source": peak_kind},
+            "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
+    buf.free()
+    eng.close()
+    return 0
+
+
 # -------------------------------------------------------------------- main --
 
 def main(argv=None):
@@ -230,6 +281,8 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--batch", type=int, default=16, help="ciphertext pairs per step")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="hmult", choices=["hmult", "ntt"],
+                    help="hmult: the headline; ntt: forward NTT of --batch x 24 limbs at N=2^16")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args(argv)
     rank, world, local = dist_env()
@@ -255,8 +308,13 @@ def main(argv=None):
     from fhe_b200 import Engine, NTT_FORM, INCLUDE_SPECIAL, RELINEARIZATION_KEY
     from inputs import uniform_limbs
 
+    # A dedicated stream for the engine and for the timing events (the legacy
+    # default stream does not order work on the engine's non-blocking streams).
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    if args.workload == "ntt":
+        return run_ntt_microbench(args, torch, np, rank, world, local, backend, stream)
     eng = Engine(log_coeff_count=LOG_N, special_prime_count=SPECIAL)
-    stream = torch.cuda.current_stream()
     eng.set_stream(stream.cuda_stream)
     n = eng.coeff_count
     level = eng.max_key_switching_level

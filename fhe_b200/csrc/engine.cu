@@ -85,6 +85,13 @@ Engine::Engine(const Config &config) : params(config) {
   tables_.n_inverse = upload_table(p.n_inverse);
   tables_.root = upload_table(p.root);
   tables_.root_inverse = upload_table(p.root_inverse);
+  std::vector<double> inv_q(P), inv_2q(P);
+  for (int i = 0; i < P; i++) {
+    inv_q[i] = 1.0 / static_cast<double>(p.q[i]);
+    inv_2q[i] = 1.0 / (2.0 * static_cast<double>(p.q[i]));
+  }
+  tables_.inv_q = upload_table(inv_q);
+  tables_.inv_2q = upload_table(inv_2q);
   tables_.log_n = p.log_n;
 
   std::vector<int64_t> pinv(static_cast<size_t>(std::max(p.special_prime_count, 1)) * P, 0);

@@ -31,7 +31,7 @@ __global__ void tensor_kernel(PrimeTables t, int n, int limbs, int prime_base, c
   const long long ps = total;
   for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
        i += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const int prime = prime_base + static_cast<int>(i / n);
+    const int prime = prime_base + static_cast<int>(i >> (__ffs(n) - 1));
     const uint64_t q = t.q[prime], k = t.k[prime];
     const int64_t qs = static_cast<int64_t>(q), q2 = qs << 1;
     const int64_t a0 = a[i], a1 = a[ps + i], b0 = b[i], b1 = b[ps + i];
@@ -45,7 +45,7 @@ __global__ void add_reduce_kernel(PrimeTables t, int n, int limbs, int prime_bas
                                   const int64_t *x1, const int64_t *x2, int64_t *y) {
   for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
        i += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const int prime = prime_base + static_cast<int>((i / n) % limbs);
+    const int prime = prime_base + static_cast<int>((i >> (__ffs(n) - 1)) % limbs);
     const int64_t qs = static_cast<int64_t>(t.q[prime]);
     y[i] = guard(guard(x1[i] + x2[i], qs << 1), qs);
   }
@@ -73,7 +73,7 @@ __global__ void rescale_kernel(PrimeTables t, KeySwitchTables ks, int n, int lim
   int64_t *yp = y + poly * ys;
   for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < per_poly;
        i += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const int j = static_cast<int>(i / n);
+    const int j = static_cast<int>(i >> (__ffs(n) - 1));
     const int c = static_cast<int>(i - static_cast<long long>(j) * n);
     const int prime = moduli_id + 1 + j;
     const int64_t x0 = xp[c];
@@ -123,42 +123,89 @@ __global__ void mixed_radix_kernel(PrimeTables t, DevicePartitions dp, int n, in
   for (int c = 0; c < A; c++) digits[static_cast<long long>(start + c) * n + coeff] = y[c];
 }
 
-// ModUp contraction of one extended limb (core_key_switch.cpp:92-106), evaluated
-// while the forward NTT loads its input.
-struct ModUpLoad {
-  DevicePartitions dp;
-  const int64_t *digits;
-  const int64_t *r_squared;
-  const uint64_t *q;
-  const uint64_t *k;
-  __device__ __forceinline__ int64_t operator()(int p, int limb, int prime, int gi, int n) const {
-    const int start = dp.start[p];
-    const int size = dp.size[p];
-    const uint64_t qq = q[prime], kk = k[prime];
-    const int64_t q2 = static_cast<int64_t>(qq << 1);
-    const int64_t *d = digits + static_cast<long long>(start) * n + gi;
-    int64_t acc = mont_mult(d[0], r_squared[prime], qq, kk);
-    const int64_t *c = dp.product_r_squared + static_cast<long long>(p) * 16 * dp.extended + limb;
-    for (int ci = 0; ci < size - 1; ci++) {
-      acc = guard(mont_mult(d[static_cast<long long>(ci + 1) * n], c[static_cast<long long>(ci) * dp.extended], qq, kk) + acc, q2);
-    }
-    return acc;
+// ModUp contraction (core_key_switch.cpp:92-106): extended limb j of partition p
+// is the chain acc = guard(REDC(d_i c_ij) + acc, 2q) over the partition's digits
+// (c_0j = R^2 mod q_j).  A thread owns one coefficient of one partition, keeps its
+// alpha digits in registers and walks all extended limbs.  The chain is evaluated as
+// one lazy sum (RedcSum) when every digit is in [0, 2^61), which holds for all
+// digits produced from canonical inputs, and term by term otherwise; both give the
+// same word.
+template <int A>
+__global__ void __launch_bounds__(256)
+    mod_up_contract_kernel(PrimeTables t, DevicePartitions dp, int n, int moduli_id,
+                           const int64_t *digits, int64_t *ext) {
+  const int p = blockIdx.y;
+  if (dp.size[p] != A) return;
+  const int coeff = blockIdx.x * blockDim.x + threadIdx.x;
+  if (coeff >= n) return;
+  const int start = dp.start[p];
+  const int E = dp.extended;
+  int64_t d[A];
+  bool fast = true;
+#pragma unroll
+  for (int i = 0; i < A; i++) {
+    d[i] = digits[static_cast<long long>(start + i) * n + coeff];
+    fast = fast && redc_operand_ok(d[i]);
   }
-};
+  const int64_t *cst = dp.product_r_squared + static_cast<long long>(p) * 16 * E;
+  int64_t *out = ext + static_cast<long long>(p) * E * n + coeff;
+  for (int j = 0; j < E; j++) {
+    const int prime = moduli_id + j;
+    const uint64_t q = t.q[prime], k = t.k[prime];
+    int64_t v;
+    if (fast) {
+      RedcSum sum;
+      sum.add(static_cast<uint64_t>(d[0]), static_cast<uint64_t>(t.r_squared[prime]), k);
+#pragma unroll
+      for (int i = 1; i < A; i++)
+        sum.add(static_cast<uint64_t>(d[i]), static_cast<uint64_t>(cst[(i - 1) * E + j]), k);
+      v = sum.reduce(q, q << 1, t.inv_2q[prime]);
+    } else {
+      const int64_t q2 = static_cast<int64_t>(q << 1);
+      v = mont_mult(d[0], t.r_squared[prime], q, k);
+#pragma unroll
+      for (int i = 1; i < A; i++) v = guard(mont_mult(d[i], cst[(i - 1) * E + j], q, k) + v, q2);
+    }
+    out[static_cast<long long>(j) * n] = v;
+  }
+}
 
 // ------------------------------------------------------ key inner product --
 
+// With two or more partitions the reference chain (mont_mult, then mont_mult_add
+// and reduce_2q_to_q per further partition) equals (sum t_p) mod q; it is evaluated
+// as a lazy sum when every operand is in [0, 2^61) and term by term otherwise.
 __global__ void key_inner_product_kernel(PrimeTables t, DevicePartitions dp, int n, int moduli_id,
                                          const int64_t *ext, const int64_t *key, int key_primes,
                                          int view_offset, int64_t *acc) {
   const int E = dp.extended;
   const long long total = static_cast<long long>(E) * n;
+  const int log_n = __ffs(n) - 1;
   for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
        i += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const int j = static_cast<int>(i / n);
+    const int j = static_cast<int>(i >> log_n);
     const int prime = moduli_id + j;
     const uint64_t q = t.q[prime], k = t.k[prime];
     const int64_t qs = static_cast<int64_t>(q), q2 = qs << 1;
+    bool fast = dp.count >= 2;
+    RedcSum s0, s1;
+    for (int p = 0; p < dp.count && fast; p++) {
+      const int64_t e = ext[static_cast<long long>(p) * total + i];
+      const int kidx = dp.key_index[p];
+      const int64_t k0 = key[(static_cast<long long>(2 * kidx) * key_primes + view_offset) * n + i];
+      const int64_t k1 = key[(static_cast<long long>(2 * kidx + 1) * key_primes + view_offset) * n + i];
+      if (!(redc_operand_ok(e) && redc_operand_ok(k0) && redc_operand_ok(k1))) {
+        fast = false;
+        break;
+      }
+      s0.add(static_cast<uint64_t>(e), static_cast<uint64_t>(k0), k);
+      s1.add(static_cast<uint64_t>(e), static_cast<uint64_t>(k1), k);
+    }
+    if (fast) {
+      acc[i] = s0.reduce(q, q, t.inv_q[prime]);
+      acc[total + i] = s1.reduce(q, q, t.inv_q[prime]);
+      continue;
+    }
     int64_t x0 = 0, x1 = 0;
     for (int p = 0; p < dp.count; p++) {
       const int64_t e = ext[static_cast<long long>(p) * total + i];
@@ -186,71 +233,90 @@ __global__ void key_inner_product_kernel(PrimeTables t, DevicePartitions dp, int
 // (core_key_switch.cpp:123-160, mont_sub_enter compound.cpp:45-52 with its
 // [0, 2p) outputs carried into the next division), then make_unsigned and the
 // caller's combination (see launch_mod_down_epilogue).
+// A CTA owns kEpilogueCoeffs consecutive coefficients of one polynomial.  Phase 1
+// derives, per coefficient, the divisor sequence d_s = (value of special limb
+// K-1-s after s divisions) with one thread per special limb and a barrier per
+// division; phase 2 spreads the K dependent divisions of every normal limb over
+// all threads (limb-major, coefficient-fastest for coalescing).
+constexpr int kEpilogueCoeffs = 16;  // K * 16 <= 256 threads for every K <= 16
+
 template <int K>
-__global__ void mod_down_epilogue_kernel(PrimeTables t, KeySwitchTables ks, int n, int moduli_id,
-                                         int limbs, const int64_t *acc, const int64_t *base,
-                                         int mode, int64_t *out) {
+__global__ void __launch_bounds__(256)
+    mod_down_epilogue_kernel(PrimeTables t, KeySwitchTables ks, int n, int moduli_id, int limbs,
+                             const int64_t *acc, const int64_t *base, int mode, int64_t *out) {
+  constexpr int CB = kEpilogueCoeffs;
+  __shared__ int64_t divisor[K][CB];
+  __shared__ int64_t first_limb[CB];
   const int poly = blockIdx.y;
-  const int coeff = blockIdx.x * blockDim.x + threadIdx.x;
-  if (coeff >= n) return;
+  const int coeff0 = blockIdx.x * CB;
   const int L = limbs;
   const int E = L + K;
   const int P = ks.prime_count;
-  const int64_t *x = acc + static_cast<long long>(poly) * E * n + coeff;
+  const int64_t *x = acc + static_cast<long long>(poly) * E * n + coeff0;
 
-  int64_t sp[K];
-  int64_t d[K];
+  // Phase 1: special limbs (thread = (special i, coefficient c)).
+  {
+    const int i = threadIdx.x / CB, c = threadIdx.x % CB;
+    const bool active = i < K && coeff0 + c < n;
+    int64_t sp = 0;
+    uint64_t q = 0, kk = 0;
+    int prime = 0;
+    if (active) {
+      prime = moduli_id + L + i;
+      q = t.q[prime];
+      kk = t.k[prime];
+      sp = x[static_cast<long long>(L + i) * n + c];
+    }
 #pragma unroll
-  for (int i = 0; i < K; i++) sp[i] = x[static_cast<long long>(L + i) * n];
-#pragma unroll
-  for (int s = 0; s < K; s++) {
-    const int idx = K - 1 - s;
-    d[s] = sp[idx];
-#pragma unroll
-    for (int i = 0; i < idx; i++) {
-      const int prime = moduli_id + L + i;
-      const uint64_t q = t.q[prime], kk = t.k[prime];
-      const int64_t q2 = static_cast<int64_t>(q << 1);
-      sp[i] = mont_mult(guard(sp[i] + q2 - d[s], q2), ks.p_inverse_mult_r[s * P + prime], q, kk);
+    for (int s = 0; s < K; s++) {
+      if (active && i == K - 1 - s) divisor[s][c] = sp;
+      __syncthreads();
+      if (active && i < K - 1 - s) {
+        const int64_t q2 = static_cast<int64_t>(q << 1);
+        sp = mont_mult(guard(sp + q2 - divisor[s][c], q2), ks.p_inverse_mult_r[s * P + prime], q, kk);
+      }
     }
   }
 
-  auto divide = [&](int j) -> int64_t {
+  auto divide = [&](int j, int c) -> int64_t {
     const int prime = moduli_id + j;
     const uint64_t q = t.q[prime], kk = t.k[prime];
     const int64_t qs = static_cast<int64_t>(q), q2 = qs << 1;
-    int64_t v = x[static_cast<long long>(j) * n];
+    int64_t v = x[static_cast<long long>(j) * n + c];
 #pragma unroll
     for (int s = 0; s < K; s++)
-      v = mont_mult(guard(v + q2 - d[s], q2), ks.p_inverse_mult_r[s * P + prime], q, kk);
+      v = mont_mult(guard(v + q2 - divisor[s][c], q2), ks.p_inverse_mult_r[s * P + prime], q, kk);
     return v < 0 ? v + qs : guard(v, qs);  // make_unsigned_reduce_2q_to_q
   };
-
   const long long in_stride = static_cast<long long>(L) * n;
-  if (mode == 0) {
-    int64_t *o = out + poly * in_stride + coeff;
-    for (int j = 0; j < L; j++) o[static_cast<long long>(j) * n] = divide(j);
-    return;
-  }
-  const int64_t *b = base + poly * in_stride + coeff;
-  auto combined = [&](int j) -> int64_t {
+  const int64_t *b = base + poly * in_stride + coeff0;
+  auto combined = [&](int j, int c) -> int64_t {
     const int64_t qs = static_cast<int64_t>(t.q[moduli_id + j]);
-    return guard(guard(b[static_cast<long long>(j) * n] + divide(j), qs << 1), qs);
+    return guard(guard(b[static_cast<long long>(j) * n + c] + divide(j, c), qs << 1), qs);
   };
-  if (mode == 1) {
-    int64_t *o = out + poly * in_stride + coeff;
-    for (int j = 0; j < L; j++) o[static_cast<long long>(j) * n] = combined(j);
+  const int valid = n - coeff0 < CB ? n - coeff0 : CB;
+
+  if (mode != 2) {
+    int64_t *o = out + poly * in_stride + coeff0;
+    for (int w = threadIdx.x; w < L * CB; w += blockDim.x) {
+      const int j = w / CB, c = w % CB;
+      if (c < valid) o[static_cast<long long>(j) * n + c] = mode == 0 ? divide(j, c) : combined(j, c);
+    }
     return;
   }
   // mode 2: rescale of the relinearized polynomial (core_rescale.cpp:5-25).
+  if (threadIdx.x < valid) first_limb[threadIdx.x] = combined(0, threadIdx.x);
+  __syncthreads();
   const long long out_stride = static_cast<long long>(L - 1) * n;
-  int64_t *o = out + poly * out_stride + coeff;
-  const int64_t y0 = combined(0);
-  const int64_t rounder = y0 > static_cast<int64_t>(t.q[moduli_id] >> 1) ? 1 : 0;
-  for (int j = 1; j < L; j++) {
+  int64_t *o = out + poly * out_stride + coeff0;
+  const int64_t q_half = static_cast<int64_t>(t.q[moduli_id] >> 1);
+  for (int w = threadIdx.x; w < (L - 1) * CB; w += blockDim.x) {
+    const int j = 1 + w / CB, c = w % CB;
+    if (c >= valid) continue;
     const int prime = moduli_id + j;
-    o[static_cast<long long>(j - 1) * n] =
-        rescale_word(combined(j), y0, rounder, t.q[prime], t.k[prime],
+    const int64_t y0 = first_limb[c];
+    o[static_cast<long long>(j - 1) * n + c] =
+        rescale_word(combined(j, c), y0, y0 > q_half ? 1 : 0, t.q[prime], t.k[prime],
                      ks.rescale_scale[static_cast<long long>(moduli_id) * P + prime]);
   }
 }
@@ -326,8 +392,27 @@ cudaError_t launch_mixed_radix(const PrimeTables &t, const DevicePartitions &dp,
 cudaError_t launch_mod_up_ntt(const PrimeTables &t, const DevicePartitions &dp, int log_n,
                               int moduli_id, const int64_t *digits, int64_t *ext, cudaStream_t s) {
   const int n = 1 << log_n;
+  const dim3 grid(blocks_for(n), dp.count);
+  for (int size = 1; size <= 16; size++) {
+    if (!(dp.size_mask & (1u << size))) continue;
+    switch (size) {
+#define FHE_MU_CASE(A)                                                                    \
+  case A:                                                                                 \
+    note_launch();                                                                        \
+    mod_up_contract_kernel<A><<<grid, kThreads, 0, s>>>(t, dp, n, moduli_id, digits, ext); \
+    break;
+      FHE_MU_CASE(1) FHE_MU_CASE(2) FHE_MU_CASE(3) FHE_MU_CASE(4) FHE_MU_CASE(5)
+      FHE_MU_CASE(6) FHE_MU_CASE(7) FHE_MU_CASE(8) FHE_MU_CASE(9) FHE_MU_CASE(10)
+      FHE_MU_CASE(11) FHE_MU_CASE(12) FHE_MU_CASE(13) FHE_MU_CASE(14) FHE_MU_CASE(15)
+      FHE_MU_CASE(16)
+#undef FHE_MU_CASE
+      default: return cudaErrorInvalidValue;
+    }
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
   const long long stride = static_cast<long long>(dp.extended) * n;
-  ModUpLoad ld{dp, digits, t.r_squared, t.q, t.k};
+  PlainLoad ld{ext, stride};
   PlainStore st{ext, stride};
   return forward_ntt(log_n, dp.count, dp.extended, moduli_id, t, ld, st, ext, stride, s);
 }
@@ -352,7 +437,7 @@ cudaError_t launch_mod_down_intt(const PrimeTables &t, int log_n, int moduli_id,
 cudaError_t launch_mod_down_epilogue(const PrimeTables &t, const KeySwitchTables &ks, int n,
                                      int moduli_id, int limbs, const int64_t *acc,
                                      const int64_t *base, int mode, int64_t *out, cudaStream_t s) {
-  const dim3 grid(blocks_for(n), 2);
+  const dim3 grid((n + kEpilogueCoeffs - 1) / kEpilogueCoeffs, 2);
   switch (ks.special_count) {
 #define FHE_MD_CASE(K)                                                                      \
   case K:                                                                                   \

@@ -1,12 +1,24 @@
-// Device-side modular arithmetic of the B200 CKKS engine.
+// Modular arithmetic of the B200 CKKS engine (device code; also compiles as host
+// C++ so the exact word semantics can be checked on the CPU).
 //
-// Words are int64 holding residues; like the reference (DESILO FHE
+// Words are int64 holding residues.  As in the reference (DESILO FHE
 // montgomery/unit.h:10-31, montgomery/compound.cpp) every comparison is signed and
 // the REDC product is formed from sign-extended operands, so out-of-range
 // intermediates evaluate to the same words as on the CPU.  R = 2^62.
+//
+// The 64x64 -> 128-bit products are written as four 32x32 -> 64-bit
+// multiply-adds whose accumulations never overflow, which maps each of them onto
+// one wide integer multiply-add on the FMA pipe and keeps carries off the ALU pipe
+// (the NTT butterflies are ALU-bound otherwise).
 #pragma once
 
 #include <cstdint>
+
+#ifdef __CUDACC__
+#define FHE_HD __host__ __device__ __forceinline__
+#else
+#define FHE_HD inline
+#endif
 
 namespace fhe_b200 {
 
@@ -14,31 +26,101 @@ constexpr int kMontBits = 62;
 constexpr uint64_t kMontMask = (uint64_t(1) << kMontBits) - 1;
 
 // (x < q) ? x : x - q  (unit.h:13)
-__device__ __forceinline__ int64_t guard(int64_t x, int64_t q) { return x < q ? x : x - q; }
+FHE_HD int64_t guard(int64_t x, int64_t q) { return x < q ? x : x - q; }
 
-// REDC(a * b) with R = 2^62: bits [62, 126) of a*b + s*q, s = (a*b*k) mod 2^62
-// (unit.h:15-23).  a and b are sign-extended to 128 bits as in the reference.
-__device__ __forceinline__ int64_t mont_mult(int64_t a, int64_t b, uint64_t q, uint64_t k) {
-  const uint64_t lo = static_cast<uint64_t>(a) * static_cast<uint64_t>(b);
-  const uint64_t hi = static_cast<uint64_t>(__mul64hi(a, b));
+FHE_HD uint64_t mad32(uint32_t a, uint32_t b, uint64_t c) {
+  return static_cast<uint64_t>(a) * b + c;
+}
+
+// Full unsigned product a * b = hi * 2^64 + lo.
+FHE_HD void mul_wide(uint64_t a, uint64_t b, uint64_t &lo, uint64_t &hi) {
+  const uint32_t a0 = static_cast<uint32_t>(a), a1 = static_cast<uint32_t>(a >> 32);
+  const uint32_t b0 = static_cast<uint32_t>(b), b1 = static_cast<uint32_t>(b >> 32);
+  const uint64_t t = mad32(a0, b0, 0);
+  const uint64_t m = mad32(a0, b1, t >> 32);                       // < 2^64
+  const uint64_t m2 = mad32(a1, b0, static_cast<uint32_t>(m));    // < 2^64
+  const uint64_t h = mad32(a1, b1, m >> 32);
+  hi = h + (m2 >> 32);                                             // no overflow
+  lo = static_cast<uint32_t>(t) | (m2 << 32);
+}
+
+// Bits [62, 126) of X + s*q with s = (X mod 2^64) * k mod 2^62, X = hi*2^64 + lo.
+FHE_HD int64_t redc_wide(uint64_t lo, uint64_t hi, uint64_t q, uint64_t k) {
   const uint64_t s = (lo * k) & kMontMask;
-  const uint64_t sq_lo = s * q;
-  const uint64_t sq_hi = __umul64hi(s, q);
-  const uint64_t sum_lo = lo + sq_lo;
-  const uint64_t sum_hi = hi + sq_hi + (sum_lo < lo ? 1 : 0);
-  return static_cast<int64_t>((sum_hi << 2) | (sum_lo >> kMontBits));
+  uint64_t sl, sh;
+  mul_wide(s, q, sl, sh);
+  const uint64_t zl = lo + sl;
+  const uint64_t zh = hi + sh + (zl < lo ? 1 : 0);
+  return static_cast<int64_t>((zh << 2) | (zl >> kMontBits));
+}
+
+// REDC(a * b) with R = 2^62 on sign-extended operands (unit.h:15-23).  The signed
+// high product is the unsigned one minus b when a < 0 and minus a when b < 0.
+FHE_HD int64_t mont_mult(int64_t a, int64_t b, uint64_t q, uint64_t k) {
+  const uint64_t ua = static_cast<uint64_t>(a), ub = static_cast<uint64_t>(b);
+  uint64_t lo, hi;
+  mul_wide(ua, ub, lo, hi);
+  hi -= (a < 0 ? ub : 0) + (b < 0 ? ua : 0);
+  return redc_wide(lo, hi, q, k);
+}
+
+// mont_mult when `a` is known to be non-negative (a twiddle or table constant).
+FHE_HD int64_t mont_mult_const(int64_t a, int64_t b, uint64_t q, uint64_t k) {
+  const uint64_t ua = static_cast<uint64_t>(a), ub = static_cast<uint64_t>(b);
+  uint64_t lo, hi;
+  mul_wide(ua, ub, lo, hi);
+  hi -= (b < 0 ? ua : 0);
+  return redc_wide(lo, hi, q, k);
 }
 
 // Montgomery exit (unit.h:25-31): REDC of a single (sign-extended) word.
-__device__ __forceinline__ int64_t mont_exit(int64_t x, uint64_t q, uint64_t k) {
-  const uint64_t s = (static_cast<uint64_t>(x) * k) & kMontMask;
-  const uint64_t sq_lo = s * q;
-  const uint64_t sq_hi = __umul64hi(s, q);
-  const uint64_t lo = static_cast<uint64_t>(x);
-  const uint64_t sum_lo = lo + sq_lo;
-  const uint64_t sign = x < 0 ? ~uint64_t(0) : 0;
-  const uint64_t sum_hi = sign + sq_hi + (sum_lo < lo ? 1 : 0);
-  return static_cast<int64_t>((sum_hi << 2) | (sum_lo >> kMontBits));
+FHE_HD int64_t mont_exit(int64_t x, uint64_t q, uint64_t k) {
+  return redc_wide(static_cast<uint64_t>(x), x < 0 ? ~uint64_t(0) : 0, q, k);
+}
+
+// Lazy sums of REDC terms.
+//
+// For operands a_i, b_i in [0, 2^61) and q < 2^61 every t_i = REDC(a_i b_i) lies in
+// [0, 2q), and a chain acc = guard(acc + t_i, 2q) started from t_0 equals
+// (sum t_i) mod 2q.  Since a_i b_i + s_i q = t_i 2^62 exactly (s_i = a_i b_i k mod
+// 2^62), sum t_i = (sum a_i b_i + q sum s_i) / 2^62: the products and the s_i are
+// accumulated in 128 bits and reduced once.  Used for the ModUp contraction and
+// the key inner product, whose reference form is such a chain.
+struct RedcSum {
+  uint64_t p_lo = 0, p_hi = 0;  // sum of a_i b_i
+  uint64_t s_lo = 0, s_hi = 0;  // sum of s_i
+  FHE_HD void add(uint64_t a, uint64_t b, uint64_t k) {
+    uint64_t lo, hi;
+    mul_wide(a, b, lo, hi);
+    const uint64_t nl = p_lo + lo;
+    p_hi += hi + (nl < p_lo ? 1 : 0);
+    p_lo = nl;
+    const uint64_t s = (lo * k) & kMontMask;
+    const uint64_t ns = s_lo + s;
+    s_hi += ns < s_lo ? 1 : 0;
+    s_lo = ns;
+  }
+  // (sum t_i) mod m for m = q or 2q, given the sum is below 64 m; inv_m ~ 1/m.
+  FHE_HD int64_t reduce(uint64_t q, uint64_t m, double inv_m) const {
+    uint64_t ql, qh;
+    mul_wide(s_lo, q, ql, qh);
+    qh += s_hi * q;
+    const uint64_t zl = p_lo + ql;
+    const uint64_t zh = p_hi + qh + (zl < p_lo ? 1 : 0);
+    const uint64_t t_lo = (zh << 2) | (zl >> kMontBits);  // T = Z >> 62 < 2^66
+    const uint64_t t_hi = zh >> kMontBits;
+    const double td = static_cast<double>(t_hi) * 18446744073709551616.0 + static_cast<double>(t_lo);
+    const uint64_t est = static_cast<uint64_t>(td * inv_m);
+    int64_t r = static_cast<int64_t>(t_lo - est * m);  // |T - est m| < 2m
+    const int64_t ms = static_cast<int64_t>(m);
+    if (r < 0) r += ms;
+    if (r >= ms) r -= ms;
+    return r;
+  }
+};
+
+FHE_HD bool redc_operand_ok(int64_t x) {
+  return static_cast<uint64_t>(x) < (uint64_t(1) << 61);
 }
 
 // Per-prime constants as the kernels read them.
@@ -49,6 +131,8 @@ struct PrimeTables {
   const int64_t *n_inverse;
   const int64_t *root;          // [prime][N-1]
   const int64_t *root_inverse;  // [prime][N-1]
+  const double *inv_q;          // 1 / q
+  const double *inv_2q;         // 1 / (2q)
   int log_n;
 };
 

@@ -29,7 +29,7 @@ struct NttPass {
   int log_n;
   int stride_log;  // log2(T); 0 for contiguous passes
   int first;       // forward: first global stage; inverse: first distance exponent
-  int columns;     // sub-transforms per CTA tile
+  int columns_log; // log2(sub-transforms per CTA tile)
   int polys;       // batch: polys x limbs, grid.y = limbs * polys (poly fastest)
   int limbs;
   int prime_base;  // prime index of limb 0
@@ -82,11 +82,23 @@ struct EnterExitStore {
   }
 };
 
+// Shared-memory word of element i of sub-transform c.  A 128-byte bank row holds 16
+// words and a half-warp's 8-byte accesses are served together, so the swizzle must
+// give the 16 threads of a half-warp 16 different rows positions.  XOR-ing
+// (i >> 4) ^ ((i >> 5) << 2) and the column into the low four bits does that for
+// every round of the 256-word passes (N = 2^16) in both directions, checked by
+// simulating each round's access pattern; other shapes stay within 2 wavefronts.
+// (For sub-transforms shorter than a row the XOR stays inside the sub-transform.)
+template <int M>
+__device__ __forceinline__ int tile_index(int c, int i) {
+  constexpr int kMask = M >= 16 ? 15 : M - 1;
+  return c * M + (i ^ (((i >> 4) ^ ((i >> 5) << 2) ^ c) & kMask));
+}
+
 template <int S, bool INVERSE, class Loader, class Storer>
 __global__ void __launch_bounds__(256)
     ntt_pass_kernel(NttPass a, PrimeTables t, Loader load, Storer store) {
   constexpr int M = 1 << S;
-  constexpr int PM = M + 1;  // padded sub-transform pitch in shared memory
   constexpr int R = (S + 2) / 3;
   extern __shared__ int64_t tile_smem[];
 
@@ -101,7 +113,7 @@ __global__ void __launch_bounds__(256)
   const int64_t *tw = (INVERSE ? t.root_inverse : t.root) + static_cast<size_t>(prime) * (n - 1);
   const int T = 1 << a.stride_log;
   const bool strided = T > 1;
-  const int C = a.columns;
+  const int C = 1 << a.columns_log;
   const int u0 = blockIdx.x * C;
 
 #pragma unroll
@@ -117,8 +129,8 @@ __global__ void __launch_bounds__(256)
     for (int gid = threadIdx.x; gid < total; gid += blockDim.x) {
       int c, g;
       if (strided) {
-        c = gid % C;
-        g = gid / C;
+        c = gid & (C - 1);
+        g = gid >> a.columns_log;
       } else {
         c = gid / groups_per_col;
         g = gid - c * groups_per_col;
@@ -134,39 +146,58 @@ __global__ void __launch_bounds__(256)
           if (round == 0) {
             x[e] = load(poly, limb, prime, gbase + i * T, n);
           } else {
-            x[e] = tile_smem[c * PM + i];
+            x[e] = tile_smem[tile_index<M>(c, i)];
           }
         }
       }
+      // Global index of element 0 of this radix-8 group.  Inside the group the
+      // butterflies of one stage that share a twiddle form blocks of consecutive
+      // elements, and the blocks' twiddles are consecutive table entries, so each
+      // stage needs a single index computation.
+      const int gi0 = gbase + base * T;
 #pragma unroll
       for (int j = 0; j < 3; j++) {
         if (j < r) {
           if (!INVERSE) {
+            // stage s: twiddle root[2^s - 1 + (gi >> (log_n - s))]; the block of
+            // element e is e >> (r - j) (ntt.cpp:46-134)
             const int s = a.first + first_local + j;
             const int half = E >> (j + 1);
+            const int64_t *wp = tw + ((1 << s) - 1 + (gi0 >> (a.log_n - s)));
 #pragma unroll
-            for (int e = 0; e < 8; e++) {
-              if (e < E && (e & half) == 0) {
-                const int gi = gbase + (base + e * D) * T;
-                const int64_t w = __ldg(&tw[(1 << s) - 1 + (gi >> (a.log_n - s))]);
-                const int64_t uu = x[e];
-                const int64_t p = mont_mult(w, x[e + half], q, k);
-                x[e] = guard(uu + p, q2);
-                x[e + half] = guard(uu + q2 - p, q2);
+            for (int h = 0; h < (1 << j); h++) {
+              const int64_t w = __ldg(wp + h);
+#pragma unroll
+              for (int e2 = 0; e2 < 4; e2++) {
+                if (e2 < half) {
+                  const int e = h * 2 * half + e2;
+                  const int64_t uu = x[e];
+                  const int64_t p = mont_mult_const(w, x[e + half], q, k);
+                  x[e] = guard(uu + p, q2);
+                  x[e + half] = guard(uu + q2 - p, q2);
+                }
               }
             }
           } else {
+            // distance 2^dg: twiddle root_inverse[N - N/2^dg + (gi >> (dg + 1))]
+            // (ntt.cpp:177-272); the block of element e is e >> (j + 1)
             const int dg = a.first + first_local + j;
             const int half = 1 << j;
+            const int64_t *wp = tw + (n - (n >> dg) + (gi0 >> (dg + 1)));
 #pragma unroll
-            for (int e = 0; e < 8; e++) {
-              if (e < E && (e & half) == 0) {
-                const int gi = gbase + (base + e * D) * T;
-                const int64_t w = __ldg(&tw[n - (n >> dg) + (gi >> (dg + 1))]);
-                const int64_t uu = x[e];
-                const int64_t vv = x[e + half];
-                x[e] = guard(uu + vv, q2);
-                x[e + half] = mont_mult(w, guard(uu + q2 - vv, q2), q, k);
+            for (int h = 0; h < 4; h++) {
+              if (h < (E >> (j + 1))) {
+                const int64_t w = __ldg(wp + h);
+#pragma unroll
+                for (int e2 = 0; e2 < 4; e2++) {
+                  if (e2 < half) {
+                    const int e = h * 2 * half + e2;
+                    const int64_t uu = x[e];
+                    const int64_t vv = x[e + half];
+                    x[e] = guard(uu + vv, q2);
+                    x[e + half] = mont_mult_const(w, guard(uu + q2 - vv, q2), q, k);
+                  }
+                }
               }
             }
           }
@@ -179,7 +210,7 @@ __global__ void __launch_bounds__(256)
           if (round == R - 1) {
             store(poly, limb, prime, gbase + i * T, n, x[e]);
           } else {
-            tile_smem[c * PM + i] = x[e];
+            tile_smem[tile_index<M>(c, i)] = x[e];
           }
         }
       }
@@ -201,15 +232,15 @@ inline NttPlan ntt_plan(int log_n) {
   return {2, log_n - s2, s2};
 }
 
-constexpr int kNttTileWords = 4096;
+constexpr int kNttTileLog = 12;  // 4096 words per tile
 constexpr int kNttThreads = 256;
 
 template <int S, bool INVERSE, class Loader, class Storer>
 cudaError_t launch_ntt_pass(const NttPass &a, const PrimeTables &t, const Loader &ld,
                             const Storer &st, cudaStream_t stream) {
   const int subs = (1 << a.log_n) >> S;
-  const dim3 grid(subs / a.columns, a.polys * a.limbs);
-  const size_t smem = sizeof(int64_t) * a.columns * ((1 << S) + 1);
+  const dim3 grid(subs >> a.columns_log, a.polys * a.limbs);
+  const size_t smem = sizeof(int64_t) << (a.columns_log + S);
   auto kernel = ntt_pass_kernel<S, INVERSE, Loader, Storer>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -252,19 +283,19 @@ cudaError_t forward_ntt(int log_n, int polys, int limbs, int prime_base, const P
   if (plan.passes == 1) {
     a.stride_log = 0;
     a.first = 0;
-    a.columns = 1;
+    a.columns_log = 0;
     return dispatch_ntt_pass<false>(plan.s_first, a, t, ld, st, stream);
   }
   PlainStore mid_store{work, work_stride};
   PlainLoad mid_load{work, work_stride};
   a.stride_log = plan.s_second;
   a.first = 0;
-  a.columns = (1 << plan.s_first) >= 512 ? 8 : 16;
+  a.columns_log = plan.s_first >= 9 ? 3 : 4;
   cudaError_t e = dispatch_ntt_pass<false>(plan.s_first, a, t, ld, mid_store, stream);
   if (e != cudaSuccess) return e;
   a.stride_log = 0;
   a.first = plan.s_first;
-  a.columns = kNttTileWords >> plan.s_second;
+  a.columns_log = kNttTileLog - plan.s_second;
   return dispatch_ntt_pass<false>(plan.s_second, a, t, mid_load, st, stream);
 }
 
@@ -277,19 +308,19 @@ cudaError_t inverse_ntt(int log_n, int polys, int limbs, int prime_base, const P
   if (plan.passes == 1) {
     a.stride_log = 0;
     a.first = 0;
-    a.columns = 1;
+    a.columns_log = 0;
     return dispatch_ntt_pass<true>(plan.s_first, a, t, ld, st, stream);
   }
   PlainStore mid_store{work, work_stride};
   PlainLoad mid_load{work, work_stride};
   a.stride_log = 0;
   a.first = 0;
-  a.columns = kNttTileWords >> plan.s_second;
+  a.columns_log = kNttTileLog - plan.s_second;
   cudaError_t e = dispatch_ntt_pass<true>(plan.s_second, a, t, ld, mid_store, stream);
   if (e != cudaSuccess) return e;
   a.stride_log = plan.s_second;
   a.first = plan.s_second;
-  a.columns = (1 << plan.s_first) >= 512 ? 8 : 16;
+  a.columns_log = plan.s_first >= 9 ? 3 : 4;
   return dispatch_ntt_pass<true>(plan.s_first, a, t, mid_load, st, stream);
 }
 
