@@ -130,6 +130,8 @@ __global__ void mixed_radix_kernel(PrimeTables t, DevicePartitions dp, int n, in
 // one lazy sum (RedcSum) when every digit is in [0, 2^61), which holds for all
 // digits produced from canonical inputs, and term by term otherwise; both give the
 // same word.
+constexpr int kContractChunk = 8;  // extended limbs per thread
+
 template <int A>
 __global__ void __launch_bounds__(256)
     mod_up_contract_kernel(PrimeTables t, DevicePartitions dp, int n, int moduli_id,
@@ -140,6 +142,8 @@ __global__ void __launch_bounds__(256)
   if (coeff >= n) return;
   const int start = dp.start[p];
   const int E = dp.extended;
+  const int j_begin = blockIdx.z * kContractChunk;
+  if (j_begin >= E) return;
   int64_t d[A];
   bool fast = true;
 #pragma unroll
@@ -149,23 +153,46 @@ __global__ void __launch_bounds__(256)
   }
   const int64_t *cst = dp.product_r_squared + static_cast<long long>(p) * 16 * E;
   int64_t *out = ext + static_cast<long long>(p) * E * n + coeff;
-  for (int j = 0; j < E; j++) {
+  if (fast) {
+    // Four extended limbs at a time: four independent accumulation chains.
+    constexpr int kLanes = 4;
+#pragma unroll
+    for (int j0 = j_begin; j0 < j_begin + kContractChunk; j0 += kLanes) {
+      if (j0 >= E) break;
+      RedcSum sum[kLanes];
+      uint64_t kl[kLanes];
+      int jl[kLanes];
+#pragma unroll
+      for (int l = 0; l < kLanes; l++) {
+        jl[l] = j0 + l < E ? j0 + l : E - 1;
+        kl[l] = t.k[moduli_id + jl[l]];
+        sum[l].add(static_cast<uint64_t>(d[0]), static_cast<uint64_t>(t.r_squared[moduli_id + jl[l]]),
+                   kl[l]);
+      }
+#pragma unroll
+      for (int i = 1; i < A; i++) {
+#pragma unroll
+        for (int l = 0; l < kLanes; l++)
+          sum[l].add(static_cast<uint64_t>(d[i]), static_cast<uint64_t>(cst[(i - 1) * E + jl[l]]), kl[l]);
+      }
+#pragma unroll
+      for (int l = 0; l < kLanes; l++) {
+        if (j0 + l < E) {
+          const int prime = moduli_id + jl[l];
+          const uint64_t q = t.q[prime];
+          out[static_cast<long long>(jl[l]) * n] = sum[l].reduce(q, q << 1, t.inv_2q[prime]);
+        }
+      }
+    }
+    return;
+  }
+  for (int j = j_begin; j < j_begin + kContractChunk && j < E; j++) {
     const int prime = moduli_id + j;
     const uint64_t q = t.q[prime], k = t.k[prime];
-    int64_t v;
-    if (fast) {
-      RedcSum sum;
-      sum.add(static_cast<uint64_t>(d[0]), static_cast<uint64_t>(t.r_squared[prime]), k);
+    const int64_t q2 = static_cast<int64_t>(q << 1);
+    int64_t v = mont_mult(d[0], t.r_squared[prime], q, k);
 #pragma unroll
-      for (int i = 1; i < A; i++)
-        sum.add(static_cast<uint64_t>(d[i]), static_cast<uint64_t>(cst[(i - 1) * E + j]), k);
-      v = sum.reduce(q, q << 1, t.inv_2q[prime]);
-    } else {
-      const int64_t q2 = static_cast<int64_t>(q << 1);
-      v = mont_mult(d[0], t.r_squared[prime], q, k);
-#pragma unroll
-      for (int i = 1; i < A; i++) v = guard(mont_mult(d[i], cst[(i - 1) * E + j], q, k) + v, q2);
-    }
+    for (int i = 1; i < A; i++) v = guard(mont_mult(d[i], cst[(i - 1) * E + j], q, k) + v, q2);
     out[static_cast<long long>(j) * n] = v;
   }
 }
@@ -392,7 +419,7 @@ cudaError_t launch_mixed_radix(const PrimeTables &t, const DevicePartitions &dp,
 cudaError_t launch_mod_up_ntt(const PrimeTables &t, const DevicePartitions &dp, int log_n,
                               int moduli_id, const int64_t *digits, int64_t *ext, cudaStream_t s) {
   const int n = 1 << log_n;
-  const dim3 grid(blocks_for(n), dp.count);
+  const dim3 grid(blocks_for(n), dp.count, (dp.extended + kContractChunk - 1) / kContractChunk);
   for (int size = 1; size <= 16; size++) {
     if (!(dp.size_mask & (1u << size))) continue;
     switch (size) {
