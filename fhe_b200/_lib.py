@@ -81,6 +81,7 @@ SIGNATURES = {
     "fhe_to_ntt": (_i, [_vp, _vp, _pp]),
     "fhe_to_intt": (_i, [_vp, _vp, _pp]),
     "fhe_ntt_limbs": (_i, [_vp, _i64p, _i, _i, _i, ctypes.c_longlong, _i]),
+    "fhe_relinearize_noalloc": (_i, [_vp, _i64p, _i, _i64p, _i, _i, _i64p]),
 }
 
 _lib = None

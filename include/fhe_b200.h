@@ -197,6 +197,23 @@ int fhe_multiply_relinearize_rescale(fhe_engine *engine, const fhe_data *a, cons
 int fhe_to_ntt(fhe_engine *engine, const fhe_data *text, fhe_data **out);
 int fhe_to_intt(fhe_engine *engine, const fhe_data *text, fhe_data **out);
 
+/* Relinearize without allocating (no counterpart in the reference, which has no
+ * device memory).  For callers that cannot call cudaMalloc while they run -- code
+ * inside a CUDA graph capture, real-time loops with a fixed memory budget, hosts
+ * whose allocator policy forbids device allocation after start-up.  Same words as
+ * fhe_relinearize; inputs and output are caller-owned device buffers on the
+ * engine's device: ct [3][L][N] in NTT form at moduli_id, the key switching key
+ * [key_polys][prime_count(key_moduli_id)][N] at key_moduli_id, out [2][L][N].
+ * All temporaries come from one fixed 32 MiB device array per GPU, held until the
+ * process exits; a call whose temporaries would not fit is rejected with
+ * FHE_ERR_INVALID_ARGUMENT.  The first call on a device resolves that array's
+ * address (cudaGetSymbolAddress) and should come before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
+int fhe_relinearize_noalloc(fhe_engine *engine, const int64_t *ct_device, int moduli_id,
+                            const int64_t *key_device, int key_moduli_id, int key_polys,
+                            int64_t *out_device);
+
 /* ---- processor-level kernels on device limbs (src/processor/single.h) --------------- */
 
 /* SingleProcessor::ntt / intt (single.cpp:420-454) on `polys` x `chains` device limbs
