@@ -692,6 +692,141 @@ void oracle_mult_relin_rescale(const oracle_ctx *c, int mid, const int64_t *a,
   free(rl);
 }
 
+/* ------------------------------------------------- key switch variants -- */
+
+/* CKKSCore::switch_key: core.cpp:1058-1083.  ct: [2][L][N] coefficient form. */
+void oracle_switch_key(const oracle_ctx *c, int mid, const int64_t *ct, int key_mid,
+                       const int64_t *key, int64_t *out) {
+  const int n = c->n, L = oracle_chain_count(c, mid);
+  const size_t PS = (size_t)L * n;
+  int64_t *ks = malloc(sizeof(int64_t) * 2 * PS);
+  oracle_key_switch(c, mid, ct + PS, key_mid, key, ks);
+  for (int j = 0; j < L; j++) {
+    const int64_t q = (int64_t)c->q[mid + j], q2 = q << 1;
+    for (int t = 0; t < n; t++) {
+      const size_t i = (size_t)j * n + t;
+      out[i] = guard(guard(ks[i] + ct[i], q2), q);
+      out[PS + i] = ks[PS + i];
+    }
+  }
+  free(ks);
+}
+
+/* rotate_ with a (permutation, sign) pair: core.cpp:846-868, encode.cpp:567-575 */
+static void rotate_coefficients(const oracle_ctx *c, int mid, int polys, const int32_t *perm,
+                                const int32_t *sign, const int64_t *x, int64_t *y) {
+  const int n = c->n, L = oracle_chain_count(c, mid);
+  for (int p = 0; p < polys; p++)
+    for (int j = 0; j < L; j++) {
+      const int64_t q = (int64_t)c->q[mid + j];
+      const int64_t *xs = x + ((size_t)p * L + j) * n;
+      int64_t *ys = y + ((size_t)p * L + j) * n;
+      for (int t = 0; t < n; t++) ys[perm[t]] = sign[t] * xs[t];
+      for (int t = 0; t < n; t++) ys[t] = ys[t] < 0 ? ys[t] + q : guard(ys[t], q);
+    }
+}
+
+/* CKKSCore::conjugate: core.cpp:1035-1056 (delta -1 permutation of both polys,
+ * then a key switch of the permuted c1). */
+void oracle_conjugate(const oracle_ctx *c, int mid, const int64_t *ct, int key_mid,
+                      const int64_t *key, int64_t *out) {
+  const int n = c->n, L = oracle_chain_count(c, mid);
+  int32_t *perm = malloc(sizeof(int32_t) * n), *sign = malloc(sizeof(int32_t) * n);
+  oracle_permutation_and_sign(perm, sign, n, -1);
+  int64_t *conj = malloc(sizeof(int64_t) * 2 * (size_t)L * n);
+  rotate_coefficients(c, mid, 2, perm, sign, ct, conj);
+  oracle_switch_key(c, mid, conj, key_mid, key, out);
+  free(conj);
+  free(perm);
+  free(sign);
+}
+
+/* CKKSCore::rotate(ct, fixed_rotation_key): core.cpp:939-963 with decompose
+ * (core_key_switch.cpp:434-466), create_key_switcher_for_rotate (:550-576) and
+ * key_switch_mod_down (core.cpp:916-937).  `delta` is the key's normalised step. */
+void oracle_rotate(const oracle_ctx *c, int mid, const int64_t *ct, int key_mid,
+                   const int64_t *key, int delta, int64_t *out) {
+  const int n = c->n;
+  const int L = oracle_chain_count(c, mid);
+  const int P = c->prime_count - mid;
+  const int key_P = c->prime_count - key_mid;
+  const int key_offset = mid - key_mid;
+  const size_t PS = (size_t)L * n;
+  partition_t parts[64];
+  /* decompose uses the partitions of (mid, mid); the key product re-indexes them
+   * against the key's moduli id (create_key_switcher(decomposed, key), :510-548). */
+  const int pcount = make_partitions(c, mid, mid, parts);
+  partition_t kparts[64];
+  make_partitions(c, mid, key_mid, kparts);
+  int64_t *x0 = malloc(sizeof(int64_t) * (size_t)P * n);
+  int64_t *x1 = malloc(sizeof(int64_t) * (size_t)P * n);
+  int64_t *ext = malloc(sizeof(int64_t) * (size_t)P * n);
+  int64_t *mrs = malloc(sizeof(int64_t) * (size_t)c->special_count * n);
+  for (int pi = 0; pi < pcount; pi++) {
+    const partition_t *pt = &parts[pi];
+    if (c->special_count == 1) {
+      mod_up_single(c, mid, ct + PS, pt->start, ext);
+    } else {
+      partition_params_t pp;
+      make_partition_params(c, mid, pt, &pp);
+      rns_to_mrs(c, mid, ct + PS, pt, &pp, mrs);
+      mod_up(c, mid, mrs, pt, &pp, ext);
+      free(pp.prod_r2);
+    }
+    const int kidx = kparts[pi].partition_index;
+    const int64_t *k0 = key + ((size_t)(kidx * 2) * key_P + key_offset) * n;
+    const int64_t *k1 = key + ((size_t)(kidx * 2 + 1) * key_P + key_offset) * n;
+    for (int j = 0; j < P; j++) {
+      const int pq = mid + j;
+      const uint64_t q = c->q[pq], k = c->k[pq];
+      const int64_t q2 = (int64_t)(q << 1), qs = (int64_t)q;
+      for (int t = 0; t < n; t++) {
+        const size_t i = (size_t)j * n + t;
+        const int64_t a0 = MM(ext[i], k0[i], q, k);
+        const int64_t a1 = MM(ext[i], k1[i], q, k);
+        if (pi == 0) {
+          x0[i] = a0;
+          x1[i] = a1;
+        } else {
+          x0[i] = guard(guard(a0 + x0[i], q2), qs);
+          x1[i] = guard(guard(a1 + x1[i], q2), qs);
+        }
+      }
+    }
+  }
+  /* b * P (p_product_mult_r), Montgomery enter, NTT, added to x0 on the L limbs. */
+  int64_t *bp = malloc(sizeof(int64_t) * PS);
+  for (int j = 0; j < L; j++) {
+    const int pq = mid + j;
+    const uint64_t q = c->q[pq], k = c->k[pq];
+    for (int t = 0; t < n; t++) {
+      const size_t i = (size_t)j * n + t;
+      bp[i] = MM(MM(ct[i], c->p_product_mult_r[pq], q, k), c->r_squared[pq], q, k);
+    }
+    oracle_ntt_limb(bp + (size_t)j * n, bp + (size_t)j * n, c->root + (size_t)pq * (n - 1), q, k,
+                    n, c->log_n);
+    const int64_t q2 = (int64_t)(q << 1), qs = (int64_t)q;
+    for (int t = 0; t < n; t++) {
+      const size_t i = (size_t)j * n + t;
+      x0[i] = guard(guard(x0[i] + bp[i], q2), qs);
+    }
+  }
+  int64_t *md = malloc(sizeof(int64_t) * 2 * PS);
+  mod_down(c, mid, x0, md);
+  mod_down(c, mid, x1, md + PS);
+  int32_t *perm = malloc(sizeof(int32_t) * n), *sign = malloc(sizeof(int32_t) * n);
+  oracle_permutation_and_sign(perm, sign, n, delta);
+  rotate_coefficients(c, mid, 2, perm, sign, md, out);
+  free(perm);
+  free(sign);
+  free(md);
+  free(bp);
+  free(x0);
+  free(x1);
+  free(ext);
+  free(mrs);
+}
+
 /* ------------------------------------------------------------ rotation -- */
 
 /* get_jump: ckks/encode.cpp:44-56 */

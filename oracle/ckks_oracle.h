@@ -88,6 +88,16 @@ void oracle_mult_relin_rescale(const oracle_ctx *ctx, int moduli_id,
                                int key_moduli_id, const int64_t *key,
                                int64_t *out);
 
+/* CKKSCore::switch_key (core.cpp:1058): ct [2][L][N] coefficient form -> out. */
+void oracle_switch_key(const oracle_ctx *ctx, int moduli_id, const int64_t *ct,
+                       int key_moduli_id, const int64_t *key, int64_t *out);
+/* CKKSCore::conjugate (core.cpp:1035): ct [2][L][N] coefficient form -> out. */
+void oracle_conjugate(const oracle_ctx *ctx, int moduli_id, const int64_t *ct,
+                      int key_moduli_id, const int64_t *key, int64_t *out);
+/* CKKSCore::rotate(ct, fixed key) (core.cpp:939-963); delta = the key's step. */
+void oracle_rotate(const oracle_ctx *ctx, int moduli_id, const int64_t *ct,
+                   int key_moduli_id, const int64_t *key, int delta, int64_t *out);
+
 /* Rotation permutations (ckks/encode.cpp:513-557). */
 void oracle_permutation_and_sign(int32_t *permutation, int32_t *sign,
                                  int coeff_count, int delta);

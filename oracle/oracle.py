@@ -71,6 +71,13 @@ def lib():
         L.oracle_mult_relin_rescale.restype = None
         L.oracle_mult_relin_rescale.argtypes = [ctypes.c_void_p, ctypes.c_int, _i64p, _i64p,
                                                 ctypes.c_int, _i64p, _i64p]
+        for name in ("oracle_switch_key", "oracle_conjugate"):
+            f = getattr(L, name)
+            f.restype = None
+            f.argtypes = [ctypes.c_void_p, ctypes.c_int, _i64p, ctypes.c_int, _i64p, _i64p]
+        L.oracle_rotate.restype = None
+        L.oracle_rotate.argtypes = [ctypes.c_void_p, ctypes.c_int, _i64p, ctypes.c_int, _i64p,
+                                    ctypes.c_int, _i64p]
         L.oracle_permutation_and_sign.restype = None
         L.oracle_permutation_and_sign.argtypes = [_i32p, _i32p, ctypes.c_int, ctypes.c_int]
         L.oracle_ntt_permutation.restype = None
@@ -211,6 +218,22 @@ class Context:
         y = np.empty((polys, L - 1, self.n), dtype=np.int64)
         lib().oracle_rescale(self._ctx, moduli_id, polys, _p(x), _p(y))
         return y
+
+    def _ks_call(self, fn, moduli_id, ct, key_moduli_id, key, *extra):
+        ct = np.ascontiguousarray(ct, dtype=np.int64)
+        key = np.ascontiguousarray(key, dtype=np.int64)
+        out = np.empty((2, self.chains(moduli_id), self.n), dtype=np.int64)
+        fn(self._ctx, moduli_id, _p(ct), key_moduli_id, _p(key), *extra, _p(out))
+        return out
+
+    def switch_key(self, moduli_id, ct, key_moduli_id, key):
+        return self._ks_call(lib().oracle_switch_key, moduli_id, ct, key_moduli_id, key)
+
+    def conjugate(self, moduli_id, ct, key_moduli_id, key):
+        return self._ks_call(lib().oracle_conjugate, moduli_id, ct, key_moduli_id, key)
+
+    def rotate(self, moduli_id, ct, key_moduli_id, key, delta):
+        return self._ks_call(lib().oracle_rotate, moduli_id, ct, key_moduli_id, key, delta)
 
     def mult_relin_rescale(self, moduli_id, a, b, key_moduli_id, key):
         a = np.ascontiguousarray(a, dtype=np.int64)

@@ -48,6 +48,9 @@ def lib():
             "ref_text_new": (vp, [vp, ci, ci, ci, ci, ctypes.c_longdouble, _i64p]),
             "ref_key_new": (vp, [vp, ci, ci, ci, _i64p]),
             "ref_handle_free": (None, [vp]),
+            "ref_rotation_key_new": (vp, [vp, ci, ci, ci, ci, _i64p]),
+            "ref_core_rotate": (vp, [vp, vp, vp]),
+            "ref_core_conjugate": (vp, [vp, vp, vp]),
             "ref_handle_info": (ctypes.c_longdouble, [vp, ctypes.POINTER(ci)]),
             "ref_handle_dump": (None, [vp, vp, _i64p]),
             "ref_create_secret_key": (vp, [vp, ci]),
@@ -173,6 +176,22 @@ class Engine:
         limbs = np.ascontiguousarray(limbs, dtype=np.int64)
         return Handle(self, lib().ref_key_new(self.ptr, 8, moduli_id, limbs.shape[0],
                                               limbs.ctypes.data_as(_i64p)))
+
+    def fixed_rotation_key(self, limbs, moduli_id, delta):
+        limbs = np.ascontiguousarray(limbs, dtype=np.int64)
+        return Handle(self, lib().ref_rotation_key_new(self.ptr, 6, moduli_id, limbs.shape[0], delta,
+                                                       limbs.ctypes.data_as(_i64p)))
+
+    def conjugation_key(self, limbs, moduli_id):
+        limbs = np.ascontiguousarray(limbs, dtype=np.int64)
+        return Handle(self, lib().ref_rotation_key_new(self.ptr, 7, moduli_id, limbs.shape[0], -1,
+                                                       limbs.ctypes.data_as(_i64p)))
+
+    def core_rotate(self, ct, fixed_key):
+        return self._h(lib().ref_core_rotate(self.ptr, ct.ptr, fixed_key.ptr))
+
+    def core_conjugate(self, ct, ck):
+        return self._h(lib().ref_core_conjugate(self.ptr, ct.ptr, ck.ptr))
 
     def _h(self, ptr):
         return Handle(self, ptr)

@@ -258,6 +258,29 @@ void *ref_key_new(void *e, int kind, int moduli_id, int polys,
   return wrap(8, key, key);
 }
 
+// A fixed rotation key (kind 6, step delta) or a conjugation key (kind 7) from
+// key switching key limbs; permutations as CKKSCore::rotate(key, ...) makes them
+// (core_key.cpp:209-236).
+void *ref_rotation_key_new(void *e, int kind, int moduli_id, int polys, int delta,
+                           const int64_t *data) {
+  auto core = static_cast<RefEngine *>(e)->core();
+  auto key = core->allocate_data<KeySwitchingKey>(
+      DataFlag::NTT_FORM | DataFlag::INCLUDE_SPECIAL, moduli_id, polys);
+  const int chains = key->chain_count_;
+  const int n = core->get_coeff_count();
+  for (int p = 0; p < polys; p++)
+    for (int c = 0; c < chains; c++)
+      std::memcpy(key->get_polynomial(p)->get(c),
+                  data + (size_t(p) * chains + c) * n, sizeof(int64_t) * n);
+  auto [perm, sign] = core->precomputed_.make_permutation_parameters(kind == 7 ? -1 : delta);
+  if (kind == 7) {
+    auto ck = new ConjugationKey(key, perm, sign);
+    return wrap(7, key, ck);
+  }
+  auto fk = new FixedRotationKey(key, perm, sign, delta);
+  return wrap(6, key, fk);
+}
+
 void ref_handle_free(void *h) {
   auto handle = static_cast<Handle *>(h);
   switch (handle->kind) {
@@ -463,6 +486,28 @@ void *ref_engine_rescale(void *e, void *a) {
   auto eng = static_cast<RefEngine *>(e)->engine.get();
   auto r = eng->rescale(static_cast<UnitCiphertext *>(static_cast<Handle *>(a)->data));
   return wrap(4, r, r);
+  } catch (...) {
+    return nullptr;
+  }
+}
+
+void *ref_core_rotate(void *e, void *a, void *fk) {
+  try {
+    auto core = static_cast<RefEngine *>(e)->core();
+    auto r = core->rotate(static_cast<UnitCiphertext *>(static_cast<Handle *>(a)->data),
+                          static_cast<FixedRotationKey *>(static_cast<Handle *>(fk)->owner));
+    return wrap(4, r, r);
+  } catch (...) {
+    return nullptr;
+  }
+}
+
+void *ref_core_conjugate(void *e, void *a, void *ck) {
+  try {
+    auto core = static_cast<RefEngine *>(e)->core();
+    auto r = core->conjugate(static_cast<UnitCiphertext *>(static_cast<Handle *>(a)->data),
+                             static_cast<ConjugationKey *>(static_cast<Handle *>(ck)->owner));
+    return wrap(4, r, r);
   } catch (...) {
     return nullptr;
   }
