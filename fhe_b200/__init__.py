@@ -10,7 +10,10 @@ from .engine import (  # noqa: F401
     CKKS_54_60_BOOTSTRAP,
     CKKS_54_60_BOOTSTRAP_ENGINE_TEST,
     COMPLEX,
+    CONJUGATION_KEY,
+    FIXED_ROTATION_KEY,
     INCLUDE_SPECIAL,
+    KEY_SWITCHING_KEY,
     NONE,
     NTT_FORM,
     RELINEARIZATION_KEY,

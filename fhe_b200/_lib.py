@@ -80,6 +80,13 @@ SIGNATURES = {
     "fhe_multiply_relinearize_rescale": (_i, [_vp, _vp, _vp, _vp, _pp]),
     "fhe_to_ntt": (_i, [_vp, _vp, _pp]),
     "fhe_to_intt": (_i, [_vp, _vp, _pp]),
+    "fhe_level_down": (_i, [_vp, _vp, _i, _pp]),
+    "fhe_rotate": (_i, [_vp, _vp, _vp, _pp]),
+    "fhe_rotate_with_keys": (_i, [_vp, _vp, ctypes.POINTER(_vp), _i, _i, _i, _pp]),
+    "fhe_rotate_plaintext": (_i, [_vp, _vp, _i, _pp]),
+    "fhe_conjugate": (_i, [_vp, _vp, _vp, _pp]),
+    "fhe_conjugate_plaintext": (_i, [_vp, _vp, _pp]),
+    "fhe_switch_key": (_i, [_vp, _vp, _vp, _pp]),
     "fhe_ntt_limbs": (_i, [_vp, _i64p, _i, _i, _i, ctypes.c_longlong, _i]),
     "fhe_relinearize_noalloc": (_i, [_vp, _i64p, _i, _i64p, _i, _i, _i64p]),
 }

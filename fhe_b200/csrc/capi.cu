@@ -343,3 +343,77 @@ int fhe_ntt_limbs(fhe_engine *engine, int64_t *device_limbs, int moduli_id, int 
 }
 
 }  // extern "C"
+
+extern "C" {
+
+int fhe_level_down(fhe_engine *engine, const fhe_data *text, int level, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(text);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] { *out = wrap(engine->impl->level_down(live(engine, text), level)); });
+}
+
+int fhe_rotate(fhe_engine *engine, const fhe_data *ct, const fhe_data *key, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(ct);
+  REQUIRE_HANDLE(key);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] { *out = wrap(engine->impl->rotate(live(engine, ct), live(engine, key))); });
+}
+
+int fhe_rotate_with_keys(fhe_engine *engine, const fhe_data *ct, const fhe_data *const *keys,
+                         int key_count, int delta, int normalize_by_slot_count, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(ct);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  if (key_count < 1 || keys == nullptr) {
+    fhe_b200::set_last_error(
+        "Rotate Unit Ciphertext With Rotation Key: the input fixed rotation key vector is empty.");
+    return FHE_ERR_INVALID_ARGUMENT;
+  }
+  for (int i = 0; i < key_count; i++) REQUIRE_HANDLE(keys[i]);
+  return guarded([&] {
+    std::vector<const fhe_b200::Data *> list;
+    for (int i = 0; i < key_count; i++) list.push_back(&live(engine, keys[i]));
+    *out = wrap(engine->impl->rotate(live(engine, ct), list, delta, normalize_by_slot_count != 0));
+  });
+}
+
+int fhe_rotate_plaintext(fhe_engine *engine, const fhe_data *pt, int delta, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(pt);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] { *out = wrap(engine->impl->rotate_plain(live(engine, pt), delta)); });
+}
+
+int fhe_conjugate(fhe_engine *engine, const fhe_data *ct, const fhe_data *key, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(ct);
+  REQUIRE_HANDLE(key);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] { *out = wrap(engine->impl->conjugate(live(engine, ct), live(engine, key))); });
+}
+
+int fhe_conjugate_plaintext(fhe_engine *engine, const fhe_data *pt, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(pt);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] { *out = wrap(engine->impl->conjugate_plain(live(engine, pt))); });
+}
+
+int fhe_switch_key(fhe_engine *engine, const fhe_data *ct, const fhe_data *key, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(ct);
+  REQUIRE_HANDLE(key);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] { *out = wrap(engine->impl->switch_key(live(engine, ct), live(engine, key))); });
+}
+
+}  // extern "C"

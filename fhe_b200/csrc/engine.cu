@@ -101,8 +101,11 @@ Engine::Engine(const Config &config) : params(config) {
   for (int from = 0; from + 1 < P; from++)
     for (int to = from + 1; to < P; to++)
       rs[static_cast<size_t>(from) * P + to] = p.rescale_scale[from][to - from - 1];
+  std::vector<int64_t> ppr(P, 0);
+  for (size_t i = 0; i < p.p_product_mult_r.size(); i++) ppr[i] = p.p_product_mult_r[i];
   ks_.p_inverse_mult_r = upload_table(pinv);
   ks_.rescale_scale = upload_table(rs);
+  ks_.p_product_mult_r = upload_table(ppr);
   ks_.prime_count = P;
   ks_.special_count = p.special_prime_count;
 }
@@ -127,6 +130,8 @@ Engine::~Engine() {
   for (auto &kv : partition_cache_) {
     cudaFree(kv.second.start);
   }
+  for (auto &kv : signed_perm_cache_) cudaFree(kv.second);
+  for (auto &kv : ntt_perm_cache_) cudaFree(kv.second);
   for (auto *b : table_buffers_) cudaFree(b);
   if (own_stream_) cudaStreamDestroy(own_stream_);
 }
@@ -313,8 +318,10 @@ std::unique_ptr<Data> Engine::prepare_for_multiply(const Data &text, int level) 
     cur = to_intt(*t);
     t = cur.get();
   }
-  if (t->level() != level)
-    throw std::invalid_argument("multiplying texts at different levels is not supported yet.");
+  if (t->level() != level) {
+    cur = level_down_any(*t, level);
+    t = cur.get();
+  }
   if (!t->is_rescaled()) {
     std::unique_ptr<Data> r;
     if (t->is_ntt()) {
@@ -336,7 +343,7 @@ std::unique_ptr<Data> Engine::prepare_for_multiply(const Data &text, int level) 
 }
 
 void Engine::require_key_level(const std::string &fn, const Data &text, const Data &key,
-                               bool for_multiply) {
+                               bool for_multiply, const char *key_name) {
   // is_key_compatible (engine_require.cpp:24-32) with the multiply relaxation
   // (engine_require.cpp:787-798).
   const int key_level = key.level();
@@ -344,7 +351,7 @@ void Engine::require_key_level(const std::string &fn, const Data &text, const Da
   if (params.preset.one_more_level && text.moduli_id == 0 && key.moduli_id == 1) ok = true;
   if (!ok && !(for_multiply && text.level() - 1 == key_level))
     throw std::runtime_error(fn + ": the level of the input " + text.type_name() +
-                             " is greater than that of the input relinearization key.");
+                             " is greater than that of the input " + key_name + ".");
 }
 
 static void require_text(const std::string &fn, const Data &t, int index, int count,
@@ -373,22 +380,22 @@ std::unique_ptr<Data> Engine::multiply(const Data &a, const Data &b) {
   return out;
 }
 
-void Engine::relinearize_tail(const int64_t *t3, int moduli_id, const Data &rk, int mode,
-                              int64_t *out) {
+void Engine::key_switch_pipeline(const int64_t *c1, int moduli_id, const Data &key,
+                                 const int64_t *rotate_c0, const EpilogueOps &ops, int64_t *out) {
   const int n = params.n;
   const int L = params.chains(moduli_id);
   const int E = params.chains(moduli_id, true);
-  if (moduli_id < rk.moduli_id)
+  if (moduli_id < key.moduli_id)
     throw std::invalid_argument(
         "the key switching key was created at a lower level than the text.");
-  const DevicePartitions &dp = partitions(moduli_id, rk.moduli_id);
-  if (rk.polys < 2 * (dp.max_key_index + 1))
-    throw std::invalid_argument("the relinearization key has too few polynomials.");
+  const DevicePartitions &dp = partitions(moduli_id, key.moduli_id);
+  if (key.polys < 2 * (dp.max_key_index + 1))
+    throw std::invalid_argument("the key switching key has too few polynomials.");
   int64_t *digits = alloc_words(static_cast<size_t>(L) * n);
   int64_t *ext = alloc_words(static_cast<size_t>(dp.count) * E * n);
   int64_t *acc = alloc_words(static_cast<size_t>(2) * E * n);
   cudaError_t e = timed("mixed_radix", [&] {
-    return launch_mixed_radix(tables_, dp, n, moduli_id, t3 + 2LL * L * n, digits, stream_);
+    return launch_mixed_radix(tables_, dp, n, moduli_id, c1, digits, stream_);
   });
   if (e == cudaSuccess)
     e = timed("mod_up_ntt", [&] {
@@ -396,8 +403,14 @@ void Engine::relinearize_tail(const int64_t *t3, int moduli_id, const Data &rk, 
     });
   if (e == cudaSuccess)
     e = timed("key_inner_product", [&] {
-      return launch_key_inner_product(tables_, dp, n, moduli_id, ext, rk.d, rk.chains,
-                                      moduli_id - rk.moduli_id, acc, stream_);
+      return launch_key_inner_product(tables_, dp, n, moduli_id, ext, key.d, key.chains,
+                                      moduli_id - key.moduli_id, acc, stream_);
+    });
+  if (e == cudaSuccess && rotate_c0 != nullptr)
+    e = timed("rotate_base", [&] {
+      // `digits` is free again and serves as the NTT's intermediate buffer.
+      return launch_rotate_base(tables_, ks_, params.log_n, moduli_id, L, rotate_c0, digits, acc,
+                                stream_);
     });
   if (e == cudaSuccess)
     e = timed("mod_down_intt", [&] {
@@ -405,12 +418,22 @@ void Engine::relinearize_tail(const int64_t *t3, int moduli_id, const Data &rk, 
     });
   if (e == cudaSuccess)
     e = timed("mod_down_epilogue", [&] {
-      return launch_mod_down_epilogue(tables_, ks_, n, moduli_id, L, acc, t3, mode, out, stream_);
+      return launch_mod_down_epilogue_ops(tables_, ks_, n, moduli_id, L, acc, ops, out, stream_);
     });
   free_words(digits);
   free_words(ext);
   free_words(acc);
   check(e, "key switch");
+}
+
+void Engine::relinearize_tail(const int64_t *t3, int moduli_id, const Data &rk, int mode,
+                              int64_t *out) {
+  EpilogueOps ops;
+  ops.base = t3;
+  ops.base_polys = mode == 0 ? 0 : 2;
+  ops.rescale = mode == 2;
+  const long long L = params.chains(moduli_id);
+  key_switch_pipeline(t3 + 2 * L * params.n, moduli_id, rk, nullptr, ops, out);
 }
 
 std::unique_ptr<Data> Engine::relinearize(const Data &ct, const Data &rk) {
@@ -544,6 +567,278 @@ std::string Engine::profile_report() {
 void Engine::profile_reset() {
   collect_timings();
   stats_.clear();
+}
+
+// --------------------------------------------------------------- level down --
+
+// CKKSCore::level_down_after_rescale (core.cpp:743-778) for rescaled text in any
+// form and CKKSCore::level_down (core.cpp:786-838) for coefficient-form text:
+// multiply by the level-down multiplier, then (not rescaled) rescale by the first
+// prime and keep the destination's limbs.
+std::unique_ptr<Data> Engine::core_level_down(const Data &text, int level) {
+  const int n = params.n;
+  const int dst_mid = params.moduli_id(level);
+  const int out_chains = params.chains(dst_mid);
+  auto to_scalars = [](const std::vector<int64_t> &v, int count) {
+    if (count > kMaxScalarLimbs || static_cast<int>(v.size()) < count)
+      throw std::invalid_argument("level down: too many limbs.");
+    LimbScalars s{};
+    for (int i = 0; i < count; i++) s.v[i] = v[i];
+    return s;
+  };
+  if (text.is_rescaled()) {
+    const LimbScalars s = to_scalars(params.level_down_multiplier_after_rescale(text.level(), level), out_chains);
+    auto out = make_data(text.type, text.flag & ~kFlagRescaled, dst_mid, text.polys,
+                         params.level_down_scale(level));
+    check(timed("level_down", [&] {
+            return launch_scalar_enter(tables_, n, text.polys, out_chains, dst_mid, text.d,
+                                       text.poly_stride(), dst_mid - text.moduli_id, s, out->d,
+                                       out->poly_stride(), stream_);
+          }),
+          "level_down");
+    return out;
+  }
+  const int src_mid = text.moduli_id;
+  const int L = text.chains;
+  const int next_mid = params.moduli_id(text.level() - 1);
+  const LimbScalars s = to_scalars(params.level_down_multiplier(text.level(), level), L);
+  const long long in_stride = static_cast<long long>(L) * n;
+  const long long mid_stride = static_cast<long long>(L - 1) * n;
+  int64_t *entered = alloc_words(static_cast<size_t>(text.polys) * in_stride);
+  int64_t *rescaled = alloc_words(static_cast<size_t>(text.polys) * mid_stride);
+  auto out = make_data(text.type, text.flag, dst_mid, text.polys, params.level_down_scale(level));
+  cudaError_t e = timed("level_down", [&] {
+    return launch_scalar_enter(tables_, n, text.polys, L, src_mid, text.d, text.poly_stride(), 0, s,
+                               entered, in_stride, stream_);
+  });
+  if (e == cudaSuccess)
+    e = timed("rescale", [&] {
+      return launch_rescale(tables_, ks_, n, text.polys, L, src_mid, entered, in_stride, rescaled,
+                            mid_stride, stream_);
+    });
+  if (e == cudaSuccess) {
+    const int offset = dst_mid - next_mid;
+    e = cudaMemcpy2DAsync(out->d, out->poly_stride() * sizeof(int64_t),
+                          rescaled + static_cast<long long>(offset) * n, mid_stride * sizeof(int64_t),
+                          static_cast<size_t>(out_chains) * n * sizeof(int64_t), text.polys,
+                          cudaMemcpyDeviceToDevice, stream_);
+  }
+  free_words(entered);
+  free_words(rescaled);
+  check(e, "level_down");
+  return out;
+}
+
+// CKKSEngine::level_down_ (engine_level_down.cpp:5-36).
+std::unique_ptr<Data> Engine::level_down_any(const Data &text, int level) {
+  if (text.level() == level) return clone(text);
+  if (text.is_rescaled()) return core_level_down(text, level);
+  if (text.is_ntt()) {
+    auto intt = to_intt(text);
+    auto down = core_level_down(*intt, level);
+    return to_ntt(*down);
+  }
+  return core_level_down(text, level);
+}
+
+std::unique_ptr<Data> Engine::level_down(const Data &text, int level) {
+  const bool cipher = text.type == kUnitCiphertext;
+  const std::string fn = cipher ? "Level Down Unit Ciphertext" : "Level Down Unit Plaintext";
+  if (cipher && text.polys != 2 && text.polys != 3)
+    throw std::runtime_error(fn + ": the input " + text.type_name() +
+                             " should have either 2 or 3 polynomials.");
+  if (level < 0 || level > text.level())
+    throw std::runtime_error(fn + ": the target level cannot be reached.");
+  return level_down_any(text, level);
+}
+
+// ------------------------------------------------- rotation and conjugation --
+
+int Engine::normalized_delta(int delta, bool normalize_by_slot_count) const {
+  // CKKSEngine::to_normalized_delta (engine.cpp:227-235) with positive_modulo.
+  const int m = normalize_by_slot_count ? params.slot_count : params.n / 2;
+  return (m + delta % m) % m;
+}
+
+const int32_t *Engine::device_signed_permutation(int delta) {
+  auto it = signed_perm_cache_.find(delta);
+  if (it != signed_perm_cache_.end()) return it->second;
+  const auto host = signed_permutation(params.n, delta);
+  void *p = nullptr;
+  check(cudaMalloc(&p, host.size() * sizeof(int32_t)), "cudaMalloc(permutation)");
+  check(cudaMemcpy(p, host.data(), host.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
+        "upload permutation");
+  return signed_perm_cache_.emplace(delta, static_cast<int32_t *>(p)).first->second;
+}
+
+const int32_t *Engine::device_ntt_permutation(int delta) {
+  auto it = ntt_perm_cache_.find(delta);
+  if (it != ntt_perm_cache_.end()) return it->second;
+  const auto host = ntt_permutation(params.n, delta);
+  void *p = nullptr;
+  check(cudaMalloc(&p, host.size() * sizeof(int32_t)), "cudaMalloc(permutation)");
+  check(cudaMemcpy(p, host.data(), host.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
+        "upload permutation");
+  return ntt_perm_cache_.emplace(delta, static_cast<int32_t *>(p)).first->second;
+}
+
+// CKKSCore::rotate (core.cpp:939-963): key switch of c1 with the b * P term, ModDown,
+// then the key's signed coefficient permutation.
+std::unique_ptr<Data> Engine::core_rotate(const Data &ct, const Data &key) {
+  auto out = make_data(kUnitCiphertext, ct.flag, ct.moduli_id, 2, ct.scale);
+  EpilogueOps ops;
+  ops.signed_perm = device_signed_permutation(key.delta);
+  key_switch_pipeline(ct.d + ct.poly_stride(), ct.moduli_id, key, ct.d, ops, out->d);
+  return out;
+}
+
+std::unique_ptr<Data> Engine::rotate(const Data &ct, const Data &key) {
+  const std::string fn = "Rotate Unit Ciphertext With Fixed Rotation Key";
+  require_text(fn, ct, 0, 1, 2, false);
+  if (key.type != kFixedRotationKey)
+    throw std::invalid_argument(fn + ": the key is not a fixed rotation key.");
+  require_key_level(fn, ct, key, false, "fixed rotation key");
+  std::unique_ptr<Data> hold;
+  const Data *x = &ct;
+  if (params.preset.one_more_level && ct.moduli_id == 0) {
+    hold = level_down_any(ct, ct.level() - 1);
+    x = hold.get();
+  }
+  if (x->is_ntt()) {
+    hold = to_intt(*x);
+    x = hold.get();
+  }
+  return core_rotate(*x, key);
+}
+
+std::unique_ptr<Data> Engine::rotate(const Data &ct, const std::vector<const Data *> &keys,
+                                     int delta, bool normalize_by_slot_count) {
+  const std::string fn = "Rotate Unit Ciphertext With Rotation Key";
+  require_text(fn, ct, 0, 1, 2, false);
+  for (const Data *k : keys) {
+    if (k == nullptr || k->type != kFixedRotationKey)
+      throw std::invalid_argument(fn + ": the key is not a fixed rotation key.");
+    require_key_level(fn, ct, *k, false, "rotation key");
+  }
+  const int nd = normalized_delta(delta, normalize_by_slot_count);
+  if (nd == 0) return to_intt(ct);
+  std::unique_ptr<Data> cur;
+  for (const Data *k : keys) {
+    if ((nd & k->delta) == 0) continue;
+    auto next = rotate(cur ? *cur : ct, *k);
+    cur = std::move(next);
+  }
+  if (!cur)
+    throw std::invalid_argument(fn + ": no fixed rotation key matches the delta.");
+  return cur;
+}
+
+std::unique_ptr<Data> Engine::rotate_plain(const Data &pt, int delta) {
+  // CKKSEngine::rotate(UnitPlaintext*, int) (engine_rotate.cpp:10-24).
+  const int nd = normalized_delta(delta);
+  auto out = make_data(pt.type, pt.flag, pt.moduli_id, pt.polys, pt.scale);
+  out->delta = pt.delta;
+  if (pt.is_ntt()) {
+    check(timed("permute", [&] {
+            return launch_permute_gather(params.n, pt.polys, pt.chains, pt.d, pt.poly_stride(),
+                                         device_ntt_permutation(nd), out->d, out->poly_stride(),
+                                         stream_);
+          }),
+          "rotate");
+  } else {
+    check(timed("permute", [&] {
+            return launch_permute_signed(tables_, params.n, pt.polys, pt.chains, pt.moduli_id, pt.d,
+                                         pt.poly_stride(), device_signed_permutation(nd), out->d,
+                                         out->poly_stride(), stream_);
+          }),
+          "rotate");
+  }
+  return out;
+}
+
+std::unique_ptr<Data> Engine::conjugate_plain(const Data &pt) {
+  // conjugate_intt_form / conjugate_ntt_form (core.cpp:1020-1033): delta -1.
+  auto out = make_data(pt.type, pt.flag, pt.moduli_id, pt.polys, pt.scale);
+  if (pt.is_ntt()) {
+    check(timed("permute", [&] {
+            return launch_permute_gather(params.n, pt.polys, pt.chains, pt.d, pt.poly_stride(),
+                                         device_ntt_permutation(-1), out->d, out->poly_stride(),
+                                         stream_);
+          }),
+          "conjugate");
+  } else {
+    check(timed("permute", [&] {
+            return launch_permute_signed(tables_, params.n, pt.polys, pt.chains, pt.moduli_id, pt.d,
+                                         pt.poly_stride(), device_signed_permutation(-1), out->d,
+                                         out->poly_stride(), stream_);
+          }),
+          "conjugate");
+  }
+  return out;
+}
+
+std::unique_ptr<Data> Engine::conjugate(const Data &ct, const Data &key) {
+  // CKKSEngine::conjugate (engine_conjugate.cpp:53-73) and CKKSCore::conjugate
+  // (core.cpp:1035-1056): permute both polynomials, key switch the permuted c1 and
+  // add the permuted c0.
+  const std::string fn = "Conjugate Unit Ciphertext";
+  require_text(fn, ct, 0, 1, 2, false);
+  if (key.type != kConjugationKey)
+    throw std::invalid_argument(fn + ": the key is not a conjugation key.");
+  require_key_level(fn, ct, key, false, "conjugation key");
+  std::unique_ptr<Data> hold;
+  const Data *x = &ct;
+  if (params.preset.one_more_level && ct.moduli_id == 0) {
+    hold = level_down_any(ct, ct.level() - 1);
+    x = hold.get();
+  }
+  if (x->is_ntt()) {
+    hold = to_intt(*x);
+    x = hold.get();
+  }
+  const int n = params.n;
+  const long long ps = x->poly_stride();
+  int64_t *permuted = alloc_words(static_cast<size_t>(2) * ps);
+  cudaError_t e = timed("permute", [&] {
+    return launch_permute_signed(tables_, n, 2, x->chains, x->moduli_id, x->d, ps,
+                                 device_signed_permutation(-1), permuted, ps, stream_);
+  });
+  if (e != cudaSuccess) {
+    free_words(permuted);
+    check(e, "conjugate");
+  }
+  auto out = make_data(kUnitCiphertext, x->flag, x->moduli_id, 2, x->scale);
+  EpilogueOps ops;
+  ops.base = permuted;
+  ops.base_polys = 1;
+  try {
+    key_switch_pipeline(permuted + ps, x->moduli_id, key, nullptr, ops, out->d);
+  } catch (...) {
+    free_words(permuted);
+    throw;
+  }
+  free_words(permuted);
+  return out;
+}
+
+std::unique_ptr<Data> Engine::switch_key(const Data &ct, const Data &key) {
+  const std::string fn = "Switch Key";
+  require_text(fn, ct, 0, 1, 2, false);
+  if (key.type != kKeySwitchingKey)
+    throw std::invalid_argument(fn + ": the key is not a key switching key.");
+  require_key_level(fn, ct, key, false, "key switching key");
+  std::unique_ptr<Data> hold;
+  const Data *x = &ct;
+  if (x->is_ntt()) {
+    hold = to_intt(*x);
+    x = hold.get();
+  }
+  auto out = make_data(x->type, x->flag, x->moduli_id, 2, x->scale);
+  EpilogueOps ops;
+  ops.base = x->d;
+  ops.base_polys = 1;
+  key_switch_pipeline(x->d + x->poly_stride(), x->moduli_id, key, nullptr, ops, out->d);
+  return out;
 }
 
 }  // namespace fhe_b200

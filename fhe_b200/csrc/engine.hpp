@@ -99,6 +99,19 @@ class Engine {
   std::unique_ptr<Data> rescale(const Data &ct);
   std::unique_ptr<Data> to_ntt(const Data &text);
   std::unique_ptr<Data> to_intt(const Data &text);
+  std::unique_ptr<Data> level_down(const Data &text, int level);
+  // Ciphertext rotation by one fixed rotation key (engine_rotate.cpp:52-74) and by
+  // a set of power-of-two keys selected by the bits of `delta` (:106-139).
+  std::unique_ptr<Data> rotate(const Data &ct, const Data &fixed_rotation_key);
+  std::unique_ptr<Data> rotate(const Data &ct, const std::vector<const Data *> &keys, int delta,
+                               bool normalize_by_slot_count = false);
+  // Plaintext rotation and conjugation (no key): engine_rotate.cpp:10-24.
+  std::unique_ptr<Data> rotate_plain(const Data &pt, int delta);
+  std::unique_ptr<Data> conjugate_plain(const Data &pt);
+  std::unique_ptr<Data> conjugate(const Data &ct, const Data &conjugation_key);
+  // CKKSCore::switch_key (core.cpp:1058-1083): coefficient-form input.
+  std::unique_ptr<Data> switch_key(const Data &ct, const Data &key_switching_key);
+  int normalized_delta(int delta, bool normalize_by_slot_count = false) const;
 
   void ntt_limbs(int64_t *limbs, int moduli_id, int chains, int polys, long long stride,
                  bool inverse);
@@ -120,6 +133,10 @@ class Engine {
   PrimeTables tables_{};
   KeySwitchTables ks_{};
   std::map<std::pair<int, int>, DevicePartitions> partition_cache_;
+  std::map<int, int32_t *> signed_perm_cache_;  // delta -> signed permutation [N]
+  std::map<int, int32_t *> ntt_perm_cache_;     // delta -> NTT-form gather indices [N]
+  const int32_t *device_signed_permutation(int delta);
+  const int32_t *device_ntt_permutation(int delta);
   std::set<Data *> live_;
 
   struct PendingTiming {
@@ -151,11 +168,19 @@ class Engine {
   // Core steps.
   std::unique_ptr<Data> core_rescale(const Data &ct);          // coefficient form
   std::unique_ptr<Data> prepare_for_multiply(const Data &text, int level);
+  // Hybrid key switch of the coefficient-form polynomial c1 at moduli_id (L limbs):
+  // decompose, ModUp, key product, optional rotation term b * P (rotate_c0 = the
+  // coefficient-form c0), ModDown and the epilogue operations `ops` into `out`.
+  void key_switch_pipeline(const int64_t *c1, int moduli_id, const Data &key,
+                           const int64_t *rotate_c0, const EpilogueOps &ops, int64_t *out);
   // Key switch tail shared by relinearize variants; t3 is [3][L][N] coefficient
   // form at moduli_id (poly 2 is switched).
   void relinearize_tail(const int64_t *t3, int moduli_id, const Data &rk, int mode, int64_t *out);
   void require_key_level(const std::string &fn, const Data &text, const Data &key,
-                         bool for_multiply);
+                         bool for_multiply, const char *key_name = "relinearization key");
+  std::unique_ptr<Data> core_level_down(const Data &text, int level);  // coefficient form
+  std::unique_ptr<Data> level_down_any(const Data &text, int level);   // level_down_ (any form)
+  std::unique_ptr<Data> core_rotate(const Data &ct, const Data &key);   // coefficient form
 };
 
 // Thread-local last error of the C ABI.

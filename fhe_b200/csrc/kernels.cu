@@ -68,7 +68,9 @@ __global__ void rescale_kernel(PrimeTables t, KeySwitchTables ks, int n, int lim
                                const int64_t *x, long long xs, int64_t *y, long long ys) {
   const int poly = blockIdx.y;
   const long long per_poly = static_cast<long long>(limbs - 1) * n;
-  const int64_t q_half = static_cast<int64_t>(t.q[moduli_id] >> 1);
+  // get_rounder compares the signed word with the unsigned q/2 (unit.cpp:67-70), so
+  // a negative word counts as above it.
+  const uint64_t q_half = t.q[moduli_id] >> 1;
   const int64_t *xp = x + poly * xs;
   int64_t *yp = y + poly * ys;
   for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < per_poly;
@@ -77,7 +79,7 @@ __global__ void rescale_kernel(PrimeTables t, KeySwitchTables ks, int n, int lim
     const int c = static_cast<int>(i - static_cast<long long>(j) * n);
     const int prime = moduli_id + 1 + j;
     const int64_t x0 = xp[c];
-    const int64_t rounder = x0 > q_half ? 1 : 0;  // get_rounder (unit.cpp:66-70)
+    const int64_t rounder = static_cast<uint64_t>(x0) > q_half ? 1 : 0;  // get_rounder
     yp[i] = rescale_word(xp[static_cast<long long>(j + 1) * n + c], x0, rounder, t.q[prime],
                          t.k[prime], ks.rescale_scale[static_cast<long long>(moduli_id) * ks.prime_count + prime]);
   }
@@ -270,7 +272,7 @@ constexpr int kEpilogueCoeffs = 16;  // K * 16 <= 256 threads for every K <= 16
 template <int K>
 __global__ void __launch_bounds__(256)
     mod_down_epilogue_kernel(PrimeTables t, KeySwitchTables ks, int n, int moduli_id, int limbs,
-                             const int64_t *acc, const int64_t *base, int mode, int64_t *out) {
+                             const int64_t *acc, EpilogueOps ops, int64_t *out) {
   constexpr int CB = kEpilogueCoeffs;
   __shared__ int64_t divisor[K][CB];
   __shared__ int64_t first_limb[CB];
@@ -316,18 +318,34 @@ __global__ void __launch_bounds__(256)
     return v < 0 ? v + qs : guard(v, qs);  // make_unsigned_reduce_2q_to_q
   };
   const long long in_stride = static_cast<long long>(L) * n;
-  const int64_t *b = base + poly * in_stride + coeff0;
+  const bool add_base = poly < ops.base_polys;  // uniform per CTA
+  const int64_t *b = add_base ? ops.base + poly * in_stride + coeff0 : nullptr;
   auto combined = [&](int j, int c) -> int64_t {
     const int64_t qs = static_cast<int64_t>(t.q[moduli_id + j]);
+    if (!add_base) return divide(j, c);
     return guard(guard(b[static_cast<long long>(j) * n + c] + divide(j, c), qs << 1), qs);
   };
   const int valid = n - coeff0 < CB ? n - coeff0 : CB;
 
-  if (mode != 2) {
-    int64_t *o = out + poly * in_stride + coeff0;
+  if (!ops.rescale) {
+    int64_t *o = out + poly * in_stride;
+    if (ops.signed_perm == nullptr) {
+      for (int w = threadIdx.x; w < L * CB; w += blockDim.x) {
+        const int j = w / CB, c = w % CB;
+        if (c < valid) o[static_cast<long long>(j) * n + coeff0 + c] = combined(j, c);
+      }
+      return;
+    }
+    // Permuted store (rotate_ after key_switch_mod_down, core.cpp:939-952).
     for (int w = threadIdx.x; w < L * CB; w += blockDim.x) {
       const int j = w / CB, c = w % CB;
-      if (c < valid) o[static_cast<long long>(j) * n + c] = mode == 0 ? divide(j, c) : combined(j, c);
+      if (c >= valid) continue;
+      const int64_t qs = static_cast<int64_t>(t.q[moduli_id + j]);
+      const int32_t pc = ops.signed_perm[coeff0 + c];
+      int64_t v = combined(j, c);
+      if (pc < 0) v = -v;
+      v = v < 0 ? v + qs : guard(v, qs);
+      o[static_cast<long long>(j) * n + (pc < 0 ? ~pc : pc)] = v;
     }
     return;
   }
@@ -336,14 +354,14 @@ __global__ void __launch_bounds__(256)
   __syncthreads();
   const long long out_stride = static_cast<long long>(L - 1) * n;
   int64_t *o = out + poly * out_stride + coeff0;
-  const int64_t q_half = static_cast<int64_t>(t.q[moduli_id] >> 1);
+  const uint64_t q_half = t.q[moduli_id] >> 1;  // unsigned comparison, as get_rounder
   for (int w = threadIdx.x; w < (L - 1) * CB; w += blockDim.x) {
     const int j = 1 + w / CB, c = w % CB;
     if (c >= valid) continue;
     const int prime = moduli_id + j;
     const int64_t y0 = first_limb[c];
     o[static_cast<long long>(j - 1) * n + c] =
-        rescale_word(combined(j, c), y0, y0 > q_half ? 1 : 0, t.q[prime], t.k[prime],
+        rescale_word(combined(j, c), y0, static_cast<uint64_t>(y0) > q_half ? 1 : 0, t.q[prime], t.k[prime],
                      ks.rescale_scale[static_cast<long long>(moduli_id) * P + prime]);
   }
 }
@@ -461,16 +479,18 @@ cudaError_t launch_mod_down_intt(const PrimeTables &t, int log_n, int moduli_id,
   return inverse_ntt(log_n, 2, extended, moduli_id, t, ld, st, acc, stride, s);
 }
 
-cudaError_t launch_mod_down_epilogue(const PrimeTables &t, const KeySwitchTables &ks, int n,
-                                     int moduli_id, int limbs, const int64_t *acc,
-                                     const int64_t *base, int mode, int64_t *out, cudaStream_t s) {
+cudaError_t launch_mod_down_epilogue_ops(const PrimeTables &t, const KeySwitchTables &ks, int n,
+                                         int moduli_id, int limbs, const int64_t *acc,
+                                         const EpilogueOps &ops, int64_t *out, cudaStream_t s) {
+  if ((ops.base_polys > 0 && ops.base == nullptr) || (ops.rescale && ops.signed_perm != nullptr))
+    return cudaErrorInvalidValue;
   const dim3 grid((n + kEpilogueCoeffs - 1) / kEpilogueCoeffs, 2);
   switch (ks.special_count) {
 #define FHE_MD_CASE(K)                                                                      \
   case K:                                                                                   \
     note_launch();                                                                          \
-    mod_down_epilogue_kernel<K><<<grid, kThreads, 0, s>>>(t, ks, n, moduli_id, limbs, acc, base, \
-                                                          mode, out);                       \
+    mod_down_epilogue_kernel<K><<<grid, kThreads, 0, s>>>(t, ks, n, moduli_id, limbs, acc, ops, \
+                                                          out);                             \
     break;
     FHE_MD_CASE(1) FHE_MD_CASE(2) FHE_MD_CASE(3) FHE_MD_CASE(4) FHE_MD_CASE(5) FHE_MD_CASE(6)
     FHE_MD_CASE(7) FHE_MD_CASE(8) FHE_MD_CASE(9) FHE_MD_CASE(10) FHE_MD_CASE(11) FHE_MD_CASE(12)
@@ -479,6 +499,18 @@ cudaError_t launch_mod_down_epilogue(const PrimeTables &t, const KeySwitchTables
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
+}
+
+// mode 0: divide only; 1: + base on both polynomials (relinearize); 2: + base and
+// rescale (multiply-relinearize-rescale).
+cudaError_t launch_mod_down_epilogue(const PrimeTables &t, const KeySwitchTables &ks, int n,
+                                     int moduli_id, int limbs, const int64_t *acc,
+                                     const int64_t *base, int mode, int64_t *out, cudaStream_t s) {
+  EpilogueOps ops;
+  ops.base = base;
+  ops.base_polys = mode == 0 ? 0 : 2;
+  ops.rescale = mode == 2;
+  return launch_mod_down_epilogue_ops(t, ks, n, moduli_id, limbs, acc, ops, out, s);
 }
 
 cudaError_t launch_to_ntt(const PrimeTables &t, int log_n, int polys, int limbs, int prime_base,

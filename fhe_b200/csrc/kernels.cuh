@@ -34,8 +34,20 @@ unsigned long long kernel_launch_count();
 struct KeySwitchTables {
   const int64_t *p_inverse_mult_r;  // [K][P] (entry for prime i at [s*P + i])
   const int64_t *rescale_scale;     // [P][P] (entry for from,to at [from*P + to])
+  const int64_t *p_product_mult_r;  // [P] P mod q * R (zero for the special primes)
   int prime_count;
   int special_count;
+};
+
+// What the ModDown epilogue does with the divided limbs of each polynomial.
+struct EpilogueOps {
+  const int64_t *base = nullptr;  // [2][L][N] coefficient-form addend (mont_add_reduce_2q_to_q)
+  int base_polys = 0;             // polynomials 0 .. base_polys-1 receive the addend
+  bool rescale = false;           // rescale by the first prime of the chain (output L-1 limbs)
+  // Signed coefficient permutation applied last (rotate_, core.cpp:846-868):
+  // word c goes to index perm[c] when perm[c] >= 0, negated to ~perm[c] otherwise,
+  // then make_unsigned_reduce_2q_to_q.
+  const int32_t *signed_perm = nullptr;
 };
 
 // z = tensor of two NTT-form ciphertexts (core.cpp:284-314): z0 = a0 b0,
@@ -90,6 +102,41 @@ cudaError_t launch_mod_down_epilogue(const PrimeTables &t, const KeySwitchTables
                                      int moduli_id, int limbs, const int64_t *acc,
                                      const int64_t *base, int mode, int64_t *out,
                                      cudaStream_t s);
+// The same epilogue with an explicit list of operations (switch_key adds the base
+// to polynomial 0 only, rotate permutes).
+cudaError_t launch_mod_down_epilogue_ops(const PrimeTables &t, const KeySwitchTables &ks, int n,
+                                         int moduli_id, int limbs, const int64_t *acc,
+                                         const EpilogueOps &ops, int64_t *out, cudaStream_t s);
+
+// Rotation's b * P term (create_key_switcher_for_rotate, core_key_switch.cpp:550-576):
+// acc0[j] = reduce(acc0[j] + NTT(mont(mont(c0[j], P mod q * R), R^2))) for the L
+// limbs of the ciphertext; `work` holds L limbs of intermediate data.
+cudaError_t launch_rotate_base(const PrimeTables &t, const KeySwitchTables &ks, int log_n,
+                               int moduli_id, int limbs, const int64_t *c0, int64_t *work,
+                               int64_t *acc0, cudaStream_t s);
+
+// rotate_ (core.cpp:846-868): y[perm[c]] = sign[c] * x[c], make_unsigned, over polys x
+// limbs, with the signed permutation encoding of EpilogueOps.
+cudaError_t launch_permute_signed(const PrimeTables &t, int n, int polys, int limbs,
+                                  int prime_base, const int64_t *x, long long x_stride,
+                                  const int32_t *signed_perm, int64_t *y, long long y_stride,
+                                  cudaStream_t s);
+// permute_chain (encode.cpp:575-580): y[c] = x[perm[c]] (NTT-form rotation).
+cudaError_t launch_permute_gather(int n, int polys, int limbs, const int64_t *x,
+                                  long long x_stride, const int32_t *perm, int64_t *y,
+                                  long long y_stride, cudaStream_t s);
+
+// Per-limb Montgomery constants passed by value.
+constexpr int kMaxScalarLimbs = 128;
+struct LimbScalars {
+  int64_t v[kMaxScalarLimbs];
+};
+// y[p][j] = reduce_2q_to_q(mont(x[p][j + x_limb_offset], s[j])) for j < limbs: the
+// mont_enter_scalar_ + reduce_2q_to_q pair of level_down (core.cpp:743-838).
+cudaError_t launch_scalar_enter(const PrimeTables &t, int n, int polys, int limbs,
+                                int prime_base, const int64_t *x, long long x_stride,
+                                int x_limb_offset, const LimbScalars &s, int64_t *y,
+                                long long y_stride, cudaStream_t st);
 
 // Forward NTT with Montgomery enter (to_ntt_) of polys x limbs, in place or not.
 cudaError_t launch_to_ntt(const PrimeTables &t, int log_n, int polys, int limbs, int prime_base,

@@ -445,3 +445,112 @@ long double Parameters::rescaled_scale(long double s, int moduli_id) const {
 }
 
 }  // namespace fhe_b200
+
+namespace fhe_b200 {
+
+namespace {
+
+// (round(value) * 2^62) mod q for the non-negative double `value`: the
+// BigInt::from_double(std::round(value)) * r_ % q of precomputed.cpp:418-462.
+int64_t rounded_times_r_mod(double value, uint64_t q) {
+  const double r = std::round(value);
+  if (!(r >= 0.0) || r >= 18446744073709551616.0)
+    throw std::invalid_argument("level down multiplier out of range");
+  const unsigned __int128 v = static_cast<unsigned __int128>(static_cast<uint64_t>(r)) << 62;
+  return static_cast<int64_t>(v % q);
+}
+
+// get_jump: ckks/encode.cpp:44-56.
+int64_t rotation_jump(unsigned long shift, unsigned long double_size) {
+  if (shift == double_size - 1) return static_cast<int64_t>(shift);
+  int64_t jump = 1;
+  for (unsigned long power = 0; power < double_size - shift; power++) {
+    jump *= 5;
+    jump &= static_cast<int64_t>(double_size - 1);
+  }
+  return jump;
+}
+
+int reverse_low_bits(int x, int bits) {
+  int y = 0;
+  for (int b = 0; b < bits; b++) y |= ((x >> b) & 1) << (bits - 1 - b);
+  return y;
+}
+
+}  // namespace
+
+std::vector<int32_t> signed_permutation(int n, int delta) {
+  const unsigned long double_size = static_cast<unsigned long>(n) * 2;
+  const unsigned long shift =
+      (static_cast<unsigned long>(static_cast<long>(delta)) + double_size) % double_size;
+  const int64_t jump = rotation_jump(shift, double_size);
+  std::vector<int32_t> out(n);
+  for (int c = 0; c < n; c++) {
+    const unsigned long index = static_cast<unsigned long>(jump) * c % double_size;
+    const int32_t to = static_cast<int32_t>(index % n);
+    out[c] = ((index / n) & 1) ? ~to : to;
+  }
+  return out;
+}
+
+std::vector<int32_t> ntt_permutation(int n, int delta) {
+  const int mask = n - 1;
+  const uint32_t m2 = static_cast<uint32_t>(n) * 2;
+  // modulus_power<uint32_t>(5, delta, 2N): arithmetic/arithmetic.cpp:40-52.
+  uint64_t power = 1, base = 5;
+  for (uint32_t e = static_cast<uint32_t>(delta); e > 0; e >>= 1) {
+    if (e & 1) power = power * base % m2;
+    base = base * base % m2;
+  }
+  const int64_t power_of_five = static_cast<int64_t>(power) & mask;
+  const int diff = delta == -1 ? -1 : static_cast<int>(((power - 1) >> 1) & mask);
+  const int64_t inverse = delta == -1 ? n - 1 : mod_invert(power_of_five, n);
+  int log_n = 0;
+  while ((1 << log_n) < n) log_n++;
+  std::vector<int32_t> tmp(n), out(n);
+  for (int i = 0; i < n; i++) {
+    const int64_t index = ((i - diff) % n + n) % n;
+    tmp[i] = static_cast<int32_t>(index * inverse % n);
+  }
+  for (int i = 0; i < n; i++) out[i] = reverse_low_bits(tmp[reverse_low_bits(i, log_n)], log_n);
+  return out;
+}
+
+std::vector<int64_t> Parameters::level_down_multiplier(int source_level,
+                                                       int destination_level) const {
+  // CKKSPrecomputed::make_level_down_multiplier (precomputed.cpp:438-462); the
+  // deviations are the double copies the precomputed tables hold.
+  const int source_moduli_id = moduli_id(source_level);
+  const double source_deviation = static_cast<double>(deviations[source_level]);
+  const double destination_deviation = static_cast<double>(deviations[destination_level]);
+  const double diff = destination_deviation / source_deviation;
+  double delta;
+  if (preset.one_more_level && source_moduli_id == 0)
+    delta = scale * diff;
+  else
+    delta = static_cast<double>(q[source_moduli_id]) * diff;
+  std::vector<int64_t> out;
+  for (int i = source_moduli_id; i < chain_count; i++) out.push_back(rounded_times_r_mod(delta, q[i]));
+  return out;
+}
+
+std::vector<int64_t> Parameters::level_down_multiplier_after_rescale(int source_level,
+                                                                     int destination_level) const {
+  // make_level_down_multiplier_after_rescale (precomputed.cpp:418-436).
+  const double source_deviation = static_cast<double>(deviations[source_level - 1]);
+  const double destination_deviation = static_cast<double>(deviations[destination_level]);
+  const double diff = destination_deviation / std::sqrt(source_deviation);
+  const double delta = scale * diff;
+  std::vector<int64_t> out;
+  for (int i = moduli_id(destination_level); i < chain_count; i++)
+    out.push_back(rounded_times_r_mod(delta, q[i]));
+  return out;
+}
+
+long double Parameters::level_down_scale(int level) const {
+  // core.cpp:743-750: deviation (double) * scale * scale in long double.
+  const long double s = scale;
+  return static_cast<double>(deviations[level]) * s * s;
+}
+
+}  // namespace fhe_b200

@@ -100,7 +100,19 @@ class Parameters {
   PartitionConstants partition_constants(int moduli_id, const Partition &p) const;
   uint64_t base_prime() const;
   long double rescaled_scale(long double scale, int moduli_id) const;
+  // Per-limb Montgomery multipliers of level_down, from the moduli id of the
+  // source level (resp. destination level after a rescale) to the last scaling prime.
+  std::vector<int64_t> level_down_multiplier(int source_level, int destination_level) const;
+  std::vector<int64_t> level_down_multiplier_after_rescale(int source_level,
+                                                           int destination_level) const;
+  long double level_down_scale(int level) const;
 };
+
+// get_permutation_and_sign (ckks/encode.cpp:513-526) for a rotation by `delta`
+// (-1: conjugation), encoded as perm[c] or ~perm[c] where the sign is -1.
+std::vector<int32_t> signed_permutation(int n, int delta);
+// get_ntt_permutation (ckks/encode.cpp:528-557): NTT-form rotation gather indices.
+std::vector<int32_t> ntt_permutation(int n, int delta);
 
 // Modular helpers shared with the engine (arithmetic/arithmetic.cpp semantics).
 int64_t mod_invert(int64_t x, int64_t modulus);

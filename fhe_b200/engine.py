@@ -51,6 +51,9 @@ class Data:
         check(_lib.load().fhe_data_download(self._h, out.ctypes.data_as(_lib._i64p)))
         return out
 
+    def set_delta(self, delta: int) -> None:
+        check(_lib.load().fhe_data_set_delta(self._h, delta))
+
     def device_pointer(self) -> int:
         p = _lib._i64p()
         check(_lib.load().fhe_data_device_pointer(self._h, ctypes.byref(p)))
@@ -178,6 +181,18 @@ class Engine:
     def upload_relinearization_key(self, limbs, moduli_id: int) -> Data:
         return self.upload(limbs, moduli_id, NTT_FORM | INCLUDE_SPECIAL, RELINEARIZATION_KEY)
 
+    def upload_fixed_rotation_key(self, limbs, moduli_id: int, delta: int) -> Data:
+        """A FixedRotationKey: its key switching key limbs and its normalised delta."""
+        key = self.upload(limbs, moduli_id, NTT_FORM | INCLUDE_SPECIAL, FIXED_ROTATION_KEY)
+        key.set_delta(delta)
+        return key
+
+    def upload_conjugation_key(self, limbs, moduli_id: int) -> Data:
+        return self.upload(limbs, moduli_id, NTT_FORM | INCLUDE_SPECIAL, CONJUGATION_KEY)
+
+    def upload_key_switching_key(self, limbs, moduli_id: int) -> Data:
+        return self.upload(limbs, moduli_id, NTT_FORM | INCLUDE_SPECIAL, KEY_SWITCHING_KEY)
+
     def _call(self, fn, *args) -> Data:
         h = ctypes.c_void_p()
         check(getattr(_lib.load(), fn)(self._h, *[a.handle for a in args], ctypes.byref(h)))
@@ -203,6 +218,36 @@ class Engine:
 
     def intt(self, text: Data) -> Data:
         return self._call("fhe_to_intt", text)
+
+    def level_down(self, text: Data, level: int) -> Data:
+        h = ctypes.c_void_p()
+        check(_lib.load().fhe_level_down(self._h, text.handle, level, ctypes.byref(h)))
+        return Data(self, h)
+
+    def rotate(self, ct: Data, key, delta: int | None = None,
+               normalize_by_slot_count: bool = False) -> Data:
+        """Rotate a ciphertext by one fixed rotation key, or by a list of fixed
+        rotation keys (a RotationKey) and a delta; plaintexts rotate without a key."""
+        if isinstance(key, (list, tuple)):
+            arr = (ctypes.c_void_p * len(key))(*[k.handle for k in key])
+            h = ctypes.c_void_p()
+            check(_lib.load().fhe_rotate_with_keys(self._h, ct.handle, arr, len(key), delta,
+                                                   int(normalize_by_slot_count), ctypes.byref(h)))
+            return Data(self, h)
+        return self._call("fhe_rotate", ct, key)
+
+    def rotate_plaintext(self, pt: Data, delta: int) -> Data:
+        h = ctypes.c_void_p()
+        check(_lib.load().fhe_rotate_plaintext(self._h, pt.handle, delta, ctypes.byref(h)))
+        return Data(self, h)
+
+    def conjugate(self, text: Data, conjugation_key: Data | None = None) -> Data:
+        if conjugation_key is None:
+            return self._call("fhe_conjugate_plaintext", text)
+        return self._call("fhe_conjugate", text, conjugation_key)
+
+    def switch_key(self, ct: Data, key_switching_key: Data) -> Data:
+        return self._call("fhe_switch_key", ct, key_switching_key)
 
     def ntt_limbs(self, device_ptr: int, moduli_id: int, chains: int, polys: int,
                   poly_stride: int, inverse: bool = False) -> None:

@@ -197,6 +197,39 @@ int fhe_multiply_relinearize_rescale(fhe_engine *engine, const fhe_data *a, cons
 int fhe_to_ntt(fhe_engine *engine, const fhe_data *text, fhe_data **out);
 int fhe_to_intt(fhe_engine *engine, const fhe_data *text, fhe_data **out);
 
+/* CKKSEngine::level_down (engine.h:387-388, engine_level_down.cpp:44-70): the text
+ * moved to `level` (level_down_multiplier, then a rescale unless the text was
+ * rescaled); form is kept. */
+int fhe_level_down(fhe_engine *engine, const fhe_data *text, int level, fhe_data **out);
+
+/* CKKSEngine::rotate(UnitCiphertext*, FixedRotationKey*) (engine.h:341-342,
+ * engine_rotate.cpp:52-74).  The key is an object of kind FHE_FIXED_ROTATION_KEY whose
+ * delta (fhe_data_set_delta) is the key's normalised rotation step; the result is in
+ * coefficient form. */
+int fhe_rotate(fhe_engine *engine, const fhe_data *ct, const fhe_data *fixed_rotation_key,
+               fhe_data **out);
+/* CKKSEngine::rotate(UnitCiphertext*, RotationKey*, int delta, bool) (engine.h:343-345,
+ * engine_rotate.cpp:106-139): a RotationKey is the list of its fixed rotation keys;
+ * the keys whose delta shares a bit with the normalised delta are applied in list
+ * order.  A zero normalised delta returns the coefficient form of the input. */
+int fhe_rotate_with_keys(fhe_engine *engine, const fhe_data *ct,
+                         const fhe_data *const *fixed_rotation_keys, int key_count, int delta,
+                         int normalize_by_slot_count, fhe_data **out);
+/* CKKSEngine::rotate(UnitPlaintext*, int) (engine.h:340, engine_rotate.cpp:10-24):
+ * keyless rotation of a plaintext in either form. */
+int fhe_rotate_plaintext(fhe_engine *engine, const fhe_data *pt, int delta, fhe_data **out);
+/* CKKSEngine::conjugate(UnitCiphertext*, ConjugationKey*) (engine.h:334-335,
+ * engine_conjugate.cpp:53-73); the key is of kind FHE_CONJUGATION_KEY. */
+int fhe_conjugate(fhe_engine *engine, const fhe_data *ct, const fhe_data *conjugation_key,
+                  fhe_data **out);
+/* CKKSEngine::conjugate(UnitPlaintext*) (engine.h:333, engine_conjugate.cpp:10-24). */
+int fhe_conjugate_plaintext(fhe_engine *engine, const fhe_data *pt, fhe_data **out);
+/* CKKSCore::switch_key (core.h, core.cpp:1058-1083): c0 + KS(c1) with a key
+ * switching key (FHE_KEY_SWITCHING_KEY); NTT-form input is brought to coefficient
+ * form first. */
+int fhe_switch_key(fhe_engine *engine, const fhe_data *ct, const fhe_data *key_switching_key,
+                   fhe_data **out);
+
 /* Relinearize without allocating (no counterpart in the reference, which has no
  * device memory).  For callers that cannot call cudaMalloc while they run -- code
  * inside a CUDA graph capture, real-time loops with a fixed memory budget, hosts

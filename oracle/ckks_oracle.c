@@ -9,6 +9,7 @@
  */
 #include "ckks_oracle.h"
 
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -641,7 +642,7 @@ void oracle_relinearize(const oracle_ctx *c, int mid, const int64_t *ct, int key
 void oracle_rescale(const oracle_ctx *c, int mid, int polys, const int64_t *x, int64_t *y) {
   const int n = c->n, L = oracle_chain_count(c, mid);
   const int next = mid + 1, NL = L - 1;
-  const int64_t q_half = (int64_t)(c->q[mid] >> 1);
+  const uint64_t q_half = c->q[mid] >> 1;
   for (int p = 0; p < polys; p++) {
     const int64_t *xp = x + (size_t)p * L * n;
     int64_t *yp = y + (size_t)p * NL * n;
@@ -654,7 +655,9 @@ void oracle_rescale(const oracle_ctx *c, int mid, int polys, const int64_t *x, i
       const int64_t *xs = LIMB(xp, 1 + j);
       int64_t *ys = LIMB(yp, j);
       for (int t = 0; t < n; t++) {
-        const int64_t rounder = x0[t] > q_half ? 1 : 0; /* get_rounder: unit.cpp:66 */
+        /* get_rounder (unit.cpp:67-70): the int64 word meets a uint64 q/2, so the
+         * comparison is unsigned and a negative word rounds up. */
+        const int64_t rounder = (uint64_t)x0[t] > q_half ? 1 : 0;
         int64_t v = xs[t] - x0[t];                       /* mont_subtract: unit.cpp:58 */
         v = v >= 0 ? v : v + q2;
         v = guard(v, qs);
@@ -874,4 +877,126 @@ void oracle_ntt_permutation(int32_t *permutation, int n, int delta) {
   }
   for (int i = 0; i < n; i++) permutation[i] = reverse_bits(tmp[reverse_bits(i, log_n)], log_n);
   free(tmp);
+}
+
+/* ----------------------------------------------------------- level down -- */
+
+/* CKKSParameters deviations (ckks/parameters.cpp:60-104), one moduli id per
+ * level; out[level] for level 0 .. chain_count-2, as the doubles the precomputed
+ * tables keep (precomputed.h:54). */
+void oracle_deviations(const oracle_ctx *c, double scale, int one_more_level, double *out) {
+  const int full = c->chain_count - 2;
+  long double dev[256];
+  int count = 0, chain_index = 0;
+  for (int level = full; level >= 0; level--) {
+    if (level == full || (one_more_level && level == full - 1)) {
+      dev[count++] = 1.0L;
+    } else {
+      const long double qprod = (long double)c->q[chain_index - 1];
+      const long double alpha = powl((long double)scale / qprod, 2);
+      dev[count] = powl(dev[count - 1], 2) * alpha;
+      count++;
+    }
+    chain_index += 1;
+  }
+  for (int level = 0; level <= full; level++) out[level] = (double)dev[full - level];
+}
+
+/* (round(v) * 2^62) mod q: BigInt::from_double(round(v)) * r_ % q. */
+static int64_t round_times_r(double v, uint64_t q) {
+  const double r = round(v);
+  const unsigned __int128 x = (unsigned __int128)(uint64_t)r << 62;
+  return (int64_t)(x % q);
+}
+
+/* make_level_down_multiplier (precomputed.cpp:438-462) when !rescaled, else
+ * make_level_down_multiplier_after_rescale (:418-436); entries from the source
+ * (resp. destination) moduli id to the last scaling prime. Returns the count. */
+int oracle_level_down_multiplier(const oracle_ctx *c, double scale, int one_more_level,
+                                 int source_level, int destination_level, int rescaled,
+                                 int64_t *out) {
+  double dev[256];
+  oracle_deviations(c, scale, one_more_level, dev);
+  const int full = c->chain_count - 2;
+  int first;
+  double delta;
+  if (rescaled) {
+    const double diff = dev[destination_level] / sqrt(dev[source_level - 1]);
+    delta = scale * diff;
+    first = full - destination_level;
+  } else {
+    const int src_mid = full - source_level;
+    const double diff = dev[destination_level] / dev[source_level];
+    delta = (one_more_level && src_mid == 0) ? scale * diff : (double)c->q[src_mid] * diff;
+    first = src_mid;
+  }
+  int count = 0;
+  for (int i = first; i < c->chain_count; i++) out[count++] = round_times_r(delta, c->q[i]);
+  return count;
+}
+
+/* CKKSCore::level_down (core.cpp:786-838) for coefficient-form, not rescaled
+ * text at src_mid (level src_mid's not-rescaled level), and level_down_after_rescale
+ * (core.cpp:743-778) for rescaled text (either form).  x: [polys][chains(src)][N];
+ * y: [polys][chains(dst)][N]. */
+void oracle_level_down(const oracle_ctx *c, int src_mid, int polys, int rescaled,
+                       int dst_mid, const int64_t *multiplier, const int64_t *x, int64_t *y) {
+  const int n = c->n;
+  const int L = oracle_chain_count(c, src_mid);
+  const int DL = oracle_chain_count(c, dst_mid);
+  if (rescaled) {
+    const int off = dst_mid - src_mid;
+    for (int p = 0; p < polys; p++)
+      for (int j = 0; j < DL; j++) {
+        const int pq = dst_mid + j;
+        const uint64_t q = c->q[pq], k = c->k[pq];
+        const int64_t *xs = x + ((size_t)p * L + j + off) * n;
+        int64_t *ys = y + ((size_t)p * DL + j) * n;
+        for (int t = 0; t < n; t++) ys[t] = guard(MM(xs[t], multiplier[j], q, k), (int64_t)q);
+      }
+    return;
+  }
+  int64_t *entered = malloc(sizeof(int64_t) * (size_t)polys * L * n);
+  int64_t *resc = malloc(sizeof(int64_t) * (size_t)polys * (L - 1) * n);
+  for (int p = 0; p < polys; p++)
+    for (int j = 0; j < L; j++) {
+      const int pq = src_mid + j;
+      const uint64_t q = c->q[pq], k = c->k[pq];
+      const int64_t *xs = x + ((size_t)p * L + j) * n;
+      int64_t *es = entered + ((size_t)p * L + j) * n;
+      for (int t = 0; t < n; t++) es[t] = guard(MM(xs[t], multiplier[j], q, k), (int64_t)q);
+    }
+  oracle_rescale(c, src_mid, polys, entered, resc);
+  const int off = dst_mid - (src_mid + 1);
+  for (int p = 0; p < polys; p++)
+    memcpy(y + (size_t)p * DL * n, resc + ((size_t)p * (L - 1) + off) * n,
+           sizeof(int64_t) * (size_t)DL * n);
+  free(entered);
+  free(resc);
+}
+
+/* rotate_intt_form_ (core.cpp:871-880): signed permutation + make_unsigned. */
+void oracle_rotate_plain(const oracle_ctx *c, int mid, int polys, int delta, const int64_t *x,
+                         int64_t *y) {
+  const int n = c->n;
+  int32_t *perm = malloc(sizeof(int32_t) * n), *sign = malloc(sizeof(int32_t) * n);
+  oracle_permutation_and_sign(perm, sign, n, delta);
+  rotate_coefficients(c, mid, polys, perm, sign, x, y);
+  free(perm);
+  free(sign);
+}
+
+/* rotate_ntt_form_ (core.cpp:886-910): y[c] = x[ntt_permutation[c]] per limb. */
+void oracle_rotate_plain_ntt(const oracle_ctx *c, int mid, int polys, int delta,
+                             const int64_t *x, int64_t *y) {
+  const int n = c->n, L = oracle_chain_count(c, mid);
+  int32_t *perm = malloc(sizeof(int32_t) * n);
+  oracle_ntt_permutation(perm, n, delta);
+  for (int p = 0; p < polys; p++)
+    for (int j = 0; j < L; j++) {
+      const int64_t *xs = x + ((size_t)p * L + j) * n;
+      int64_t *ys = y + ((size_t)p * L + j) * n;
+      for (int t = 0; t < n; t++) ys[t] = xs[perm[t]];
+    }
+  free(perm);
 }

@@ -103,6 +103,20 @@ void oracle_permutation_and_sign(int32_t *permutation, int32_t *sign,
                                  int coeff_count, int delta);
 void oracle_ntt_permutation(int32_t *permutation, int coeff_count, int delta);
 
+/* Level down (core.cpp:743-838) and its multipliers (precomputed.cpp:418-462). */
+void oracle_deviations(const oracle_ctx *ctx, double scale, int one_more_level, double *out);
+int oracle_level_down_multiplier(const oracle_ctx *ctx, double scale, int one_more_level,
+                                 int source_level, int destination_level, int rescaled,
+                                 int64_t *out);
+void oracle_level_down(const oracle_ctx *ctx, int src_moduli_id, int polys, int rescaled,
+                       int dst_moduli_id, const int64_t *multiplier, const int64_t *x,
+                       int64_t *y);
+/* Keyless rotation of a text (core.cpp:871-910), coefficient and NTT form. */
+void oracle_rotate_plain(const oracle_ctx *ctx, int moduli_id, int polys, int delta,
+                         const int64_t *x, int64_t *y);
+void oracle_rotate_plain_ntt(const oracle_ctx *ctx, int moduli_id, int polys, int delta,
+                             const int64_t *x, int64_t *y);
+
 #ifdef __cplusplus
 }
 #endif

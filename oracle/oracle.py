@@ -82,6 +82,19 @@ def lib():
         L.oracle_permutation_and_sign.argtypes = [_i32p, _i32p, ctypes.c_int, ctypes.c_int]
         L.oracle_ntt_permutation.restype = None
         L.oracle_ntt_permutation.argtypes = [_i32p, ctypes.c_int, ctypes.c_int]
+        L.oracle_deviations.restype = None
+        L.oracle_deviations.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_double)]
+        L.oracle_level_down_multiplier.restype = ctypes.c_int
+        L.oracle_level_down_multiplier.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
+                                                   ctypes.c_int, ctypes.c_int, ctypes.c_int, _i64p]
+        L.oracle_level_down.restype = None
+        L.oracle_level_down.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, _i64p, _i64p, _i64p]
+        for name in ("oracle_rotate_plain", "oracle_rotate_plain_ntt"):
+            f = getattr(L, name)
+            f.restype = None
+            f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _i64p, _i64p]
     return _lib
 
 
@@ -234,6 +247,34 @@ class Context:
 
     def rotate(self, moduli_id, ct, key_moduli_id, key, delta):
         return self._ks_call(lib().oracle_rotate, moduli_id, ct, key_moduli_id, key, delta)
+
+    def deviations(self, scale: float, one_more_level: bool):
+        out = np.empty(self.chain_count - 1, dtype=np.float64)
+        lib().oracle_deviations(self._ctx, scale, int(one_more_level),
+                                out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return out
+
+    def level_down(self, x, source_level: int, level: int, rescaled: bool, scale: float,
+                   one_more_level: bool):
+        """Engine level_down of a coefficient-form (or rescaled) text."""
+        x = np.ascontiguousarray(x, dtype=np.int64)
+        full = self.chain_count - 2
+        src_mid = full - source_level + (1 if rescaled else 0)
+        dst_mid = full - level
+        mult = np.zeros(self.chain_count, dtype=np.int64)
+        lib().oracle_level_down_multiplier(self._ctx, scale, int(one_more_level), source_level,
+                                           level, int(rescaled), _p(mult))
+        y = np.empty((x.shape[0], self.chains(dst_mid), self.n), dtype=np.int64)
+        lib().oracle_level_down(self._ctx, src_mid, x.shape[0], int(rescaled), dst_mid, _p(mult),
+                                _p(x), _p(y))
+        return y
+
+    def rotate_plain(self, moduli_id, x, delta, ntt_form=False):
+        x = np.ascontiguousarray(x, dtype=np.int64)
+        y = np.empty_like(x)
+        fn = lib().oracle_rotate_plain_ntt if ntt_form else lib().oracle_rotate_plain
+        fn(self._ctx, moduli_id, x.shape[0], delta, _p(x), _p(y))
+        return y
 
     def mult_relin_rescale(self, moduli_id, a, b, key_moduli_id, key):
         a = np.ascontiguousarray(a, dtype=np.int64)

@@ -70,6 +70,13 @@ def lib():
             "ref_engine_rescale": (vp, [vp, vp]),
             "ref_engine_rotate": (vp, [vp, vp, vp]),
             "ref_engine_conjugate": (vp, [vp, vp, vp]),
+            "ref_engine_level_down": (vp, [vp, vp, ctypes.c_int]),
+            "ref_last_error": (ctypes.c_char_p, []),
+            "ref_deviations": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
+            "ref_engine_rotate_plain": (vp, [vp, vp, ctypes.c_int]),
+            "ref_engine_conjugate_plain": (vp, [vp, vp]),
+            "ref_engine_rotate_keys": (vp, [vp, vp, ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int]),
             "ref_engine_encode": (vp, [vp, ctypes.POINTER(cd), ctypes.POINTER(cd), ci, ci]),
             "ref_engine_decode": (ci, [vp, vp, ctypes.POINTER(cd), ctypes.POINTER(cd)]),
             "ref_engine_encrypt": (vp, [vp, vp, vp]),
@@ -94,7 +101,7 @@ class Handle:
 
     def __init__(self, engine: "Engine", ptr):
         if not ptr:
-            raise RuntimeError("reference call failed")
+            raise RuntimeError("reference call failed: " + lib().ref_last_error().decode())
         self.engine = engine
         self.ptr = ptr
 
@@ -244,8 +251,26 @@ class Engine:
     def rotate(self, a, fixed_key):
         return self._h(lib().ref_engine_rotate(self.ptr, a.ptr, fixed_key.ptr))
 
-    def conjugate(self, a, ck):
+    def conjugate(self, a, ck=None):
+        if ck is None:
+            return self._h(lib().ref_engine_conjugate_plain(self.ptr, a.ptr))
         return self._h(lib().ref_engine_conjugate(self.ptr, a.ptr, ck.ptr))
+
+    def deviations(self):
+        out = np.zeros(256, dtype=np.float64)
+        n = lib().ref_deviations(self.ptr, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 256)
+        return out[:n]
+
+    def level_down(self, a, level):
+        return self._h(lib().ref_engine_level_down(self.ptr, a.ptr, level))
+
+    def rotate_plain(self, a, delta):
+        return self._h(lib().ref_engine_rotate_plain(self.ptr, a.ptr, delta))
+
+    def rotate_keys(self, a, fixed_keys, delta, by_slot_count=False):
+        arr = (ctypes.c_void_p * len(fixed_keys))(*[k.ptr for k in fixed_keys])
+        return self._h(lib().ref_engine_rotate_keys(self.ptr, a.ptr, arr, len(fixed_keys), delta,
+                                                    int(by_slot_count)))
 
     def encode(self, values, level=-1):
         values = np.asarray(values, dtype=np.complex128)

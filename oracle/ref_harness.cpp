@@ -91,6 +91,19 @@ void dump(Data *data, int64_t *out, int n) {
   }
 }
 
+thread_local std::string g_ref_error;
+
+// Called inside a catch-all handler: records the message of the exception in flight.
+void remember_error() {
+  try {
+    throw;
+  } catch (const std::exception &ex) {
+    g_ref_error = ex.what();
+  } catch (...) {
+    g_ref_error = "unknown exception";
+  }
+}
+
 Handle *wrap(int kind, Data *data, void *owner) {
   auto h = new Handle();
   h->kind = kind;
@@ -102,6 +115,17 @@ Handle *wrap(int kind, Data *data, void *owner) {
 } // namespace
 
 extern "C" {
+
+const char *ref_last_error() { return g_ref_error.c_str(); }
+
+// The double deviations of the precomputed tables, indexed by level.
+int ref_deviations(void *e, double *out, int capacity) {
+  auto core = static_cast<RefEngine *>(e)->core();
+  const auto &d = core->precomputed_.deviation_;
+  const int count = static_cast<int>(d.size());
+  for (int i = 0; i < count && i < capacity; i++) out[i] = d[i];
+  return count;
+}
 
 int ref_cached_primes(int kind, int coeff_count, uint64_t *out, int capacity) {
   std::tuple<uint64_t *, int> cached;
@@ -140,6 +164,7 @@ void *ref_engine_new(int log_n, int log_slot, int special_prime_count,
     e->engine = std::make_unique<CKKSEngine>(config);
     return e;
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -320,6 +345,7 @@ void *ref_create_secret_key(void *e, int level) {
   auto sk = level < 0 ? eng->create_secret_key() : eng->create_secret_key(level);
   return wrap(1, sk, sk);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -331,6 +357,7 @@ void *ref_create_secret_key_from(void *e, const int64_t *secret, int level) {
   auto sk = level < 0 ? eng->create_secret_key(s) : eng->create_secret_key(s, level);
   return wrap(1, sk, sk);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -342,6 +369,7 @@ void *ref_create_public_key(void *e, void *sk, int level) {
   auto pk = level < 0 ? eng->create_public_key(s) : eng->create_public_key(s, level);
   return wrap(2, pk, pk);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -354,6 +382,7 @@ void *ref_create_relinearization_key(void *e, void *sk, int level) {
                       : eng->create_relinearization_key(s, level);
   return wrap(3, rk->key_switching_key_, rk);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -366,6 +395,7 @@ void *ref_create_fixed_rotation_key(void *e, void *sk, int delta, int level) {
                       : eng->create_fixed_rotation_key(s, delta, level);
   return wrap(6, fk->key_switching_key_, fk);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -378,6 +408,7 @@ void *ref_create_conjugation_key(void *e, void *sk, int level) {
                       : eng->create_conjugation_key(s, level);
   return wrap(7, ck->key_switching_key_, ck);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -390,6 +421,7 @@ void *ref_core_to_ntt(void *e, void *h) {
   auto r = core->to_ntt_form(static_cast<UnitCiphertext *>(static_cast<Handle *>(h)->data));
   return wrap(4, r, r);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -400,6 +432,7 @@ void *ref_core_to_intt(void *e, void *h) {
   auto r = core->to_intt_form(static_cast<UnitCiphertext *>(static_cast<Handle *>(h)->data));
   return wrap(4, r, r);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -411,6 +444,7 @@ void *ref_core_tensor(void *e, void *a, void *b) {
                           static_cast<UnitCiphertext *>(static_cast<Handle *>(b)->data));
   return wrap(4, r, r);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -423,6 +457,7 @@ void *ref_core_relinearize(void *e, void *ct, void *rk) {
       static_cast<RelinearizationKey *>(static_cast<Handle *>(rk)->owner));
   return wrap(4, r, r);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -433,6 +468,7 @@ void *ref_core_rescale(void *e, void *ct) {
   auto r = core->rescale(static_cast<UnitCiphertext *>(static_cast<Handle *>(ct)->data));
   return wrap(4, r, r);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -445,6 +481,7 @@ void *ref_core_switch_key(void *e, void *ct, void *ksk) {
       static_cast<KeySwitchingKey *>(static_cast<Handle *>(ksk)->data));
   return wrap(4, r, r);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -465,6 +502,7 @@ void *ref_engine_multiply(void *e, void *a, void *b, void *rk) {
   }
   return wrap(4, r, r);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -477,6 +515,7 @@ void *ref_engine_relinearize(void *e, void *a, void *rk) {
       static_cast<RelinearizationKey *>(static_cast<Handle *>(rk)->owner));
   return wrap(4, r, r);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -487,6 +526,7 @@ void *ref_engine_rescale(void *e, void *a) {
   auto r = eng->rescale(static_cast<UnitCiphertext *>(static_cast<Handle *>(a)->data));
   return wrap(4, r, r);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -498,6 +538,7 @@ void *ref_core_rotate(void *e, void *a, void *fk) {
                           static_cast<FixedRotationKey *>(static_cast<Handle *>(fk)->owner));
     return wrap(4, r, r);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -509,6 +550,7 @@ void *ref_core_conjugate(void *e, void *a, void *ck) {
                              static_cast<ConjugationKey *>(static_cast<Handle *>(ck)->owner));
     return wrap(4, r, r);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -520,6 +562,7 @@ void *ref_engine_rotate(void *e, void *a, void *fk) {
                        static_cast<FixedRotationKey *>(static_cast<Handle *>(fk)->owner));
   return wrap(4, r, r);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -531,8 +574,73 @@ void *ref_engine_conjugate(void *e, void *a, void *ck) {
                           static_cast<ConjugationKey *>(static_cast<Handle *>(ck)->owner));
   return wrap(4, r, r);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
+}
+
+void *ref_engine_level_down(void *e, void *a, int level) {
+  try {
+    auto eng = static_cast<RefEngine *>(e)->engine.get();
+    auto h = static_cast<Handle *>(a);
+    if (h->kind == 5) {
+      auto r = eng->level_down(static_cast<UnitPlaintext *>(h->data), level);
+      return wrap(5, r, r);
+    }
+    auto r = eng->level_down(static_cast<UnitCiphertext *>(h->data), level);
+    return wrap(4, r, r);
+  } catch (...) {
+    remember_error();
+    return nullptr;
+  }
+}
+
+void *ref_engine_rotate_plain(void *e, void *a, int delta) {
+  try {
+    auto eng = static_cast<RefEngine *>(e)->engine.get();
+    auto r = eng->rotate(static_cast<UnitPlaintext *>(static_cast<Handle *>(a)->data), delta);
+    return wrap(5, r, r);
+  } catch (...) {
+    remember_error();
+    return nullptr;
+  }
+}
+
+void *ref_engine_conjugate_plain(void *e, void *a) {
+  try {
+    auto eng = static_cast<RefEngine *>(e)->engine.get();
+    auto r = eng->conjugate(static_cast<UnitPlaintext *>(static_cast<Handle *>(a)->data));
+    return wrap(5, r, r);
+  } catch (...) {
+    remember_error();
+    return nullptr;
+  }
+}
+
+// CKKSEngine::rotate(UnitCiphertext*, RotationKey*, delta, normalize_by_slot_count)
+// with a RotationKey that borrows the given fixed rotation keys.
+void *ref_engine_rotate_keys(void *e, void *a, void **fks, int count, int delta,
+                             int by_slot_count) {
+  std::vector<FixedRotationKey *> keys;
+  for (int i = 0; i < count; i++)
+    keys.push_back(static_cast<FixedRotationKey *>(static_cast<Handle *>(fks[i])->owner));
+  RotationKey *rk = nullptr;
+  void *out = nullptr;
+  try {
+    auto eng = static_cast<RefEngine *>(e)->engine.get();
+    rk = new RotationKey(keys);
+    auto r = eng->rotate(static_cast<UnitCiphertext *>(static_cast<Handle *>(a)->data), rk, delta,
+                         by_slot_count != 0);
+    out = wrap(4, r, r);
+  } catch (...) {
+    remember_error();
+    out = nullptr;
+  }
+  if (rk) {
+    rk->fixed_rotation_keys_.clear();
+    delete rk;
+  }
+  return out;
 }
 
 void *ref_engine_encode(void *e, const double *re, const double *im, int count,
@@ -544,6 +652,7 @@ void *ref_engine_encode(void *e, const double *re, const double *im, int count,
   auto pt = level < 0 ? eng->encode_unit(v) : eng->encode_unit(v, level);
   return wrap(5, pt, pt);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -572,6 +681,7 @@ void *ref_engine_encrypt(void *e, void *pt, void *key) {
   }
   return wrap(4, ct, ct);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }
@@ -584,6 +694,7 @@ void *ref_engine_decrypt(void *e, void *ct, void *sk) {
       static_cast<SecretKey *>(static_cast<Handle *>(sk)->data));
   return wrap(5, pt, pt);
   } catch (...) {
+    remember_error();
     return nullptr;
   }
 }

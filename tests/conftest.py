@@ -50,3 +50,21 @@ def load_golden(name):
 @pytest.fixture(scope="session")
 def ref_ops():
     return load_golden("ref_ops.json")
+
+
+@pytest.fixture(scope="module")
+def engines():
+    """Engines on cuda:0, one per (log_n, special prime count, preset), per module."""
+    from fhe_b200 import Engine
+
+    cache = {}
+
+    def get(log_n, K, preset):
+        key = (log_n, K, preset)
+        if key not in cache:
+            cache[key] = Engine(log_coeff_count=log_n, special_prime_count=K, scheme_preset=preset)
+        return cache[key]
+
+    yield get
+    for e in cache.values():
+        e.close()

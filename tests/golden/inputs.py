@@ -51,3 +51,27 @@ def case_inputs(seed: int, moduli, n: int, moduli_id: int, special: int):
     ct3 = uniform_limbs(rng, qs, 3, n)
     key = uniform_limbs(rng, ext, 2 * dnum, n)
     return a, b, ct3, key
+
+
+ROTATION_KEY_DELTAS = (1, 2, 4)
+
+
+def key_switch_inputs(seed: int, moduli, n: int, moduli_id: int, special: int):
+    """Inputs of the rotation / conjugation / key-switch / level cases of one
+    op-parity case, drawn from their own stream so the other inputs keep their
+    values.  Texts at moduli id 0 are switched at moduli id 1 by the engine (the
+    one-more-level rule), so their rotation and conjugation keys live there."""
+    rng = np.random.default_rng(seed + 100000)
+    chain = len(moduli) - special
+
+    def key_at(mid):
+        dnum = (chain - mid + special - 1) // special
+        return uniform_limbs(rng, moduli[mid:], 2 * dnum, n)
+
+    key_mid = moduli_id if moduli_id > 0 else 1
+    rotation_keys = [key_at(key_mid) for _ in ROTATION_KEY_DELTAS]
+    conjugation_key = key_at(key_mid)
+    switching_key = key_at(moduli_id)
+    b_next = uniform_limbs(rng, moduli[moduli_id + 1:chain], 2, n)
+    return dict(key_moduli_id=key_mid, rotation_keys=rotation_keys,
+                conjugation_key=conjugation_key, switching_key=switching_key, b_next=b_next)

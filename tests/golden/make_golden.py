@@ -25,7 +25,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
-from inputs import TIERS, case_inputs, digest  # noqa: E402
+from inputs import ROTATION_KEY_DELTAS, key_switch_inputs, TIERS, case_inputs, digest  # noqa: E402
 
 REF = os.environ.get("FHE_REFERENCE", "/root/reference")
 
@@ -87,6 +87,41 @@ def parse_precomputed_kats():
     return out
 
 
+def key_switch_ops(e, seed, q, n, mid, K, a, rk):
+    """Rotation, conjugation, key switch, level down and mixed-level multiply
+    through the reference's engine (and core, for switch_key)."""
+    x = key_switch_inputs(seed, q, n, mid, K)
+    kmid = x["key_moduli_id"]
+    res = {}
+    fks = [e.fixed_rotation_key(k, kmid, d) for k, d in zip(x["rotation_keys"], ROTATION_KEY_DELTAS)]
+    ck = e.conjugation_key(x["conjugation_key"], kmid)
+    scale = 2.0 ** 40
+    level = e.chains(mid) - 2
+    res["rotate_1"] = e.rotate(e.text(a, mid, flag=0, scale=scale), fks[0]).limbs()
+    res["rotate_4_ntt"] = e.rotate(e.text(a, mid, flag=2, scale=scale), fks[2]).limbs()
+    res["rotate_keys_7"] = e.rotate_keys(e.text(a, mid, flag=0, scale=scale), fks, 7).limbs()
+    res["conjugate"] = e.conjugate(e.text(a, mid, flag=0, scale=scale), ck).limbs()
+    res["switch_key"] = e.core_switch_key(e.text(a, mid, flag=0),
+                                          e.switching_key(x["switching_key"], mid)).limbs()
+    res["rotate_plain_3"] = e.rotate_plain(e.text(a[:1], mid, flag=0, kind=5), 3).limbs()
+    res["rotate_plain_3_ntt"] = e.rotate_plain(e.text(a[:1], mid, flag=2, kind=5), 3).limbs()
+    res["conjugate_plain"] = e.conjugate(e.text(a[:1], mid, flag=0, kind=5)).limbs()
+    res["conjugate_plain_ntt"] = e.conjugate(e.text(a[:1], mid, flag=2, kind=5)).limbs()
+    if level >= 1:
+        res["level_down"] = e.level_down(e.text(a, mid, flag=0, scale=scale), level - 1).limbs()
+        res["level_down_ntt"] = e.level_down(e.text(a, mid, flag=2, scale=scale), 0).limbs()
+    if level >= 1 and mid >= 1:  # a rescaled text never sits at moduli id 0
+        res["level_down_rescaled"] = e.level_down(e.text(a, mid, flag=4, scale=scale),
+                                                  level).limbs()
+    try:
+        m = e.multiply(e.text(a, mid, flag=0, scale=scale), e.text(x["b_next"], mid + 1, flag=0,
+                                                                   scale=scale), rk)
+        res["multiply_mixed_levels"] = m.limbs()
+    except RuntimeError:
+        pass
+    return res
+
+
 def reference_ops():
     from oracle import ref
 
@@ -116,11 +151,13 @@ def reference_ops():
                 res["mult_relin_rescale"] = e.rescale(m).limbs()
             except RuntimeError:
                 pass
+            arrays = {k: v.tolist() for k, v in res.items()} if n <= 16 else None
+            res.update(key_switch_ops(e, seed, q, n, mid, K, a, rk))
             entry = dict(tier=tier, log_n=log_n, special_prime_count=K, preset=preset,
                          moduli_id=mid, seed=seed, moduli=[int(v) for v in q],
                          digests={k: digest(v) for k, v in res.items()})
-            if n <= 16:
-                entry["arrays"] = {k: v.tolist() for k, v in res.items()}
+            if arrays is not None:
+                entry["arrays"] = arrays
             cases.append(entry)
     return cases
 
@@ -130,8 +167,9 @@ def main():
         json.dump(parse_ntt_kats(), f, indent=1)
     with open(os.path.join(HERE, "precomputed_kat.json"), "w") as f:
         json.dump(parse_precomputed_kats(), f, indent=1)
+    cases = reference_ops()  # computed before the file is opened: a failure keeps the old one
     with open(os.path.join(HERE, "ref_ops.json"), "w") as f:
-        json.dump(reference_ops(), f, indent=1)
+        json.dump(cases, f, indent=1)
 
 
 if __name__ == "__main__":

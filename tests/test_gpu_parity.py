@@ -12,23 +12,6 @@ pytestmark = pytest.mark.gpu
 NTT, RESCALED, SPECIAL = 2, 4, 16
 
 
-@pytest.fixture(scope="module")
-def engines():
-    from fhe_b200 import Engine
-
-    cache = {}
-
-    def get(log_n, K, preset):
-        key = (log_n, K, preset)
-        if key not in cache:
-            cache[key] = Engine(log_coeff_count=log_n, special_prime_count=K, scheme_preset=preset)
-        return cache[key]
-
-    yield get
-    for e in cache.values():
-        e.close()
-
-
 CASES = load_golden("ref_ops.json")
 
 

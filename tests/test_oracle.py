@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 from conftest import load_golden
-from inputs import TIERS, case_inputs, digest
+from inputs import ROTATION_KEY_DELTAS, key_switch_inputs, TIERS, case_inputs, digest
 from oracle import oracle, ref
 
 
@@ -82,6 +82,74 @@ def test_oracle_matches_recorded_reference_outputs(case):
 
 def _chain(case):
     return np.array(case["moduli"], dtype=np.uint64)
+
+
+def _engine_scale(case):
+    return 2.0 ** (54 if case["preset"] in (2, 4) else 40)
+
+
+def _switch_input(ctx, case, mid, x, ntt):
+    """The engine's preparation of a rotation/conjugation input (engine_rotate.cpp:52-74):
+    a text at moduli id 0 drops one level first (one-more-level rule), then leaves NTT form."""
+    if mid == 0:
+        level = ctx.chains(0) - 2
+        y = ctx.to_intt(0, x) if ntt else x
+        y = ctx.level_down(y, level, level - 1, False, _engine_scale(case), True)
+        if ntt:
+            y = ctx.to_ntt(1, y)
+        return 1, (ctx.to_intt(1, y) if ntt else y)
+    return mid, (ctx.to_intt(mid, x) if ntt else x)
+
+
+@pytest.mark.parametrize("case", _cases(), ids=lambda c: f"{c['tier']}-m{c['moduli_id']}")
+def test_oracle_key_switch_ops_match_recorded_reference(case):
+    """Rotation, conjugation, switch_key, keyless rotations, level down and a
+    mixed-level multiply composed from oracle steps, against the reference's engine."""
+    log_n, K = case["log_n"], case["special_prime_count"]
+    q = _chain(case)
+    ctx = oracle.Context(log_n, q, K)
+    mid, n = case["moduli_id"], ctx.n
+    a, _, _, key = case_inputs(case["seed"], q, n, mid, K)
+    x = key_switch_inputs(case["seed"], q, n, mid, K)
+    kmid, keys = x["key_moduli_id"], x["rotation_keys"]
+    d = case["digests"]
+    scale = _engine_scale(case)
+
+    def rotate(m, y, i):
+        return ctx.rotate(m, y, kmid, keys[i], ROTATION_KEY_DELTAS[i])
+
+    m, y = _switch_input(ctx, case, mid, a, False)
+    assert digest(rotate(m, y, 0)) == d["rotate_1"]
+    m4, y4 = _switch_input(ctx, case, mid, a, True)
+    assert digest(rotate(m4, y4, 2)) == d["rotate_4_ntt"]
+    nd, cur, cm = 7 % (n // 2), a, mid
+    for i, delta in enumerate(ROTATION_KEY_DELTAS):
+        if nd & delta:
+            cm, cur = _switch_input(ctx, case, cm, cur, False)
+            cur = rotate(cm, cur, i)
+    assert digest(cur) == d["rotate_keys_7"]
+    assert digest(ctx.conjugate(m, y, kmid, x["conjugation_key"])) == d["conjugate"]
+    assert digest(ctx.switch_key(mid, a, mid, x["switching_key"])) == d["switch_key"]
+    p = a[:1]
+    assert digest(ctx.rotate_plain(mid, p, 3 % (n // 2))) == d["rotate_plain_3"]
+    assert digest(ctx.rotate_plain(mid, p, 3 % (n // 2), True)) == d["rotate_plain_3_ntt"]
+    assert digest(ctx.rotate_plain(mid, p, -1)) == d["conjugate_plain"]
+    assert digest(ctx.rotate_plain(mid, p, -1, True)) == d["conjugate_plain_ntt"]
+    level = ctx.chains(mid) - 2
+    full = ctx.chain_count - 2
+    if "level_down" in d:
+        assert digest(ctx.level_down(a, level, level - 1, False, scale, True)) == d["level_down"]
+        down = ctx.level_down(ctx.to_intt(mid, a), level, 0, False, scale, True)
+        assert digest(ctx.to_ntt(full, down)) == d["level_down_ntt"]
+    if "level_down_rescaled" in d:
+        got = ctx.level_down(a, level + 1, level, True, scale, True)
+        assert digest(got) == d["level_down_rescaled"]
+    if "multiply_mixed_levels" in d:
+        la = ctx.level_down(a, level, level - 1, False, scale, True)
+        na = ctx.to_ntt(mid + 2, ctx.rescale(mid + 1, la))
+        nb = ctx.to_ntt(mid + 2, ctx.rescale(mid + 1, x["b_next"]))
+        got = ctx.relinearize(mid + 2, ctx.tensor(mid + 2, na, nb), mid, key)
+        assert digest(got) == d["multiply_mixed_levels"]
 
 
 @pytest.mark.skipif(not ref.available(), reason="reference library not built")
