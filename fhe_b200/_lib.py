@@ -25,6 +25,7 @@ STATUS_NAMES = {
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
 _pp = ctypes.POINTER(ctypes.c_void_p)
+_f64p = ctypes.POINTER(ctypes.c_double)
 _i64p = ctypes.POINTER(ctypes.c_int64)
 
 
@@ -87,6 +88,8 @@ SIGNATURES = {
     "fhe_conjugate": (_i, [_vp, _vp, _vp, _pp]),
     "fhe_conjugate_plaintext": (_i, [_vp, _vp, _pp]),
     "fhe_switch_key": (_i, [_vp, _vp, _vp, _pp]),
+    "fhe_encode": (_i, [_vp, _f64p, _f64p, _i, _i, _i, _pp]),
+    "fhe_decode": (_i, [_vp, _vp, _f64p, _f64p]),
     "fhe_ntt_limbs": (_i, [_vp, _i64p, _i, _i, _i, ctypes.c_longlong, _i]),
     "fhe_relinearize_noalloc": (_i, [_vp, _i64p, _i, _i64p, _i, _i, _i64p]),
 }

@@ -417,3 +417,22 @@ int fhe_switch_key(fhe_engine *engine, const fhe_data *ct, const fhe_data *key, 
 }
 
 }  // extern "C"
+
+extern "C" {
+
+int fhe_encode(fhe_engine *engine, const double *re, const double *im, int count, int level,
+               int include_special, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded(
+      [&] { *out = wrap(engine->impl->encode(re, im, count, level, include_special != 0)); });
+}
+
+int fhe_decode(fhe_engine *engine, const fhe_data *pt, double *re, double *im) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(pt);
+  return guarded([&] { engine->impl->decode(live(engine, pt), re, im); });
+}
+
+}  // extern "C"

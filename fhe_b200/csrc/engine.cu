@@ -54,16 +54,6 @@ void Engine::check(cudaError_t e, const char *what) {
   }
 }
 
-template <class T>
-T *Engine::upload_table(const std::vector<T> &v) {
-  const size_t bytes = std::max<size_t>(v.size(), 1) * sizeof(T);
-  void *p = nullptr;
-  check(cudaMalloc(&p, bytes), "cudaMalloc(table)");
-  table_buffers_.push_back(static_cast<int64_t *>(p));
-  if (!v.empty()) check(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload table");
-  return static_cast<T *>(p);
-}
-
 Engine::Engine(const Config &config) : params(config) {
   int device = 0;
   check(cudaGetDevice(&device), "cudaGetDevice");

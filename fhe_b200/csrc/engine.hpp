@@ -112,6 +112,12 @@ class Engine {
   // CKKSCore::switch_key (core.cpp:1058-1083): coefficient-form input.
   std::unique_ptr<Data> switch_key(const Data &ct, const Data &key_switching_key);
   int normalized_delta(int delta, bool normalize_by_slot_count = false) const;
+  // CKKSCore::encode (core_encode.cpp:33-150) of up to slot_count values (im null:
+  // real input) at `level`; CKKSCore::decode / decode_complex_plaintext
+  // (core_decode.cpp) into host arrays of slot_count doubles.
+  std::unique_ptr<Data> encode(const double *re, const double *im, int count, int level,
+                               bool include_special = false);
+  void decode(const Data &pt, double *re, double *im);
 
   void ntt_limbs(int64_t *limbs, int moduli_id, int chains, int polys, long long stride,
                  bool inverse);
@@ -162,8 +168,32 @@ class Engine {
   }
 
   void check(cudaError_t e, const char *what);
+  // Device copy of a host table, freed with the engine.
   template <class T>
-  T *upload_table(const std::vector<T> &v);
+  T *upload_table(const std::vector<T> &v) {
+    const size_t bytes = (v.empty() ? 1 : v.size()) * sizeof(T);
+    void *p = nullptr;
+    check(cudaMalloc(&p, bytes), "cudaMalloc(table)");
+    table_buffers_.push_back(static_cast<int64_t *>(p));
+    if (!v.empty())
+      check(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload table");
+    return static_cast<T *>(p);
+  }
+
+  // Codec tables on the device (built on first encode/decode).
+  struct DeviceCodec {
+    int codec = 0;
+    int log_codec = 0;
+    const int32_t *pre = nullptr;
+    const int32_t *post = nullptr;
+    const double2 *fft = nullptr;    // (cos, sin) of the forward twiddles
+    const double2 *ifft = nullptr;
+    const double2 *twist = nullptr;  // apply_twister factors
+    const double2 *skew = nullptr;   // apply_skewer factors
+  };
+  DeviceCodec codec_;
+  const DeviceCodec &codec();
+  void fft_on_device(double2 *y, const double2 *twiddle, int log_codec);
 
   // Core steps.
   std::unique_ptr<Data> core_rescale(const Data &ct);          // coefficient form

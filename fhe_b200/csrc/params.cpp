@@ -554,3 +554,154 @@ long double Parameters::level_down_scale(int level) const {
 }
 
 }  // namespace fhe_b200
+
+// ------------------------------------------------------------ encode/decode --
+
+namespace fhe_b200 {
+
+namespace {
+
+// circular_shift_permutation, fold_canon_permutation, get_permutation_cycles,
+// conjugate_permutations and invert_permutation of ckks/encode.cpp:25-154.
+std::vector<uint64_t> circular_shift(int size) {
+  const int half = size / 2;
+  std::vector<uint64_t> out(size);
+  out[0] = half - 1;
+  for (int i = 1; i < half; i++) out[i] = i - 1;
+  for (int i = half; i < size - 1; i++) out[i] = i + 1;
+  out[size - 1] = half;
+  return out;
+}
+
+std::vector<uint64_t> fold_canon(int size) {
+  const int double_size = size * 2;
+  const int64_t jump = rotation_jump(1, double_size);
+  std::vector<uint64_t> out(size);
+  int64_t jm = jump;
+  for (int i = 0; i < size; i++) {
+    out[i] = static_cast<uint64_t>((jm - 1) >> 1);
+    jm = (jm + jump * 2) % double_size;
+  }
+  return out;
+}
+
+std::vector<uint64_t> permutation_cycles(const std::vector<uint64_t> &p) {
+  const int size = static_cast<int>(p.size());
+  std::vector<bool> visited(size, false);
+  std::vector<uint64_t> out;
+  out.reserve(size);
+  int start = 0;
+  while (start < size) {
+    uint64_t cur = p[start], next = p[cur];
+    while (true) {
+      out.push_back(cur);
+      visited[cur] = true;
+      cur = next;
+      if (visited[next]) break;
+      next = p[cur];
+    }
+    start++;
+    while (start < size && visited[start]) start++;
+  }
+  return out;
+}
+
+}  // namespace
+
+CodecTables Parameters::codec_tables() const {
+  CodecTables t;
+  const int codec = slot_count * 2;
+  t.codec = codec;
+  const auto c1 = permutation_cycles(fold_canon(codec));
+  const auto c2 = permutation_cycles(circular_shift(codec));
+  std::vector<uint64_t> post(codec), pre(codec);
+  for (int i = 0; i < codec; i++) post[c1[i]] = c2[i];
+  for (int i = 0; i < codec; i++) pre[post[i]] = i;
+  t.pre.assign(pre.begin(), pre.end());
+  t.post.assign(post.begin(), post.end());
+  // precomputed.cpp:67-74 (std::numbers::pi).
+  const double pi = 3.141592653589793;
+  const double unit_angle = -2 * pi / codec;
+  t.fft_cos.resize(codec);
+  t.fft_sin.resize(codec);
+  t.ifft_cos.resize(codec);
+  t.ifft_sin.resize(codec);
+  for (int i = 0; i < codec; i++) {
+    const double angle = i * unit_angle;
+    t.fft_cos[i] = std::cos(angle);
+    t.fft_sin[i] = std::sin(angle);
+    t.ifft_cos[i] = std::cos(angle);
+    t.ifft_sin[i] = std::sin(-angle);
+  }
+  // apply_twister_ / apply_skewer_ (core_calculate.cpp:539-566, encode.cpp:279-301).
+  const int y_count = codec * 2;
+  const double twist_step = -pi / y_count;
+  const double skew_step = pi / y_count;
+  t.twist_cos.resize(codec);
+  t.twist_sin.resize(codec);
+  t.skew_cos.resize(codec);
+  t.skew_sin.resize(codec);
+  for (int i = 0; i < codec; i++) {
+    const int real_index = 2 * i;
+    t.twist_cos[i] = std::cos(real_index * twist_step);
+    t.twist_sin[i] = std::sin(real_index * twist_step);
+    t.skew_cos[i] = std::cos(real_index * skew_step);
+    t.skew_sin[i] = std::sin(real_index * skew_step);
+  }
+  return t;
+}
+
+long double Parameters::ckks_scale(int level) const {
+  // precomputed.cpp:144-155.
+  const int mid = moduli_id(level);
+  const double deviation = static_cast<double>(deviations[level]);
+  long double s = static_cast<long double>(deviation) * scale * scale;
+  if (preset.one_more_level && mid == 0) s = scale * static_cast<long double>(q[0]);
+  return s;
+}
+
+EncodeLevel Parameters::encode_level(int level) const {
+  // precomputed.cpp:139-215 (no flexible chain: its scale bit is always 0).
+  EncodeLevel e;
+  int mid = moduli_id(level);
+  int chains_here = chains(mid, true);
+  const int log_scale = preset.scale_bits;
+  const long double ckks = ckks_scale(level);
+  e.ckks_scale = ckks;
+  const uint64_t p0 = q[mid];
+  e.max_level_in_one_more_level = preset.one_more_level && mid == 0 && (ckks >= p0 * scale);
+  if (e.max_level_in_one_more_level) {
+    e.scale_before_tile = static_cast<double>(ckks / p0);
+    chains_here -= 1;
+    mid = moduli_id(level - 1);
+  } else {
+    int exponent = 0;
+    const double mantissa = static_cast<double>(std::frexp(ckks, &exponent));
+    if (exponent >= log_scale) {
+      e.scale_before_tile = mantissa * scale;
+      e.log_scale_after_tile = exponent - log_scale;
+    } else {
+      e.scale_before_tile = static_cast<double>(ckks);
+      e.log_scale_after_tile = 0;
+    }
+  }
+  e.first_moduli_id = mid;
+  const int64_t r = INT64_C(1) << 62;
+  e.r_mult_scale_after_tile.resize(chains_here);
+  if (e.max_level_in_one_more_level) {
+    for (int j = 0; j < chains_here; j++)
+      e.r_mult_scale_after_tile[j] = mod_mul(r, static_cast<int64_t>(p0), static_cast<int64_t>(q[mid + j]));
+  } else {
+    for (int j = 0; j < chains_here; j++)
+      e.r_mult_scale_after_tile[j] = r % static_cast<int64_t>(q[mid + j]);
+    for (int64_t ls = e.log_scale_after_tile; ls > 0; ls -= 60) {
+      const int64_t partial = INT64_C(1) << std::min<int64_t>(60, ls);
+      for (int j = 0; j < chains_here; j++)
+        e.r_mult_scale_after_tile[j] =
+            mod_mul(e.r_mult_scale_after_tile[j], partial, static_cast<int64_t>(q[mid + j]));
+    }
+  }
+  return e;
+}
+
+}  // namespace fhe_b200

@@ -62,6 +62,25 @@ struct PartitionConstants {
   std::vector<int64_t> product_r_squared;         // [(size-1) * prime_count(moduli_id)]
 };
 
+// Host tables of the canonical-embedding codec (precomputed.cpp:49-74 and the
+// cos/sin factors of apply_twister / apply_skewer), for codec = 2 * slot_count.
+struct CodecTables {
+  int codec = 0;
+  std::vector<int32_t> pre, post;  // pre_permutation_, post_permutation_
+  std::vector<double> fft_cos, fft_sin, ifft_cos, ifft_sin;
+  std::vector<double> twist_cos, twist_sin, skew_cos, skew_sin;
+};
+
+// Per-level encode constants (precomputed.cpp:139-215).
+struct EncodeLevel {
+  long double ckks_scale = 0;
+  double scale_before_tile = 0;
+  int64_t log_scale_after_tile = 0;
+  bool max_level_in_one_more_level = false;
+  int first_moduli_id = 0;  // moduli id of r_mult_scale_after_tile[0]
+  std::vector<int64_t> r_mult_scale_after_tile;
+};
+
 class Parameters {
  public:
   explicit Parameters(const Config &config);
@@ -106,6 +125,9 @@ class Parameters {
   std::vector<int64_t> level_down_multiplier_after_rescale(int source_level,
                                                            int destination_level) const;
   long double level_down_scale(int level) const;
+  CodecTables codec_tables() const;
+  long double ckks_scale(int level) const;
+  EncodeLevel encode_level(int level) const;
 };
 
 // get_permutation_and_sign (ckks/encode.cpp:513-526) for a rotation by `delta`

@@ -246,6 +246,30 @@ class Engine:
             return self._call("fhe_conjugate_plaintext", text)
         return self._call("fhe_conjugate", text, conjugation_key)
 
+    def encode(self, values, level: int | None = None, include_special: bool = False) -> Data:
+        """encode_unit: real or complex slot values into a coefficient-form plaintext."""
+        v = np.asarray(values)
+        lvl = self.max_level if level is None else level
+        h = ctypes.c_void_p()
+        if np.iscomplexobj(v):
+            re = np.ascontiguousarray(v.real, dtype=np.float64)
+            im = np.ascontiguousarray(v.imag, dtype=np.float64)
+            imp = im.ctypes.data_as(_lib._f64p)
+        else:
+            re = np.ascontiguousarray(v, dtype=np.float64)
+            imp = None
+        check(_lib.load().fhe_encode(self._h, re.ctypes.data_as(_lib._f64p), imp, re.size, lvl,
+                                     int(include_special), ctypes.byref(h)))
+        return Data(self, h)
+
+    def decode(self, pt: Data, complex_output: bool = False) -> np.ndarray:
+        """decode_unit (real parts) or decode_complex_unit_plaintext."""
+        re = np.empty(self.slot_count, dtype=np.float64)
+        im = np.empty(self.slot_count, dtype=np.float64) if complex_output else None
+        check(_lib.load().fhe_decode(self._h, pt.handle, re.ctypes.data_as(_lib._f64p),
+                                     im.ctypes.data_as(_lib._f64p) if im is not None else None))
+        return re + 1j * im if complex_output else re
+
     def switch_key(self, ct: Data, key_switching_key: Data) -> Data:
         return self._call("fhe_switch_key", ct, key_switching_key)
 

@@ -224,6 +224,18 @@ int fhe_conjugate(fhe_engine *engine, const fhe_data *ct, const fhe_data *conjug
                   fhe_data **out);
 /* CKKSEngine::conjugate(UnitPlaintext*) (engine.h:333, engine_conjugate.cpp:10-24). */
 int fhe_conjugate_plaintext(fhe_engine *engine, const fhe_data *pt, fhe_data **out);
+/* CKKSEngine::encode_unit (engine.h:50-54, engine_encode.cpp:6-36; CKKSCore::encode,
+ * core_encode.cpp:33-150): `count` slot values (im NULL: real input; fewer than the
+ * slot count are zero-padded, more are ignored) encoded at `level` into a plaintext
+ * in coefficient form.  The FFT, twist and rounding run on the device in IEEE
+ * double with the reference's operation order, so the limbs are bit-identical. */
+int fhe_encode(fhe_engine *engine, const double *re, const double *im, int count, int level,
+               int include_special, fhe_data **out);
+/* CKKSEngine::decode_unit / decode_complex_unit_plaintext (engine.h:75-77,
+ * engine_decode.cpp:6-19; core_decode.cpp:11-124): slot_count values into re (and
+ * im unless NULL).  CRT reconstruction, skew, FFT and permutation run on the device. */
+int fhe_decode(fhe_engine *engine, const fhe_data *pt, double *re, double *im);
+
 /* CKKSCore::switch_key (core.h, core.cpp:1058-1083): c0 + KS(c1) with a key
  * switching key (FHE_KEY_SWITCHING_KEY); NTT-form input is brought to coefficient
  * form first. */

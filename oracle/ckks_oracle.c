@@ -1000,3 +1000,388 @@ void oracle_rotate_plain_ntt(const oracle_ctx *c, int mid, int polys, int delta,
     }
   free(perm);
 }
+
+/* ------------------------------------------------------- encode / decode -- */
+
+typedef struct {
+  double re, im;
+} cplx;
+
+/* std::complex<double> product as the reference's compiler expands it. */
+static cplx cmul_(cplx a, cplx b) {
+  cplx r = {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+  return r;
+}
+
+/* ckks/encode.cpp:25-154: the codec permutations for codec = 2 * slot_count. */
+static int32_t jump_of(unsigned shift, int double_size) {
+  if (shift == (unsigned)(double_size - 1)) return (int32_t)shift;
+  int64_t jump = 1;
+  for (int power = 0; power < double_size - (int)shift; power++) {
+    jump *= 5;
+    jump &= double_size - 1;
+  }
+  return (int32_t)jump;
+}
+
+static void cycles_of(const uint64_t *p, int size, uint64_t *out) {
+  char *visited = calloc(size, 1);
+  int start = 0, o = 0;
+  while (start < size) {
+    uint64_t cur = p[start], next = p[cur];
+    for (;;) {
+      out[o++] = cur;
+      visited[cur] = 1;
+      cur = next;
+      if (visited[next]) break;
+      next = p[cur];
+    }
+    start++;
+    while (start < size && visited[start]) start++;
+  }
+  free(visited);
+}
+
+static void codec_permutations(int codec, uint64_t *pre, uint64_t *post) {
+  uint64_t *cs = calloc(codec, sizeof(uint64_t)), *fc = calloc(codec, sizeof(uint64_t));
+  uint64_t *c1 = calloc(codec, sizeof(uint64_t)), *c2 = calloc(codec, sizeof(uint64_t));
+  const int half = codec / 2;
+  cs[0] = half - 1;
+  for (int i = 1; i < half; i++) cs[i] = i - 1;
+  for (int i = half; i < codec - 1; i++) cs[i] = i + 1;
+  cs[codec - 1] = half;
+  const int double_size = codec * 2;
+  const int32_t jump = jump_of(1, double_size);
+  int32_t jm = jump;
+  for (int i = 0; i < codec; i++) {
+    fc[i] = (uint64_t)((jm - 1) >> 1);
+    jm = (jm + jump * 2) % double_size;
+  }
+  cycles_of(fc, codec, c1);
+  cycles_of(cs, codec, c2);
+  for (int i = 0; i < codec; i++) post[c1[i]] = c2[i];
+  for (int i = 0; i < codec; i++) pre[post[i]] = i;
+  free(cs);
+  free(fc);
+  free(c1);
+  free(c2);
+}
+
+static void bit_reverse_(cplx *y, int size) { /* fft.cpp:56-75 */
+  for (int i = 1, j = 0; i < size; i++) {
+    int bit = size >> 1;
+    while (j & bit) {
+      j ^= bit;
+      bit >>= 1;
+    }
+    j ^= bit;
+    if (i < j) {
+      cplx t = y[i];
+      y[i] = y[j];
+      y[j] = t;
+    }
+  }
+}
+
+static void fft_(cplx *y, const cplx *tw, int size) { /* fft.cpp:77-102 */
+  for (int step = 2, ts = size / 2; step <= size; step <<= 1, ts >>= 1) {
+    const int half = step >> 1;
+    for (int off = 0; off < size; off += step) {
+      int ti = 0;
+      for (int d = off; d < off + half; d++) {
+        const cplx l = y[d], r = cmul_(tw[ti], y[d + half]);
+        y[d].re = l.re + r.re;
+        y[d].im = l.im + r.im;
+        y[d + half].re = l.re - r.re;
+        y[d + half].im = l.im - r.im;
+        ti += ts;
+      }
+    }
+  }
+}
+
+static const double PI_ = 3.141592653589793;
+
+/* precomputed.cpp:139-215 for one level: scale before the tile, the
+ * one-more-level flag and r_mult_scale_after_tile from moduli id *first_mid. */
+void oracle_encode_level(const oracle_ctx *c, double scale, int scale_bits, int one_more_level,
+                         int level, long double *ckks_scale_out, double *scale_before_tile,
+                         int *max_level_flag, int *first_mid, int64_t *r_mult) {
+  double dev[256];
+  oracle_deviations(c, scale, one_more_level, dev);
+  const int full = c->chain_count - 2;
+  int mid = full - level;
+  int chains = c->prime_count - mid;
+  long double ckks = (long double)dev[level] * scale * scale;
+  if (one_more_level && mid == 0) ckks = scale * (long double)c->q[0];
+  *ckks_scale_out = ckks;
+  const uint64_t p0 = c->q[mid];
+  const int max_flag = one_more_level && mid == 0 && (ckks >= p0 * scale);
+  int64_t log_after = 0;
+  if (max_flag) {
+    *scale_before_tile = (double)(ckks / p0);
+    chains -= 1;
+    mid = full - (level - 1);
+  } else {
+    int e = 0;
+    const double m = (double)frexpl(ckks, &e);
+    if (e >= scale_bits) {
+      *scale_before_tile = m * scale;
+      log_after = e - scale_bits;
+    } else {
+      *scale_before_tile = (double)ckks;
+    }
+  }
+  const int64_t r = (int64_t)1 << 62;
+  for (int j = 0; j < chains; j++) {
+    const int64_t qj = (int64_t)c->q[mid + j];
+    if (max_flag) {
+      r_mult[j] = mod_mul(r, (int64_t)p0, qj);
+    } else {
+      int64_t v = r % qj;
+      for (int64_t ls = log_after; ls > 0; ls -= 60)
+        v = mod_mul(v, (int64_t)1 << (ls < 60 ? ls : 60), qj);
+      r_mult[j] = v;
+    }
+  }
+  *max_level_flag = max_flag;
+  *first_mid = mid;
+}
+
+static int64_t pmod_(int64_t x, int64_t m) { return (m + x % m) % m; }
+
+/* CKKSCore::encode_polynomial (core_encode.cpp:33-150) for odd moduli.  Writes
+ * `limbs` limbs (the plaintext's chain at its level, with or without specials)
+ * [limbs][N]; im may be NULL (real input). */
+void oracle_encode(const oracle_ctx *c, const double *re, const double *im, int log_slot,
+                   double scale_before_tile, int max_level_flag, int first_mid,
+                   const int64_t *r_mult, int limbs, int64_t *out) {
+  const int n = c->n, slot = 1 << log_slot, codec = 2 * slot, jump = n / codec;
+  uint64_t *pre = calloc(codec, sizeof(uint64_t)), *post = calloc(codec, sizeof(uint64_t));
+  codec_permutations(codec, pre, post);
+  cplx *y = calloc(codec, sizeof(cplx));
+  for (int i = 0; i < slot; i++) { /* pre_permute, encode.cpp:156-185 */
+    const uint64_t p = pre[i];
+    const double r = re[i], m = im ? im[i] : 0.0;
+    y[p].re = r;
+    y[p].im = m;
+    y[codec - p - 1].re = r;
+    y[codec - p - 1].im = im ? -m : 0.0;
+  }
+  bit_reverse_(y, codec);
+  cplx *tw = calloc(codec, sizeof(cplx));
+  const double unit = -2 * PI_ / codec;
+  for (int i = 0; i < codec; i++) {
+    const double a = i * unit;
+    tw[i].re = cos(a);
+    tw[i].im = sin(a);
+  }
+  fft_(y, tw, codec);
+  double *v = calloc(codec, sizeof(double));
+  const double step = -PI_ / (codec * 2);
+  double max_abs = 0.0;
+  for (int i = 0; i < codec; i++) { /* normalize + apply_twister */
+    const double a = y[i].re / codec, b = y[i].im / codec;
+    const int ri = 2 * i;
+    v[i] = (a * cos(ri * step) - b * sin(ri * step)) * scale_before_tile;
+    if (fabs(v[i]) > max_abs) max_abs = fabs(v[i]);
+  }
+  const int offset = max_level_flag ? 1 : 0;
+  const int filled = limbs - offset;
+  memset(out, 0, sizeof(int64_t) * (size_t)limbs * n);
+  for (int j = 0; j < filled; j++) {
+    const int pq = first_mid + j;
+    const uint64_t q = c->q[pq], k = c->k[pq];
+    const int64_t qs = (int64_t)q;
+    int64_t *o = out + (size_t)(j + offset) * n;
+    for (int i = 0; i < codec; i++) {
+      int64_t t;
+      if (max_abs > (double)(1UL << 59)) { /* double_to_rns, arithmetic.cpp:242-270 */
+        if (fabs(v[i]) < (double)(1L << 62)) {
+          t = pmod_((int64_t)(v[i] + 0.5), qs);
+        } else {
+          int e;
+          const double m = frexp(v[i] + 0.5, &e);
+          t = pmod_((int64_t)(m * (double)(1L << 52)), qs);
+          for (int le = 52; le < e; le++) {
+            t <<= 1;
+            t %= qs;
+          }
+        }
+      } else { /* llround, then make_unsigned_reduce_2q_to_q */
+        const int64_t r = llround(v[i]);
+        t = r < 0 ? r + qs : guard(r, qs);
+      }
+      o[(size_t)i * jump] = MM(t, r_mult[j], q, k);
+    }
+  }
+  free(pre);
+  free(post);
+  free(y);
+  free(tw);
+  free(v);
+}
+
+/* convert_plaintext_to_double after the rescale loop + decode_ (core_decode.cpp:
+ * 77-124): x [limbs][N] coefficient form at mid; output_scale = the plaintext's
+ * ckks_scale then; writes slot values (im may be NULL). */
+void oracle_decode(const oracle_ctx *c, const int64_t *x, int mid, int limbs, int log_slot,
+                   long double output_scale, double *re, double *im) {
+  const int n = c->n, slot = 1 << log_slot, codec = 2 * slot, jump = n / codec;
+  double *plain = calloc(codec, sizeof(double));
+  const int words = (limbs * 61 + 63) / 64 + 2;
+  uint64_t *Q = calloc(words, 8), *cof = calloc((size_t)limbs * words, 8);
+  uint64_t *acc = calloc(words + 1, 8);
+  int64_t *inv = calloc(limbs, sizeof(int64_t));
+#define MULW(a, m)                                                  \
+  do {                                                              \
+    unsigned __int128 cr = 0;                                       \
+    for (int w_ = 0; w_ < words; w_++) {                            \
+      unsigned __int128 p_ = (unsigned __int128)(a)[w_] * (m) + cr; \
+      (a)[w_] = (uint64_t)p_;                                       \
+      cr = p_ >> 64;                                                \
+    }                                                               \
+  } while (0)
+  Q[0] = 1;
+  for (int j = 0; j < limbs; j++) MULW(Q, c->q[mid + j]);
+  for (int j = 0; j < limbs; j++) { /* Q/q_j and (Q/q_j)^-1 mod q_j */
+    uint64_t *cj = cof + (size_t)j * words;
+    cj[0] = 1;
+    const int64_t qj = (int64_t)c->q[mid + j];
+    int64_t iv = 1;
+    for (int i = 0; i < limbs; i++) {
+      if (i == j) continue;
+      MULW(cj, c->q[mid + i]);
+      iv = mod_mul(iv, mod_invert((int64_t)(c->q[mid + i] % (uint64_t)qj), qj), qj);
+    }
+    inv[j] = iv;
+  }
+#undef MULW
+  for (int i = 0; i < codec; i++) {
+    const size_t pos = (size_t)i * jump;
+    if (limbs == 1) { /* make_signed, unsigned q/2 comparison (unit.cpp:36-42) */
+      const int64_t v = x[pos];
+      const uint64_t q = c->q[mid];
+      plain[i] = (double)((uint64_t)v <= (q >> 1) ? v : v - (int64_t)q);
+      continue;
+    }
+    memset(acc, 0, 8 * (words + 1));
+    for (int j = 0; j < limbs; j++) {
+      const int64_t qj = (int64_t)c->q[mid + j];
+      int64_t v = x[(size_t)j * n + pos];
+      v = v < 0 ? v + qj : guard(v, qj);
+      const int64_t d = mod_mul(v, inv[j], qj);
+      unsigned __int128 cr = 0;
+      const uint64_t *cj = cof + (size_t)j * words;
+      for (int w = 0; w < words; w++) {
+        unsigned __int128 s = (unsigned __int128)cj[w] * (uint64_t)d + acc[w] + cr;
+        acc[w] = (uint64_t)s;
+        cr = s >> 64;
+      }
+      acc[words] += (uint64_t)cr;
+    }
+    for (;;) { /* reduce modulo Q */
+      int ge = acc[words] != 0;
+      if (!ge) {
+        ge = 1;
+        for (int w = words - 1; w >= 0; w--)
+          if (acc[w] != Q[w]) {
+            ge = acc[w] > Q[w];
+            break;
+          }
+      }
+      if (!ge) break;
+      unsigned __int128 br = 0;
+      for (int w = 0; w < words; w++) {
+        unsigned __int128 d = (unsigned __int128)acc[w] - Q[w] - br;
+        acc[w] = (uint64_t)d;
+        br = (d >> 64) ? 1 : 0;
+      }
+      acc[words] -= (uint64_t)br;
+    }
+    /* centre: X >= floor(Q/2) -> -(Q - X); then BigInt::get_double */
+    int neg = 1;
+    for (int w = words - 1; w >= 0; w--) {
+      const uint64_t h = (Q[w] >> 1) | (w + 1 < words ? Q[w + 1] << 63 : 0);
+      if (acc[w] != h) {
+        neg = acc[w] > h;
+        break;
+      }
+    }
+    if (neg) {
+      unsigned __int128 br = 0;
+      for (int w = 0; w < words; w++) {
+        unsigned __int128 d = (unsigned __int128)Q[w] - acc[w] - br;
+        acc[w] = (uint64_t)d;
+        br = (d >> 64) ? 1 : 0;
+      }
+    }
+    int top = words - 1;
+    while (top > 0 && acc[top] == 0) top--;
+    double yv = 0;
+    for (int w = 0; w <= top; w++) yv += (double)acc[w] * pow(2.0, 64 * w);
+    plain[i] = neg ? -yv : yv;
+  }
+  /* apply_skewer, bit_reversal_permute, fft with the inverse twiddles,
+   * permute_after_ifft */
+  cplx *z = calloc(codec, sizeof(cplx)), *tw = calloc(codec, sizeof(cplx));
+  const double step = PI_ / (codec * 2);
+  for (int i = 0; i < codec; i++) {
+    z[i].re = plain[i] * cos(2 * i * step);
+    z[i].im = plain[i] * sin(2 * i * step);
+  }
+  bit_reverse_(z, codec);
+  const double unit = -2 * PI_ / codec;
+  for (int i = 0; i < codec; i++) {
+    const double a = i * unit;
+    tw[i].re = cos(a);
+    tw[i].im = sin(-a);
+  }
+  fft_(z, tw, codec);
+  uint64_t *pre = calloc(codec, sizeof(uint64_t)), *post = calloc(codec, sizeof(uint64_t));
+  codec_permutations(codec, pre, post);
+  const double sinv = (double)(1.0 / output_scale);
+  for (int i = 0; i < codec; i++) {
+    const uint64_t p = post[i];
+    if (p < (uint64_t)slot) {
+      re[p] = z[i].re * sinv;
+      if (im) im[p] = z[i].im * sinv;
+    }
+  }
+  free(plain);
+  free(Q);
+  free(cof);
+  free(acc);
+  free(inv);
+  free(z);
+  free(tw);
+  free(pre);
+  free(post);
+}
+
+/* Engine decode of a coefficient-form plaintext x [limbs][N] at moduli_id (no
+ * specials) whose ckks_scale is *scale: the rescale loop of
+ * convert_plaintext_to_double (core_decode.cpp:36-54, with get_rescaled_scale =
+ * scale / q[moduli_id]), then decode. */
+void oracle_decode_plaintext(const oracle_ctx *c, const int64_t *x, int mid, int log_slot,
+                             const long double *scale, double engine_scale, double *re,
+                             double *im) {
+  const int n = c->n;
+  int limbs = oracle_chain_count(c, mid);
+  int64_t *cur = malloc(sizeof(int64_t) * (size_t)limbs * n);
+  memcpy(cur, x, sizeof(int64_t) * (size_t)limbs * n);
+  long double s = *scale;
+  while (mid <= c->chain_count - 2) {
+    const long double next = s / c->q[mid];
+    if (next <= engine_scale) break;
+    int64_t *y = malloc(sizeof(int64_t) * (size_t)(limbs - 1) * n);
+    oracle_rescale(c, mid, 1, cur, y);
+    free(cur);
+    cur = y;
+    s = next;
+    mid++;
+    limbs--;
+  }
+  oracle_decode(c, cur, mid, limbs, log_slot, s, re, im);
+  free(cur);
+}

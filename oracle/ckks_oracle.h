@@ -117,6 +117,19 @@ void oracle_rotate_plain(const oracle_ctx *ctx, int moduli_id, int polys, int de
 void oracle_rotate_plain_ntt(const oracle_ctx *ctx, int moduli_id, int polys, int delta,
                              const int64_t *x, int64_t *y);
 
+/* Encode / decode (core_encode.cpp:33-150, core_decode.cpp:11-124). */
+void oracle_encode_level(const oracle_ctx *ctx, double scale, int scale_bits, int one_more_level,
+                         int level, long double *ckks_scale, double *scale_before_tile,
+                         int *max_level_flag, int *first_moduli_id, int64_t *r_mult);
+void oracle_encode(const oracle_ctx *ctx, const double *re, const double *im, int log_slot,
+                   double scale_before_tile, int max_level_flag, int first_moduli_id,
+                   const int64_t *r_mult, int limbs, int64_t *out);
+void oracle_decode(const oracle_ctx *ctx, const int64_t *x, int moduli_id, int limbs,
+                   int log_slot, long double output_scale, double *re, double *im);
+void oracle_decode_plaintext(const oracle_ctx *ctx, const int64_t *x, int moduli_id, int log_slot,
+                             const long double *scale, double engine_scale, double *re,
+                             double *im);
+
 #ifdef __cplusplus
 }
 #endif

@@ -91,6 +91,16 @@ def lib():
         L.oracle_level_down.restype = None
         L.oracle_level_down.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_int, _i64p, _i64p, _i64p]
+        _f64 = ctypes.POINTER(ctypes.c_double)
+        L.oracle_encode_level.restype = None
+        L.oracle_encode_level.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_void_p, _f64, _i32p, _i32p, _i64p]
+        L.oracle_encode.restype = None
+        L.oracle_encode.argtypes = [ctypes.c_void_p, _f64, _f64, ctypes.c_int, ctypes.c_double,
+                                    ctypes.c_int, ctypes.c_int, _i64p, ctypes.c_int, _i64p]
+        L.oracle_decode_plaintext.restype = None
+        L.oracle_decode_plaintext.argtypes = [ctypes.c_void_p, _i64p, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_void_p, ctypes.c_double, _f64, _f64]
         for name in ("oracle_rotate_plain", "oracle_rotate_plain_ntt"):
             f = getattr(L, name)
             f.restype = None
@@ -268,6 +278,51 @@ class Context:
         lib().oracle_level_down(self._ctx, src_mid, x.shape[0], int(rescaled), dst_mid, _p(mult),
                                 _p(x), _p(y))
         return y
+
+    def encode(self, values, log_slot: int, level: int, scale_bits: int,
+               include_special: bool = False, one_more_level: bool = True):
+        """CKKSCore::encode of real (float) or complex slot values; returns
+        (limbs [1][L][N], ckks_scale as a numpy longdouble)."""
+        f64 = ctypes.POINTER(ctypes.c_double)
+        scale = float(2 ** scale_bits)
+        ckks = np.zeros(1, dtype=np.longdouble)  # x87 extended, as the C long double
+        sbt = ctypes.c_double()
+        flag = ctypes.c_int()
+        first = ctypes.c_int()
+        mult = np.zeros(self.prime_count, dtype=np.int64)
+        lib().oracle_encode_level(self._ctx, scale, scale_bits, int(one_more_level), level,
+                                  ckks.ctypes.data, ctypes.byref(sbt), ctypes.byref(flag),
+                                  ctypes.byref(first), _p(mult))
+        slot = 1 << log_slot
+        v = np.asarray(values)
+        re = np.zeros(slot)
+        im = np.zeros(slot) if np.iscomplexobj(v) else None
+        m = min(len(v), slot)
+        re[:m] = np.real(v[:m])
+        if im is not None:
+            im[:m] = np.imag(v[:m])
+        mid = self.chain_count - 2 - level
+        limbs = self.prime_count - mid if include_special else self.chain_count - mid
+        out = np.zeros((1, limbs, self.n), dtype=np.int64)
+        lib().oracle_encode(self._ctx, re.ctypes.data_as(f64),
+                            im.ctypes.data_as(f64) if im is not None else None, log_slot, sbt.value,
+                            flag.value, first.value, _p(mult), limbs, _p(out))
+        return out, ckks[0]
+
+    def decode_plaintext(self, x, moduli_id: int, log_slot: int, ckks_scale, scale_bits: int,
+                         complex_output: bool = True):
+        """Engine decode of a coefficient-form plaintext [L][N] (rescale loop
+        included); ckks_scale is a numpy longdouble."""
+        x = np.ascontiguousarray(x, dtype=np.int64)
+        f64 = ctypes.POINTER(ctypes.c_double)
+        s = np.array([ckks_scale], dtype=np.longdouble)
+        slot = 1 << log_slot
+        re = np.zeros(slot)
+        im = np.zeros(slot)
+        lib().oracle_decode_plaintext(self._ctx, _p(x), moduli_id, log_slot, s.ctypes.data,
+                                      float(2 ** scale_bits), re.ctypes.data_as(f64),
+                                      im.ctypes.data_as(f64) if complex_output else None)
+        return re + 1j * im if complex_output else re
 
     def rotate_plain(self, moduli_id, x, delta, ntt_form=False):
         x = np.ascontiguousarray(x, dtype=np.int64)

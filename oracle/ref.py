@@ -72,6 +72,7 @@ def lib():
             "ref_engine_conjugate": (vp, [vp, vp, vp]),
             "ref_engine_level_down": (vp, [vp, vp, ctypes.c_int]),
             "ref_last_error": (ctypes.c_char_p, []),
+            "ref_engine_decode_real": (ctypes.c_int, [vp, vp, ctypes.POINTER(ctypes.c_double)]),
             "ref_deviations": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
             "ref_engine_rotate_plain": (vp, [vp, vp, ctypes.c_int]),
             "ref_engine_conjugate_plain": (vp, [vp, vp]),
@@ -272,13 +273,23 @@ class Engine:
         return self._h(lib().ref_engine_rotate_keys(self.ptr, a.ptr, arr, len(fixed_keys), delta,
                                                     int(by_slot_count)))
 
-    def encode(self, values, level=-1):
+    def encode(self, values, level=-1, real=False):
+        cd = ctypes.POINTER(ctypes.c_double)
+        if real:
+            re = np.ascontiguousarray(np.asarray(values, dtype=np.float64))
+            return self._h(lib().ref_engine_encode(self.ptr, re.ctypes.data_as(cd), None,
+                                                   len(re), level))
         values = np.asarray(values, dtype=np.complex128)
         re = np.ascontiguousarray(values.real)
         im = np.ascontiguousarray(values.imag)
-        cd = ctypes.POINTER(ctypes.c_double)
         return self._h(lib().ref_engine_encode(self.ptr, re.ctypes.data_as(cd),
                                                im.ctypes.data_as(cd), len(values), level))
+
+    def decode_real(self, pt):
+        re = np.empty(self.slot_count)
+        cd = ctypes.POINTER(ctypes.c_double)
+        cnt = lib().ref_engine_decode_real(self.ptr, pt.ptr, re.ctypes.data_as(cd))
+        return re[:cnt]
 
     def decode(self, pt):
         re = np.empty(self.slot_count)

@@ -647,14 +647,26 @@ void *ref_engine_encode(void *e, const double *re, const double *im, int count,
                         int level) {
   try {
   auto eng = static_cast<RefEngine *>(e)->engine.get();
+  if (im == nullptr) {  // encode_unit(std::vector<double>&)
+    std::vector<double> v(re, re + count);
+    auto pt = level < 0 ? eng->encode_unit(v) : eng->encode_unit(v, level);
+    return wrap(5, pt, pt);
+  }
   std::vector<std::complex<double>> v(count);
-  for (int i = 0; i < count; i++) v[i] = {re[i], im ? im[i] : 0.0};
+  for (int i = 0; i < count; i++) v[i] = {re[i], im[i]};
   auto pt = level < 0 ? eng->encode_unit(v) : eng->encode_unit(v, level);
   return wrap(5, pt, pt);
   } catch (...) {
     remember_error();
     return nullptr;
   }
+}
+
+int ref_engine_decode_real(void *e, void *pt, double *re) {
+  auto eng = static_cast<RefEngine *>(e)->engine.get();
+  auto v = eng->decode_unit(static_cast<UnitPlaintext *>(static_cast<Handle *>(pt)->data));
+  for (size_t i = 0; i < v.size(); i++) re[i] = v[i];
+  return static_cast<int>(v.size());
 }
 
 int ref_engine_decode(void *e, void *pt, double *re, double *im) {

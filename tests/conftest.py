@@ -59,10 +59,11 @@ def engines():
 
     cache = {}
 
-    def get(log_n, K, preset):
-        key = (log_n, K, preset)
+    def get(log_n, K, preset, log_slot=-1):
+        key = (log_n, K, preset, log_slot)
         if key not in cache:
-            cache[key] = Engine(log_coeff_count=log_n, special_prime_count=K, scheme_preset=preset)
+            cache[key] = Engine(log_coeff_count=log_n, special_prime_count=K, scheme_preset=preset,
+                                log_slot_count=log_slot)
         return cache[key]
 
     yield get

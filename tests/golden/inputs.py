@@ -75,3 +75,18 @@ def key_switch_inputs(seed: int, moduli, n: int, moduli_id: int, special: int):
     b_next = uniform_limbs(rng, moduli[moduli_id + 1:chain], 2, n)
     return dict(key_moduli_id=key_mid, rotation_keys=rotation_keys,
                 conjugation_key=conjugation_key, switching_key=switching_key, b_next=b_next)
+
+
+def codec_values(seed: int, slot_count: int, complex_values: bool) -> np.ndarray:
+    """Slot values uniform in [-1, 1) (real and imaginary parts) for codec cases."""
+    rng = np.random.default_rng(seed)
+    re = rng.uniform(-1.0, 1.0, slot_count)
+    if not complex_values:
+        return re
+    return re + 1j * rng.uniform(-1.0, 1.0, slot_count)
+
+
+def digest_doubles(a) -> str:
+    """Digest of the IEEE bit patterns of a float64 / complex128 array."""
+    a = np.ascontiguousarray(a)
+    return hashlib.sha256(a.view(np.uint8).tobytes()).hexdigest()

@@ -25,7 +25,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
-from inputs import ROTATION_KEY_DELTAS, key_switch_inputs, TIERS, case_inputs, digest  # noqa: E402
+from inputs import ROTATION_KEY_DELTAS, codec_values, digest_doubles, key_switch_inputs, TIERS, case_inputs, digest  # noqa: E402
 
 REF = os.environ.get("FHE_REFERENCE", "/root/reference")
 
@@ -162,6 +162,40 @@ def reference_ops():
     return cases
 
 
+# (tier, log_slot_count): full slots, plus one sparse-slot engine.
+CODEC_PLAN = [("pebble", -1), ("bronze", -1), ("bronze", 10), ("bootstrap_gold", -1)]
+
+
+def codec_cases():
+    """Encode / decode through the reference's engine (encode_unit, decode_unit,
+    decode_complex_unit_plaintext) on seeded slot values."""
+    from oracle import ref
+
+    cases = []
+    seed = 5000
+    for tier, log_slot in CODEC_PLAN:
+        log_n, K, preset = TIERS[tier]
+        e = ref.Engine(log_n=log_n, special_prime_count=K, preset=preset, log_slot=log_slot)
+        full = e.chain_count - 2
+        for level in sorted({full, full - 1, 1}):
+            for kind in ("real", "complex"):
+                seed += 1
+                vals = codec_values(seed, e.slot_count, kind == "complex")
+                pt = e.encode(vals, level, real=kind == "real")
+                # digest before decoding: the reference's decode reduces the limbs of
+                # its input in place (make_unsigned_reduce_2q_to_q, core_decode.cpp:82)
+                encoded = digest(pt.limbs())
+                dec = e.decode_real(pt) if kind == "real" else e.decode(pt)
+                info = pt.info()
+                cases.append(dict(tier=tier, log_n=log_n, special_prime_count=K, preset=preset,
+                                  log_slot=log_slot, level=level, kind=kind, seed=seed,
+                                  moduli_id=info["moduli_id"], scale_bits=e.scale_bits,
+                                  moduli=[int(v) for v in e.tables()["q"]],
+                                  encode=encoded, decode=digest_doubles(dec),
+                                  max_error=float(np.max(np.abs(dec - vals)))))
+    return cases
+
+
 def main():
     with open(os.path.join(HERE, "ntt_kat.json"), "w") as f:
         json.dump(parse_ntt_kats(), f, indent=1)
@@ -170,6 +204,9 @@ def main():
     cases = reference_ops()  # computed before the file is opened: a failure keeps the old one
     with open(os.path.join(HERE, "ref_ops.json"), "w") as f:
         json.dump(cases, f, indent=1)
+    codec = codec_cases()
+    with open(os.path.join(HERE, "codec.json"), "w") as f:
+        json.dump(codec, f, indent=1)
 
 
 if __name__ == "__main__":

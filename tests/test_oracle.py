@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 from conftest import load_golden
-from inputs import ROTATION_KEY_DELTAS, key_switch_inputs, TIERS, case_inputs, digest
+from inputs import ROTATION_KEY_DELTAS, codec_values, digest_doubles, key_switch_inputs, TIERS, case_inputs, digest
 from oracle import oracle, ref
 
 
@@ -174,3 +174,20 @@ def test_rotation_permutations_are_permutations(n, delta):
     assert set(sign.tolist()) <= {-1, 1}
     nperm = oracle.ntt_permutation(n, delta)
     assert sorted(nperm.tolist()) == list(range(n))
+
+
+@pytest.mark.parametrize("case", load_golden("codec.json"),
+                         ids=lambda c: f"{c['tier']}-s{c['log_slot']}-l{c['level']}-{c['kind']}")
+def test_oracle_codec_matches_recorded_reference(case):
+    """Encode limbs and decoded doubles (bit patterns) of the oracle's restatement
+    against the reference's encode_unit / decode_unit on the same slot values."""
+    log_n, K = case["log_n"], case["special_prime_count"]
+    ctx = oracle.Context(log_n, _chain(case), K)
+    log_slot = log_n - 1 if case["log_slot"] < 0 else case["log_slot"]
+    complex_values = case["kind"] == "complex"
+    vals = codec_values(case["seed"], 1 << log_slot, complex_values)
+    limbs, ckks_scale = ctx.encode(vals, log_slot, case["level"], case["scale_bits"])
+    assert digest(limbs) == case["encode"]
+    dec = ctx.decode_plaintext(limbs[0], case["moduli_id"], log_slot, ckks_scale,
+                               case["scale_bits"], complex_output=complex_values)
+    assert digest_doubles(dec) == case["decode"]
