@@ -89,6 +89,18 @@ SIGNATURES = {
     "fhe_conjugate_plaintext": (_i, [_vp, _vp, _pp]),
     "fhe_switch_key": (_i, [_vp, _vp, _vp, _pp]),
     "fhe_encode": (_i, [_vp, _f64p, _f64p, _i, _i, _i, _pp]),
+    "fhe_engine_seed": (_i, [_vp, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint8)]),
+    "fhe_create_secret_key": (_i, [_vp, _i, _pp]),
+    "fhe_create_secret_key_from": (_i, [_vp, _i64p, _i, _i, _pp]),
+    "fhe_create_sparse_secret_key": (_i, [_vp, _i, _i, _pp]),
+    "fhe_create_public_key": (_i, [_vp, _vp, _i, _pp]),
+    "fhe_create_relinearization_key": (_i, [_vp, _vp, _i, _pp]),
+    "fhe_create_fixed_rotation_key": (_i, [_vp, _vp, _i, _i, _i, _pp]),
+    "fhe_create_rotation_keys": (_i, [_vp, _vp, _i, ctypes.POINTER(_vp), _i,
+                                      ctypes.POINTER(ctypes.c_int)]),
+    "fhe_create_conjugation_key": (_i, [_vp, _vp, _i, _pp]),
+    "fhe_encrypt": (_i, [_vp, _vp, _vp, _pp]),
+    "fhe_decrypt": (_i, [_vp, _vp, _vp, _pp]),
     "fhe_decode": (_i, [_vp, _vp, _f64p, _f64p]),
     "fhe_ntt_limbs": (_i, [_vp, _i64p, _i, _i, _i, ctypes.c_longlong, _i]),
     "fhe_relinearize_noalloc": (_i, [_vp, _i64p, _i, _i64p, _i, _i, _i64p]),

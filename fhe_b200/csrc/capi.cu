@@ -436,3 +436,132 @@ int fhe_decode(fhe_engine *engine, const fhe_data *pt, double *re, double *im) {
 }
 
 }  // extern "C"
+
+extern "C" {
+
+int fhe_engine_seed(fhe_engine *engine, const uint32_t *seed, const uint8_t *nonce) {
+  REQUIRE_HANDLE(engine);
+  return guarded([&] { engine->impl->seed(seed, nonce); });
+}
+
+int fhe_create_secret_key(fhe_engine *engine, int level, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] {
+    auto &e = *engine->impl;
+    *out = wrap(e.create_secret_key(level < 0 ? e.params.max_level() : level));
+  });
+}
+
+int fhe_create_secret_key_from(fhe_engine *engine, const int64_t *secret, int count, int level,
+                               fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] {
+    auto &e = *engine->impl;
+    *out = wrap(e.create_secret_key(secret, count, level < 0 ? e.params.max_level() : level));
+  });
+}
+
+int fhe_create_sparse_secret_key(fhe_engine *engine, int hamming_weight, int level,
+                                 fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] {
+    auto &e = *engine->impl;
+    *out = wrap(e.create_sparse_secret_key(hamming_weight, level < 0 ? e.params.max_level() : level));
+  });
+}
+
+int fhe_create_public_key(fhe_engine *engine, const fhe_data *sk, int level, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(sk);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] {
+    auto &e = *engine->impl;
+    *out = wrap(e.create_public_key(live(engine, sk), level < 0 ? e.params.max_level() : level));
+  });
+}
+
+int fhe_create_relinearization_key(fhe_engine *engine, const fhe_data *sk, int level,
+                                   fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(sk);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] {
+    auto &e = *engine->impl;
+    *out = wrap(e.create_relinearization_key(
+        live(engine, sk), level < 0 ? e.params.max_key_switching_level() : level));
+  });
+}
+
+int fhe_create_fixed_rotation_key(fhe_engine *engine, const fhe_data *sk, int delta, int level,
+                                  int normalize_by_slot_count, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(sk);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] {
+    auto &e = *engine->impl;
+    const int nd = e.normalized_delta(delta, normalize_by_slot_count != 0);
+    *out = wrap(e.create_fixed_rotation_key(
+        live(engine, sk), nd, level < 0 ? e.params.max_key_switching_level() : level));
+  });
+}
+
+int fhe_create_rotation_keys(fhe_engine *engine, const fhe_data *sk, int level, fhe_data **keys,
+                             int capacity, int *count) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(sk);
+  REQUIRE_OUT(keys);
+  REQUIRE_OUT(count);
+  *count = 0;
+  return guarded([&] {
+    auto &e = *engine->impl;
+    int needed = 0;
+    for (int d = 1; d < e.params.n / 2; d <<= 1) needed++;
+    if (capacity < needed)
+      throw std::invalid_argument("Create Rotation Key: the output array holds fewer than " +
+                                  std::to_string(needed) + " keys.");
+    auto made = e.create_rotation_keys(live(engine, sk),
+                                       level < 0 ? e.params.max_key_switching_level() : level);
+    for (auto &k : made) keys[(*count)++] = wrap(std::move(k));
+  });
+}
+
+int fhe_create_conjugation_key(fhe_engine *engine, const fhe_data *sk, int level, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(sk);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] {
+    auto &e = *engine->impl;
+    *out = wrap(e.create_conjugation_key(live(engine, sk),
+                                         level < 0 ? e.params.max_key_switching_level() : level));
+  });
+}
+
+int fhe_encrypt(fhe_engine *engine, const fhe_data *pt, const fhe_data *key, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(pt);
+  REQUIRE_HANDLE(key);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] { *out = wrap(engine->impl->encrypt(live(engine, pt), live(engine, key))); });
+}
+
+int fhe_decrypt(fhe_engine *engine, const fhe_data *ct, const fhe_data *sk, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(ct);
+  REQUIRE_HANDLE(sk);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] { *out = wrap(engine->impl->decrypt(live(engine, ct), live(engine, sk))); });
+}
+
+}  // extern "C"

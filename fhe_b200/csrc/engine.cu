@@ -98,6 +98,7 @@ Engine::Engine(const Config &config) : params(config) {
   ks_.p_product_mult_r = upload_table(ppr);
   ks_.prime_count = P;
   ks_.special_count = p.special_prime_count;
+  seed(nullptr, nullptr);
 }
 
 Engine::~Engine() {

@@ -45,6 +45,13 @@ class CudaError : public std::runtime_error {
 
 class Engine;
 
+// The ChaCha20 key and nonce of the engine's random stream (RandomNumberGenerator,
+// random_number_generator.cpp:9-55); the block counter is kept by the engine.
+struct RngState {
+  uint32_t seed[8];
+  uint32_t nonce[2];
+};
+
 // One HBM-resident object (key, ciphertext or plaintext).
 struct Data {
   Engine *engine = nullptr;
@@ -119,6 +126,21 @@ class Engine {
                                bool include_special = false);
   void decode(const Data &pt, double *re, double *im);
 
+  // Randomness and keys (core_key.cpp, core.cpp:35-200).  seed: 8 words and a
+  // 2-byte nonce (null: from the system random device), block counter reset.
+  void seed(const uint32_t *seed_words, const uint8_t *nonce);
+  unsigned long long random_counter() const { return rng_counter_; }
+  std::unique_ptr<Data> create_secret_key(int level);
+  std::unique_ptr<Data> create_secret_key(const int64_t *secret, int count, int level);
+  std::unique_ptr<Data> create_sparse_secret_key(int hamming_weight, int level);
+  std::unique_ptr<Data> create_public_key(const Data &sk, int level);
+  std::unique_ptr<Data> create_relinearization_key(const Data &sk, int level);
+  std::unique_ptr<Data> create_fixed_rotation_key(const Data &sk, int delta, int level);
+  std::vector<std::unique_ptr<Data>> create_rotation_keys(const Data &sk, int level);
+  std::unique_ptr<Data> create_conjugation_key(const Data &sk, int level);
+  std::unique_ptr<Data> encrypt(const Data &pt, const Data &key);  // public or secret key
+  std::unique_ptr<Data> decrypt(const Data &ct, const Data &sk);
+
   void ntt_limbs(int64_t *limbs, int moduli_id, int chains, int polys, long long stride,
                  bool inverse);
 
@@ -139,6 +161,21 @@ class Engine {
   PrimeTables tables_{};
   KeySwitchTables ks_{};
   std::map<std::pair<int, int>, DevicePartitions> partition_cache_;
+  RngState rng_{};
+  unsigned long long rng_counter_ = 0;
+  bool cdt_uploaded_ = false;
+  void ensure_rng_tables();
+  void draw_uniform(int64_t *out, long long row_stride, int rows, int prime_base, uint64_t fixed_max,
+                    int64_t shift);
+  void draw_gaussian(int64_t *out);
+  void tile(const int64_t *chain, int limbs, int prime_base, int64_t *y, long long y_stride);
+  void pointwise(int op, int limbs, int prime_base, const int64_t *a, const int64_t *b,
+                 const int64_t *constants, int64_t *y);
+  void ntt_in_place(int64_t *x, int limbs, int prime_base, long long stride, int polys);
+  void intt_in_place(int64_t *x, int limbs, int prime_base, long long stride, int polys);
+  std::unique_ptr<Data> create_key_switching_key(const Data &from, const Data &to, int level,
+                                                 int type);
+  std::unique_ptr<Data> rotated_secret_key(const Data &sk, int ntt_delta);
   std::map<int, int32_t *> signed_perm_cache_;  // delta -> signed permutation [N]
   std::map<int, int32_t *> ntt_perm_cache_;     // delta -> NTT-form gather indices [N]
   const int32_t *device_signed_permutation(int delta);

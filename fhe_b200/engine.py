@@ -270,6 +270,54 @@ class Engine:
                                      im.ctypes.data_as(_lib._f64p) if im is not None else None))
         return re + 1j * im if complex_output else re
 
+    # ------------------------------------------------------ keys, encryption --
+    def seed(self, seed_words=None, nonce=None) -> None:
+        """Reseed the engine's ChaCha20 stream (8 words, 2 nonce bytes; None: random)."""
+        sw = (ctypes.c_uint32 * 8)(*seed_words) if seed_words is not None else None
+        nn = (ctypes.c_uint8 * 2)(*nonce) if nonce is not None else None
+        check(_lib.load().fhe_engine_seed(self._h, sw, nn))
+
+    def _make(self, fn, *args) -> Data:
+        h = ctypes.c_void_p()
+        check(getattr(_lib.load(), fn)(self._h, *args, ctypes.byref(h)))
+        return Data(self, h)
+
+    def create_secret_key(self, level: int = -1, secret=None) -> Data:
+        if secret is None:
+            return self._make("fhe_create_secret_key", level)
+        s = np.ascontiguousarray(secret, dtype=np.int64)
+        return self._make("fhe_create_secret_key_from", s.ctypes.data_as(_lib._i64p), s.size, level)
+
+    def create_sparse_secret_key(self, hamming_weight: int = 128, level: int = -1) -> Data:
+        return self._make("fhe_create_sparse_secret_key", hamming_weight, level)
+
+    def create_public_key(self, secret_key: Data, level: int = -1) -> Data:
+        return self._make("fhe_create_public_key", secret_key.handle, level)
+
+    def create_relinearization_key(self, secret_key: Data, level: int = -1) -> Data:
+        return self._make("fhe_create_relinearization_key", secret_key.handle, level)
+
+    def create_fixed_rotation_key(self, secret_key: Data, delta: int, level: int = -1,
+                                  normalize_by_slot_count: bool = True) -> Data:
+        return self._make("fhe_create_fixed_rotation_key", secret_key.handle, delta, level,
+                          int(normalize_by_slot_count))
+
+    def create_rotation_key(self, secret_key: Data, level: int = -1) -> list:
+        arr = (ctypes.c_void_p * 64)()
+        count = ctypes.c_int()
+        check(_lib.load().fhe_create_rotation_keys(self._h, secret_key.handle, level, arr, 64,
+                                                   ctypes.byref(count)))
+        return [Data(self, ctypes.c_void_p(arr[i])) for i in range(count.value)]
+
+    def create_conjugation_key(self, secret_key: Data, level: int = -1) -> Data:
+        return self._make("fhe_create_conjugation_key", secret_key.handle, level)
+
+    def encrypt(self, plaintext: Data, key: Data) -> Data:
+        return self._call("fhe_encrypt", plaintext, key)
+
+    def decrypt(self, ciphertext: Data, secret_key: Data) -> Data:
+        return self._call("fhe_decrypt", ciphertext, secret_key)
+
     def switch_key(self, ct: Data, key_switching_key: Data) -> Data:
         return self._call("fhe_switch_key", ct, key_switching_key)
 

@@ -236,6 +236,52 @@ int fhe_encode(fhe_engine *engine, const double *re, const double *im, int count
  * im unless NULL).  CRT reconstruction, skew, FFT and permutation run on the device. */
 int fhe_decode(fhe_engine *engine, const fhe_data *pt, double *re, double *im);
 
+/* ---- randomness, keys, encryption ------------------------------------------------ */
+
+/* RandomNumberGenerator(1, N, seed, nonce) (src/random/random_number_generator.cpp:9-55)
+ * for the engine's ChaCha20 stream: 8 seed words and 2 nonce bytes; NULL draws them
+ * from the system random device.  The block counter restarts at zero.  With the
+ * reference engine reseeded the same way, keys and ciphertexts made afterwards by
+ * the same sequence of calls are bit-identical. */
+int fhe_engine_seed(fhe_engine *engine, const uint32_t *seed, const uint8_t *nonce);
+/* CKKSEngine::create_secret_key([level]) (engine.h:23-24, core_key.cpp:9-28);
+ * level -1: the maximum level. */
+int fhe_create_secret_key(fhe_engine *engine, int level, fhe_data **out);
+/* create_secret_key(std::vector<int64_t>&, level) (engine.h:25-26, core_key.cpp:30-50):
+ * `count` signed coefficients, zero-padded to N. */
+int fhe_create_secret_key_from(fhe_engine *engine, const int64_t *secret, int count, int level,
+                               fhe_data **out);
+/* create_sparse_secret_key (engine.cpp:41-48, core_key.cpp:52-77): ternary with
+ * `hamming_weight` nonzero coefficients (the engine's default is 128). */
+int fhe_create_sparse_secret_key(fhe_engine *engine, int hamming_weight, int level,
+                                 fhe_data **out);
+/* create_public_key(sk[, level]) (engine.h:27-28, core_key.cpp:79-109). */
+int fhe_create_public_key(fhe_engine *engine, const fhe_data *secret_key, int level,
+                          fhe_data **out);
+/* create_relinearization_key(sk[, level]) (engine.h:33-35, core_key.cpp:168-190);
+ * level -1: the maximum key-switching level. */
+int fhe_create_relinearization_key(fhe_engine *engine, const fhe_data *secret_key, int level,
+                                   fhe_data **out);
+/* create_fixed_rotation_key(sk, delta[, level, normalize_by_slot_count]) (engine.h:37-42,
+ * engine.cpp:98-124, core_key.cpp:229-242). */
+int fhe_create_fixed_rotation_key(fhe_engine *engine, const fhe_data *secret_key, int delta,
+                                  int level, int normalize_by_slot_count, fhe_data **out);
+/* create_rotation_key(sk[, level]) (engine.h:44-45, core_key.cpp:258-268): one fixed
+ * rotation key per power of two below N/2, written to keys[0..*count). */
+int fhe_create_rotation_keys(fhe_engine *engine, const fhe_data *secret_key, int level,
+                             fhe_data **keys, int capacity, int *count);
+/* create_conjugation_key(sk[, level]) (engine.h:30-31, core_key.cpp:244-256). */
+int fhe_create_conjugation_key(fhe_engine *engine, const fhe_data *secret_key, int level,
+                               fhe_data **out);
+/* CKKSCore::encrypt(UnitPlaintext*, PublicKey* | SecretKey*) (core.cpp:35-122), as
+ * CKKSEngine::encrypt_unit uses it after encoding (engine_encrypt.cpp:104-112). */
+int fhe_encrypt(fhe_engine *engine, const fhe_data *plaintext, const fhe_data *key,
+                fhe_data **out);
+/* CKKSEngine::decrypt_to_unit_plaintext (engine_decrypt.cpp:99-126): a plaintext in
+ * coefficient form (fhe_decode gives the slots). */
+int fhe_decrypt(fhe_engine *engine, const fhe_data *ciphertext, const fhe_data *secret_key,
+                fhe_data **out);
+
 /* CKKSCore::switch_key (core.h, core.cpp:1058-1083): c0 + KS(c1) with a key
  * switching key (FHE_KEY_SWITCHING_KEY); NTT-form input is brought to coefficient
  * form first. */

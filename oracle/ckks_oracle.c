@@ -1385,3 +1385,81 @@ void oracle_decode_plaintext(const oracle_ctx *c, const int64_t *x, int mid, int
   oracle_decode(c, cur, mid, limbs, log_slot, s, re, im);
   free(cur);
 }
+
+/* ---------------------------------------------------------------- random -- */
+
+#define ROTL32(x, s) (((x) << (s)) | ((x) >> (32 - (s))))
+#define QR_(a, b, c, d)              \
+  x[a] += x[b];                      \
+  x[d] = ROTL32(x[d] ^ x[a], 16);    \
+  x[c] += x[d];                      \
+  x[b] = ROTL32(x[b] ^ x[c], 12);    \
+  x[a] += x[b];                      \
+  x[d] = ROTL32(x[d] ^ x[a], 8);     \
+  x[c] += x[d];                      \
+  x[b] = ROTL32(x[b] ^ x[c], 7)
+
+/* chacha20 (random.cpp:76-92) for the state (constants, seed[8], counter, nonce[2]). */
+void oracle_chacha_block(const uint32_t *seed, const uint32_t *nonce, uint64_t counter,
+                         uint32_t *out) {
+  uint32_t in[16] = {1634760805u, 857760878u, 2036477234u, 1797285236u};
+  for (int i = 0; i < 8; i++) in[4 + i] = seed[i];
+  in[12] = (uint32_t)counter;
+  in[13] = (uint32_t)(counter >> 32);
+  in[14] = nonce[0];
+  in[15] = nonce[1];
+  uint32_t x[16];
+  memcpy(x, in, sizeof x);
+  for (int r = 0; r < 10; r++) {
+    QR_(0, 4, 8, 12);
+    QR_(1, 5, 9, 13);
+    QR_(2, 6, 10, 14);
+    QR_(3, 7, 11, 15);
+    QR_(0, 5, 10, 15);
+    QR_(1, 6, 11, 12);
+    QR_(2, 7, 8, 13);
+    QR_(3, 4, 9, 14);
+  }
+  for (int i = 0; i < 16; i++) out[i] = x[i] + in[i];
+}
+#undef QR_
+#undef ROTL32
+
+/* rand_int (random.cpp:94-131): count samples from blocks counter0, counter0+1, ... */
+void oracle_rand_int(const uint32_t *seed, const uint32_t *nonce, uint64_t counter0, int count,
+                     uint64_t max_value, int64_t shift, int64_t *out) {
+  uint32_t w[16];
+  for (int i = 0; i < count; i++) {
+    if (i % 4 == 0) oracle_chacha_block(seed, nonce, counter0 + (uint64_t)(i / 4), w);
+    const uint32_t *l = w + 4 * (i % 4);
+    const uint64_t x_low = ((uint64_t)l[0] << 32) | l[1];
+    const uint64_t x_high = ((uint64_t)l[2] << 32) | l[3];
+    const unsigned __int128 t =
+        (unsigned __int128)max_value * x_high + (uint64_t)(((unsigned __int128)max_value * x_low) >> 64);
+    out[i] = (int64_t)(uint64_t)(t >> 64) + shift;
+  }
+}
+
+/* discrete_gaussian (random.cpp:133-170) with the CDT tree (low words [size],
+ * then high words [size]) of depth `depth`. */
+void oracle_discrete_gaussian(const uint32_t *seed, const uint32_t *nonce, uint64_t counter0,
+                              int count, const uint64_t *tree, int size, int depth, int64_t *out) {
+  uint32_t w[16];
+  for (int i = 0; i < count; i++) {
+    if (i % 4 == 0) oracle_chacha_block(seed, nonce, counter0 + (uint64_t)(i / 4), w);
+    const uint32_t *l = w + 4 * (i % 4);
+    const uint64_t x_low = ((uint64_t)l[0] << 32) | l[1];
+    uint64_t x_high = ((uint64_t)l[2] << 32) | l[3];
+    const int64_t sign = (int64_t)(x_high & 1);
+    x_high >>= 1;
+    int jump = 1, current = 0, counter = 0;
+    for (int d = 0; d < depth; d++) {
+      const uint64_t th = tree[counter + current + size], tl = tree[counter + current];
+      const int ge = (x_high > th) || (x_high == th && x_low >= tl);
+      current = 2 * current + ge;
+      counter += jump;
+      jump *= 2;
+    }
+    out[i] = (sign * 2 - 1) * (int64_t)current;
+  }
+}

@@ -130,6 +130,14 @@ void oracle_decode_plaintext(const oracle_ctx *ctx, const int64_t *x, int moduli
                              const long double *scale, double engine_scale, double *re,
                              double *im);
 
+/* ChaCha20 stream and samplers (random.cpp:76-170). */
+void oracle_chacha_block(const uint32_t *seed, const uint32_t *nonce, uint64_t counter,
+                         uint32_t *out);
+void oracle_rand_int(const uint32_t *seed, const uint32_t *nonce, uint64_t counter0, int count,
+                     uint64_t max_value, int64_t shift, int64_t *out);
+void oracle_discrete_gaussian(const uint32_t *seed, const uint32_t *nonce, uint64_t counter0,
+                              int count, const uint64_t *tree, int size, int depth, int64_t *out);
+
 #ifdef __cplusplus
 }
 #endif

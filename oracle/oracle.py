@@ -101,6 +101,15 @@ def lib():
         L.oracle_decode_plaintext.restype = None
         L.oracle_decode_plaintext.argtypes = [ctypes.c_void_p, _i64p, ctypes.c_int, ctypes.c_int,
                                               ctypes.c_void_p, ctypes.c_double, _f64, _f64]
+        _u32p = ctypes.POINTER(ctypes.c_uint32)
+        L.oracle_chacha_block.restype = None
+        L.oracle_chacha_block.argtypes = [_u32p, _u32p, ctypes.c_uint64, _u32p]
+        L.oracle_rand_int.restype = None
+        L.oracle_rand_int.argtypes = [_u32p, _u32p, ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64,
+                                      ctypes.c_int64, _i64p]
+        L.oracle_discrete_gaussian.restype = None
+        L.oracle_discrete_gaussian.argtypes = [_u32p, _u32p, ctypes.c_uint64, ctypes.c_int, _u64p,
+                                               ctypes.c_int, ctypes.c_int, _i64p]
         for name in ("oracle_rotate_plain", "oracle_rotate_plain_ntt"):
             f = getattr(L, name)
             f.restype = None
@@ -158,6 +167,32 @@ def ntt_permutation(n: int, delta: int):
     perm = np.empty(n, dtype=np.int32)
     lib().oracle_ntt_permutation(_p(perm, _i32p), n, delta)
     return perm
+
+
+def _u32(values):
+    return (ctypes.c_uint32 * len(values))(*values)
+
+
+def chacha_block(seed, nonce, counter: int):
+    out = (ctypes.c_uint32 * 16)()
+    lib().oracle_chacha_block(_u32(seed), _u32(nonce), counter, out)
+    return list(out)
+
+
+def rand_int(seed, nonce, counter0: int, count: int, max_value: int, shift: int = 0):
+    out = np.empty(count, dtype=np.int64)
+    lib().oracle_rand_int(_u32(seed), _u32(nonce), counter0, count, max_value, shift, _p(out))
+    return out
+
+
+def discrete_gaussian(seed, nonce, counter0: int, count: int, tree):
+    t = np.ascontiguousarray(np.asarray(tree, dtype=np.uint64))
+    size = len(t) // 2
+    depth = size.bit_length()
+    out = np.empty(count, dtype=np.int64)
+    lib().oracle_discrete_gaussian(_u32(seed), _u32(nonce), counter0, count, _p(t, _u64p), size,
+                                   depth, _p(out))
+    return out
 
 
 class Context:

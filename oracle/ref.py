@@ -72,6 +72,7 @@ def lib():
             "ref_engine_conjugate": (vp, [vp, vp, vp]),
             "ref_engine_level_down": (vp, [vp, vp, ctypes.c_int]),
             "ref_last_error": (ctypes.c_char_p, []),
+            "ref_cdt_tree": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]),
             "ref_engine_decode_real": (ctypes.c_int, [vp, vp, ctypes.POINTER(ctypes.c_double)]),
             "ref_deviations": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
             "ref_engine_rotate_plain": (vp, [vp, vp, ctypes.c_int]),
@@ -310,3 +311,10 @@ def bench_mult_relin_rescale(log_n, special_prime_count, level, threads, warmup,
     med = lib().ref_bench_mult_relin_rescale(log_n, special_prime_count, level, threads, warmup,
                                              steps, times)
     return med, list(times)[:steps]
+
+
+def cdt_tree():
+    """The reference sampler's CDT tree words."""
+    out = (ctypes.c_uint64 * 256)()
+    n = lib().ref_cdt_tree(out, 256)
+    return [int(out[i]) for i in range(n)]

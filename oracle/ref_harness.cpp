@@ -25,6 +25,7 @@
 #include "arithmetic/prime.h"
 #include "ckks/core.h"
 #include "ckks/engine.h"
+#include "random/gaussian_sampler.h"
 #include "operation/ntt.h"
 #include "montgomery/unit.h"
 #undef private
@@ -117,6 +118,13 @@ Handle *wrap(int kind, Data *data, void *owner) {
 extern "C" {
 
 const char *ref_last_error() { return g_ref_error.c_str(); }
+
+// The discrete-Gaussian CDT tree (sigma 3.2, 128 bits) the sampler walks.
+int ref_cdt_tree(uint64_t *out, int capacity) {
+  GaussianSamplingTree tree;
+  for (int i = 0; i < tree.data_size_ && i < capacity; i++) out[i] = tree.data_[i];
+  return tree.data_size_;
+}
 
 // The double deviations of the precomputed tables, indexed by level.
 int ref_deviations(void *e, double *out, int capacity) {

@@ -66,6 +66,24 @@ def parse_ntt_kats():
     return kats
 
 
+def parse_random_kats():
+    """test/random/random.cpp: ChaCha20 blocks and the rand_int / discrete_gaussian
+    outputs for the test state (seed words 1..8, nonce 9, 10, counter 0), plus the
+    sampler's CDT tree literal from src/random/gaussian_sampler.cpp."""
+    text = open(os.path.join(REF, "test/random/random.cpp")).read()
+    blocks = re.search(r"expected_chacha20\[4\]\[16\]\{(.*?)\};", text, re.S).group(1)
+    chacha = [_ints(b) for b in re.findall(r"\{([^{}]*)\}", blocks)]
+    arrays = {m.group(1): _ints(m.group(2))
+              for m in re.finditer(r"int64_t\s+(expected_\w+)\[\d+\]\{([^}]*)\}", text)}
+    sampler = open(os.path.join(REF, "src/random/gaussian_sampler.cpp")).read()
+    tree = re.search(r"tree_128_3_2\[\d+\]\{(.*?)\};", sampler, re.S).group(1)
+    tree_words = [int(v.strip().rstrip("u")) for v in tree.replace("\n", " ").split(",") if v.strip()]
+    return dict(seed=[1, 2, 3, 4, 5, 6, 7, 8], nonce=[9, 10], chacha20=chacha,
+                rand_int_10=arrays["expected_rand_int"],
+                rand_int_10_shift_10=arrays["expected_rand_int_shifted"],
+                discrete_gaussian=arrays["expected_discrete_gaussian"], cdt_tree=tree_words)
+
+
 def parse_precomputed_kats():
     text = open(os.path.join(REF, "test/ckks/precomputed/default.cpp")).read()
     out = {}
@@ -196,17 +214,69 @@ def codec_cases():
     return cases
 
 
+KEYGEN_TIERS = ["pebble", "iron", "bronze", "silver", "bootstrap_gold"]
+KEYGEN_SEED = (11, 22, 33, 44, 55, 66, 77, 88)
+KEYGEN_NONCE = (5, 9)
+
+
+def keygen_cases():
+    """Keys, encryptions and decryptions through the reference's engine after
+    reseeding its ChaCha20 stream; the calls run in this order, so each output
+    depends on the stream position the previous calls left."""
+    from oracle import ref
+
+    cases = []
+    for tier in KEYGEN_TIERS:
+        log_n, K, preset = TIERS[tier]
+        e = ref.Engine(log_n=log_n, special_prime_count=K, preset=preset)
+        e.seed(KEYGEN_SEED, KEYGEN_NONCE)
+        out = {}
+        sk = e.create_secret_key()
+        out["secret_key"] = sk.limbs()
+        pk = e.create_public_key(sk)
+        out["public_key"] = pk.limbs()
+        rk = e.create_relinearization_key(sk)
+        out["relinearization_key"] = rk.limbs()
+        fk = e.create_fixed_rotation_key(sk, 3)
+        out["fixed_rotation_key_3"] = fk.limbs()
+        ck = e.create_conjugation_key(sk)
+        out["conjugation_key"] = ck.limbs()
+        vals = codec_values(7000 + log_n, e.slot_count, True)
+        level = e.max_level
+        pt = e.encode(vals, level)
+        out["plaintext"] = pt.limbs()
+        ct_pk = e.encrypt(pt, pk)
+        out["encrypt_public"] = ct_pk.limbs()
+        ct_sk = e.encrypt(pt, sk)
+        out["encrypt_secret"] = ct_sk.limbs()
+        dec = e.decrypt(ct_pk, sk)
+        out["decrypt_public"] = dec.limbs()
+        slots = e.decode(dec)
+        cases.append(dict(tier=tier, log_n=log_n, special_prime_count=K, preset=preset,
+                          seed=list(KEYGEN_SEED), nonce=list(KEYGEN_NONCE), values_seed=7000 + log_n,
+                          level=level, moduli=[int(v) for v in e.tables()["q"]],
+                          digests={k: digest(v) for k, v in out.items()},
+                          decoded=digest_doubles(slots),
+                          max_error=float(np.max(np.abs(slots - vals)))))
+    return cases
+
+
 def main():
     with open(os.path.join(HERE, "ntt_kat.json"), "w") as f:
         json.dump(parse_ntt_kats(), f, indent=1)
     with open(os.path.join(HERE, "precomputed_kat.json"), "w") as f:
         json.dump(parse_precomputed_kats(), f, indent=1)
+    with open(os.path.join(HERE, "random_kat.json"), "w") as f:
+        json.dump(parse_random_kats(), f, indent=1)
     cases = reference_ops()  # computed before the file is opened: a failure keeps the old one
     with open(os.path.join(HERE, "ref_ops.json"), "w") as f:
         json.dump(cases, f, indent=1)
     codec = codec_cases()
     with open(os.path.join(HERE, "codec.json"), "w") as f:
         json.dump(codec, f, indent=1)
+    keygen = keygen_cases()
+    with open(os.path.join(HERE, "keygen.json"), "w") as f:
+        json.dump(keygen, f, indent=1)
 
 
 if __name__ == "__main__":

@@ -1,5 +1,7 @@
 """Pin the CPU oracle: the reference's own known-answer tests, recorded reference
 outputs on seeded inputs, and (where it is built) the reference library itself."""
+import os
+
 import numpy as np
 import pytest
 
@@ -191,3 +193,26 @@ def test_oracle_codec_matches_recorded_reference(case):
     dec = ctx.decode_plaintext(limbs[0], case["moduli_id"], log_slot, ckks_scale,
                                case["scale_bits"], complex_output=complex_values)
     assert digest_doubles(dec) == case["decode"]
+
+
+def test_oracle_random_stream_matches_known_answers():
+    """test/random/random.cpp: ChaCha20 blocks 0-3, rand_int (max 10, shift 0 and 10)
+    and discrete_gaussian outputs of the test state."""
+    kat = load_golden("random_kat.json")
+    seed, nonce = kat["seed"], kat["nonce"]
+    for counter, block in enumerate(kat["chacha20"]):
+        assert oracle.chacha_block(seed, nonce, counter) == block
+    assert oracle.rand_int(seed, nonce, 0, 32, 10).tolist() == kat["rand_int_10"]
+    assert oracle.rand_int(seed, nonce, 0, 32, 10, 10).tolist() == kat["rand_int_10_shift_10"]
+    got = oracle.discrete_gaussian(seed, nonce, 0, 32, kat["cdt_tree"])
+    assert got.tolist() == kat["discrete_gaussian"]
+
+
+def test_engine_cdt_table_is_the_reference_tree():
+    """fhe_b200/csrc/cdt_table.inc holds the tree literal of gaussian_sampler.cpp."""
+    import re
+
+    text = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                             "fhe_b200", "csrc", "cdt_table.inc")).read()
+    words = [int(w) for w in re.findall(r"(\d+)ULL", text)]
+    assert words == load_golden("random_kat.json")["cdt_tree"]
