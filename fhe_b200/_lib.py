@@ -89,6 +89,18 @@ SIGNATURES = {
     "fhe_conjugate_plaintext": (_i, [_vp, _vp, _pp]),
     "fhe_switch_key": (_i, [_vp, _vp, _vp, _pp]),
     "fhe_encode": (_i, [_vp, _f64p, _f64p, _i, _i, _i, _pp]),
+    "fhe_add": (_i, [_vp, _vp, _vp, _pp]),
+    "fhe_subtract": (_i, [_vp, _vp, _vp, _pp]),
+    "fhe_add_plaintext": (_i, [_vp, _vp, _vp, _pp]),
+    "fhe_subtract_plaintext": (_i, [_vp, _vp, _vp, _pp]),
+    "fhe_subtract_from_plaintext": (_i, [_vp, _vp, _vp, _pp]),
+    "fhe_multiply_plaintext": (_i, [_vp, _vp, _vp, _pp]),
+    "fhe_add_scalar": (_i, [_vp, _vp, ctypes.c_double, _pp]),
+    "fhe_subtract_scalar": (_i, [_vp, _vp, ctypes.c_double, _pp]),
+    "fhe_multiply_scalar": (_i, [_vp, _vp, ctypes.c_double, _pp]),
+    "fhe_multiply_integer": (_i, [_vp, _vp, ctypes.c_longlong, _pp]),
+    "fhe_negate": (_i, [_vp, _vp, _pp]),
+    "fhe_square": (_i, [_vp, _vp, _vp, _pp]),
     "fhe_engine_seed": (_i, [_vp, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint8)]),
     "fhe_create_secret_key": (_i, [_vp, _i, _pp]),
     "fhe_create_secret_key_from": (_i, [_vp, _i64p, _i, _i, _pp]),

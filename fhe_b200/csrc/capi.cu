@@ -565,3 +565,66 @@ int fhe_decrypt(fhe_engine *engine, const fhe_data *ct, const fhe_data *sk, fhe_
 }
 
 }  // extern "C"
+
+extern "C" {
+
+#define FHE_BINARY_OP(name, call)                                                      \
+  int name(fhe_engine *engine, const fhe_data *a, const fhe_data *b, fhe_data **out) { \
+    REQUIRE_HANDLE(engine);                                                            \
+    REQUIRE_HANDLE(a);                                                                 \
+    REQUIRE_HANDLE(b);                                                                 \
+    REQUIRE_OUT(out);                                                                  \
+    *out = nullptr;                                                                    \
+    return guarded([&] {                                                               \
+      auto &e = *engine->impl;                                                         \
+      const Data &x = live(engine, a);                                                 \
+      const Data &y = live(engine, b);                                                 \
+      *out = wrap(call);                                                               \
+    });                                                                                \
+  }
+FHE_BINARY_OP(fhe_add, e.add(x, y))
+FHE_BINARY_OP(fhe_subtract, e.subtract(x, y))
+FHE_BINARY_OP(fhe_add_plaintext, e.add_plain(x, y))
+FHE_BINARY_OP(fhe_subtract_plaintext, e.subtract_plain(x, y))
+FHE_BINARY_OP(fhe_subtract_from_plaintext, e.subtract_from_plain(x, y))
+FHE_BINARY_OP(fhe_multiply_plaintext, e.multiply_plain(x, y))
+#undef FHE_BINARY_OP
+
+#define FHE_SCALAR_OP(name, type, call)                                            \
+  int name(fhe_engine *engine, const fhe_data *a, type value, fhe_data **out) {    \
+    REQUIRE_HANDLE(engine);                                                        \
+    REQUIRE_HANDLE(a);                                                             \
+    REQUIRE_OUT(out);                                                              \
+    *out = nullptr;                                                                \
+    return guarded([&] {                                                           \
+      auto &e = *engine->impl;                                                     \
+      const Data &x = live(engine, a);                                             \
+      *out = wrap(call);                                                           \
+    });                                                                            \
+  }
+FHE_SCALAR_OP(fhe_add_scalar, double, e.add_scalar(x, value))
+FHE_SCALAR_OP(fhe_subtract_scalar, double, e.subtract_scalar(x, value))
+FHE_SCALAR_OP(fhe_multiply_scalar, double, e.multiply_scalar(x, value))
+FHE_SCALAR_OP(fhe_multiply_integer, long long, e.multiply_integer(x, value))
+#undef FHE_SCALAR_OP
+
+int fhe_negate(fhe_engine *engine, const fhe_data *ct, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(ct);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] { *out = wrap(engine->impl->negate(live(engine, ct))); });
+}
+
+int fhe_square(fhe_engine *engine, const fhe_data *ct, const fhe_data *rk, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(ct);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] {
+    const Data *key = rk ? &live(engine, rk) : nullptr;
+    *out = wrap(engine->impl->square(live(engine, ct), key));
+  });
+}
+
+}  // extern "C"

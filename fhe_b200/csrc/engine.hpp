@@ -45,6 +45,18 @@ class CudaError : public std::runtime_error {
 
 class Engine;
 
+// Element-wise operations of Engine::pointwise over [limbs][N] views.
+enum PointwiseOp : int {
+  kOpMult = 0,            // mont_mult(a, b)
+  kOpAddReduce = 1,       // mont_add_reduce_2q_to_q(a, b)
+  kOpSubReduce = 2,       // mont_sub_reduce_2q_to_q: a - b
+  kOpReduce = 3,          // reduce_2q_to_q(a)
+  kOpEnter = 4,           // mont_enter(a, c[limb])
+  kOpNegate = 5,          // negate_make_unsigned: q - a
+  kOpAddScalarFirst = 6,  // add_scalar (c[limb] on coefficient 0) then reduce_2q_to_q
+  kOpEnterReduce = 7,     // mont_enter(a, c[limb]) then reduce_2q_to_q
+};
+
 // The ChaCha20 key and nonce of the engine's random stream (RandomNumberGenerator,
 // random_number_generator.cpp:9-55); the block counter is kept by the engine.
 struct RngState {
@@ -141,6 +153,22 @@ class Engine {
   std::unique_ptr<Data> encrypt(const Data &pt, const Data &key);  // public or secret key
   std::unique_ptr<Data> decrypt(const Data &ct, const Data &sk);
 
+  // Ciphertext arithmetic (engine_add.cpp, engine_subtract.cpp, engine_multiply.cpp,
+  // engine_negate.cpp): operands are brought to a common level, rescale state and
+  // form first (match_form / prepare_for_multiply), then the core operation.
+  std::unique_ptr<Data> add(const Data &a, const Data &b);
+  std::unique_ptr<Data> subtract(const Data &a, const Data &b);
+  std::unique_ptr<Data> add_plain(const Data &ct, const Data &pt);
+  std::unique_ptr<Data> subtract_plain(const Data &ct, const Data &pt);
+  std::unique_ptr<Data> subtract_from_plain(const Data &pt, const Data &ct);
+  std::unique_ptr<Data> add_scalar(const Data &ct, double value);
+  std::unique_ptr<Data> subtract_scalar(const Data &ct, double value);
+  std::unique_ptr<Data> multiply_plain(const Data &ct, const Data &pt);
+  std::unique_ptr<Data> multiply_scalar(const Data &ct, double value);
+  std::unique_ptr<Data> multiply_integer(const Data &ct, int64_t value);
+  std::unique_ptr<Data> negate(const Data &ct);
+  std::unique_ptr<Data> square(const Data &ct, const Data *rk);
+
   void ntt_limbs(int64_t *limbs, int moduli_id, int chains, int polys, long long stride,
                  bool inverse);
 
@@ -176,6 +204,12 @@ class Engine {
   std::unique_ptr<Data> create_key_switching_key(const Data &from, const Data &to, int level,
                                                  int type);
   std::unique_ptr<Data> rotated_secret_key(const Data &sk, int ntt_delta);
+  std::unique_ptr<Data> rescale_any(const Data &text);  // CKKSEngine::rescale_
+  struct Matched;
+  Matched match_texts(const Data &a, const Data &b, bool b_is_plain);
+  std::vector<int64_t> add_multiplier(double value, int level) const;
+  std::vector<int64_t> mult_multiplier(double value, int level) const;
+  int64_t *upload_constants(const std::vector<int64_t> &v);
   std::map<int, int32_t *> signed_perm_cache_;  // delta -> signed permutation [N]
   std::map<int, int32_t *> ntt_perm_cache_;     // delta -> NTT-form gather indices [N]
   const int32_t *device_signed_permutation(int delta);

@@ -157,14 +157,6 @@ __global__ void tile_kernel(PrimeTables t, int log_n, int limbs, int prime_base,
   y[j * y_stride + c] = v < 0 ? v + q : guard(v, q);
 }
 
-enum PointwiseOp : int {
-  kOpMult = 0,       // mont_mult
-  kOpAddReduce = 1,  // mont_add_reduce_2q_to_q
-  kOpSubReduce = 2,  // mont_sub_reduce_2q_to_q: a - b
-  kOpReduce = 3,     // reduce_2q_to_q
-  kOpEnter = 4,      // mont_enter by a per-limb constant c[j]
-};
-
 // y[j] = op(a[j], b[j]) over `limbs` limbs of N words; a, b, y are [limbs][N]
 // views (any may alias).
 __global__ void pointwise_kernel(PrimeTables t, int op, int log_n, int limbs, int prime_base,
@@ -182,6 +174,9 @@ __global__ void pointwise_kernel(PrimeTables t, int op, int log_n, int limbs, in
     case kOpSubReduce: v = guard(guard(a[i] + q2 - b[i], q2), qs); break;
     case kOpReduce: v = guard(a[i], qs); break;
     case kOpEnter: v = mont_mult(a[i], c[j], q, k); break;
+    case kOpNegate: v = qs - a[i]; break;
+    case kOpAddScalarFirst: v = guard(a[i] + ((i & ((1LL << log_n) - 1)) == 0 ? c[j] : 0), qs); break;
+    case kOpEnterReduce: v = guard(mont_mult(a[i], c[j], q, k), qs); break;
   }
   y[i] = v;
 }

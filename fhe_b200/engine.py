@@ -270,6 +270,49 @@ class Engine:
                                      im.ctypes.data_as(_lib._f64p) if im is not None else None))
         return re + 1j * im if complex_output else re
 
+    # ------------------------------------------------------------ arithmetic --
+    def add(self, a: Data, b) -> Data:
+        """add(ct, ct | pt | float)."""
+        if isinstance(b, (int, float)):
+            return self._scalar("fhe_add_scalar", a, float(b))
+        if b.info()["type"] == UNIT_PLAINTEXT:
+            return self._call("fhe_add_plaintext", a, b)
+        return self._call("fhe_add", a, b)
+
+    def subtract(self, a, b) -> Data:
+        """subtract(ct, ct | pt | float) or subtract(pt, ct)."""
+        if isinstance(b, (int, float)):
+            return self._scalar("fhe_subtract_scalar", a, float(b))
+        if a.info()["type"] == UNIT_PLAINTEXT:
+            return self._call("fhe_subtract_from_plaintext", a, b)
+        if b.info()["type"] == UNIT_PLAINTEXT:
+            return self._call("fhe_subtract_plaintext", a, b)
+        return self._call("fhe_subtract", a, b)
+
+    def multiply_plaintext(self, ct: Data, pt: Data) -> Data:
+        return self._call("fhe_multiply_plaintext", ct, pt)
+
+    def multiply_scalar(self, ct: Data, value: float) -> Data:
+        return self._scalar("fhe_multiply_scalar", ct, float(value))
+
+    def multiply_integer(self, ct: Data, value: int) -> Data:
+        return self._scalar("fhe_multiply_integer", ct, int(value))
+
+    def negate(self, ct: Data) -> Data:
+        return self._call("fhe_negate", ct)
+
+    def square(self, ct: Data, relinearization_key: Data | None = None) -> Data:
+        h = ctypes.c_void_p()
+        check(_lib.load().fhe_square(self._h, ct.handle,
+                                     relinearization_key.handle if relinearization_key else None,
+                                     ctypes.byref(h)))
+        return Data(self, h)
+
+    def _scalar(self, fn, ct: Data, value) -> Data:
+        h = ctypes.c_void_p()
+        check(getattr(_lib.load(), fn)(self._h, ct.handle, value, ctypes.byref(h)))
+        return Data(self, h)
+
     # ------------------------------------------------------ keys, encryption --
     def seed(self, seed_words=None, nonce=None) -> None:
         """Reseed the engine's ChaCha20 stream (8 words, 2 nonce bytes; None: random)."""

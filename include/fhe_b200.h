@@ -236,6 +236,37 @@ int fhe_encode(fhe_engine *engine, const double *re, const double *im, int count
  * im unless NULL).  CRT reconstruction, skew, FFT and permutation run on the device. */
 int fhe_decode(fhe_engine *engine, const fhe_data *pt, double *re, double *im);
 
+/* ---- arithmetic (engine_add.cpp, engine_subtract.cpp, engine_multiply.cpp,
+ *      engine_negate.cpp): operands are brought to a common level, rescale state and
+ *      form first, as the reference's match_form / prepare_for_multiply do ---------- */
+
+/* CKKSEngine::add / subtract(UnitCiphertext*, UnitCiphertext*) (engine.h:158-159,
+ * engine_add.cpp:82-104, engine_subtract.cpp:5-30); 2- and 3-polynomial operands. */
+int fhe_add(fhe_engine *engine, const fhe_data *a, const fhe_data *b, fhe_data **out);
+int fhe_subtract(fhe_engine *engine, const fhe_data *a, const fhe_data *b, fhe_data **out);
+/* add(ct, pt) / subtract(ct, pt) / subtract(pt, ct) (engine_add.cpp:221-234,
+ * engine_subtract.cpp:91-157). */
+int fhe_add_plaintext(fhe_engine *engine, const fhe_data *ct, const fhe_data *pt, fhe_data **out);
+int fhe_subtract_plaintext(fhe_engine *engine, const fhe_data *ct, const fhe_data *pt,
+                           fhe_data **out);
+int fhe_subtract_from_plaintext(fhe_engine *engine, const fhe_data *pt, const fhe_data *ct,
+                                fhe_data **out);
+/* multiply(ct, pt) (engine_multiply.cpp:210-227): the tensor with a plaintext. */
+int fhe_multiply_plaintext(fhe_engine *engine, const fhe_data *ct, const fhe_data *pt,
+                           fhe_data **out);
+/* add / subtract(ct, double) (engine_add.cpp:518-536, engine_subtract.cpp:319-325). */
+int fhe_add_scalar(fhe_engine *engine, const fhe_data *ct, double value, fhe_data **out);
+int fhe_subtract_scalar(fhe_engine *engine, const fhe_data *ct, double value, fhe_data **out);
+/* multiply(ct, double) with its rescale (engine_multiply.cpp:418-432) and
+ * multiply(ct, int64_t) (:443-457). */
+int fhe_multiply_scalar(fhe_engine *engine, const fhe_data *ct, double value, fhe_data **out);
+int fhe_multiply_integer(fhe_engine *engine, const fhe_data *ct, long long value, fhe_data **out);
+/* negate (engine_negate.cpp:5-12); square([relinearization key]) (engine_multiply.cpp:
+ * 86-101, 175-188; relinearization_key may be NULL). */
+int fhe_negate(fhe_engine *engine, const fhe_data *ct, fhe_data **out);
+int fhe_square(fhe_engine *engine, const fhe_data *ct, const fhe_data *relinearization_key,
+               fhe_data **out);
+
 /* ---- randomness, keys, encryption ------------------------------------------------ */
 
 /* RandomNumberGenerator(1, N, seed, nonce) (src/random/random_number_generator.cpp:9-55)

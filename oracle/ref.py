@@ -72,6 +72,8 @@ def lib():
             "ref_engine_conjugate": (vp, [vp, vp, vp]),
             "ref_engine_level_down": (vp, [vp, vp, ctypes.c_int]),
             "ref_last_error": (ctypes.c_char_p, []),
+            "ref_engine_arith": (vp, [vp, ctypes.c_int, vp, vp]),
+            "ref_engine_scalar": (vp, [vp, ctypes.c_int, vp, ctypes.c_double, ctypes.c_longlong]),
             "ref_cdt_tree": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]),
             "ref_engine_decode_real": (ctypes.c_int, [vp, vp, ctypes.POINTER(ctypes.c_double)]),
             "ref_deviations": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
@@ -262,6 +264,18 @@ class Engine:
         out = np.zeros(256, dtype=np.float64)
         n = lib().ref_deviations(self.ptr, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 256)
         return out[:n]
+
+    ARITH = dict(add=0, subtract=1, add_plain=2, subtract_plain=3, subtract_from_plain=4,
+                 multiply_plain=5, negate=6, square=7, square_relinearize=8)
+    SCALAR = dict(add_scalar=0, subtract_scalar=1, multiply_scalar=2, multiply_integer=3)
+
+    def arith(self, op, a, b=None):
+        return self._h(lib().ref_engine_arith(self.ptr, self.ARITH[op], a.ptr,
+                                              b.ptr if b is not None else None))
+
+    def scalar(self, op, a, value):
+        return self._h(lib().ref_engine_scalar(self.ptr, self.SCALAR[op], a.ptr, float(value),
+                                               int(value) if op == "multiply_integer" else 0))
 
     def level_down(self, a, level):
         return self._h(lib().ref_engine_level_down(self.ptr, a.ptr, level))

@@ -651,6 +651,56 @@ void *ref_engine_rotate_keys(void *e, void *a, void **fks, int count, int delta,
   return out;
 }
 
+// Engine arithmetic (engine_add.cpp, engine_subtract.cpp, engine_multiply.cpp,
+// engine_negate.cpp).  op: 0 add, 1 subtract, 2 add plaintext, 3 subtract plaintext,
+// 4 plaintext minus ciphertext, 5 multiply plaintext, 6 negate, 7 square, 8 square and
+// relinearize (b = key); scalar ops: 0 add, 1 subtract, 2 multiply.
+void *ref_engine_arith(void *e, int op, void *a, void *b) {
+  try {
+    auto eng = static_cast<RefEngine *>(e)->engine.get();
+    auto ct = [](void *h) { return static_cast<UnitCiphertext *>(static_cast<Handle *>(h)->data); };
+    auto pt = [](void *h) { return static_cast<UnitPlaintext *>(static_cast<Handle *>(h)->data); };
+    UnitCiphertext *r = nullptr;
+    switch (op) {
+      case 0: r = eng->add(ct(a), ct(b)); break;
+      case 1: r = eng->subtract(ct(a), ct(b)); break;
+      case 2: r = eng->add(ct(a), pt(b)); break;
+      case 3: r = eng->subtract(ct(a), pt(b)); break;
+      case 4: r = eng->subtract(pt(b), ct(a)); break;
+      case 5: r = eng->multiply(ct(a), pt(b)); break;
+      case 6: r = eng->negate(ct(a)); break;
+      case 7: r = eng->square(ct(a)); break;
+      case 8:
+        r = eng->square(ct(a), static_cast<RelinearizationKey *>(static_cast<Handle *>(b)->owner));
+        break;
+      default: return nullptr;
+    }
+    return wrap(4, r, r);
+  } catch (...) {
+    remember_error();
+    return nullptr;
+  }
+}
+
+void *ref_engine_scalar(void *e, int op, void *a, double value, long long integer) {
+  try {
+    auto eng = static_cast<RefEngine *>(e)->engine.get();
+    auto c = static_cast<UnitCiphertext *>(static_cast<Handle *>(a)->data);
+    UnitCiphertext *r = nullptr;
+    switch (op) {
+      case 0: r = eng->add(c, value); break;
+      case 1: r = eng->subtract(c, value); break;
+      case 2: r = eng->multiply(c, value); break;
+      case 3: r = eng->multiply(c, static_cast<int64_t>(integer)); break;
+      default: return nullptr;
+    }
+    return wrap(4, r, r);
+  } catch (...) {
+    remember_error();
+    return nullptr;
+  }
+}
+
 void *ref_engine_encode(void *e, const double *re, const double *im, int count,
                         int level) {
   try {

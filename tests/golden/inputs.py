@@ -90,3 +90,17 @@ def digest_doubles(a) -> str:
     """Digest of the IEEE bit patterns of a float64 / complex128 array."""
     a = np.ascontiguousarray(a)
     return hashlib.sha256(a.view(np.uint8).tobytes()).hexdigest()
+
+
+def arith_inputs(seed: int, moduli, n: int, moduli_id: int, special: int):
+    """Operands of the arithmetic cases at `moduli_id` (uniform residues): two
+    2-polynomial texts, one a level lower, a 3-polynomial text, a plaintext and a
+    relinearization key."""
+    rng = np.random.default_rng(seed + 200000)
+    chain = len(moduli) - special
+    qs = moduli[moduli_id:chain]
+    dnum = (chain - moduli_id + special - 1) // special
+    return dict(a=uniform_limbs(rng, qs, 2, n), b=uniform_limbs(rng, qs, 2, n),
+                low=uniform_limbs(rng, moduli[moduli_id + 1:chain], 2, n),
+                trio=uniform_limbs(rng, qs, 3, n), plain=uniform_limbs(rng, qs, 1, n),
+                key=uniform_limbs(rng, moduli[moduli_id:], 2 * dnum, n))

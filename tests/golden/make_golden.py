@@ -25,7 +25,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
-from inputs import ROTATION_KEY_DELTAS, codec_values, digest_doubles, key_switch_inputs, TIERS, case_inputs, digest  # noqa: E402
+from inputs import ROTATION_KEY_DELTAS, arith_inputs, codec_values, digest_doubles, key_switch_inputs, TIERS, case_inputs, digest  # noqa: E402
 
 REF = os.environ.get("FHE_REFERENCE", "/root/reference")
 
@@ -261,6 +261,68 @@ def keygen_cases():
     return cases
 
 
+ARITH_PLAN = [("pebble", 2), ("bronze", 1), ("silver", 2), ("bootstrap_gold", 3)]
+
+
+def arith_cases():
+    """Ciphertext arithmetic through the reference's engine on uniform operands.
+    Each case lists (op, operand names, flags); flags: 2 NTT form, 4 rescaled.  Every
+    call gets fresh input objects: the reference reduces some NTT-form inputs in place."""
+    from oracle import ref
+
+    plan = [
+        ("add", "a:0", "b:0"), ("add", "a:2", "low:2"), ("add", "trio:2", "a:2"),
+        ("add", "a:4", "b:0"), ("subtract", "a:0", "b:0"), ("subtract", "a:2", "trio:2"),
+        ("subtract", "trio:0", "low:0"), ("add_plain", "a:0", "plain:0"),
+        ("add_plain", "a:2", "plain:0"), ("subtract_plain", "a:2", "plain:0"),
+        ("subtract_from_plain", "a:2", "plain:0"), ("subtract_from_plain", "a:0", "plain:0"),
+        ("multiply_plain", "a:0", "plain:0"), ("multiply_plain", "a:2", "plain:2"),
+        ("negate", "a:2"), ("negate", "trio:0"), ("square", "a:0"), ("square_relinearize", "a:2"),
+        ("add_scalar", "a:0", 0.37), ("add_scalar", "a:2", -1.25), ("subtract_scalar", "b:0", 2.5),
+        ("multiply_scalar", "a:0", 0.71), ("multiply_scalar", "b:2", -2.5),
+        ("multiply_integer", "a:2", -3),
+    ]
+    cases = []
+    seed = 9000
+    for tier, mid in ARITH_PLAN:
+        log_n, K, preset = TIERS[tier]
+        e = ref.Engine(log_n=log_n, special_prime_count=K, preset=preset)
+        q = e.tables()["q"]
+        seed += 1
+        x = arith_inputs(seed, q, e.n, mid, K)
+        level = e.chains(mid) - 2
+        probe = e.encode(np.zeros(e.slot_count), level)
+        scale = probe.info()["scale"]
+        low_scale = e.encode(np.zeros(e.slot_count), level - 1).info()["scale"]
+
+        def text(spec):
+            name, flag = spec.split(":")
+            flag = int(flag)
+            m = mid + 1 if name == "low" else mid
+            kind = 5 if name == "plain" else 4
+            s = low_scale if name == "low" else scale
+            return e.text(x[name], m, flag=flag, kind=kind, scale=s)
+
+        rk = e.relin_key(x["key"], mid)
+        digests = {}
+        for step in plan:
+            op = step[0]
+            key = "|".join(str(v) for v in step)
+            if op in ref.Engine.SCALAR:
+                out = e.scalar(op, text(step[1]), step[2])
+            elif op == "square_relinearize":
+                out = e.arith(op, text(step[1]), rk)
+            elif len(step) == 2:
+                out = e.arith(op, text(step[1]))
+            else:
+                out = e.arith(op, text(step[1]), text(step[2]))
+            digests[key] = digest(out.limbs())
+        cases.append(dict(tier=tier, log_n=log_n, special_prime_count=K, preset=preset,
+                          moduli_id=mid, seed=seed, scale=scale, low_scale=low_scale,
+                          moduli=[int(v) for v in q], digests=digests))
+    return cases
+
+
 def main():
     with open(os.path.join(HERE, "ntt_kat.json"), "w") as f:
         json.dump(parse_ntt_kats(), f, indent=1)
@@ -274,6 +336,9 @@ def main():
     codec = codec_cases()
     with open(os.path.join(HERE, "codec.json"), "w") as f:
         json.dump(codec, f, indent=1)
+    arith = arith_cases()
+    with open(os.path.join(HERE, "arith.json"), "w") as f:
+        json.dump(arith, f, indent=1)
     keygen = keygen_cases()
     with open(os.path.join(HERE, "keygen.json"), "w") as f:
         json.dump(keygen, f, indent=1)
