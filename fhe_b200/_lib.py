@@ -89,6 +89,8 @@ SIGNATURES = {
     "fhe_conjugate_plaintext": (_i, [_vp, _vp, _pp]),
     "fhe_switch_key": (_i, [_vp, _vp, _vp, _pp]),
     "fhe_encode": (_i, [_vp, _f64p, _f64p, _i, _i, _i, _pp]),
+    "fhe_create_small_bootstrap_key": (_i, [_vp, _vp, _pp, _pp]),
+    "fhe_bootstrap": (_i, [_vp, _vp, _vp, _vp, ctypes.POINTER(_vp), _i, _vp, _vp, _i, _pp]),
     "fhe_add": (_i, [_vp, _vp, _vp, _pp]),
     "fhe_subtract": (_i, [_vp, _vp, _vp, _pp]),
     "fhe_add_plaintext": (_i, [_vp, _vp, _vp, _pp]),

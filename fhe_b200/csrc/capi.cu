@@ -628,3 +628,48 @@ int fhe_square(fhe_engine *engine, const fhe_data *ct, const fhe_data *rk, fhe_d
 }
 
 }  // extern "C"
+
+extern "C" {
+
+int fhe_create_small_bootstrap_key(fhe_engine *engine, const fhe_data *sk, fhe_data **to_sparse,
+                                   fhe_data **to_dense) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(sk);
+  REQUIRE_OUT(to_sparse);
+  REQUIRE_OUT(to_dense);
+  *to_sparse = nullptr;
+  *to_dense = nullptr;
+  return guarded([&] {
+    auto keys = engine->impl->create_small_bootstrap_key(live(engine, sk));
+    *to_sparse = wrap(std::move(keys.first));
+    *to_dense = wrap(std::move(keys.second));
+  });
+}
+
+int fhe_bootstrap(fhe_engine *engine, const fhe_data *ct, const fhe_data *rk, const fhe_data *ck,
+                  const fhe_data *const *rotation_keys, int rotation_key_count,
+                  const fhe_data *to_sparse, const fhe_data *to_dense, int stage_count,
+                  fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(ct);
+  REQUIRE_HANDLE(rk);
+  REQUIRE_HANDLE(ck);
+  REQUIRE_HANDLE(to_sparse);
+  REQUIRE_HANDLE(to_dense);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  if (rotation_keys == nullptr || rotation_key_count < 1) {
+    fhe_b200::set_last_error("Bootstrap Unit Ciphertext With Rotation Key: the rotation key is empty.");
+    return FHE_ERR_INVALID_ARGUMENT;
+  }
+  for (int i = 0; i < rotation_key_count; i++) REQUIRE_HANDLE(rotation_keys[i]);
+  return guarded([&] {
+    std::vector<const Data *> keys;
+    for (int i = 0; i < rotation_key_count; i++) keys.push_back(&live(engine, rotation_keys[i]));
+    *out = wrap(engine->impl->bootstrap(live(engine, ct), live(engine, rk), live(engine, ck), keys,
+                                        live(engine, to_sparse), live(engine, to_dense),
+                                        stage_count));
+  });
+}
+
+}  // extern "C"

@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <complex>
 #include <map>
 #include <memory>
 #include <set>
@@ -123,14 +124,14 @@ class Engine {
   // a set of power-of-two keys selected by the bits of `delta` (:106-139).
   std::unique_ptr<Data> rotate(const Data &ct, const Data &fixed_rotation_key);
   std::unique_ptr<Data> rotate(const Data &ct, const std::vector<const Data *> &keys, int delta,
-                               bool normalize_by_slot_count = false);
+                               bool normalize_by_slot_count = true);
   // Plaintext rotation and conjugation (no key): engine_rotate.cpp:10-24.
   std::unique_ptr<Data> rotate_plain(const Data &pt, int delta);
   std::unique_ptr<Data> conjugate_plain(const Data &pt);
   std::unique_ptr<Data> conjugate(const Data &ct, const Data &conjugation_key);
   // CKKSCore::switch_key (core.cpp:1058-1083): coefficient-form input.
   std::unique_ptr<Data> switch_key(const Data &ct, const Data &key_switching_key);
-  int normalized_delta(int delta, bool normalize_by_slot_count = false) const;
+  int normalized_delta(int delta, bool normalize_by_slot_count = true) const;  // engine.h:370
   // CKKSCore::encode (core_encode.cpp:33-150) of up to slot_count values (im null:
   // real input) at `level`; CKKSCore::decode / decode_complex_plaintext
   // (core_decode.cpp) into host arrays of slot_count doubles.
@@ -169,6 +170,20 @@ class Engine {
   std::unique_ptr<Data> negate(const Data &ct);
   std::unique_ptr<Data> square(const Data &ct, const Data *rk);
 
+  // Bootstrapping with a rotation key (engine_bootstrap.cpp:712-754) and its parts.
+  std::pair<std::unique_ptr<Data>, std::unique_ptr<Data>> create_small_bootstrap_key(const Data &sk);
+  std::unique_ptr<Data> bootstrap(const Data &ct, const Data &rk, const Data &ck,
+                                  const std::vector<const Data *> &rotation_keys,
+                                  const Data &to_sparse, const Data &to_dense, int stage_count);
+  std::unique_ptr<Data> mod_raise(const Data &ct, const Data &to_sparse, const Data &to_dense);
+  std::unique_ptr<Data> multiply_imaginary(const Data &ct, int64_t value);
+  std::unique_ptr<Data> weighted_sum(const std::vector<const Data *> &basis,
+                                     const std::vector<double> &weights);
+  std::vector<std::unique_ptr<Data>> rotate_batch(const Data &ct,
+                                                  const std::vector<const Data *> &keys,
+                                                  const std::vector<int> &deltas);
+  void add_inplace(Data &a, const Data &b);
+
   void ntt_limbs(int64_t *limbs, int moduli_id, int chains, int polys, long long stride,
                  bool inverse);
 
@@ -205,6 +220,22 @@ class Engine {
                                                  int type);
   std::unique_ptr<Data> rotated_secret_key(const Data &sk, int ntt_delta);
   std::unique_ptr<Data> rescale_any(const Data &text);  // CKKSEngine::rescale_
+  void signed_tile(const int64_t *chain, int64_t q_src, int limbs, int prime_base, int64_t *y,
+                   long long y_stride);
+  std::unique_ptr<Data> apply_butterfly(const Data &ct,
+                                        const std::vector<std::vector<std::complex<double>>> &tw,
+                                        const std::vector<const Data *> &keys, int rotate_count);
+  std::pair<std::unique_ptr<Data>, std::unique_ptr<Data>> coeff_to_slot(
+      const Data &ct, const Data &conjugation_key, const std::vector<const Data *> &keys,
+      int stage_count);
+  std::unique_ptr<Data> slot_to_coeff(const Data &real_part, const Data &imaginary_part,
+                                      const std::vector<const Data *> &keys, int stage_count);
+  std::unique_ptr<Data> chebyshev_ps(const std::vector<const Data *> &baby, const Data &giant,
+                                     const Data *rk,
+                                     const std::vector<std::vector<double>> &coefficients);
+  std::unique_ptr<Data> sine(const Data &ct, const Data &rk);
+  std::unique_ptr<Data> round_to_integer(const Data &ct, const Data &rk);
+  std::unique_ptr<Data> make_signed_tile(const Data &ct);
   struct Matched;
   Matched match_texts(const Data &a, const Data &b, bool b_is_plain);
   std::vector<int64_t> add_multiplier(double value, int level) const;

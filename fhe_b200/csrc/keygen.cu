@@ -157,6 +157,21 @@ __global__ void tile_kernel(PrimeTables t, int log_n, int limbs, int prime_base,
   y[j * y_stride + c] = v < 0 ? v + q : guard(v, q);
 }
 
+// make_signed (unit.cpp:36-42, unsigned comparison with q/2) of one chain modulo
+// q_src, then tile_unsigned_reduce_2q_to_q onto `limbs` (make_signed_tile, core.cpp:
+// 1085-1108).
+__global__ void signed_tile_kernel(PrimeTables t, int log_n, int limbs, int prime_base,
+                                   const int64_t *x, int64_t q_src, int64_t *y, long long y_stride) {
+  const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (i >= (static_cast<long long>(limbs) << log_n)) return;
+  const int j = static_cast<int>(i >> log_n);
+  const int c = static_cast<int>(i & ((1LL << log_n) - 1));
+  const int64_t v = x[c];
+  const int64_t s = static_cast<uint64_t>(v) <= static_cast<uint64_t>(q_src >> 1) ? v : v - q_src;
+  const int64_t q = static_cast<int64_t>(t.q[prime_base + j]);
+  y[j * y_stride + c] = s < 0 ? s + q : guard(s, q);
+}
+
 // y[j] = op(a[j], b[j]) over `limbs` limbs of N words; a, b, y are [limbs][N]
 // views (any may alias).
 __global__ void pointwise_kernel(PrimeTables t, int op, int log_n, int limbs, int prime_base,
@@ -227,6 +242,15 @@ void Engine::tile(const int64_t *chain, int limbs, int prime_base, int64_t *y, l
   tile_kernel<<<grid_for(static_cast<long long>(limbs) << params.log_n), kThreads, 0, stream_>>>(
       tables_, params.log_n, limbs, prime_base, chain, y, y_stride);
   check(cudaGetLastError(), "tile");
+}
+
+void Engine::signed_tile(const int64_t *chain, int64_t q_src, int limbs, int prime_base,
+                         int64_t *y, long long y_stride) {
+  note_launch();
+  signed_tile_kernel<<<grid_for(static_cast<long long>(limbs) << params.log_n), kThreads, 0,
+                       stream_>>>(tables_, params.log_n, limbs, prime_base, chain, q_src, y,
+                                  y_stride);
+  check(cudaGetLastError(), "signed tile");
 }
 
 void Engine::pointwise(int op, int limbs, int prime_base, const int64_t *a, const int64_t *b,

@@ -225,7 +225,7 @@ class Engine:
         return Data(self, h)
 
     def rotate(self, ct: Data, key, delta: int | None = None,
-               normalize_by_slot_count: bool = False) -> Data:
+               normalize_by_slot_count: bool = True) -> Data:
         """Rotate a ciphertext by one fixed rotation key, or by a list of fixed
         rotation keys (a RotationKey) and a delta; plaintexts rotate without a key."""
         if isinstance(key, (list, tuple)):
@@ -360,6 +360,25 @@ class Engine:
 
     def decrypt(self, ciphertext: Data, secret_key: Data) -> Data:
         return self._call("fhe_decrypt", ciphertext, secret_key)
+
+    # --------------------------------------------------------- bootstrapping --
+    def create_small_bootstrap_key(self, secret_key: Data):
+        """Returns (to_sparse, to_dense) key switching keys."""
+        a, b = ctypes.c_void_p(), ctypes.c_void_p()
+        check(_lib.load().fhe_create_small_bootstrap_key(self._h, secret_key.handle,
+                                                         ctypes.byref(a), ctypes.byref(b)))
+        return Data(self, a), Data(self, b)
+
+    def bootstrap(self, ct: Data, relinearization_key: Data, conjugation_key: Data,
+                  rotation_keys, small_bootstrap_key, stage_count: int = 3) -> Data:
+        arr = (ctypes.c_void_p * len(rotation_keys))(*[k.handle for k in rotation_keys])
+        to_sparse, to_dense = small_bootstrap_key
+        h = ctypes.c_void_p()
+        check(_lib.load().fhe_bootstrap(self._h, ct.handle, relinearization_key.handle,
+                                        conjugation_key.handle, arr, len(rotation_keys),
+                                        to_sparse.handle, to_dense.handle, stage_count,
+                                        ctypes.byref(h)))
+        return Data(self, h)
 
     def switch_key(self, ct: Data, key_switching_key: Data) -> Data:
         return self._call("fhe_switch_key", ct, key_switching_key)

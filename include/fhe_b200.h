@@ -313,6 +313,23 @@ int fhe_encrypt(fhe_engine *engine, const fhe_data *plaintext, const fhe_data *k
 int fhe_decrypt(fhe_engine *engine, const fhe_data *ciphertext, const fhe_data *secret_key,
                 fhe_data **out);
 
+/* ---- bootstrapping ---------------------------------------------------------------- */
+
+/* CKKSEngine::create_small_bootstrap_key (engine.h, engine.cpp:141-160): key switching
+ * keys to a sparse secret (Hamming weight 128) at level 0 and back at the maximum
+ * key-switching level.  Needs a bootstrapping preset. */
+int fhe_create_small_bootstrap_key(fhe_engine *engine, const fhe_data *secret_key,
+                                   fhe_data **to_sparse, fhe_data **to_dense);
+/* CKKSEngine::bootstrap(UnitCiphertext*, RelinearizationKey*, ConjugationKey*,
+ * RotationKey*, SmallBootstrapKey*, int stage_count) (engine_bootstrap.cpp:712-754):
+ * level down to 0, mod raise, coefficients-to-slots, EvalRound, slots-to-coefficients
+ * and the correction, on a coefficient-form ciphertext.  The rotation key is the list
+ * of fixed rotation keys fhe_create_rotation_keys made. */
+int fhe_bootstrap(fhe_engine *engine, const fhe_data *ct, const fhe_data *relinearization_key,
+                  const fhe_data *conjugation_key, const fhe_data *const *rotation_keys,
+                  int rotation_key_count, const fhe_data *to_sparse, const fhe_data *to_dense,
+                  int stage_count, fhe_data **out);
+
 /* CKKSCore::switch_key (core.h, core.cpp:1058-1083): c0 + KS(c1) with a key
  * switching key (FHE_KEY_SWITCHING_KEY); NTT-form input is brought to coefficient
  * form first. */

@@ -72,6 +72,12 @@ def lib():
             "ref_engine_conjugate": (vp, [vp, vp, vp]),
             "ref_engine_level_down": (vp, [vp, vp, ctypes.c_int]),
             "ref_last_error": (ctypes.c_char_p, []),
+            "ref_create_rotation_key": (vp, [vp, vp, ctypes.c_int]),
+            "ref_rotation_key_count": (ctypes.c_int, [vp]),
+            "ref_rotation_key_get": (vp, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+            "ref_create_small_bootstrap_key": (vp, [vp, vp]),
+            "ref_small_bootstrap_key_part": (vp, [vp, ctypes.c_int]),
+            "ref_engine_bootstrap": (vp, [vp, vp, vp, vp, vp, vp, ctypes.c_int]),
             "ref_engine_arith": (vp, [vp, ctypes.c_int, vp, vp]),
             "ref_engine_scalar": (vp, [vp, ctypes.c_int, vp, ctypes.c_double, ctypes.c_longlong]),
             "ref_cdt_tree": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]),
@@ -276,6 +282,24 @@ class Engine:
     def scalar(self, op, a, value):
         return self._h(lib().ref_engine_scalar(self.ptr, self.SCALAR[op], a.ptr, float(value),
                                                int(value) if op == "multiply_integer" else 0))
+
+    def create_rotation_key(self, sk, level=-1):
+        """Returns (owner handle, [(fixed key view, delta), ...])."""
+        owner = self._h(lib().ref_create_rotation_key(self.ptr, sk.ptr, level))
+        views = []
+        for i in range(lib().ref_rotation_key_count(owner.ptr)):
+            d = ctypes.c_int()
+            views.append((self._h(lib().ref_rotation_key_get(owner.ptr, i, ctypes.byref(d))),
+                          d.value))
+        return owner, views
+
+    def create_small_bootstrap_key(self, sk):
+        owner = self._h(lib().ref_create_small_bootstrap_key(self.ptr, sk.ptr))
+        return owner, [self._h(lib().ref_small_bootstrap_key_part(owner.ptr, i)) for i in (0, 1)]
+
+    def bootstrap(self, ct, rk, ck, rotk, sbk, stage_count):
+        return self._h(lib().ref_engine_bootstrap(self.ptr, ct.ptr, rk.ptr, ck.ptr, rotk.ptr,
+                                                  sbk.ptr, stage_count))
 
     def level_down(self, a, level):
         return self._h(lib().ref_engine_level_down(self.ptr, a.ptr, level))

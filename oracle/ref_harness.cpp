@@ -320,6 +320,9 @@ void ref_handle_free(void *h) {
   case 3: delete static_cast<RelinearizationKey *>(handle->owner); break;
   case 6: delete static_cast<FixedRotationKey *>(handle->owner); break;
   case 7: delete static_cast<ConjugationKey *>(handle->owner); break;
+  case 9: delete static_cast<RotationKey *>(handle->owner); break;
+  case 10: delete static_cast<SmallBootstrapKey *>(handle->owner); break;
+  case 11: break;  // a view into another handle's key
   default: delete static_cast<Data *>(handle->owner); break;
   }
   delete handle;
@@ -694,6 +697,69 @@ void *ref_engine_scalar(void *e, int op, void *a, double value, long long intege
       case 3: r = eng->multiply(c, static_cast<int64_t>(integer)); break;
       default: return nullptr;
     }
+    return wrap(4, r, r);
+  } catch (...) {
+    remember_error();
+    return nullptr;
+  }
+}
+
+// ---- bootstrapping --------------------------------------------------------------
+
+// create_rotation_key(sk[, level]): kind 9 owns the RotationKey; its fixed keys are
+// reached with ref_rotation_key_get.
+void *ref_create_rotation_key(void *e, void *sk, int level) {
+  try {
+    auto eng = static_cast<RefEngine *>(e)->engine.get();
+    auto s = static_cast<SecretKey *>(static_cast<Handle *>(sk)->data);
+    auto rk = level < 0 ? eng->create_rotation_key(s) : eng->create_rotation_key(s, level);
+    return wrap(9, nullptr, rk);
+  } catch (...) {
+    remember_error();
+    return nullptr;
+  }
+}
+
+int ref_rotation_key_count(void *h) {
+  return static_cast<int>(
+      static_cast<RotationKey *>(static_cast<Handle *>(h)->owner)->fixed_rotation_keys_.size());
+}
+
+// A non-owning view (kind 11) of fixed key i: its key switching key limbs and delta.
+void *ref_rotation_key_get(void *h, int i, int *delta) {
+  auto rk = static_cast<RotationKey *>(static_cast<Handle *>(h)->owner);
+  auto fk = rk->fixed_rotation_keys_[i];
+  *delta = fk->delta_;
+  return wrap(11, fk->key_switching_key_, nullptr);
+}
+
+// create_small_bootstrap_key(sk): kind 10; part 0 = to_sparse, 1 = to_dense (views).
+void *ref_create_small_bootstrap_key(void *e, void *sk) {
+  try {
+    auto eng = static_cast<RefEngine *>(e)->engine.get();
+    auto s = static_cast<SecretKey *>(static_cast<Handle *>(sk)->data);
+    return wrap(10, nullptr, eng->create_small_bootstrap_key(s));
+  } catch (...) {
+    remember_error();
+    return nullptr;
+  }
+}
+
+void *ref_small_bootstrap_key_part(void *h, int part) {
+  auto k = static_cast<SmallBootstrapKey *>(static_cast<Handle *>(h)->owner);
+  return wrap(11, part == 0 ? k->to_sparse_ : k->to_dense_, nullptr);
+}
+
+void *ref_engine_bootstrap(void *e, void *ct, void *rk, void *ck, void *rotk, void *sbk,
+                           int stage_count) {
+  try {
+    auto eng = static_cast<RefEngine *>(e)->engine.get();
+    auto r = eng->bootstrap(
+        static_cast<UnitCiphertext *>(static_cast<Handle *>(ct)->data),
+        static_cast<RelinearizationKey *>(static_cast<Handle *>(rk)->owner),
+        static_cast<ConjugationKey *>(static_cast<Handle *>(ck)->owner),
+        static_cast<RotationKey *>(static_cast<Handle *>(rotk)->owner),
+        static_cast<SmallBootstrapKey *>(static_cast<Handle *>(sbk)->owner), stage_count);
     return wrap(4, r, r);
   } catch (...) {
     remember_error();

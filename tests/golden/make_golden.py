@@ -323,6 +323,47 @@ def arith_cases():
     return cases
 
 
+BOOTSTRAP_SEED = (101, 202, 303, 404, 505, 606, 707, 808)
+BOOTSTRAP_NONCE = (7, 3)
+
+
+def bootstrap_cases():
+    """Bootstrapping through the reference's engine (bootstrap preset, N = 2^16,
+    4 special primes, 3 stages) after reseeding: secret, relinearization, conjugation,
+    rotation and small bootstrap keys, a secret-key encryption at level 3, then
+    bootstrap(ct, rk, ck, rotation key, small bootstrap key, 3)."""
+    from oracle import ref
+
+    log_n, K, preset = TIERS["bootstrap_gold"]
+    e = ref.Engine(log_n=log_n, special_prime_count=K, preset=preset, threads=os.cpu_count())
+    e.seed(BOOTSTRAP_SEED, BOOTSTRAP_NONCE)
+    out = {}
+    sk = e.create_secret_key()
+    out["secret_key"] = sk.limbs()
+    rk = e.create_relinearization_key(sk)
+    out["relinearization_key"] = rk.limbs()
+    ck = e.create_conjugation_key(sk)
+    rotk, views = e.create_rotation_key(sk)
+    out["rotation_key_1"] = views[0][0].limbs()
+    sbk, (to_sparse, to_dense) = e.create_small_bootstrap_key(sk)
+    out["to_sparse"] = to_sparse.limbs()
+    out["to_dense"] = to_dense.limbs()
+    vals = codec_values(4242, e.slot_count, True)
+    pt = e.encode(vals, 3)
+    ct = e.encrypt(pt, sk)
+    out["ciphertext"] = ct.limbs()
+    boot = e.bootstrap(ct, rk, ck, rotk, sbk, 3)
+    out["bootstrapped"] = boot.limbs()
+    info = boot.info()
+    dec = e.decode(e.decrypt(boot, sk))
+    return [dict(tier="bootstrap_gold", log_n=log_n, special_prime_count=K, preset=preset,
+                 seed=list(BOOTSTRAP_SEED), nonce=list(BOOTSTRAP_NONCE), values_seed=4242,
+                 encrypt_level=3, stage_count=3, moduli=[int(v) for v in e.tables()["q"]],
+                 rotation_deltas=[d for _, d in views], output_moduli_id=info["moduli_id"],
+                 output_level=info["level"], digests={k: digest(v) for k, v in out.items()},
+                 decoded=digest_doubles(dec), max_error=float(np.max(np.abs(dec - vals))))]
+
+
 def main():
     with open(os.path.join(HERE, "ntt_kat.json"), "w") as f:
         json.dump(parse_ntt_kats(), f, indent=1)
@@ -339,6 +380,9 @@ def main():
     arith = arith_cases()
     with open(os.path.join(HERE, "arith.json"), "w") as f:
         json.dump(arith, f, indent=1)
+    boot = bootstrap_cases()
+    with open(os.path.join(HERE, "bootstrap.json"), "w") as f:
+        json.dump(boot, f, indent=1)
     keygen = keygen_cases()
     with open(os.path.join(HERE, "keygen.json"), "w") as f:
         json.dump(keygen, f, indent=1)
