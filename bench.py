@@ -272,6 +272,104 @@ def run_ntt_microbench(args, torch, np, rank, world, local, backend, stream):
     return 0
 
 
+# -------------------------------------------------------------- bootstrap --
+
+def run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream):
+    """Bootstrapping at N = 2^16 (bootstrap preset, 4 special primes, 2^15 complex
+    slots uniform in [-1, 1], 3 stages): each step bootstraps `batch` ciphertexts
+    encrypted at level 3.  Keys are made on the device before timing."""
+    from fhe_b200 import Engine
+    from inputs import codec_values
+
+    eng = Engine(log_coeff_count=16, special_prime_count=4, scheme_preset=2)
+    eng.set_stream(stream.cuda_stream)
+    B = args.batch
+    eng.seed([11 + rank, 22, 33, 44, 55, 66, 77, 88], [1, 2])
+    sk = eng.create_secret_key()
+    rk = eng.create_relinearization_key(sk)
+    ck = eng.create_conjugation_key(sk)
+    rot = eng.create_rotation_key(sk)
+    sbk = eng.create_small_bootstrap_key(sk)
+    values = [codec_values(100 + i, eng.slot_count, True) for i in range(B)]
+    cts = [eng.encrypt(eng.encode(v, 3), sk) for v in values]
+
+    def step(inputs):
+        return [eng.bootstrap(c, rk, ck, rot, sbk, 3) for c in inputs]
+
+    for _ in range(args.warmup):
+        step(cts)
+    torch.cuda.synchronize()
+    if backend:
+        torch.distributed.barrier()
+    launches0 = Engine.kernel_launch_count()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            outs = step(cts)
+        stop.record(stream)
+        torch.cuda.synchronize()
+    elapsed = start.elapsed_time(stop)
+    launches = Engine.kernel_launch_count() - launches0
+    elapsed_max, units = aggregate(elapsed, float(B * args.steps), world, backend)
+    ms_per_bootstrap = elapsed_max / (args.steps * B)
+    # Precision of one output against the input slots (float64 oracle = the values).
+    dec = eng.decode(eng.decrypt(outs[0], sk), complex_output=True)
+    err = float(np.max(np.abs(dec - values[0])))
+    bits = float(-np.log2(err)) if err > 0 else 64.0
+    # Per-family device time of one bootstrap.
+    eng.set_profiling(True)
+    eng.profile_reset()
+    step(cts[:1])
+    families = {k: v[1] for k, v in eng.profile().items()}
+    eng.set_profiling(False)
+    # End to end: ciphertext limbs from pinned host memory, bootstrap, result back.
+    host_ct = [torch.from_numpy(c.download()).pin_memory() for c in cts]
+    out_host = torch.empty(tuple(outs[0].download().shape), dtype=torch.int64).pin_memory()
+    info = cts[0].info()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for h in host_ct:
+            c = eng.upload_from_pointer(h.data_ptr(), info["moduli_id"], 2, info["flag"],
+                                        scale=float(info["scale"]))
+            o = eng.bootstrap(c, rk, ck, rot, sbk, 3)
+            eng.download_to_pointer(o, out_host.data_ptr())
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / (args.steps * B)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import ref
+
+            if ref.available():
+                threads = os.cpu_count() or 1
+                ms = ref.bench_bootstrap(threads)
+                cpu = {"value": ms, "unit": "ms/bootstrap", "cores": threads, "kind": "reference",
+                       "sample": "1 bootstrap (N=2^16, 3 stages, rotation key) through the "
+                                 "reference CKKSEngine with CPU_PARALLEL, keygen excluded"}
+        except Exception as exc:
+            cpu = {"value": None, "unit": "ms/bootstrap", "cores": 0, "kind": "reference",
+                   "sample": f"failed: {exc}"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "bootstrap ms at N=2^16 (2^15 slots, 3 stages)", "value": ms_per_bootstrap,
+            "unit": "ms/bootstrap", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": elapsed_max / args.steps, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic (seeded uniform complex slots in [-1, 1], keys made on the device)",
+            "config": {"workload": "engine.bootstrap(ct, rk, ck, rotation key, small bootstrap "
+                                   "key, 3), bootstrap preset, N=2^16, K=4, input level 3",
+                       "ciphertexts_per_step": B, "precision_bits": bits,
+                       "kernel_ms_per_bootstrap": families},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_ms, "unit": "ms/bootstrap",
+                    "h2d_bytes_per_step": int(sum(h.numel() * 8 for h in host_ct)),
+                    "d2h_bytes_per_step": int(out_host.numel() * 8 * B)},
+            "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
+    eng.close()
+    return 0
+
+
 # -------------------------------------------------------------------- main --
 
 def main(argv=None):
@@ -281,8 +379,9 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--batch", type=int, default=16, help="ciphertext pairs per step")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="hmult", choices=["hmult", "ntt"],
-                    help="hmult: the headline; ntt: forward NTT of --batch x 24 limbs at N=2^16")
+    ap.add_argument("--workload", default="hmult", choices=["hmult", "ntt", "bootstrap"],
+                    help="hmult: the headline; ntt: forward NTT of --batch x 24 limbs at N=2^16; "
+                         "bootstrap: --batch ciphertexts bootstrapped per step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args(argv)
     rank, world, local = dist_env()
@@ -314,6 +413,8 @@ def main(argv=None):
     torch.cuda.set_stream(stream)
     if args.workload == "ntt":
         return run_ntt_microbench(args, torch, np, rank, world, local, backend, stream)
+    if args.workload == "bootstrap":
+        return run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream)
     eng = Engine(log_coeff_count=LOG_N, special_prime_count=SPECIAL)
     eng.set_stream(stream.cuda_stream)
     n = eng.coeff_count

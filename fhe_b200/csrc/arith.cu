@@ -38,13 +38,6 @@ struct Engine::Matched {
   const Data *b = nullptr;
 };
 
-int64_t *Engine::upload_constants(const std::vector<int64_t> &v) {
-  int64_t *d = alloc_words(v.size());
-  check(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream_),
-        "upload constants");
-  return d;
-}
-
 std::vector<int64_t> Engine::add_multiplier(double value, int level) const {
   // make_add_multiplier (precomputed.cpp:476-498) with scale_modulo
   // (arithmetic.cpp:60-76).
@@ -266,11 +259,9 @@ std::unique_ptr<Data> Engine::add_scalar(const Data &ct, double value) {
     return add_plain(ct, *pt);
   }
   const auto mult = add_multiplier(value, ct.level());
-  int64_t *c = upload_constants(mult);
   auto out = clone(ct);
-  pointwise(kOpAddScalarFirst, params.chains(ct.moduli_id), ct.moduli_id, ct.d, nullptr, c, out->d);
-  free_words(c);
-  synchronize();  // the host constants are released on return
+  pointwise(kOpAddScalarFirst, params.chains(ct.moduli_id), ct.moduli_id, ct.d, nullptr,
+            mult.data(), out->d);
   return out;
 }
 
@@ -320,19 +311,16 @@ std::unique_ptr<Data> Engine::multiply_scalar(const Data &ct, double value) {
   const int mid = x->moduli_id;
   const int L = x->chains;
   const auto mult = mult_multiplier(value, level);
-  int64_t *c = upload_constants(mult);
   int64_t *entered = alloc_words(static_cast<size_t>(x->polys) * x->poly_stride());
   const long long ps = x->poly_stride();
   for (int q = 0; q < x->polys; q++)
-    pointwise(kOpEnterReduce, L, mid, x->d + q * ps, nullptr, c, entered + q * ps);
+    pointwise(kOpEnterReduce, L, mid, x->d + q * ps, nullptr, mult.data(), entered + q * ps);
   const long double rs = params.rescaled_scale(x->scale, mid);
   auto out = make_data(kUnitCiphertext, x->flag, params.moduli_id(level - 1), x->polys, rs * rs);
   const cudaError_t e = launch_rescale(tables_, ks_, params.n, x->polys, L, mid, entered, ps,
                                        out->d, out->poly_stride(), stream_);
-  free_words(c);
   free_words(entered);
   check(e, "rescale");
-  synchronize();  // the host constants are released on return
   return out;
 }
 
@@ -354,13 +342,11 @@ std::unique_ptr<Data> Engine::multiply_integer(const Data &ct, int64_t value) {
   std::vector<int64_t> mult(x->chains);
   for (int j = 0; j < x->chains; j++)
     mult[j] = mod_mul(value, INT64_C(1) << 62, static_cast<int64_t>(params.q[x->moduli_id + j]));
-  int64_t *c = upload_constants(mult);
   auto out = make_data(kUnitCiphertext, x->flag, x->moduli_id, x->polys, x->scale);
   const long long ps = x->poly_stride();
   for (int q = 0; q < x->polys; q++)
-    pointwise(kOpEnterReduce, x->chains, x->moduli_id, x->d + q * ps, nullptr, c, out->d + q * ps);
-  free_words(c);
-  synchronize();
+    pointwise(kOpEnterReduce, x->chains, x->moduli_id, x->d + q * ps, nullptr, mult.data(),
+              out->d + q * ps);
   return out;
 }
 

@@ -192,20 +192,16 @@ std::unique_ptr<Data> Engine::multiply_imaginary(const Data &ct, int64_t value) 
     hold = to_ntt(*x);
     x = hold.get();
   }
-  const int n = params.n, mid = x->moduli_id, L = params.chains(mid);
+  const int mid = x->moduli_id, L = params.chains(mid);
   auto pt = make_data(kUnitPlaintext, kFlagComplex, mid, 1, 1.0L);
-  std::vector<int64_t> chain(n, 0);
-  chain[n / 2] = value;
-  int64_t *d_chain = upload_constants(chain);
-  tile(d_chain, L, mid, pt->d, n);
-  free_words(d_chain);
+  const std::vector<int64_t> monomial(L, value);
+  pointwise(kOpMonomial, L, mid, nullptr, nullptr, monomial.data(), pt->d);
   ntt_in_place(pt->d, L, mid, pt->poly_stride(), 1);
   auto out = make_data(kUnitCiphertext, (x->flag | kFlagComplex) & ~kFlagRescaled, mid, x->polys,
                        x->scale);
   const long long ps = x->poly_stride();
   for (int p = 0; p < x->polys; p++)
     pointwise(kOpMult, x->chains, mid, x->d + p * ps, pt->d, nullptr, out->d + p * ps);
-  synchronize();  // the host chain is released on return
   if (!ct.is_ntt()) return to_intt(*out);
   return out;
 }
@@ -274,10 +270,26 @@ std::vector<std::unique_ptr<Data>> Engine::rotate_batch(const Data &ct,
 
 // ------------------------------------------------------------- the stages --
 
-std::unique_ptr<Data> Engine::apply_butterfly(const Data &ct, const std::vector<cvec> &twiddle,
-                                              const std::vector<const Data *> &keys,
+const std::vector<std::vector<std::vector<std::complex<double>>>> &Engine::bootstrap_twiddles(
+    bool to_slot, int stage_count) {
+  const auto key = std::make_pair(to_slot, stage_count);
+  auto it = twiddle_cache_.find(key);
+  if (it == twiddle_cache_.end())
+    it = twiddle_cache_
+             .emplace(key, butterfly_twiddles(params.slot_count, params.log_slot_count, stage_count,
+                                              to_slot))
+             .first;
+  return it->second;
+}
+
+std::unique_ptr<Data> Engine::apply_butterfly(const Data &ct, bool to_slot, int stage_count,
+                                              int stage, const std::vector<const Data *> &keys,
                                               int rotate_count) {
-  // CKKSEngine::apply_butterfly with a rotation key (engine_bootstrap.cpp:155-216).
+  // CKKSEngine::apply_butterfly with a rotation key (engine_bootstrap.cpp:155-216).  The
+  // reference encodes each diagonal at every call and multiplies through
+  // prepare_for_multiply; the prepared (rescaled, NTT-form) diagonal depends only on
+  // the stage, its position and the level, so it is made once and kept on the device.
+  const auto &twiddle = bootstrap_twiddles(to_slot, stage_count)[stage];
   const int count = static_cast<int>(twiddle.size());
   const auto [inner, outer] = stage_loop_counts(count);
   std::vector<int> inner_deltas;
@@ -290,14 +302,28 @@ std::unique_ptr<Data> Engine::apply_butterfly(const Data &ct, const std::vector<
     Owned inner_sum;
     for (int i = (o == 0 ? 1 : 0); i < inner; i++) {
       const int index = inner * norm_o + i;
-      const cvec factor = rotate_vector(twiddle[pmod(index, count)], -factor_delta);
-      std::vector<double> re(factor.size()), im(factor.size());
-      for (size_t s = 0; s < factor.size(); s++) {
-        re[s] = factor[s].real();
-        im[s] = factor[s].imag();
+      const int level = rotated[i]->level();
+      const auto key = std::make_tuple(to_slot, stage_count, stage, o, i, level);
+      auto cached = diagonal_cache_.find(key);
+      if (cached == diagonal_cache_.end()) {
+        const cvec factor = rotate_vector(twiddle[pmod(index, count)], -factor_delta);
+        std::vector<double> re(factor.size()), im(factor.size());
+        for (size_t s = 0; s < factor.size(); s++) {
+          re[s] = factor[s].real();
+          im[s] = factor[s].imag();
+        }
+        auto pt = encode(re.data(), im.data(), static_cast<int>(factor.size()), level);
+        cached = diagonal_cache_.emplace(key, prepare_for_multiply(*pt, level)).first;
       }
-      auto pt = encode(re.data(), im.data(), static_cast<int>(factor.size()), rotated[i]->level());
-      auto product = multiply_plain(*rotated[i], *pt);
+      // multiply(ct, encoded diagonal): CKKSCore::multiply(ct, pt) (core.cpp:257-282).
+      const Data &p = *cached->second;
+      auto c = prepare_for_multiply(*rotated[i], level);
+      auto product = make_data(kUnitCiphertext, (c->flag | p.flag) & ~kFlagRescaled, c->moduli_id,
+                               c->polys, c->scale * p.scale);
+      const long long ps = c->poly_stride();
+      for (int q = 0; q < c->polys; q++)
+        pointwise(kOpMult, c->chains, c->moduli_id, c->d + q * ps, p.d, nullptr,
+                  product->d + q * ps);
       if (!inner_sum)
         inner_sum = std::move(product);
       else
@@ -317,12 +343,11 @@ std::pair<std::unique_ptr<Data>, std::unique_ptr<Data>> Engine::coeff_to_slot(
     int stage_count) {
   // engine_bootstrap.cpp:331-371.
   const int slot = params.slot_count, log_slot = params.log_slot_count;
-  const Stages tw = butterfly_twiddles(slot, log_slot, stage_count, true);
   int rotate_count = slot;
   Owned current;
   for (int stage = 0; stage < stage_count; stage++) {
     rotate_count >>= cts_log_radix(stage, stage_count, log_slot);
-    current = apply_butterfly(current ? *current : ct, tw[stage], keys, rotate_count);
+    current = apply_butterfly(current ? *current : ct, true, stage_count, stage, keys, rotate_count);
   }
   auto conjugated = conjugate(*current, conjugation_key);
   auto real_part = add(*current, *conjugated);
@@ -335,13 +360,12 @@ std::unique_ptr<Data> Engine::slot_to_coeff(const Data &real_part, const Data &i
                                             const std::vector<const Data *> &keys,
                                             int stage_count) {
   // engine_bootstrap.cpp:405-434.
-  const int slot = params.slot_count, log_slot = params.log_slot_count;
+  const int log_slot = params.log_slot_count;
   auto multiplied = multiply_imaginary(imaginary_part, 1);
   auto current = add(real_part, *multiplied);
-  const Stages tw = butterfly_twiddles(slot, log_slot, stage_count, false);
   int rotate_count = 1;
   for (int stage = 0; stage < stage_count; stage++) {
-    current = apply_butterfly(*current, tw[stage], keys, rotate_count);
+    current = apply_butterfly(*current, false, stage_count, stage, keys, rotate_count);
     rotate_count <<= stc_log_radix(stage, stage_count, log_slot);
   }
   return current;

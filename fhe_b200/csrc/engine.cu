@@ -129,6 +129,11 @@ Engine::~Engine() {
 
 void Engine::synchronize() { check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize"); }
 
+void Engine::upload_bytes(void *dst, const void *src, size_t bytes, const char *what) {
+  check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_), what);
+  synchronize();
+}
+
 int64_t *Engine::alloc_words(size_t words) {
   void *p = nullptr;
   check(cudaMallocAsync(&p, std::max<size_t>(words, 1) * sizeof(int64_t), stream_), "cudaMallocAsync");
@@ -228,7 +233,7 @@ const DevicePartitions &Engine::partitions(int moduli_id, int key_moduli_id) {
   }
   void *dev = nullptr;
   check(cudaMalloc(&dev, words * sizeof(int64_t)), "cudaMalloc(partitions)");
-  check(cudaMemcpy(dev, host.data(), words * sizeof(int64_t), cudaMemcpyHostToDevice), "upload partitions");
+  upload_bytes(dev, host.data(), words * sizeof(int64_t), "upload partitions");
   int *dints = static_cast<int *>(dev);
   dp.start = dints;
   dp.size = dints + count;
@@ -657,8 +662,7 @@ const int32_t *Engine::device_signed_permutation(int delta) {
   const auto host = signed_permutation(params.n, delta);
   void *p = nullptr;
   check(cudaMalloc(&p, host.size() * sizeof(int32_t)), "cudaMalloc(permutation)");
-  check(cudaMemcpy(p, host.data(), host.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
-        "upload permutation");
+  upload_bytes(p, host.data(), host.size() * sizeof(int32_t), "upload permutation");
   return signed_perm_cache_.emplace(delta, static_cast<int32_t *>(p)).first->second;
 }
 
@@ -668,8 +672,7 @@ const int32_t *Engine::device_ntt_permutation(int delta) {
   const auto host = ntt_permutation(params.n, delta);
   void *p = nullptr;
   check(cudaMalloc(&p, host.size() * sizeof(int32_t)), "cudaMalloc(permutation)");
-  check(cudaMemcpy(p, host.data(), host.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
-        "upload permutation");
+  upload_bytes(p, host.data(), host.size() * sizeof(int32_t), "upload permutation");
   return ntt_perm_cache_.emplace(delta, static_cast<int32_t *>(p)).first->second;
 }
 

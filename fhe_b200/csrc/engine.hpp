@@ -11,6 +11,7 @@
 #include <set>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -56,6 +57,7 @@ enum PointwiseOp : int {
   kOpNegate = 5,          // negate_make_unsigned: q - a
   kOpAddScalarFirst = 6,  // add_scalar (c[limb] on coefficient 0) then reduce_2q_to_q
   kOpEnterReduce = 7,     // mont_enter(a, c[limb]) then reduce_2q_to_q
+  kOpMonomial = 8,        // c[limb] X^(N/2), signed c tiled per limb (encode_imaginary)
 };
 
 // The ChaCha20 key and nonce of the engine's random stream (RandomNumberGenerator,
@@ -96,7 +98,12 @@ class Engine {
   const Parameters params;
 
   cudaStream_t stream() const { return stream_; }
-  void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
+  // Work queued on the previous stream finishes first, so results made there are
+  // ready for the new one.
+  void set_stream(cudaStream_t s) {
+    synchronize();
+    stream_ = s ? s : own_stream_;
+  }
   void synchronize();
 
   // Device memory from the stream-ordered pool.
@@ -212,6 +219,7 @@ class Engine {
                     int64_t shift);
   void draw_gaussian(int64_t *out);
   void tile(const int64_t *chain, int limbs, int prime_base, int64_t *y, long long y_stride);
+  // constants: host array of `limbs` per-limb values (or null), passed by value.
   void pointwise(int op, int limbs, int prime_base, const int64_t *a, const int64_t *b,
                  const int64_t *constants, int64_t *y);
   void ntt_in_place(int64_t *x, int limbs, int prime_base, long long stride, int polys);
@@ -222,9 +230,15 @@ class Engine {
   std::unique_ptr<Data> rescale_any(const Data &text);  // CKKSEngine::rescale_
   void signed_tile(const int64_t *chain, int64_t q_src, int limbs, int prime_base, int64_t *y,
                    long long y_stride);
-  std::unique_ptr<Data> apply_butterfly(const Data &ct,
-                                        const std::vector<std::vector<std::complex<double>>> &tw,
+  std::unique_ptr<Data> apply_butterfly(const Data &ct, bool to_slot, int stage_count, int stage,
                                         const std::vector<const Data *> &keys, int rotate_count);
+  // Host twiddles per (direction, stage count) and device diagonals prepared for the
+  // product (rescaled, NTT form) per (direction, stage count, stage, outer, inner, level).
+  std::map<std::pair<bool, int>, std::vector<std::vector<std::vector<std::complex<double>>>>>
+      twiddle_cache_;
+  std::map<std::tuple<bool, int, int, int, int, int>, std::unique_ptr<Data>> diagonal_cache_;
+  const std::vector<std::vector<std::vector<std::complex<double>>>> &bootstrap_twiddles(
+      bool to_slot, int stage_count);
   std::pair<std::unique_ptr<Data>, std::unique_ptr<Data>> coeff_to_slot(
       const Data &ct, const Data &conjugation_key, const std::vector<const Data *> &keys,
       int stage_count);
@@ -240,7 +254,7 @@ class Engine {
   Matched match_texts(const Data &a, const Data &b, bool b_is_plain);
   std::vector<int64_t> add_multiplier(double value, int level) const;
   std::vector<int64_t> mult_multiplier(double value, int level) const;
-  int64_t *upload_constants(const std::vector<int64_t> &v);
+
   std::map<int, int32_t *> signed_perm_cache_;  // delta -> signed permutation [N]
   std::map<int, int32_t *> ntt_perm_cache_;     // delta -> NTT-form gather indices [N]
   const int32_t *device_signed_permutation(int delta);
@@ -270,6 +284,11 @@ class Engine {
   }
 
   void check(cudaError_t e, const char *what);
+  // Copies a host table to the device on the engine's stream and waits for it.  A
+  // plain cudaMemcpy is not enough: from pageable memory it may return before the
+  // DMA lands, and it runs on the legacy stream, which a non-blocking stream does
+  // not wait for.  Waiting also makes the table visible to every other stream.
+  void upload_bytes(void *dst, const void *src, size_t bytes, const char *what);
   // Device copy of a host table, freed with the engine.
   template <class T>
   T *upload_table(const std::vector<T> &v) {
@@ -277,8 +296,7 @@ class Engine {
     void *p = nullptr;
     check(cudaMalloc(&p, bytes), "cudaMalloc(table)");
     table_buffers_.push_back(static_cast<int64_t *>(p));
-    if (!v.empty())
-      check(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload table");
+    if (!v.empty()) upload_bytes(p, v.data(), v.size() * sizeof(T), "upload table");
     return static_cast<T *>(p);
   }
 

@@ -175,7 +175,7 @@ __global__ void signed_tile_kernel(PrimeTables t, int log_n, int limbs, int prim
 // y[j] = op(a[j], b[j]) over `limbs` limbs of N words; a, b, y are [limbs][N]
 // views (any may alias).
 __global__ void pointwise_kernel(PrimeTables t, int op, int log_n, int limbs, int prime_base,
-                                 const int64_t *a, const int64_t *b, const int64_t *c, int64_t *y) {
+                                 const int64_t *a, const int64_t *b, LimbScalars c, int64_t *y) {
   const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
   if (i >= (static_cast<long long>(limbs) << log_n)) return;
   const int j = static_cast<int>(i >> log_n);
@@ -188,10 +188,15 @@ __global__ void pointwise_kernel(PrimeTables t, int op, int log_n, int limbs, in
     case kOpAddReduce: v = guard(guard(a[i] + b[i], q2), qs); break;
     case kOpSubReduce: v = guard(guard(a[i] + q2 - b[i], q2), qs); break;
     case kOpReduce: v = guard(a[i], qs); break;
-    case kOpEnter: v = mont_mult(a[i], c[j], q, k); break;
+    case kOpEnter: v = mont_mult(a[i], c.v[j], q, k); break;
     case kOpNegate: v = qs - a[i]; break;
-    case kOpAddScalarFirst: v = guard(a[i] + ((i & ((1LL << log_n) - 1)) == 0 ? c[j] : 0), qs); break;
-    case kOpEnterReduce: v = guard(mont_mult(a[i], c[j], q, k), qs); break;
+    case kOpAddScalarFirst: v = guard(a[i] + ((i & ((1LL << log_n) - 1)) == 0 ? c.v[j] : 0), qs); break;
+    case kOpEnterReduce: v = guard(mont_mult(a[i], c.v[j], q, k), qs); break;
+    case kOpMonomial: {
+      const int64_t m = c.v[j];
+      v = (i & ((1LL << log_n) - 1)) == (1LL << (log_n - 1)) ? (m < 0 ? m + qs : guard(m, qs)) : 0;
+      break;
+    }
   }
   y[i] = v;
 }
@@ -212,7 +217,10 @@ void Engine::seed(const uint32_t *seed_words, const uint8_t *nonce) {
 void Engine::ensure_rng_tables() {
   if (cdt_uploaded_) return;
   static_assert(sizeof(kCdtTree) == 2 * kCdtSize * sizeof(unsigned long long), "CDT tree size");
-  check(cudaMemcpyToSymbol(c_cdt, kCdtTree, sizeof(kCdtTree)), "upload CDT tree");
+  check(cudaMemcpyToSymbolAsync(c_cdt, kCdtTree, sizeof(kCdtTree), 0, cudaMemcpyHostToDevice,
+                                stream_),
+        "upload CDT tree");
+  synchronize();
   cdt_uploaded_ = true;
 }
 
@@ -255,9 +263,15 @@ void Engine::signed_tile(const int64_t *chain, int64_t q_src, int limbs, int pri
 
 void Engine::pointwise(int op, int limbs, int prime_base, const int64_t *a, const int64_t *b,
                        const int64_t *constants, int64_t *y) {
+  // The per-limb constants travel by value in the launch (no copy, no wait).
+  LimbScalars c{};
+  if (constants) {
+    if (limbs > kMaxScalarLimbs) throw std::invalid_argument("pointwise: too many limbs.");
+    for (int j = 0; j < limbs; j++) c.v[j] = constants[j];
+  }
   note_launch();
   pointwise_kernel<<<grid_for(static_cast<long long>(limbs) << params.log_n), kThreads, 0,
-                     stream_>>>(tables_, op, params.log_n, limbs, prime_base, a, b, constants, y);
+                     stream_>>>(tables_, op, params.log_n, limbs, prime_base, a, b, c, y);
   check(cudaGetLastError(), "pointwise");
 }
 
@@ -374,14 +388,11 @@ std::unique_ptr<Data> Engine::create_key_switching_key(const Data &from, const D
   auto ksk = make_data(type, kFlagNtt | kFlagSpecial, mid, 2 * static_cast<int>(parts.size()), 1.0L);
   std::vector<int64_t> ppr(L);
   for (int j = 0; j < L; j++) ppr[j] = params.p_product_mult_r[mid + j];
-  int64_t *consts = alloc_words(L);
   int64_t *p_from = alloc_words(static_cast<size_t>(L) * n);
   int64_t *chain = alloc_words(n);
   int64_t *error = alloc_words(static_cast<size_t>(ps));
-  check(cudaMemcpyAsync(consts, ppr.data(), L * sizeof(int64_t), cudaMemcpyHostToDevice, stream_),
-        "upload constants");
   pointwise(kOpEnter, L, mid, from.d + static_cast<long long>(mid - from.moduli_id) * n, nullptr,
-            consts, p_from);
+            ppr.data(), p_from);
   const int64_t *s_to = to.d + static_cast<long long>(mid - to.moduli_id) * n;
   for (size_t pi = 0; pi < parts.size(); pi++) {
     int64_t *b = ksk->d + static_cast<long long>(2 * pi) * ps;
@@ -396,11 +407,9 @@ std::unique_ptr<Data> Engine::create_key_switching_key(const Data &from, const D
     pointwise(kOpAddReduce, size, mid + start, p_from + static_cast<long long>(start) * n,
               b + static_cast<long long>(start) * n, nullptr, b + static_cast<long long>(start) * n);
   }
-  free_words(consts);
   free_words(p_from);
   free_words(chain);
   free_words(error);
-  synchronize();  // the host constants are released on return
   return ksk;
 }
 

@@ -72,6 +72,7 @@ def lib():
             "ref_engine_conjugate": (vp, [vp, vp, vp]),
             "ref_engine_level_down": (vp, [vp, vp, ctypes.c_int]),
             "ref_last_error": (ctypes.c_char_p, []),
+            "ref_bench_bootstrap": (ctypes.c_double, [ctypes.c_int]),
             "ref_create_rotation_key": (vp, [vp, vp, ctypes.c_int]),
             "ref_rotation_key_count": (ctypes.c_int, [vp]),
             "ref_rotation_key_get": (vp, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
@@ -356,3 +357,8 @@ def cdt_tree():
     out = (ctypes.c_uint64 * 256)()
     n = lib().ref_cdt_tree(out, 256)
     return [int(out[i]) for i in range(n)]
+
+
+def bench_bootstrap(threads: int) -> float:
+    """Milliseconds of one reference bootstrap (N = 2^16, 3 stages, all given threads)."""
+    return float(lib().ref_bench_bootstrap(threads))

@@ -879,4 +879,35 @@ double ref_bench_mult_relin_rescale(int log_n, int special_prime_count, int leve
   return times[times.size() / 2];
 }
 
+// Times one engine.bootstrap(ct, rk, ck, rotation key, small bootstrap key, 3) on the
+// bootstrap preset at N = 2^16 (keys and encryption outside the timing); returns ms.
+double ref_bench_bootstrap(int threads) {
+  auto config = make_config(16, -1, 4, -1, 2, threads);
+  CKKSEngine engine(config);
+  auto sk = engine.create_secret_key();
+  auto rk = engine.create_relinearization_key(sk);
+  auto ck = engine.create_conjugation_key(sk);
+  auto rot = engine.create_rotation_key(sk);
+  auto sbk = engine.create_small_bootstrap_key(sk);
+  const int slots = engine.get_slot_count();
+  std::mt19937_64 gen(1);
+  std::uniform_real_distribution<double> u(-1.0, 1.0);
+  std::vector<std::complex<double>> v(slots);
+  for (auto &z : v) z = {u(gen), u(gen)};
+  auto pt = engine.encode_unit(v, 3);
+  auto ct = engine.encrypt_unit(v, sk, 3);
+  auto t0 = std::chrono::steady_clock::now();
+  auto out = engine.bootstrap(ct, rk, ck, rot, sbk, 3);
+  auto t1 = std::chrono::steady_clock::now();
+  delete out;
+  delete ct;
+  delete pt;
+  delete sbk;
+  delete rot;
+  delete ck;
+  delete rk;
+  delete sk;
+  return std::chrono::duration<double, std::milli>(t1 - t0).count();
+}
+
 } // extern "C"

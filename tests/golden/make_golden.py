@@ -343,8 +343,10 @@ def bootstrap_cases():
     rk = e.create_relinearization_key(sk)
     out["relinearization_key"] = rk.limbs()
     ck = e.create_conjugation_key(sk)
+    out["conjugation_key"] = ck.limbs()
     rotk, views = e.create_rotation_key(sk)
     out["rotation_key_1"] = views[0][0].limbs()
+    rotation_keys = [digest(v.limbs()) for v, _ in views]
     sbk, (to_sparse, to_dense) = e.create_small_bootstrap_key(sk)
     out["to_sparse"] = to_sparse.limbs()
     out["to_dense"] = to_dense.limbs()
@@ -359,7 +361,8 @@ def bootstrap_cases():
     return [dict(tier="bootstrap_gold", log_n=log_n, special_prime_count=K, preset=preset,
                  seed=list(BOOTSTRAP_SEED), nonce=list(BOOTSTRAP_NONCE), values_seed=4242,
                  encrypt_level=3, stage_count=3, moduli=[int(v) for v in e.tables()["q"]],
-                 rotation_deltas=[d for _, d in views], output_moduli_id=info["moduli_id"],
+                 rotation_deltas=[d for _, d in views], rotation_keys=rotation_keys,
+                 output_moduli_id=info["moduli_id"],
                  output_level=info["level"], digests={k: digest(v) for k, v in out.items()},
                  decoded=digest_doubles(dec), max_error=float(np.max(np.abs(dec - vals))))]
 

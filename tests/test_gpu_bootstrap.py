@@ -25,9 +25,11 @@ def test_bootstrap_matches_recorded_reference(engines, case):
     rk = e.create_relinearization_key(sk)
     assert digest(rk.download()) == d["relinearization_key"]
     ck = e.create_conjugation_key(sk)
+    assert digest(ck.download()) == d["conjugation_key"]
     rot = e.create_rotation_key(sk)
     assert [k.info()["delta"] for k in rot] == case["rotation_deltas"]
     assert digest(rot[0].download()) == d["rotation_key_1"]
+    assert [digest(k.download()) for k in rot] == case["rotation_keys"]
     to_sparse, to_dense = e.create_small_bootstrap_key(sk)
     assert digest(to_sparse.download()) == d["to_sparse"]
     assert digest(to_dense.download()) == d["to_dense"]
