@@ -277,10 +277,13 @@ def run_ntt_microbench(args, torch, np, rank, world, local, backend, stream):
 def run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream):
     """Bootstrapping at N = 2^16 (bootstrap preset, 4 special primes, 2^15 complex
     slots uniform in [-1, 1], 3 stages): each step bootstraps `batch` ciphertexts
-    encrypted at level 3.  Keys are made on the device before timing."""
+    encrypted at level 3.  Keys are made on the device before timing.  Workload
+    "bootstrap" uses a "medium" bootstrap key (hoisted baby-step giant-step
+    transforms); "bootstrap_rotation" the rotation key and small bootstrap key."""
     from fhe_b200 import Engine
     from inputs import codec_values
 
+    with_key = args.workload == "bootstrap"
     eng = Engine(log_coeff_count=16, special_prime_count=4, scheme_preset=2)
     eng.set_stream(stream.cuda_stream)
     B = args.batch
@@ -288,13 +291,23 @@ def run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream):
     sk = eng.create_secret_key()
     rk = eng.create_relinearization_key(sk)
     ck = eng.create_conjugation_key(sk)
-    rot = eng.create_rotation_key(sk)
-    sbk = eng.create_small_bootstrap_key(sk)
+    if with_key:
+        bk = eng.create_bootstrap_key(sk, 3, "medium")
+        key_bytes = bk.info()["bytes"]
+    else:
+        rot = eng.create_rotation_key(sk)
+        sbk = eng.create_small_bootstrap_key(sk)
+        key_bytes = None
     values = [codec_values(100 + i, eng.slot_count, True) for i in range(B)]
     cts = [eng.encrypt(eng.encode(v, 3), sk) for v in values]
 
+    def boot(c):
+        if with_key:
+            return eng.bootstrap(c, rk, ck, bk)
+        return eng.bootstrap(c, rk, ck, rot, sbk, 3)
+
     def step(inputs):
-        return [eng.bootstrap(c, rk, ck, rot, sbk, 3) for c in inputs]
+        return [boot(c) for c in inputs]
 
     for _ in range(args.warmup):
         step(cts)
@@ -333,7 +346,7 @@ def run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream):
         for h in host_ct:
             c = eng.upload_from_pointer(h.data_ptr(), info["moduli_id"], 2, info["flag"],
                                         scale=float(info["scale"]))
-            o = eng.bootstrap(c, rk, ck, rot, sbk, 3)
+            o = boot(c)
             eng.download_to_pointer(o, out_host.data_ptr())
     e2e_ms = (time.perf_counter() - t0) * 1e3 / (args.steps * B)
     cpu = None
@@ -343,9 +356,10 @@ def run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream):
 
             if ref.available():
                 threads = os.cpu_count() or 1
-                ms = ref.bench_bootstrap(threads)
+                ms = (ref.bench_bootstrap_with_key if with_key else ref.bench_bootstrap)(threads)
+                kind = "medium bootstrap key" if with_key else "rotation key"
                 cpu = {"value": ms, "unit": "ms/bootstrap", "cores": threads, "kind": "reference",
-                       "sample": "1 bootstrap (N=2^16, 3 stages, rotation key) through the "
+                       "sample": f"1 bootstrap (N=2^16, 3 stages, {kind}) through the "
                                  "reference CKKSEngine with CPU_PARALLEL, keygen excluded"}
         except Exception as exc:
             cpu = {"value": None, "unit": "ms/bootstrap", "cores": 0, "kind": "reference",
@@ -357,9 +371,12 @@ def run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream):
             "ms_per_step": elapsed_max / args.steps, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "int64",
             "data": "synthetic (seeded uniform complex slots in [-1, 1], keys made on the device)",
-            "config": {"workload": "engine.bootstrap(ct, rk, ck, rotation key, small bootstrap "
-                                   "key, 3), bootstrap preset, N=2^16, K=4, input level 3",
+            "config": {"workload": ("engine.bootstrap(ct, rk, ck, medium bootstrap key of 3 "
+                                    "stages)" if with_key else
+                                    "engine.bootstrap(ct, rk, ck, rotation key, small bootstrap "
+                                    "key, 3)") + ", bootstrap preset, N=2^16, K=4, input level 3",
                        "ciphertexts_per_step": B, "precision_bits": bits,
+                       "bootstrap_key_bytes": key_bytes,
                        "kernel_ms_per_bootstrap": families},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_ms, "unit": "ms/bootstrap",
@@ -379,9 +396,11 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--batch", type=int, default=16, help="ciphertext pairs per step")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="hmult", choices=["hmult", "ntt", "bootstrap"],
+    ap.add_argument("--workload", default="hmult",
+                    choices=["hmult", "ntt", "bootstrap", "bootstrap_rotation"],
                     help="hmult: the headline; ntt: forward NTT of --batch x 24 limbs at N=2^16; "
-                         "bootstrap: --batch ciphertexts bootstrapped per step")
+                         "bootstrap: --batch ciphertexts bootstrapped per step with a medium "
+                         "bootstrap key; bootstrap_rotation: the same with a rotation key")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args(argv)
     rank, world, local = dist_env()
@@ -413,7 +432,7 @@ def main(argv=None):
     torch.cuda.set_stream(stream)
     if args.workload == "ntt":
         return run_ntt_microbench(args, torch, np, rank, world, local, backend, stream)
-    if args.workload == "bootstrap":
+    if args.workload in ("bootstrap", "bootstrap_rotation"):
         return run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream)
     eng = Engine(log_coeff_count=LOG_N, special_prime_count=SPECIAL)
     eng.set_stream(stream.cuda_stream)

@@ -25,6 +25,7 @@ STATUS_NAMES = {
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
 _pp = ctypes.POINTER(ctypes.c_void_p)
+_ip = ctypes.POINTER(ctypes.c_int)
 _f64p = ctypes.POINTER(ctypes.c_double)
 _i64p = ctypes.POINTER(ctypes.c_int64)
 
@@ -91,6 +92,16 @@ SIGNATURES = {
     "fhe_encode": (_i, [_vp, _f64p, _f64p, _i, _i, _i, _pp]),
     "fhe_create_small_bootstrap_key": (_i, [_vp, _vp, _pp, _pp]),
     "fhe_bootstrap": (_i, [_vp, _vp, _vp, _vp, ctypes.POINTER(_vp), _i, _vp, _vp, _i, _pp]),
+    "fhe_create_bootstrap_key": (_i, [_vp, _vp, _i, ctypes.c_char_p, _pp]),
+    "fhe_bootstrap_key_destroy": (_i, [_vp]),
+    "fhe_bootstrap_key_info": (_i, [_vp, _ip, _ip, _ip, ctypes.POINTER(ctypes.c_uint64)]),
+    "fhe_bootstrap_key_deltas": (_i, [_vp, _ip, _i, _ip]),
+    "fhe_bootstrap_key_rotation_key": (_i, [_vp, _vp, _i, _pp]),
+    "fhe_bootstrap_key_stage": (_i, [_vp, _i, _i, _ip, _ip, _ip]),
+    "fhe_bootstrap_key_diagonal": (_i, [_vp, _vp, _i, _i, _i, _i, _pp]),
+    "fhe_bootstrap_key_small": (_i, [_vp, _vp, _pp, _pp]),
+    "fhe_bootstrap_with_key": (_i, [_vp, _vp, _vp, _vp, _vp, _pp]),
+    "fhe_rotate_with_bootstrap_key": (_i, [_vp, _vp, _vp, _i, _pp]),
     "fhe_add": (_i, [_vp, _vp, _vp, _pp]),
     "fhe_subtract": (_i, [_vp, _vp, _vp, _pp]),
     "fhe_add_plaintext": (_i, [_vp, _vp, _vp, _pp]),

@@ -5,6 +5,8 @@
 // final correction.  Every step is an engine operation already on the device; this
 // file composes them in the reference's order so each intermediate word matches,
 // and builds the butterfly twiddles on the host with the reference's expressions.
+#include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <complex>
 #include <map>
@@ -130,11 +132,11 @@ Stages butterfly_twiddles(int slot_count, int log_slot_count, int stage_count, b
   return out;
 }
 
-std::pair<int, int> stage_loop_counts(int twiddle_count) {
-  // get_stage_loop_counts (operation/bootstrap.cpp:265-278), inner shift 0.
+std::pair<int, int> stage_loop_counts(int twiddle_count, int inner_loop_shift = 0) {
+  // get_stage_loop_counts (operation/bootstrap.cpp:265-278).
   int bits = 0;
   for (int t = twiddle_count; t > 0; t >>= 1) bits++;
-  const int inner = 1 << ((bits + 1) / 2);
+  const int inner = 1 << ((bits + 1) / 2 + inner_loop_shift);
   return {inner, (twiddle_count + 1) / inner};
 }
 
@@ -503,8 +505,7 @@ std::unique_ptr<Data> Engine::bootstrap(const Data &ct, const Data &rk, const Da
     throw std::runtime_error(fn + ": the input unit ciphertext should have 2 polynomials.");
   if (ct.is_ntt())
     throw std::runtime_error(fn + ": the input unit ciphertext should not be in NTT form.");
-  if (stage_count < 1 || stage_count > params.log_slot_count)
-    throw std::runtime_error(fn + ": the stage count is not supported.");
+  require_bootstrap_stage_count(fn, stage_count, 0);
   auto leveled = level_down(ct, 0);
   auto raised = mod_raise(*leveled, to_sparse, to_dense);
   if (params.log_slot_count != params.log_n - 1) {
@@ -519,6 +520,437 @@ std::unique_ptr<Data> Engine::bootstrap(const Data &ct, const Data &rk, const Da
   auto rounded_imag = round_to_integer(*slot_imag, rk);
   auto coeff = slot_to_coeff(*rounded_real, *rounded_imag, keys, stage_count);
   auto bootstrapped = subtract(*raised, *coeff);
+  const int64_t ratio =
+      static_cast<int64_t>(std::round(static_cast<double>(params.base_prime()) / params.scale));
+  return multiply_integer(*bootstrapped, ratio);
+}
+
+// ------------------------------------------- bootstrap key (hoisted BSGS) --
+
+size_t BootstrapKey::bytes() const {
+  size_t total = 0;
+  auto add = [&](const Data *d) {
+    if (d) total += d->words() * sizeof(int64_t);
+  };
+  for (const auto &kv : rotation_keys) add(kv.second.get());
+  for (const auto *stages : {&coeff_to_slot, &slot_to_coeff})
+    for (const auto &stage : *stages)
+      for (const auto &row : stage.diagonals)
+        for (const auto &entry : row.second) add(entry.second.get());
+  add(to_sparse.get());
+  add(to_dense.get());
+  return total;
+}
+
+void Engine::require_bootstrap_stage_count(const std::string &fn, int stage_count,
+                                           int inner_loop_shift) const {
+  // CKKSEngine::require_bootstrap_stage_count (engine_require.cpp:1018-1100): the
+  // admissible stage counts per slot count and inner loop shift.
+  int lo = 3, hi = 5;
+  bool invalid = false;
+  const int ls = params.log_slot_count;
+  if (inner_loop_shift == 0) {
+    if (ls >= 1 && ls <= 3) lo = 1, hi = 1;
+    else if (ls <= 5 && ls >= 4) lo = 1, hi = 2;
+    else if (ls == 6) lo = 2, hi = 2;
+    else if (ls >= 7 && ls <= 9) lo = 2, hi = 3;
+    else if (ls == 10) lo = 2, hi = 4;
+    else if (ls == 11 || ls == 12) lo = 3, hi = 4;
+    else if (ls == 13 || ls == 14) lo = 3, hi = 5;
+  } else if (inner_loop_shift == 1) {
+    if (ls == 1 || ls == 2) invalid = true;
+    else if (ls >= 3 && ls <= 5) lo = 1, hi = 1;
+    else if (ls >= 6 && ls <= 8) lo = 2, hi = 2;
+    else if (ls == 9 || ls == 10) lo = 2, hi = 3;
+    else if (ls == 11) lo = 3, hi = 3;
+    else if (ls >= 12 && ls <= 14) lo = 3, hi = 4;
+  }
+  if (invalid || stage_count < lo || stage_count > hi)
+    throw std::runtime_error(fn + ": invalid stage count.");
+}
+
+void Engine::make_bootstrap_stage(BootstrapStage &stage, const std::vector<cvec> &twiddles,
+                                  int rotate_count, int level, int inner_loop_shift) {
+  // make_bootstrap_stage (engine_bootstrap.cpp:8-67): loop deltas, the order in which
+  // equal outer deltas are summed, and every diagonal encoded with the special
+  // primes at the stage's level, rescaled and put in NTT form.
+  const int count = static_cast<int>(twiddles.size());
+  const auto [inner, outer] = stage_loop_counts(count, inner_loop_shift);
+  stage.level = level;
+  stage.inner = inner;
+  stage.outer = outer;
+  stage.inner_deltas.assign(1, 0);
+  for (int i = 1; i < inner; i++) stage.inner_deltas.push_back(normalized_delta(i * rotate_count));
+  for (int o = 0; o < outer; o++) {
+    const int norm_o = o - outer / 2;
+    const int delta = normalized_delta(inner * norm_o * rotate_count);
+    stage.outer_deltas.push_back(delta);
+    bool fresh = true;
+    for (auto &entry : stage.process_order)
+      if (entry.first == delta) {
+        entry.second.push_back(o);
+        fresh = false;
+        break;
+      }
+    if (fresh) stage.process_order.push_back({delta, {o}});
+    auto &row = stage.diagonals[o];
+    for (int i = (o == 0 ? 1 : 0); i < inner; i++) {
+      const cvec factor = rotate_vector(twiddles[pmod(inner * norm_o + i, count)], -delta);
+      std::vector<double> re(factor.size()), im(factor.size());
+      for (size_t k = 0; k < factor.size(); k++) {
+        re[k] = factor[k].real();
+        im[k] = factor[k].imag();
+      }
+      auto encoded = encode(re.data(), im.data(), static_cast<int>(factor.size()), level, true);
+      auto rescaled = rescale_any(*encoded);
+      row[i] = to_ntt(*rescaled);
+    }
+  }
+}
+
+std::unique_ptr<BootstrapKey> Engine::create_bootstrap_key(const Data &sk, int stage_count,
+                                                           const std::string &size) {
+  // CKKSEngine::create_bootstrap_key (engine.cpp:162-215).
+  const std::string fn = "Create Bootstrap Key";
+  if (!params.preset.bootstrap)
+    throw std::runtime_error(fn + ": the engine is not for bootstrapping.");
+  if (sk.type != kSecretKey) throw std::invalid_argument(fn + ": the key is not a secret key.");
+  if (sk.level() < params.max_key_switching_level())
+    throw std::runtime_error(fn + ": the target level cannot be reached with the provided keys.");
+  std::string lower = size;
+  std::transform(lower.begin(), lower.end(), lower.begin(),
+                 [](unsigned char c) { return static_cast<char>(std::tolower(c)); });
+  int shift;
+  if (lower == "medium")
+    shift = 0;
+  else if (lower == "large")
+    shift = 1;
+  else
+    throw std::runtime_error(fn + ": invalid size.");
+  require_bootstrap_stage_count(fn, stage_count, shift);
+
+  auto bk = std::make_unique<BootstrapKey>();
+  bk->stage_count = stage_count;
+  bk->inner_loop_shift = shift;
+  // get_bootstrap_stage_levels (engine_bootstrap.cpp:121-130): nine levels for EvalRound.
+  const int max_level = params.max_key_switching_level();
+  const int cts_level = max_level;
+  const int stc_level = max_level - stage_count - 9;
+  const int slot = params.slot_count, log_slot = params.log_slot_count;
+
+  const auto &cts = bootstrap_twiddles(true, stage_count);
+  bk->coeff_to_slot.resize(stage_count);
+  int rotate_count = slot;
+  for (int s = 0; s < stage_count; s++) {
+    rotate_count >>= cts_log_radix(s, stage_count, log_slot);
+    make_bootstrap_stage(bk->coeff_to_slot[s], cts[s], rotate_count, cts_level - s, shift);
+  }
+  const auto &stc = bootstrap_twiddles(false, stage_count);
+  bk->slot_to_coeff.resize(stage_count);
+  rotate_count = 1;
+  for (int s = 0; s < stage_count; s++) {
+    make_bootstrap_stage(bk->slot_to_coeff[s], stc[s], rotate_count, stc_level - s, shift);
+    rotate_count <<= stc_log_radix(s, stage_count, log_slot);
+  }
+
+  // Rotation contexts in the reference's order (the random stream sees the same
+  // sequence of key generations): partial sums, then each stage's inner and outer
+  // deltas; a delta gets its key at the first level that needs it.
+  auto add_keys = [&](const std::vector<int> &deltas, int level, bool by_slot_count) {
+    for (int delta : deltas) {
+      if (delta == 0 || bk->rotation_keys.count(delta)) continue;
+      const int nd = normalized_delta(delta, by_slot_count);
+      bk->rotation_keys[delta] = create_fixed_rotation_key(sk, nd, level);
+    }
+  };
+  std::vector<int> partial;
+  for (int d = slot; d < params.n / 2; d <<= 1) partial.push_back(d);
+  add_keys(partial, max_level, false);
+  for (const auto *stages : {&bk->coeff_to_slot, &bk->slot_to_coeff})
+    for (const auto &stage : *stages) {
+      add_keys(stage.inner_deltas, stage.level, true);
+      add_keys(stage.outer_deltas, stage.level, true);
+    }
+  auto small = create_small_bootstrap_key(sk);
+  bk->to_sparse = std::move(small.first);
+  bk->to_dense = std::move(small.second);
+  return bk;
+}
+
+void Engine::decompose_into(const int64_t *x, int moduli_id, int64_t *out) {
+  const int n = params.n;
+  const DevicePartitions &dp = partitions(moduli_id, moduli_id);
+  int64_t *digits = alloc_words(static_cast<size_t>(params.chains(moduli_id)) * n);
+  cudaError_t e = timed("mixed_radix", [&] {
+    return launch_mixed_radix(tables_, dp, n, moduli_id, x, digits, stream_);
+  });
+  if (e == cudaSuccess)
+    e = timed("mod_up_ntt", [&] {
+      return launch_mod_up_ntt(tables_, dp, params.log_n, moduli_id, digits, out, stream_);
+    });
+  free_words(digits);
+  check(e, "decompose");
+}
+
+void Engine::mod_down_polys(int64_t *extended, int moduli_id, int polys, int64_t *out) {
+  const int L = params.chains(moduli_id), E = params.chains(moduli_id, true);
+  cudaError_t e = timed("mod_down_intt", [&] {
+    return launch_mod_down_intt(tables_, params.log_n, moduli_id, E, extended, stream_, polys);
+  });
+  if (e == cudaSuccess)
+    e = timed("mod_down_epilogue", [&] {
+      EpilogueOps ops;
+      ops.polys = polys;
+      return launch_mod_down_epilogue_ops(tables_, ks_, params.n, moduli_id, L, extended, ops, out,
+                                          stream_);
+    });
+  check(e, "mod down");
+}
+
+std::unique_ptr<Data> Engine::decompose(const Data &ct) {
+  // CKKSCore::decompose (core_key_switch.cpp:434-466): polynomial 1 of a
+  // coefficient-form text, every partition raised to the extended chain, NTT form.
+  if (ct.polys < 2 || (ct.flag & kFlagSpecial))
+    throw std::invalid_argument("decompose: the input should be a ciphertext without special primes.");
+  const int m = ct.moduli_id;
+  const DevicePartitions &dp = partitions(m, m);
+  auto out = make_data(kDecomposed, ct.flag | kFlagNtt | kFlagSpecial, m, dp.count, ct.scale);
+  decompose_into(ct.d + ct.poly_stride(), m, out->d);
+  return out;
+}
+
+std::unique_ptr<Data> Engine::mod_down_then_decompose(const Data &ct) {
+  // CKKSCore::mod_down_then_decompose (core_key_switch.cpp:468-508): polynomial 1 of
+  // an extended NTT-form text brought down to its chain, then decomposed.
+  const int m = ct.moduli_id, n = params.n;
+  const DevicePartitions &dp = partitions(m, m);
+  auto out = make_data(kDecomposed, ct.flag, m, dp.count, ct.scale);
+  int64_t *x = alloc_words(static_cast<size_t>(ct.chains) * n);
+  int64_t *reduced = alloc_words(static_cast<size_t>(params.chains(m)) * n);
+  cudaError_t e = cudaMemcpyAsync(x, ct.d + ct.poly_stride(), ct.chains * n * sizeof(int64_t),
+                                  cudaMemcpyDeviceToDevice, stream_);
+  if (e == cudaSuccess) {
+    try {
+      mod_down_polys(x, m, 1, reduced);
+      decompose_into(reduced, m, out->d);
+    } catch (...) {
+      free_words(x);
+      free_words(reduced);
+      throw;
+    }
+  }
+  free_words(x);
+  free_words(reduced);
+  check(e, "copy");
+  return out;
+}
+
+std::unique_ptr<Data> Engine::attach_special_primes(const Data &text) {
+  // attach_special_prime_chains_ (core.cpp:1127-1155): x * P on the chain, zero
+  // special limbs, then to_ntt_ over the extended chain.
+  if (text.flag & kFlagSpecial)
+    throw std::invalid_argument("attach special primes: the text already has them.");
+  const int m = text.moduli_id, L = text.chains, n = params.n;
+  auto out = make_data(text.type, text.flag | kFlagNtt | kFlagSpecial, m, text.polys, text.scale);
+  std::vector<int64_t> p_product(L);
+  for (int j = 0; j < L; j++) p_product[j] = params.p_product_mult_r[m + j];
+  const long long ops = out->poly_stride();
+  for (int p = 0; p < text.polys; p++) {
+    pointwise(kOpEnter, L, m, text.d + p * text.poly_stride(), nullptr, p_product.data(),
+              out->d + p * ops);
+    check(cudaMemsetAsync(out->d + p * ops + static_cast<long long>(L) * n, 0,
+                          static_cast<size_t>(out->chains - L) * n * sizeof(int64_t), stream_),
+          "zero special limbs");
+  }
+  ntt_in_place(out->d, out->chains, m, ops, text.polys);
+  return out;
+}
+
+std::unique_ptr<Data> Engine::remove_special_primes(const Data &text) {
+  // remove_special_prime_chains_ (core.cpp:1165-1187): ModDown of every polynomial.
+  if (!(text.flag & kFlagSpecial) || !text.is_ntt() || text.polys > 2)
+    throw std::invalid_argument("remove special primes: the text has no special primes.");
+  const int m = text.moduli_id;
+  auto out = make_data(text.type, text.flag & ~(kFlagNtt | kFlagSpecial), m, text.polys,
+                       text.scale);
+  int64_t *x = alloc_words(text.words());
+  cudaError_t e = cudaMemcpyAsync(x, text.d, text.words() * sizeof(int64_t),
+                                  cudaMemcpyDeviceToDevice, stream_);
+  if (e == cudaSuccess) {
+    try {
+      mod_down_polys(x, m, text.polys, out->d);
+    } catch (...) {
+      free_words(x);
+      throw;
+    }
+  }
+  free_words(x);
+  check(e, "copy");
+  return out;
+}
+
+std::unique_ptr<Data> Engine::core_ntt_rotate(const Data &ct, const Data &decomposed,
+                                              const Data &key, int delta) {
+  // CKKSCore::ntt_rotate (core.cpp:965-1000): the key switcher of the decomposition
+  // (create_key_switcher, core_key_switch.cpp:510-548), polynomial 0 added, both
+  // permuted in NTT form.
+  const int m = ct.moduli_id, n = params.n;
+  if (key.moduli_id > m)
+    throw std::runtime_error("the fixed rotation key was created at a lower level than the text.");
+  const DevicePartitions &dp = partitions(m, key.moduli_id);
+  if (dp.count != decomposed.polys || decomposed.moduli_id != m || ct.chains != decomposed.chains)
+    throw std::invalid_argument("ntt rotate: the decomposition does not match the text.");
+  if (key.polys < 2 * (dp.max_key_index + 1))
+    throw std::invalid_argument("the key switching key has too few polynomials.");
+  int64_t *acc = alloc_words(static_cast<size_t>(2) * ct.chains * n);
+  auto out = make_data(kUnitCiphertext, decomposed.flag, m, 2, ct.scale);
+  cudaError_t e = timed("key_inner_product", [&] {
+    return launch_key_inner_product(tables_, dp, n, m, decomposed.d, key.d, key.chains,
+                                    m - key.moduli_id, acc, stream_);
+  });
+  if (e == cudaSuccess) {
+    const int32_t *perm = device_ntt_permutation(delta);
+    e = timed("ntt_rotate", [&] {
+      return launch_ntt_rotate_finish(tables_, params.log_n, ct.chains, m, ct.d, acc, perm, out->d,
+                                      stream_);
+    });
+  }
+  free_words(acc);
+  check(e, "ntt rotate");
+  return out;
+}
+
+namespace {
+const Data &rotation_context(const std::string &fn, const BootstrapKey &bk, int delta) {
+  // get_rotation_context (engine_rotate.cpp:172-184).
+  auto it = bk.rotation_keys.find(delta);
+  if (it == bk.rotation_keys.end())
+    throw std::runtime_error(fn + ": the bootstrap key does not contain a rotation context for delta " +
+                             std::to_string(delta) + ".");
+  return *it->second;
+}
+}  // namespace
+
+std::unique_ptr<Data> Engine::ntt_rotate(const Data &ct, const Data &decomposed,
+                                         const BootstrapKey &bk, int delta) {
+  // CKKSEngine::ntt_rotate / ntt_rotate_ (engine_rotate.cpp:223-259).
+  const std::string fn = "Rotate Unit Ciphertext in NTT Form with Bootstrap Key";
+  if (ct.polys != 2)
+    throw std::runtime_error(fn + ": the input unit ciphertext should have 2 polynomials.");
+  if (!ct.is_ntt())
+    throw std::runtime_error(fn + ": the input unit ciphertext should be in NTT form.");
+  if (ct.level() != decomposed.level())
+    throw std::runtime_error(fn + ": the levels of the inputs do not match.");
+  const int nd = normalized_delta(delta);
+  if (nd == 0) return clone(ct);
+  return core_ntt_rotate(ct, decomposed, rotation_context(fn, bk, nd), nd);
+}
+
+std::unique_ptr<Data> Engine::rotate(const Data &ct, const BootstrapKey &bk, int delta,
+                                     bool normalize_by_slot_count) {
+  const std::string fn = "Rotate Unit Ciphertext with Bootstrap Key";
+  const int nd = normalized_delta(delta, normalize_by_slot_count);
+  if (nd == 0) return clone(ct);
+  return rotate(ct, rotation_context(fn, bk, nd));
+}
+
+std::unique_ptr<Data> Engine::apply_butterfly(const Data &ct, const BootstrapKey &bk,
+                                              const BootstrapStage &stage) {
+  // CKKSEngine::apply_butterfly(ct, bootstrap key, stage) (engine_bootstrap.cpp:216-291):
+  // one decomposition serves every inner rotation; the diagonal products of each
+  // outer group are summed in the extended domain and rotated once.
+  if (ct.level() <= 0)
+    throw std::runtime_error(
+        "Rescale Unit Ciphertext: the input unit ciphertext should have a positive level.");
+  Owned inner0;
+  std::vector<Owned> rotated;
+  {
+    auto rescaled = rescale_any(ct);
+    auto decomposed = decompose(*rescaled);
+    inner0 = attach_special_primes(*rescaled);
+    for (int delta : stage.inner_deltas) {
+      if (delta == 0) continue;
+      rotated.push_back(ntt_rotate(*inner0, *decomposed, bk, delta));
+    }
+  }
+  auto inner_text = [&](int i) -> const Data & { return i == 0 ? *inner0 : *rotated[i - 1]; };
+  Owned outer_sum;
+  for (const auto &[delta, outer_indices] : stage.process_order) {
+    Owned inner_sum;
+    for (int o : outer_indices) {
+      const auto &row = stage.diagonals.at(o);
+      for (int i = (o == 0 ? 1 : 0); i < stage.inner; i++) {
+        // multiply_for_butterfly: CKKSCore::multiply(ct, pt) (core.cpp:257-282).
+        const Data &x = inner_text(i);
+        const Data &diagonal = *row.at(i);
+        if (diagonal.moduli_id != x.moduli_id || diagonal.chains != x.chains)
+          throw std::runtime_error("apply butterfly: the diagonal does not match the text.");
+        auto product = make_data(kUnitCiphertext, (x.flag | diagonal.flag) & ~kFlagRescaled,
+                                 x.moduli_id, x.polys, x.scale * diagonal.scale);
+        const long long ps = x.poly_stride();
+        for (int p = 0; p < x.polys; p++)
+          pointwise(kOpMult, x.chains, x.moduli_id, x.d + p * ps, diagonal.d, nullptr,
+                    product->d + p * ps);
+        if (!inner_sum)
+          inner_sum = std::move(product);
+        else
+          add_inplace(*inner_sum, *product);
+      }
+    }
+    Owned turned = std::move(inner_sum);
+    if (delta != 0) {
+      auto decomposed = mod_down_then_decompose(*turned);
+      turned = ntt_rotate(*turned, *decomposed, bk, delta);
+    }
+    if (!outer_sum)
+      outer_sum = std::move(turned);
+    else
+      add_inplace(*outer_sum, *turned);
+  }
+  return remove_special_primes(*outer_sum);
+}
+
+std::unique_ptr<Data> Engine::bootstrap(const Data &ct, const Data &rk, const Data &ck,
+                                        const BootstrapKey &bk) {
+  // CKKSEngine::bootstrap(UnitCiphertext*, RelinearizationKey*, ConjugationKey*,
+  // BootstrapKey*) (engine_bootstrap.cpp:804-838).
+  const std::string fn = "Bootstrap Unit Ciphertext With Bootstrap Key";
+  if (!params.preset.bootstrap)
+    throw std::runtime_error(fn + ": the engine is not for bootstrapping.");
+  if (ct.polys != 2)
+    throw std::runtime_error(fn + ": the input unit ciphertext should have 2 polynomials.");
+  if (ct.is_ntt())
+    throw std::runtime_error(fn + ": the input unit ciphertext should not be in NTT form.");
+  if (!bk.to_sparse || !bk.to_dense || static_cast<int>(bk.coeff_to_slot.size()) != bk.stage_count ||
+      static_cast<int>(bk.slot_to_coeff.size()) != bk.stage_count)
+    throw std::invalid_argument(fn + ": the bootstrap key is incomplete.");
+  auto leveled = level_down(ct, 0);
+  auto raised = mod_raise(*leveled, *bk.to_sparse, *bk.to_dense);
+  if (params.log_slot_count != params.log_n - 1) {
+    // partial_sum_inplace with the bootstrap key (engine_bootstrap.cpp:298-313).
+    for (int delta = params.slot_count; delta < params.n / 2; delta <<= 1) {
+      auto turned = rotate(*raised, bk, delta, false);
+      add_inplace(*raised, *turned);
+    }
+  }
+  // coeff_to_slot with the bootstrap key (engine_bootstrap.cpp:370-400).
+  Owned current;
+  for (const auto &stage : bk.coeff_to_slot)
+    current = apply_butterfly(current ? *current : *raised, bk, stage);
+  auto conjugated = conjugate(*current, ck);
+  auto real_part = add(*current, *conjugated);
+  auto subtracted = subtract(*current, *conjugated);
+  auto imaginary_part = multiply_imaginary(*subtracted, -1);
+  current.reset();
+  conjugated.reset();
+  subtracted.reset();
+  auto rounded_real = round_to_integer(*real_part, rk);
+  auto rounded_imag = round_to_integer(*imaginary_part, rk);
+  // slot_to_coeff with the bootstrap key (engine_bootstrap.cpp:436-452).
+  auto multiplied = multiply_imaginary(*rounded_imag, 1);
+  current = add(*rounded_real, *multiplied);
+  for (const auto &stage : bk.slot_to_coeff) current = apply_butterfly(*current, bk, stage);
+  auto bootstrapped = subtract(*raised, *current);
   const int64_t ratio =
       static_cast<int64_t>(std::round(static_cast<double>(params.base_prime()) / params.scale));
   return multiply_integer(*bootstrapped, ratio);

@@ -19,6 +19,10 @@ struct fhe_data {
   Data *impl;
 };
 
+struct fhe_bootstrap_key {
+  fhe_b200::BootstrapKey *impl;
+};
+
 namespace fhe_b200 {
 namespace {
 thread_local std::string g_last_error;
@@ -669,6 +673,162 @@ int fhe_bootstrap(fhe_engine *engine, const fhe_data *ct, const fhe_data *rk, co
     *out = wrap(engine->impl->bootstrap(live(engine, ct), live(engine, rk), live(engine, ck), keys,
                                         live(engine, to_sparse), live(engine, to_dense),
                                         stage_count));
+  });
+}
+
+// The bootstrap key behind a handle, checked to belong to `engine`.
+static const fhe_b200::BootstrapKey &live_key(const fhe_engine *engine,
+                                              const fhe_bootstrap_key *key) {
+  const Data *part = key->impl->to_sparse.get();
+  if (!part || !part->engine) throw std::runtime_error("the engine of the bootstrap key was destroyed.");
+  if (engine && part->engine != engine->impl)
+    throw std::runtime_error("the bootstrap key is not compatible with this engine.");
+  return *key->impl;
+}
+
+int fhe_create_bootstrap_key(fhe_engine *engine, const fhe_data *secret_key, int stage_count,
+                             const char *size, fhe_bootstrap_key **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(secret_key);
+  REQUIRE_OUT(size);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] {
+    auto bk = engine->impl->create_bootstrap_key(live(engine, secret_key), stage_count, size);
+    auto h = new fhe_bootstrap_key;
+    h->impl = bk.release();
+    *out = h;
+  });
+}
+
+int fhe_bootstrap_key_destroy(fhe_bootstrap_key *key) {
+  if (!key) return FHE_OK;
+  delete key->impl;
+  delete key;
+  return FHE_OK;
+}
+
+int fhe_bootstrap_key_info(const fhe_bootstrap_key *key, int *stage_count, int *inner_loop_shift,
+                           int *rotation_key_count, uint64_t *bytes) {
+  REQUIRE_HANDLE(key);
+  return guarded([&] {
+    const auto &bk = live_key(nullptr, key);
+    if (stage_count) *stage_count = bk.stage_count;
+    if (inner_loop_shift) *inner_loop_shift = bk.inner_loop_shift;
+    if (rotation_key_count) *rotation_key_count = static_cast<int>(bk.rotation_keys.size());
+    if (bytes) *bytes = bk.bytes();
+  });
+}
+
+int fhe_bootstrap_key_deltas(const fhe_bootstrap_key *key, int *deltas, int capacity, int *count) {
+  REQUIRE_HANDLE(key);
+  REQUIRE_OUT(count);
+  return guarded([&] {
+    const auto &bk = live_key(nullptr, key);
+    int i = 0;
+    for (const auto &kv : bk.rotation_keys) {
+      if (deltas && i < capacity) deltas[i] = kv.first;
+      i++;
+    }
+    *count = i;
+  });
+}
+
+int fhe_bootstrap_key_rotation_key(fhe_engine *engine, const fhe_bootstrap_key *key, int delta,
+                                   fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(key);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] {
+    const auto &bk = live_key(engine, key);
+    auto it = bk.rotation_keys.find(delta);
+    if (it == bk.rotation_keys.end())
+      throw std::invalid_argument("the bootstrap key does not contain a rotation context for delta " +
+                                  std::to_string(delta) + ".");
+    *out = wrap(engine->impl->clone(*it->second));
+  });
+}
+
+static const fhe_b200::BootstrapStage &key_stage(const fhe_b200::BootstrapKey &bk, int to_slot,
+                                                 int stage) {
+  const auto &stages = to_slot ? bk.coeff_to_slot : bk.slot_to_coeff;
+  if (stage < 0 || stage >= static_cast<int>(stages.size()))
+    throw std::invalid_argument("the stage index is out of range.");
+  return stages[stage];
+}
+
+int fhe_bootstrap_key_stage(const fhe_bootstrap_key *key, int to_slot, int stage, int *level,
+                            int *inner_loop_count, int *outer_loop_count) {
+  REQUIRE_HANDLE(key);
+  return guarded([&] {
+    const auto &st = key_stage(live_key(nullptr, key), to_slot, stage);
+    if (level) *level = st.level;
+    if (inner_loop_count) *inner_loop_count = st.inner;
+    if (outer_loop_count) *outer_loop_count = st.outer;
+  });
+}
+
+int fhe_bootstrap_key_diagonal(fhe_engine *engine, const fhe_bootstrap_key *key, int to_slot,
+                               int stage, int outer, int inner, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(key);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] {
+    const auto &st = key_stage(live_key(engine, key), to_slot, stage);
+    auto row = st.diagonals.find(outer);
+    if (row == st.diagonals.end()) return;
+    auto entry = row->second.find(inner);
+    if (entry == row->second.end()) return;
+    *out = wrap(engine->impl->clone(*entry->second));
+  });
+}
+
+int fhe_bootstrap_key_small(fhe_engine *engine, const fhe_bootstrap_key *key,
+                            fhe_data **to_sparse, fhe_data **to_dense) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(key);
+  REQUIRE_OUT(to_sparse);
+  REQUIRE_OUT(to_dense);
+  *to_sparse = nullptr;
+  *to_dense = nullptr;
+  return guarded([&] {
+    const auto &bk = live_key(engine, key);
+    auto a = engine->impl->clone(*bk.to_sparse);
+    auto b = engine->impl->clone(*bk.to_dense);
+    *to_sparse = wrap(std::move(a));
+    *to_dense = wrap(std::move(b));
+  });
+}
+
+int fhe_bootstrap_with_key(fhe_engine *engine, const fhe_data *ct,
+                           const fhe_data *relinearization_key, const fhe_data *conjugation_key,
+                           const fhe_bootstrap_key *bootstrap_key, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(ct);
+  REQUIRE_HANDLE(relinearization_key);
+  REQUIRE_HANDLE(conjugation_key);
+  REQUIRE_HANDLE(bootstrap_key);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] {
+    *out = wrap(engine->impl->bootstrap(live(engine, ct), live(engine, relinearization_key),
+                                        live(engine, conjugation_key),
+                                        live_key(engine, bootstrap_key)));
+  });
+}
+
+int fhe_rotate_with_bootstrap_key(fhe_engine *engine, const fhe_data *ct,
+                                  const fhe_bootstrap_key *bootstrap_key, int delta,
+                                  fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(ct);
+  REQUIRE_HANDLE(bootstrap_key);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] {
+    *out = wrap(engine->impl->rotate(live(engine, ct), live_key(engine, bootstrap_key), delta));
   });
 }
 

@@ -24,6 +24,7 @@ int Data::level() const {
 
 const char *Data::type_name() const {
   switch (type) {
+    case kDecomposed: return "decomposed unit ciphertext";
     case kSecretKey: return "secret key";
     case kPublicKey: return "public key";
     case kRelinearizationKey: return "relinearization key";
@@ -278,8 +279,8 @@ void Engine::ntt_limbs(int64_t *limbs, int moduli_id, int chains, int polys, lon
 // ------------------------------------------------------------------ rescale --
 
 std::unique_ptr<Data> Engine::core_rescale(const Data &ct) {
-  if (ct.flag & kFlagSpecial)
-    throw std::invalid_argument("rescale of an extended polynomial is not supported.");
+  // rescale_once_ (core_rescale.cpp:5-25); with the special primes, their limbs are
+  // rescaled too (the prime tables run on past the chain).
   if (ct.chains < 2) throw std::runtime_error("cannot rescale a single-limb text.");
   auto out = make_data(ct.type, ct.flag | kFlagRescaled, ct.moduli_id + 1, ct.polys,
                        params.rescaled_scale(ct.scale, ct.moduli_id));

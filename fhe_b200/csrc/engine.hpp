@@ -30,6 +30,7 @@ enum DataFlag : int {
 };
 
 enum DataType : int {
+  kDecomposed = 0,  // DecomposedUnitCiphertext: [partitions][L+K][N], NTT form
   kSecretKey = 1,
   kPublicKey = 2,
   kRelinearizationKey = 3,
@@ -87,6 +88,35 @@ struct Data {
   const char *type_name() const;
   ~Data();
 };
+
+// One stage of the baby-step giant-step linear transform of bootstrapping
+// (PlainMatrix, data/plain_matrix.h; made by make_bootstrap_stage,
+// engine_bootstrap.cpp:8-67): the rotation steps and the twiddle diagonals, encoded
+// with the special primes, rescaled and in NTT form.
+struct BootstrapStage {
+  int level = 0;
+  int inner = 0;
+  int outer = 0;
+  std::vector<int> inner_deltas;  // inner_deltas[0] == 0
+  std::vector<int> outer_deltas;
+  std::vector<std::pair<int, std::vector<int>>> process_order;  // delta -> outer indices
+  std::map<int, std::map<int, std::unique_ptr<Data>>> diagonals;  // [outer][inner]
+};
+
+// BootstrapKey (data/bootstrap.h:24-44): fixed rotation keys per normalised delta
+// (with their NTT-form permutation, made on use), the coefficients-to-slots and
+// slots-to-coefficients stages, and the small bootstrap key.
+struct BootstrapKey {
+  int stage_count = 0;
+  int inner_loop_shift = 0;
+  std::map<int, std::unique_ptr<Data>> rotation_keys;
+  std::vector<BootstrapStage> coeff_to_slot;
+  std::vector<BootstrapStage> slot_to_coeff;
+  std::unique_ptr<Data> to_sparse;
+  std::unique_ptr<Data> to_dense;
+  size_t bytes() const;
+};
+
 
 class Engine {
  public:
@@ -191,6 +221,27 @@ class Engine {
                                                   const std::vector<int> &deltas);
   void add_inplace(Data &a, const Data &b);
 
+  // Bootstrapping with a bootstrap key (engine_bootstrap.cpp:804-838): hoisted
+  // baby-step giant-step transforms in the special-prime-extended NTT domain.
+  std::unique_ptr<BootstrapKey> create_bootstrap_key(const Data &sk, int stage_count,
+                                                     const std::string &size);
+  std::unique_ptr<Data> bootstrap(const Data &ct, const Data &rk, const Data &ck,
+                                  const BootstrapKey &bk);
+  // CKKSEngine::rotate(UnitCiphertext*, BootstrapKey*, delta, normalize)
+  // (engine_rotate.cpp:192-206).
+  std::unique_ptr<Data> rotate(const Data &ct, const BootstrapKey &bk, int delta,
+                               bool normalize_by_slot_count = true);
+  // CKKSCore::decompose (core_key_switch.cpp:434-466): every partition's ModUp of
+  // polynomial 1 of a coefficient-form text.
+  std::unique_ptr<Data> decompose(const Data &ct);
+  // CKKSEngine::ntt_rotate (engine_rotate.cpp:223-259) on an extended NTT-form text.
+  std::unique_ptr<Data> ntt_rotate(const Data &ct, const Data &decomposed, const BootstrapKey &bk,
+                                   int delta);
+  // CKKSCore::attach_special_prime_chains / remove_special_prime_chains
+  // (core.cpp:1127-1195).
+  std::unique_ptr<Data> attach_special_primes(const Data &text);
+  std::unique_ptr<Data> remove_special_primes(const Data &text);
+
   void ntt_limbs(int64_t *limbs, int moduli_id, int chains, int polys, long long stride,
                  bool inverse);
 
@@ -250,6 +301,22 @@ class Engine {
   std::unique_ptr<Data> sine(const Data &ct, const Data &rk);
   std::unique_ptr<Data> round_to_integer(const Data &ct, const Data &rk);
   std::unique_ptr<Data> make_signed_tile(const Data &ct);
+  void make_bootstrap_stage(BootstrapStage &stage,
+                            const std::vector<std::vector<std::complex<double>>> &twiddles,
+                            int rotate_count, int level, int inner_loop_shift);
+  void require_bootstrap_stage_count(const std::string &fn, int stage_count,
+                                     int inner_loop_shift) const;
+  std::unique_ptr<Data> mod_down_then_decompose(const Data &ct);
+  std::unique_ptr<Data> core_ntt_rotate(const Data &ct, const Data &decomposed, const Data &key,
+                                        int delta);
+  std::unique_ptr<Data> apply_butterfly(const Data &ct, const BootstrapKey &bk,
+                                        const BootstrapStage &stage);
+  // ModUp of every partition of one coefficient-form polynomial (L limbs at
+  // moduli_id) into `out` ([partitions][L+K][N]).
+  void decompose_into(const int64_t *x, int moduli_id, int64_t *out);
+  // ModDown (core_key_switch.cpp:110-160) of `polys` NTT-form extended polynomials
+  // (clobbered) into coefficient-form polynomials of L limbs.
+  void mod_down_polys(int64_t *extended, int moduli_id, int polys, int64_t *out);
   struct Matched;
   Matched match_texts(const Data &a, const Data &b, bool b_is_plain);
   std::vector<int64_t> add_multiplier(double value, int level) const;

@@ -472,19 +472,21 @@ cudaError_t launch_key_inner_product(const PrimeTables &t, const DevicePartition
 }
 
 cudaError_t launch_mod_down_intt(const PrimeTables &t, int log_n, int moduli_id, int extended,
-                                 int64_t *acc, cudaStream_t s) {
+                                 int64_t *acc, cudaStream_t s, int polys) {
+  if (polys < 1 || polys > 2) return cudaErrorInvalidValue;
   const long long stride = static_cast<long long>(extended) << log_n;
   PlainLoad ld{acc, stride};
   EnterExitStore<true> st{acc, stride, t.n_inverse, t.q, t.k};
-  return inverse_ntt(log_n, 2, extended, moduli_id, t, ld, st, acc, stride, s);
+  return inverse_ntt(log_n, polys, extended, moduli_id, t, ld, st, acc, stride, s);
 }
 
 cudaError_t launch_mod_down_epilogue_ops(const PrimeTables &t, const KeySwitchTables &ks, int n,
                                          int moduli_id, int limbs, const int64_t *acc,
                                          const EpilogueOps &ops, int64_t *out, cudaStream_t s) {
-  if ((ops.base_polys > 0 && ops.base == nullptr) || (ops.rescale && ops.signed_perm != nullptr))
+  if ((ops.base_polys > 0 && ops.base == nullptr) || (ops.rescale && ops.signed_perm != nullptr) ||
+      ops.polys < 1 || ops.polys > 2 || ops.base_polys > ops.polys)
     return cudaErrorInvalidValue;
-  const dim3 grid((n + kEpilogueCoeffs - 1) / kEpilogueCoeffs, 2);
+  const dim3 grid((n + kEpilogueCoeffs - 1) / kEpilogueCoeffs, ops.polys);
   switch (ks.special_count) {
 #define FHE_MD_CASE(K)                                                                      \
   case K:                                                                                   \

@@ -48,6 +48,7 @@ struct EpilogueOps {
   // word c goes to index perm[c] when perm[c] >= 0, negated to ~perm[c] otherwise,
   // then make_unsigned_reduce_2q_to_q.
   const int32_t *signed_perm = nullptr;
+  int polys = 2;  // polynomials of the accumulator ([polys][L+K][N]) divided
 };
 
 // z = tensor of two NTT-form ciphertexts (core.cpp:284-314): z0 = a0 b0,
@@ -89,7 +90,7 @@ cudaError_t launch_key_inner_product(const PrimeTables &t, const DevicePartition
 // Inverse NTT of both accumulators, then to_intt_ scaling and reduce_2q_to_q
 // (mod_down, core_key_switch.cpp:110-121), in place.
 cudaError_t launch_mod_down_intt(const PrimeTables &t, int log_n, int moduli_id, int extended,
-                                 int64_t *acc, cudaStream_t s);
+                                 int64_t *acc, cudaStream_t s, int polys = 2);
 
 // Epilogue of a key switch on (acc0, acc1) = INTT'd extended accumulators:
 // the sequential division by the special primes (core_key_switch.cpp:123-160),
@@ -125,6 +126,13 @@ cudaError_t launch_permute_signed(const PrimeTables &t, int n, int polys, int li
 cudaError_t launch_permute_gather(int n, int polys, int limbs, const int64_t *x,
                                   long long x_stride, const int32_t *perm, int64_t *y,
                                   long long y_stride, cudaStream_t s);
+
+// ntt_rotate's tail (core.cpp:965-1000) on extended NTT-form texts of `limbs` limbs:
+// y[0][c] = guard(x0[perm[c]] + acc[0][perm[c]], 2q), y[1][c] = acc[1][perm[c]];
+// acc and y are [2][limbs][N].
+cudaError_t launch_ntt_rotate_finish(const PrimeTables &t, int log_n, int limbs, int prime_base,
+                                     const int64_t *x0, const int64_t *acc, const int32_t *perm,
+                                     int64_t *y, cudaStream_t s);
 
 // Per-limb Montgomery constants passed by value.
 constexpr int kMaxScalarLimbs = 128;

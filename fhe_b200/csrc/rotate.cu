@@ -96,6 +96,21 @@ __global__ void scalar_enter_kernel(PrimeTables t, int log_n, int polys, int lim
   }
 }
 
+__global__ void ntt_rotate_finish_kernel(PrimeTables t, int log_n, int limbs, int prime_base,
+                                         const int64_t *x0, const int64_t *acc,
+                                         const int32_t *perm, int64_t *y) {
+  const long long per_poly = static_cast<long long>(limbs) << log_n;
+  const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (i >= 2 * per_poly) return;
+  const int poly = i >= per_poly ? 1 : 0;
+  const long long r = i - poly * per_poly;
+  const int j = static_cast<int>(r >> log_n);
+  const long long src = (static_cast<long long>(j) << log_n) + perm[r & ((1LL << log_n) - 1)];
+  int64_t v = acc[poly * per_poly + src];
+  if (poly == 0) v = guard(x0[src] + v, static_cast<int64_t>(t.q[prime_base + j] << 1));
+  y[i] = v;
+}
+
 }  // namespace
 
 cudaError_t launch_rotate_base(const PrimeTables &t, const KeySwitchTables &ks, int log_n,
@@ -139,6 +154,15 @@ cudaError_t launch_scalar_enter(const PrimeTables &t, int n, int polys, int limb
   note_launch();
   scalar_enter_kernel<<<grid_for(static_cast<long long>(polys) * limbs * n), kThreads, 0, st>>>(
       t, log_n, polys, limbs, prime_base, x, x_stride, x_limb_offset, s, y, y_stride);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ntt_rotate_finish(const PrimeTables &t, int log_n, int limbs, int prime_base,
+                                     const int64_t *x0, const int64_t *acc, const int32_t *perm,
+                                     int64_t *y, cudaStream_t s) {
+  note_launch();
+  ntt_rotate_finish_kernel<<<grid_for((2LL * limbs) << log_n), kThreads, 0, s>>>(
+      t, log_n, limbs, prime_base, x0, acc, perm, y);
   return cudaGetLastError();
 }
 

@@ -71,6 +71,69 @@ class Data:
             pass
 
 
+class BootstrapKey:
+    """A bootstrap key on the device (BootstrapKey, data/bootstrap.h:24-44)."""
+
+    def __init__(self, engine: "Engine", handle):
+        self.engine = engine
+        self._h = handle
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self) -> dict:
+        sc, shift, count = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        nbytes = ctypes.c_uint64()
+        check(_lib.load().fhe_bootstrap_key_info(self._h, ctypes.byref(sc), ctypes.byref(shift),
+                                                 ctypes.byref(count), ctypes.byref(nbytes)))
+        return dict(stage_count=sc.value, inner_loop_shift=shift.value,
+                    rotation_key_count=count.value, bytes=nbytes.value)
+
+    def deltas(self) -> list:
+        count = ctypes.c_int()
+        check(_lib.load().fhe_bootstrap_key_deltas(self._h, None, 0, ctypes.byref(count)))
+        arr = (ctypes.c_int * max(count.value, 1))()
+        check(_lib.load().fhe_bootstrap_key_deltas(self._h, arr, count.value, ctypes.byref(count)))
+        return list(arr[:count.value])
+
+    def rotation_key(self, delta: int) -> Data:
+        h = ctypes.c_void_p()
+        check(_lib.load().fhe_bootstrap_key_rotation_key(self.engine.handle, self._h, delta,
+                                                         ctypes.byref(h)))
+        return Data(self.engine, h)
+
+    def stage(self, to_slot: bool, stage: int) -> tuple:
+        """(level, inner loop count, outer loop count) of a stage."""
+        lv, inner, outer = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(_lib.load().fhe_bootstrap_key_stage(self._h, int(to_slot), stage, ctypes.byref(lv),
+                                                  ctypes.byref(inner), ctypes.byref(outer)))
+        return lv.value, inner.value, outer.value
+
+    def diagonal(self, to_slot: bool, stage: int, outer: int, inner: int):
+        h = ctypes.c_void_p()
+        check(_lib.load().fhe_bootstrap_key_diagonal(self.engine.handle, self._h, int(to_slot),
+                                                     stage, outer, inner, ctypes.byref(h)))
+        return Data(self.engine, h) if h.value else None
+
+    def small_bootstrap_key(self):
+        a, b = ctypes.c_void_p(), ctypes.c_void_p()
+        check(_lib.load().fhe_bootstrap_key_small(self.engine.handle, self._h, ctypes.byref(a),
+                                                  ctypes.byref(b)))
+        return Data(self.engine, a), Data(self.engine, b)
+
+    def free(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.load().fhe_bootstrap_key_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
 class Engine:
     """CKKS engine on one B200 (create_ckks_engine(CKKSConfig))."""
 
@@ -234,6 +297,11 @@ class Engine:
             check(_lib.load().fhe_rotate_with_keys(self._h, ct.handle, arr, len(key), delta,
                                                    int(normalize_by_slot_count), ctypes.byref(h)))
             return Data(self, h)
+        if isinstance(key, BootstrapKey):
+            h = ctypes.c_void_p()
+            check(_lib.load().fhe_rotate_with_bootstrap_key(self._h, ct.handle, key.handle, delta,
+                                                            ctypes.byref(h)))
+            return Data(self, h)
         return self._call("fhe_rotate", ct, key)
 
     def rotate_plaintext(self, pt: Data, delta: int) -> Data:
@@ -369,8 +437,23 @@ class Engine:
                                                          ctypes.byref(a), ctypes.byref(b)))
         return Data(self, a), Data(self, b)
 
+    def create_bootstrap_key(self, secret_key: Data, stage_count: int = 3,
+                             size: str = "medium") -> BootstrapKey:
+        h = ctypes.c_void_p()
+        check(_lib.load().fhe_create_bootstrap_key(self._h, secret_key.handle, stage_count,
+                                                   size.encode(), ctypes.byref(h)))
+        return BootstrapKey(self, h)
+
     def bootstrap(self, ct: Data, relinearization_key: Data, conjugation_key: Data,
-                  rotation_keys, small_bootstrap_key, stage_count: int = 3) -> Data:
+                  rotation_keys, small_bootstrap_key=None, stage_count: int = 3) -> Data:
+        """bootstrap(ct, rk, ck, bootstrap_key) or bootstrap(ct, rk, ck, rotation key,
+        small bootstrap key, stage_count), as the reference's two overloads."""
+        if isinstance(rotation_keys, BootstrapKey):
+            h = ctypes.c_void_p()
+            check(_lib.load().fhe_bootstrap_with_key(self._h, ct.handle, relinearization_key.handle,
+                                                     conjugation_key.handle, rotation_keys.handle,
+                                                     ctypes.byref(h)))
+            return Data(self, h)
         arr = (ctypes.c_void_p * len(rotation_keys))(*[k.handle for k in rotation_keys])
         to_sparse, to_dense = small_bootstrap_key
         h = ctypes.c_void_p()

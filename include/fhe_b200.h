@@ -78,6 +78,8 @@ enum {
 
 typedef struct fhe_engine fhe_engine;
 typedef struct fhe_data fhe_data;
+/* BootstrapKey (data/bootstrap.h:24-44), resident on the device. */
+typedef struct fhe_bootstrap_key fhe_bootstrap_key;
 
 /* CKKSConfig, src/ckks/config.h:11-34 (processor/stream/thread fields have no
  * GPU meaning and are absent). */
@@ -329,6 +331,51 @@ int fhe_bootstrap(fhe_engine *engine, const fhe_data *ct, const fhe_data *reline
                   const fhe_data *conjugation_key, const fhe_data *const *rotation_keys,
                   int rotation_key_count, const fhe_data *to_sparse, const fhe_data *to_dense,
                   int stage_count, fhe_data **out);
+
+/* CKKSEngine::create_bootstrap_key(SecretKey*, int stage_count, const std::string &size)
+ * (engine.h:47, engine.cpp:162-215): the baby-step giant-step stages of
+ * coefficients-to-slots and slots-to-coefficients (every twiddle diagonal encoded with
+ * the special primes, rescaled, NTT form), a fixed rotation key per step at the first
+ * level that needs it, and the small bootstrap key.  size is "medium" or "large"
+ * (inner loop shift 0 or 1, case-insensitive).  Keys are drawn from the engine's
+ * random stream in the reference's order. */
+int fhe_create_bootstrap_key(fhe_engine *engine, const fhe_data *secret_key, int stage_count,
+                             const char *size, fhe_bootstrap_key **out);
+/* Releases a bootstrap key (~BootstrapKey, data/bootstrap.cpp). */
+int fhe_bootstrap_key_destroy(fhe_bootstrap_key *key);
+/* stage_count_, inner_loop_shift_, rotation_contexts_.size() and the device bytes
+ * held (BootstrapKey::nbytes).  Any output pointer may be null. */
+int fhe_bootstrap_key_info(const fhe_bootstrap_key *key, int *stage_count, int *inner_loop_shift,
+                           int *rotation_key_count, uint64_t *bytes);
+/* The normalised deltas of the rotation contexts in ascending order; *count gets
+ * their number (at most capacity are written). */
+int fhe_bootstrap_key_deltas(const fhe_bootstrap_key *key, int *deltas, int capacity, int *count);
+/* A copy of the fixed rotation key of a normalised delta (rotation_contexts_[delta]). */
+int fhe_bootstrap_key_rotation_key(fhe_engine *engine, const fhe_bootstrap_key *key, int delta,
+                                   fhe_data **out);
+/* PlainMatrix level_, inner_loop_count_, outer_loop_count_ of a stage (to_slot 1:
+ * coefficients-to-slots, 0: slots-to-coefficients). */
+int fhe_bootstrap_key_stage(const fhe_bootstrap_key *key, int to_slot, int stage, int *level,
+                            int *inner_loop_count, int *outer_loop_count);
+/* A copy of encoded_diagonals_[outer][inner] of a stage; *out is null when the stage
+ * has no such diagonal. */
+int fhe_bootstrap_key_diagonal(fhe_engine *engine, const fhe_bootstrap_key *key, int to_slot,
+                               int stage, int outer, int inner, fhe_data **out);
+/* Copies of the small bootstrap key's two key switching keys. */
+int fhe_bootstrap_key_small(fhe_engine *engine, const fhe_bootstrap_key *key,
+                            fhe_data **to_sparse, fhe_data **to_dense);
+/* CKKSEngine::bootstrap(UnitCiphertext*, RelinearizationKey*, ConjugationKey*,
+ * BootstrapKey*) (engine_bootstrap.cpp:804-838): as fhe_bootstrap, with the hoisted
+ * baby-step giant-step transforms of the bootstrap key. */
+int fhe_bootstrap_with_key(fhe_engine *engine, const fhe_data *ct,
+                           const fhe_data *relinearization_key, const fhe_data *conjugation_key,
+                           const fhe_bootstrap_key *bootstrap_key, fhe_data **out);
+/* CKKSEngine::rotate(UnitCiphertext*, BootstrapKey*, int delta) (engine_rotate.cpp:
+ * 192-206): rotation by a delta (normalised by the slot count) whose fixed key the
+ * bootstrap key holds. */
+int fhe_rotate_with_bootstrap_key(fhe_engine *engine, const fhe_data *ct,
+                                  const fhe_bootstrap_key *bootstrap_key, int delta,
+                                  fhe_data **out);
 
 /* CKKSCore::switch_key (core.h, core.cpp:1058-1083): c0 + KS(c1) with a key
  * switching key (FHE_KEY_SWITCHING_KEY); NTT-form input is brought to coefficient

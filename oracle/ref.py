@@ -73,6 +73,16 @@ def lib():
             "ref_engine_level_down": (vp, [vp, vp, ctypes.c_int]),
             "ref_last_error": (ctypes.c_char_p, []),
             "ref_bench_bootstrap": (ctypes.c_double, [ctypes.c_int]),
+            "ref_bench_bootstrap_with_key": (ctypes.c_double, [ctypes.c_int]),
+            "ref_create_bootstrap_key": (vp, [vp, vp, ctypes.c_int, ctypes.c_char_p]),
+            "ref_bootstrap_key_delta_count": (ctypes.c_int, [vp]),
+            "ref_bootstrap_key_get": (vp, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+            "ref_bootstrap_key_stage": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int,
+                                                       ctypes.POINTER(ctypes.c_int)]),
+            "ref_bootstrap_key_diagonal": (vp, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_int]),
+            "ref_bootstrap_key_small": (vp, [vp, ctypes.c_int]),
+            "ref_engine_bootstrap_with_key": (vp, [vp, vp, vp, vp, vp]),
             "ref_create_rotation_key": (vp, [vp, vp, ctypes.c_int]),
             "ref_rotation_key_count": (ctypes.c_int, [vp]),
             "ref_rotation_key_get": (vp, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
@@ -302,6 +312,38 @@ class Engine:
         return self._h(lib().ref_engine_bootstrap(self.ptr, ct.ptr, rk.ptr, ck.ptr, rotk.ptr,
                                                   sbk.ptr, stage_count))
 
+    def create_bootstrap_key(self, sk, stage_count, size="medium"):
+        """Returns the owner handle of a BootstrapKey."""
+        return self._h(lib().ref_create_bootstrap_key(self.ptr, sk.ptr, stage_count,
+                                                      size.encode()))
+
+    def bootstrap_key_rotation_keys(self, bk):
+        """[(key switching key view, delta), ...] in ascending delta order."""
+        out = []
+        for i in range(lib().ref_bootstrap_key_delta_count(bk.ptr)):
+            d = ctypes.c_int()
+            out.append((self._h(lib().ref_bootstrap_key_get(bk.ptr, i, ctypes.byref(d))),
+                        d.value))
+        return out
+
+    def bootstrap_key_stage(self, bk, to_slot, stage):
+        """(level, inner loop count, outer loop count, process order entries)."""
+        shape = (ctypes.c_int * 4)()
+        if lib().ref_bootstrap_key_stage(bk.ptr, int(to_slot), stage, shape) != 0:
+            raise IndexError(stage)
+        return tuple(shape)
+
+    def bootstrap_key_diagonal(self, bk, to_slot, stage, outer, inner):
+        p = lib().ref_bootstrap_key_diagonal(bk.ptr, int(to_slot), stage, outer, inner)
+        return self._h(p) if p else None
+
+    def bootstrap_key_small(self, bk):
+        return [self._h(lib().ref_bootstrap_key_small(bk.ptr, i)) for i in (0, 1)]
+
+    def bootstrap_with_key(self, ct, rk, ck, bk):
+        return self._h(lib().ref_engine_bootstrap_with_key(self.ptr, ct.ptr, rk.ptr, ck.ptr,
+                                                           bk.ptr))
+
     def level_down(self, a, level):
         return self._h(lib().ref_engine_level_down(self.ptr, a.ptr, level))
 
@@ -362,3 +404,8 @@ def cdt_tree():
 def bench_bootstrap(threads: int) -> float:
     """Milliseconds of one reference bootstrap (N = 2^16, 3 stages, all given threads)."""
     return float(lib().ref_bench_bootstrap(threads))
+
+
+def bench_bootstrap_with_key(threads: int) -> float:
+    """Milliseconds of one reference bootstrap with a medium 3-stage bootstrap key."""
+    return float(lib().ref_bench_bootstrap_with_key(threads))

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <chrono>
 #include <complex>
+#include <iterator>
 #include <cstdint>
 #include <cstring>
 #include <map>
@@ -322,6 +323,7 @@ void ref_handle_free(void *h) {
   case 7: delete static_cast<ConjugationKey *>(handle->owner); break;
   case 9: delete static_cast<RotationKey *>(handle->owner); break;
   case 10: delete static_cast<SmallBootstrapKey *>(handle->owner); break;
+  case 12: delete static_cast<BootstrapKey *>(handle->owner); break;
   case 11: break;  // a view into another handle's key
   default: delete static_cast<Data *>(handle->owner); break;
   }
@@ -767,6 +769,78 @@ void *ref_engine_bootstrap(void *e, void *ct, void *rk, void *ck, void *rotk, vo
   }
 }
 
+// create_bootstrap_key(sk, stage_count, size): kind 12 owns the BootstrapKey.
+void *ref_create_bootstrap_key(void *e, void *sk, int stage_count, const char *size) {
+  try {
+    auto eng = static_cast<RefEngine *>(e)->engine.get();
+    auto s = static_cast<SecretKey *>(static_cast<Handle *>(sk)->data);
+    return wrap(12, nullptr, eng->create_bootstrap_key(s, stage_count, size));
+  } catch (...) {
+    remember_error();
+    return nullptr;
+  }
+}
+
+int ref_bootstrap_key_delta_count(void *h) {
+  auto bk = static_cast<BootstrapKey *>(static_cast<Handle *>(h)->owner);
+  return static_cast<int>(bk->rotation_contexts_.size());
+}
+
+// Rotation context i in ascending delta order: a view of its key switching key.
+void *ref_bootstrap_key_get(void *h, int i, int *delta) {
+  auto bk = static_cast<BootstrapKey *>(static_cast<Handle *>(h)->owner);
+  auto it = bk->rotation_contexts_.begin();
+  std::advance(it, i);
+  *delta = it->first;
+  return wrap(11, it->second.first->key_switching_key_, nullptr);
+}
+
+// shape: [level, inner loop count, outer loop count, process order entries].
+int ref_bootstrap_key_stage(void *h, int to_slot, int stage, int *shape) {
+  auto bk = static_cast<BootstrapKey *>(static_cast<Handle *>(h)->owner);
+  auto &stages = to_slot ? bk->coeff_to_slot_stages_ : bk->slot_to_coeff_stages_;
+  if (stage < 0 || stage >= static_cast<int>(stages.size())) return -1;
+  auto m = stages[stage];
+  shape[0] = m->level_;
+  shape[1] = m->inner_loop_count_;
+  shape[2] = m->outer_loop_count_;
+  shape[3] = static_cast<int>(m->outer_loop_process_order_.size());
+  return 0;
+}
+
+// A view of diagonal (outer, inner) of a stage, or null when the stage has none.
+void *ref_bootstrap_key_diagonal(void *h, int to_slot, int stage, int outer, int inner) {
+  auto bk = static_cast<BootstrapKey *>(static_cast<Handle *>(h)->owner);
+  auto &stages = to_slot ? bk->coeff_to_slot_stages_ : bk->slot_to_coeff_stages_;
+  auto &diagonals = stages[stage]->encoded_diagonals_;
+  auto o = diagonals.find(outer);
+  if (o == diagonals.end()) return nullptr;
+  auto i = o->second.find(inner);
+  if (i == o->second.end()) return nullptr;
+  return wrap(11, i->second, nullptr);
+}
+
+void *ref_bootstrap_key_small(void *h, int part) {
+  auto bk = static_cast<BootstrapKey *>(static_cast<Handle *>(h)->owner);
+  auto k = bk->small_bootstrap_key_;
+  return wrap(11, part == 0 ? k->to_sparse_ : k->to_dense_, nullptr);
+}
+
+void *ref_engine_bootstrap_with_key(void *e, void *ct, void *rk, void *ck, void *bk) {
+  try {
+    auto eng = static_cast<RefEngine *>(e)->engine.get();
+    auto r = eng->bootstrap(
+        static_cast<UnitCiphertext *>(static_cast<Handle *>(ct)->data),
+        static_cast<RelinearizationKey *>(static_cast<Handle *>(rk)->owner),
+        static_cast<ConjugationKey *>(static_cast<Handle *>(ck)->owner),
+        static_cast<BootstrapKey *>(static_cast<Handle *>(bk)->owner));
+    return wrap(4, r, r);
+  } catch (...) {
+    remember_error();
+    return nullptr;
+  }
+}
+
 void *ref_engine_encode(void *e, const double *re, const double *im, int count,
                         int level) {
   try {
@@ -904,6 +978,33 @@ double ref_bench_bootstrap(int threads) {
   delete pt;
   delete sbk;
   delete rot;
+  delete ck;
+  delete rk;
+  delete sk;
+  return std::chrono::duration<double, std::milli>(t1 - t0).count();
+}
+
+// Times one engine.bootstrap(ct, rk, ck, bootstrap key) with a "medium" bootstrap key
+// of 3 stages on the same workload; returns ms (key generation outside the timing).
+double ref_bench_bootstrap_with_key(int threads) {
+  auto config = make_config(16, -1, 4, -1, 2, threads);
+  CKKSEngine engine(config);
+  auto sk = engine.create_secret_key();
+  auto rk = engine.create_relinearization_key(sk);
+  auto ck = engine.create_conjugation_key(sk);
+  auto bk = engine.create_bootstrap_key(sk, 3, "medium");
+  const int slots = engine.get_slot_count();
+  std::mt19937_64 gen(1);
+  std::uniform_real_distribution<double> u(-1.0, 1.0);
+  std::vector<std::complex<double>> v(slots);
+  for (auto &z : v) z = {u(gen), u(gen)};
+  auto ct = engine.encrypt_unit(v, sk, 3);
+  auto t0 = std::chrono::steady_clock::now();
+  auto out = engine.bootstrap(ct, rk, ck, bk);
+  auto t1 = std::chrono::steady_clock::now();
+  delete out;
+  delete ct;
+  delete bk;
   delete ck;
   delete rk;
   delete sk;

@@ -86,6 +86,11 @@ def codec_values(seed: int, slot_count: int, complex_values: bool) -> np.ndarray
     return re + 1j * rng.uniform(-1.0, 1.0, slot_count)
 
 
+def digest_list(digests) -> str:
+    """One digest of an ordered list of digests (a bootstrap stage's diagonals)."""
+    return hashlib.sha256("".join(digests).encode()).hexdigest()
+
+
 def digest_doubles(a) -> str:
     """Digest of the IEEE bit patterns of a float64 / complex128 array."""
     a = np.ascontiguousarray(a)

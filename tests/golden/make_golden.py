@@ -25,7 +25,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
-from inputs import ROTATION_KEY_DELTAS, arith_inputs, codec_values, digest_doubles, key_switch_inputs, TIERS, case_inputs, digest  # noqa: E402
+from inputs import ROTATION_KEY_DELTAS, arith_inputs, codec_values, digest_doubles, digest_list, key_switch_inputs, TIERS, case_inputs, digest  # noqa: E402
 
 REF = os.environ.get("FHE_REFERENCE", "/root/reference")
 
@@ -367,6 +367,58 @@ def bootstrap_cases():
                  decoded=digest_doubles(dec), max_error=float(np.max(np.abs(dec - vals))))]
 
 
+def bootstrap_key_cases():
+    """Bootstrapping with a bootstrap key (bootstrap preset, N = 2^16, K = 4, 3 stages,
+    "medium"): after reseeding, secret, relinearization and conjugation keys, then
+    create_bootstrap_key (every fixed rotation key, the stages' diagonals, the small
+    bootstrap key), a secret-key encryption at level 3 and bootstrap(ct, rk, ck, bk)."""
+    from oracle import ref
+
+    log_n, K, preset = TIERS["bootstrap_gold"]
+    e = ref.Engine(log_n=log_n, special_prime_count=K, preset=preset, threads=os.cpu_count())
+    e.seed(BOOTSTRAP_SEED, BOOTSTRAP_NONCE)
+    out = {}
+    sk = e.create_secret_key()
+    out["secret_key"] = sk.limbs()
+    rk = e.create_relinearization_key(sk)
+    out["relinearization_key"] = rk.limbs()
+    ck = e.create_conjugation_key(sk)
+    out["conjugation_key"] = ck.limbs()
+    bk = e.create_bootstrap_key(sk, 3, "medium")
+    keys = e.bootstrap_key_rotation_keys(bk)
+    rotation_keys = [[d, digest(k.limbs())] for k, d in keys]
+    stages = []
+    for to_slot in (1, 0):
+        for stage in range(3):
+            level, inner, outer, _ = e.bootstrap_key_stage(bk, to_slot, stage)
+            diagonals = []
+            for o in range(outer):
+                for i in range(inner):
+                    d = e.bootstrap_key_diagonal(bk, to_slot, stage, o, i)
+                    if d is not None:
+                        diagonals.append(digest(d.limbs()))
+            stages.append(dict(to_slot=to_slot, stage=stage, level=level, inner=inner,
+                               outer=outer, diagonal_count=len(diagonals),
+                               diagonals=digest_list(diagonals)))
+    to_sparse, to_dense = e.bootstrap_key_small(bk)
+    out["to_sparse"] = to_sparse.limbs()
+    out["to_dense"] = to_dense.limbs()
+    vals = codec_values(4242, e.slot_count, True)
+    ct = e.encrypt(e.encode(vals, 3), sk)
+    out["ciphertext"] = ct.limbs()
+    boot = e.bootstrap_with_key(ct, rk, ck, bk)
+    out["bootstrapped"] = boot.limbs()
+    info = boot.info()
+    dec = e.decode(e.decrypt(boot, sk))
+    return [dict(tier="bootstrap_key_gold", log_n=log_n, special_prime_count=K, preset=preset,
+                 seed=list(BOOTSTRAP_SEED), nonce=list(BOOTSTRAP_NONCE), values_seed=4242,
+                 encrypt_level=3, stage_count=3, size="medium",
+                 moduli=[int(v) for v in e.tables()["q"]], rotation_keys=rotation_keys,
+                 stages=stages, output_moduli_id=info["moduli_id"], output_level=info["level"],
+                 digests={k: digest(v) for k, v in out.items()}, decoded=digest_doubles(dec),
+                 max_error=float(np.max(np.abs(dec - vals))))]
+
+
 def main():
     with open(os.path.join(HERE, "ntt_kat.json"), "w") as f:
         json.dump(parse_ntt_kats(), f, indent=1)
@@ -386,6 +438,9 @@ def main():
     boot = bootstrap_cases()
     with open(os.path.join(HERE, "bootstrap.json"), "w") as f:
         json.dump(boot, f, indent=1)
+    boot_key = bootstrap_key_cases()
+    with open(os.path.join(HERE, "bootstrap_key.json"), "w") as f:
+        json.dump(boot_key, f, indent=1)
     keygen = keygen_cases()
     with open(os.path.join(HERE, "keygen.json"), "w") as f:
         json.dump(keygen, f, indent=1)
