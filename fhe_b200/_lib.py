@@ -92,6 +92,7 @@ SIGNATURES = {
     "fhe_encode": (_i, [_vp, _f64p, _f64p, _i, _i, _i, _pp]),
     "fhe_create_small_bootstrap_key": (_i, [_vp, _vp, _pp, _pp]),
     "fhe_bootstrap": (_i, [_vp, _vp, _vp, _vp, ctypes.POINTER(_vp), _i, _vp, _vp, _i, _pp]),
+    "fhe_engine_set_tensor_cores": (_i, [_vp, _i]),
     "fhe_create_bootstrap_key": (_i, [_vp, _vp, _i, ctypes.c_char_p, _pp]),
     "fhe_bootstrap_key_destroy": (_i, [_vp]),
     "fhe_bootstrap_key_info": (_i, [_vp, _ip, _ip, _ip, ctypes.POINTER(ctypes.c_uint64)]),

@@ -697,13 +697,11 @@ void Engine::mod_down_polys(int64_t *extended, int moduli_id, int polys, int64_t
   cudaError_t e = timed("mod_down_intt", [&] {
     return launch_mod_down_intt(tables_, params.log_n, moduli_id, E, extended, stream_, polys);
   });
-  if (e == cudaSuccess)
-    e = timed("mod_down_epilogue", [&] {
-      EpilogueOps ops;
-      ops.polys = polys;
-      return launch_mod_down_epilogue_ops(tables_, ks_, params.n, moduli_id, L, extended, ops, out,
-                                          stream_);
-    });
+  if (e == cudaSuccess) {
+    EpilogueOps ops;
+    ops.polys = polys;
+    e = mod_down_epilogue(moduli_id, L, extended, ops, out);
+  }
   check(e, "mod down");
 }
 

@@ -686,6 +686,11 @@ static const fhe_b200::BootstrapKey &live_key(const fhe_engine *engine,
   return *key->impl;
 }
 
+int fhe_engine_set_tensor_cores(fhe_engine *engine, int enable) {
+  REQUIRE_HANDLE(engine);
+  return guarded([&] { engine->impl->set_tensor_cores(enable != 0); });
+}
+
 int fhe_create_bootstrap_key(fhe_engine *engine, const fhe_data *secret_key, int stage_count,
                              const char *size, fhe_bootstrap_key **out) {
   REQUIRE_HANDLE(engine);

@@ -60,6 +60,8 @@ Engine::Engine(const Config &config) : params(config) {
   check(cudaGetDevice(&device), "cudaGetDevice");
   check(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
   stream_ = own_stream_;
+  check(cudaMalloc(&device_error_, sizeof(int)), "cudaMalloc(error flag)");
+  check(cudaMemset(device_error_, 0, sizeof(int)), "clear error flag");
   // Keep freed blocks in the stream-ordered pool: key switching allocates and frees
   // the same temporaries every call.
   cudaMemPool_t pool;
@@ -125,10 +127,49 @@ Engine::~Engine() {
   for (auto &kv : signed_perm_cache_) cudaFree(kv.second);
   for (auto &kv : ntt_perm_cache_) cudaFree(kv.second);
   for (auto *b : table_buffers_) cudaFree(b);
+  if (device_error_) cudaFree(device_error_);
   if (own_stream_) cudaStreamDestroy(own_stream_);
 }
 
-void Engine::synchronize() { check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize"); }
+void Engine::synchronize() {
+  check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+  int flag = 0;
+  check(cudaMemcpy(&flag, device_error_, sizeof(int), cudaMemcpyDeviceToHost), "read error flag");
+  if (flag) {
+    check(cudaMemset(device_error_, 0, sizeof(int)), "clear error flag");
+    throw CudaError("a tensor-core wait ran out; the results since the last check are unspecified");
+  }
+}
+
+const ModDownTcTables *Engine::mod_down_tc(int moduli_id) {
+  const int L = params.chains(moduli_id), K = params.special_prime_count;
+  if (!mod_down_tc_supported(K, L, params.n)) return nullptr;
+  auto it = mod_down_tc_cache_.find(moduli_id);
+  if (it != mod_down_tc_cache_.end()) return &it->second;
+  const ModDownTcHost h = make_mod_down_tc_tables(params.q, params.p_inverse_mult_r, moduli_id, L, K);
+  ModDownTcTables tc;
+  tc.b = upload_table(h.b);
+  tc.c_r = upload_table(h.c_r);
+  tc.r40 = upload_table(h.r40);
+  tc.r80 = upload_table(h.r80);
+  tc.rounds = h.rounds;
+  tc.kb = h.kb;
+  return &mod_down_tc_cache_.emplace(moduli_id, tc).first->second;
+}
+
+cudaError_t Engine::mod_down_epilogue(int moduli_id, int limbs, const int64_t *acc,
+                                      const EpilogueOps &ops, int64_t *out) {
+  const ModDownTcTables *tc = tensor_cores_ ? mod_down_tc(moduli_id) : nullptr;
+  if (tc)
+    return timed("mod_down_epilogue_tc", [&] {
+      return launch_mod_down_epilogue_tc(tables_, ks_, *tc, params.n, moduli_id, limbs, acc, ops,
+                                         out, device_error_, stream_);
+    });
+  return timed("mod_down_epilogue", [&] {
+    return launch_mod_down_epilogue_ops(tables_, ks_, params.n, moduli_id, limbs, acc, ops, out,
+                                        stream_);
+  });
+}
 
 void Engine::upload_bytes(void *dst, const void *src, size_t bytes, const char *what) {
   check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_), what);
@@ -413,10 +454,7 @@ void Engine::key_switch_pipeline(const int64_t *c1, int moduli_id, const Data &k
     e = timed("mod_down_intt", [&] {
       return launch_mod_down_intt(tables_, params.log_n, moduli_id, E, acc, stream_);
     });
-  if (e == cudaSuccess)
-    e = timed("mod_down_epilogue", [&] {
-      return launch_mod_down_epilogue_ops(tables_, ks_, n, moduli_id, L, acc, ops, out, stream_);
-    });
+  if (e == cudaSuccess) e = mod_down_epilogue(moduli_id, L, acc, ops, out);
   free_words(digits);
   free_words(ext);
   free_words(acc);

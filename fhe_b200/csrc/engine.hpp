@@ -251,6 +251,11 @@ class Engine {
   std::string profile_report();  // "name launches total_ms" lines; synchronizes
   void profile_reset();
 
+  // The ModDown base conversion on the INT8 tensor pipe (on by default where the
+  // shape allows it) or on the CUDA cores; both give the same words.
+  void set_tensor_cores(bool on) { tensor_cores_ = on; }
+  bool tensor_cores() const { return tensor_cores_; }
+
   const PrimeTables &tables() const { return tables_; }
   const KeySwitchTables &key_switch_tables() const { return ks_; }
   const DevicePartitions &partitions(int moduli_id, int key_moduli_id);
@@ -262,6 +267,13 @@ class Engine {
   PrimeTables tables_{};
   KeySwitchTables ks_{};
   std::map<std::pair<int, int>, DevicePartitions> partition_cache_;
+  bool tensor_cores_ = true;
+  std::map<int, ModDownTcTables> mod_down_tc_cache_;  // moduli id -> tables
+  int *device_error_ = nullptr;  // set by a kernel whose bounded wait ran out
+  const ModDownTcTables *mod_down_tc(int moduli_id);
+  // The ModDown epilogue in the selected form.
+  cudaError_t mod_down_epilogue(int moduli_id, int limbs, const int64_t *acc,
+                                const EpilogueOps &ops, int64_t *out);
   RngState rng_{};
   unsigned long long rng_counter_ = 0;
   bool cdt_uploaded_ = false;

@@ -1,6 +1,7 @@
 // Device kernels of the B200 CKKS engine: element-wise families, rescale and the
 // hybrid key-switching pipeline (see kernels.cuh for the contract of each launcher).
 #include "kernels.cuh"
+#include "epilogue.cuh"
 #include "ntt.cuh"
 
 #include <atomic>
@@ -53,16 +54,6 @@ __global__ void add_reduce_kernel(PrimeTables t, int n, int limbs, int prime_bas
 
 // -------------------------------------------------------------- rescale --
 
-__device__ __forceinline__ int64_t rescale_word(int64_t xj, int64_t x0, int64_t rounder,
-                                                uint64_t q, uint64_t k, int64_t constant) {
-  const int64_t qs = static_cast<int64_t>(q), q2 = qs << 1;
-  int64_t v = xj - x0;  // mont_subtract (unit.cpp:58-64)
-  v = v >= 0 ? v : v + q2;
-  v = guard(v, qs);
-  v = mont_mult(v, constant, q, k);
-  v = guard(v + rounder, q2);  // add_tiled
-  return guard(v, qs);
-}
 
 __global__ void rescale_kernel(PrimeTables t, KeySwitchTables ks, int n, int limbs, int moduli_id,
                                const int64_t *x, long long xs, int64_t *y, long long ys) {
@@ -317,53 +308,8 @@ __global__ void __launch_bounds__(256)
       v = mont_mult(guard(v + q2 - divisor[s][c], q2), ks.p_inverse_mult_r[s * P + prime], q, kk);
     return v < 0 ? v + qs : guard(v, qs);  // make_unsigned_reduce_2q_to_q
   };
-  const long long in_stride = static_cast<long long>(L) * n;
-  const bool add_base = poly < ops.base_polys;  // uniform per CTA
-  const int64_t *b = add_base ? ops.base + poly * in_stride + coeff0 : nullptr;
-  auto combined = [&](int j, int c) -> int64_t {
-    const int64_t qs = static_cast<int64_t>(t.q[moduli_id + j]);
-    if (!add_base) return divide(j, c);
-    return guard(guard(b[static_cast<long long>(j) * n + c] + divide(j, c), qs << 1), qs);
-  };
   const int valid = n - coeff0 < CB ? n - coeff0 : CB;
-
-  if (!ops.rescale) {
-    int64_t *o = out + poly * in_stride;
-    if (ops.signed_perm == nullptr) {
-      for (int w = threadIdx.x; w < L * CB; w += blockDim.x) {
-        const int j = w / CB, c = w % CB;
-        if (c < valid) o[static_cast<long long>(j) * n + coeff0 + c] = combined(j, c);
-      }
-      return;
-    }
-    // Permuted store (rotate_ after key_switch_mod_down, core.cpp:939-952).
-    for (int w = threadIdx.x; w < L * CB; w += blockDim.x) {
-      const int j = w / CB, c = w % CB;
-      if (c >= valid) continue;
-      const int64_t qs = static_cast<int64_t>(t.q[moduli_id + j]);
-      const int32_t pc = ops.signed_perm[coeff0 + c];
-      int64_t v = combined(j, c);
-      if (pc < 0) v = -v;
-      v = v < 0 ? v + qs : guard(v, qs);
-      o[static_cast<long long>(j) * n + (pc < 0 ? ~pc : pc)] = v;
-    }
-    return;
-  }
-  // mode 2: rescale of the relinearized polynomial (core_rescale.cpp:5-25).
-  if (threadIdx.x < valid) first_limb[threadIdx.x] = combined(0, threadIdx.x);
-  __syncthreads();
-  const long long out_stride = static_cast<long long>(L - 1) * n;
-  int64_t *o = out + poly * out_stride + coeff0;
-  const uint64_t q_half = t.q[moduli_id] >> 1;  // unsigned comparison, as get_rounder
-  for (int w = threadIdx.x; w < (L - 1) * CB; w += blockDim.x) {
-    const int j = 1 + w / CB, c = w % CB;
-    if (c >= valid) continue;
-    const int prime = moduli_id + j;
-    const int64_t y0 = first_limb[c];
-    o[static_cast<long long>(j - 1) * n + c] =
-        rescale_word(combined(j, c), y0, static_cast<uint64_t>(y0) > q_half ? 1 : 0, t.q[prime], t.k[prime],
-                     ks.rescale_scale[static_cast<long long>(moduli_id) * P + prime]);
-  }
+  mod_down_store(t, ks, n, moduli_id, L, poly, coeff0, valid, ops, out, first_limb, divide);
 }
 
 struct TensorLoad {

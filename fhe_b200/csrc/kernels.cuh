@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <vector>
 
 #include "modarith.cuh"
 
@@ -108,6 +109,42 @@ cudaError_t launch_mod_down_epilogue(const PrimeTables &t, const KeySwitchTables
 cudaError_t launch_mod_down_epilogue_ops(const PrimeTables &t, const KeySwitchTables &ks, int n,
                                          int moduli_id, int limbs, const int64_t *acc,
                                          const EpilogueOps &ops, int64_t *out, cudaStream_t s);
+
+// Constants of the tensor-core ModDown at one moduli id (built by the engine):
+// the exact division by the special primes is the linear map
+//   v_j = x_j * prod_s pinv_s - sum_s d_s * prod_{t>=s} pinv_t   (mod q_j)
+// of the divisor sequence d_s, whose sum runs on the INT8 tensor pipe with 8-bit
+// limbs of d_s and of the constants (S32 accumulation, exact).
+struct ModDownTcTables {
+  const uint8_t *b = nullptr;   // [rounds][256 columns][kb bytes], UMMA K-major core matrices
+  const int64_t *c_r = nullptr; // [L] prod_s pinv_s * R mod q_j (x_j's Montgomery factor)
+  const int64_t *r40 = nullptr; // [L] 2^40 * R mod q_j
+  const int64_t *r80 = nullptr; // [L] 2^80 * R mod q_j
+  int rounds = 0;               // ceil(L / 16) MMA rounds of 16 target limbs
+  int kb = 0;                   // A row bytes: 9 K rounded up to 32
+};
+
+// The epilogue of launch_mod_down_epilogue_ops with the division as an INT8
+// tensor-core contraction (tcgen05.mma kind::i8, accumulator in tensor memory).
+// Same words as the CUDA-core form.  n must be a multiple of 128; error receives 1
+// if a tensor-core wait ran out (the outputs are then unspecified).
+cudaError_t launch_mod_down_epilogue_tc(const PrimeTables &t, const KeySwitchTables &ks,
+                                        const ModDownTcTables &tc, int n, int moduli_id,
+                                        int limbs, const int64_t *acc, const EpilogueOps &ops,
+                                        int64_t *out, int *error, cudaStream_t s);
+// Whether the tensor-core epilogue serves this shape (special primes, limbs, n).
+bool mod_down_tc_supported(int special_count, int limbs, int n);
+// Host copies of the tables of ModDownTcTables at one moduli id, from the prime
+// chain and the p^-1 R constants per division step ([K][prime]).
+struct ModDownTcHost {
+  std::vector<uint8_t> b;
+  std::vector<int64_t> c_r, r40, r80;
+  int rounds = 0;
+  int kb = 0;
+};
+ModDownTcHost make_mod_down_tc_tables(const std::vector<uint64_t> &q,
+                                      const std::vector<std::vector<int64_t>> &p_inverse_mult_r,
+                                      int moduli_id, int limbs, int special_count);
 
 // Rotation's b * P term (create_key_switcher_for_rotate, core_key_switch.cpp:550-576):
 // acc0[j] = reduce(acc0[j] + NTT(mont(mont(c0[j], P mod q * R), R^2))) for the L

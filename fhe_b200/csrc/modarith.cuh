@@ -119,6 +119,19 @@ struct RedcSum {
   }
 };
 
+// One word of rescale_once_ (core_rescale.cpp:5-25): (x_j - x_0) reduced, times
+// q_0^-1 R, plus the rounder of x_0, reduced to [0, q).
+FHE_HD int64_t rescale_word(int64_t xj, int64_t x0, int64_t rounder, uint64_t q, uint64_t k,
+                            int64_t constant) {
+  const int64_t qs = static_cast<int64_t>(q), q2 = qs << 1;
+  int64_t v = xj - x0;  // mont_subtract (unit.cpp:58-64)
+  v = v >= 0 ? v : v + q2;
+  v = guard(v, qs);
+  v = mont_mult(v, constant, q, k);
+  v = guard(v + rounder, q2);  // add_tiled
+  return guard(v, qs);
+}
+
 FHE_HD bool redc_operand_ok(int64_t x) {
   return static_cast<uint64_t>(x) < (uint64_t(1) << 61);
 }

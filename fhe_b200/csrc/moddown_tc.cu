@@ -1,0 +1,357 @@
+// Tensor-core ModDown epilogue (tcgen05.mma kind::i8 on sm_100a).
+//
+// The reference divides every normal limb by the special primes one after another
+// (core_key_switch.cpp:123-160).  Unrolled, limb j of a coefficient becomes
+//   v_j = x_j * prod_s pinv_s - sum_s d_s * prod_{t>=s} pinv_t   (mod q_j),
+// where d_s is the divisor of step s (special limb K-1-s after s divisions) and
+// pinv_s the step's inverse special prime modulo q_j; its final make_unsigned
+// leaves v_j canonical in [0, q_j), so any exact evaluation gives the same word.
+// Here the sum over s runs on the INT8 tensor pipe:
+//   * A (128 coefficients x kb bytes): the 8 little-endian bytes of every d_s as an
+//     unsigned word, then one byte [d_s < 0] per divisor (a negative d_s read as
+//     unsigned is d_s + 2^64, which the sign byte takes back);
+//   * B (per moduli id, built on the host): for target j and byte shift h, the byte
+//     h - u of w'_sj = -prod_{t>=s} pinv_t mod q_j against byte u of d_s, and byte h
+//     of z_sj = -2^64 w'_sj mod q_j against the sign byte of d_s;
+//   * D (tensor memory, S32): 16 columns per target, column h = the exact partial
+//     sum at byte shift h (h < 15; each below 2^23).
+// The epilogue folds the partial sums into three words below 2^56 (shifts 0-4,
+// 5-9 and 10-14), scales the upper two by 2^40 and 2^80 and x_j by prod pinv with
+// one Montgomery product each, and reduces the total (below 2^63) to [0, q_j).
+// The divisor triangle (K(K-1)/2 divisions per coefficient) stays on the CUDA
+// cores, as in the CUDA-core form.
+#include <cstring>
+#include <vector>
+
+#include "epilogue.cuh"
+#include "kernels.cuh"
+#include "modarith.cuh"
+
+namespace fhe_b200 {
+
+namespace {
+
+constexpr int kTcCoeffs = 128;   // MMA M = tensor memory lanes = coefficients per CTA
+constexpr int kTcThreads = 256;  // two warpgroups; warp w reads lanes 32 (w % 4) ...
+constexpr int kTcTargets = 16;   // target limbs per MMA round
+constexpr int kTcColumns = 256;  // 16 targets x 16 byte shifts = MMA N = TMEM columns
+constexpr uint32_t kTcWaitLimit = 1u << 22;
+
+constexpr int row_bytes(int K) { return (9 * K + 31) / 32 * 32; }
+
+// Byte offset of element (row, k) of a K-major operand of `rows` rows stored as
+// UMMA core matrices (8 rows x 16 bytes): [k / 16][row / 8][row % 8][k % 16].
+__host__ __device__ inline int core_offset(int row, int k, int rows) {
+  return ((k / 16) * (rows / 8) + row / 8) * 128 + (row % 8) * 16 + (k % 16);
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor: K-major without swizzle; lbo = bytes between the
+// two 16-byte halves of a 32-byte K step, sbo = bytes between 8-row groups.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return static_cast<uint64_t>((addr >> 4) & 0x3FFF) |
+         (static_cast<uint64_t>((lbo >> 4) & 0x3FFF) << 16) |
+         (static_cast<uint64_t>((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(done)
+      : "r"(addr), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+__device__ bool mbar_wait(uint32_t addr, uint32_t parity) {
+  for (uint32_t i = 0; i < kTcWaitLimit; i++)
+    if (mbar_try_wait(addr, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void tmem_load16(uint32_t addr, uint32_t (&d)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]),
+        "=r"(d[7]), "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]),
+        "=r"(d[14]), "=r"(d[15])
+      : "r"(addr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// Five partial sums (each below 2^23) at byte shifts 0, 8, ..., 32: below 2^56.
+__device__ __forceinline__ uint64_t fold5(const uint32_t *d) {
+  return static_cast<uint64_t>(d[0]) + (static_cast<uint64_t>(d[1]) << 8) +
+         (static_cast<uint64_t>(d[2]) << 16) + (static_cast<uint64_t>(d[3]) << 24) +
+         (static_cast<uint64_t>(d[4]) << 32);
+}
+
+template <int K>
+__global__ void __launch_bounds__(kTcThreads)
+    mod_down_tc_kernel(PrimeTables t, KeySwitchTables ks, ModDownTcTables tc, int n,
+                       int moduli_id, int L, const int64_t *acc, EpilogueOps ops, int64_t *out,
+                       int *error) {
+  constexpr int KB = row_bytes(K);
+  extern __shared__ __align__(128) uint8_t smem[];
+  uint8_t *sA = smem;                                   // [128 rows][KB], core matrices
+  uint8_t *sB = smem + kTcCoeffs * KB;                  // [rounds][256 rows][KB]
+  int64_t *divided = reinterpret_cast<int64_t *>(sB + static_cast<size_t>(tc.rounds) * kTcColumns * KB);
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_base;
+  __shared__ int64_t first_limb[kTcCoeffs];
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int poly = blockIdx.y;
+  const int coeff0 = blockIdx.x * kTcCoeffs;
+  const int P = ks.prime_count;
+  const int64_t *x = acc + static_cast<long long>(poly) * (L + K) * n + coeff0;
+
+  // 1. Divisor triangle of one coefficient per thread, then its A row.
+  if (tid < kTcCoeffs) {
+    int64_t sp[K];
+#pragma unroll
+    for (int i = 0; i < K; i++) sp[i] = x[static_cast<long long>(L + i) * n + tid];
+    uint64_t w[KB / 8];
+#pragma unroll
+    for (int i = 0; i < KB / 8; i++) w[i] = 0;
+#pragma unroll
+    for (int s = 0; s < K; s++) {
+      const int64_t d = sp[K - 1 - s];
+      w[s] = static_cast<uint64_t>(d);
+      if (d < 0) w[K + (s >> 3)] |= 1ull << (8 * (s & 7));
+#pragma unroll
+      for (int i = 0; i < K - 1 - s; i++) {
+        const int prime = moduli_id + L + i;
+        const uint64_t q = t.q[prime];
+        const int64_t q2 = static_cast<int64_t>(q << 1);
+        sp[i] = mont_mult(guard(sp[i] + q2 - d, q2), ks.p_inverse_mult_r[s * P + prime], q,
+                          t.k[prime]);
+      }
+    }
+#pragma unroll
+    for (int ch = 0; ch < KB / 16; ch++) {
+      const uint4 v = make_uint4(static_cast<uint32_t>(w[2 * ch]), static_cast<uint32_t>(w[2 * ch] >> 32),
+                                 static_cast<uint32_t>(w[2 * ch + 1]),
+                                 static_cast<uint32_t>(w[2 * ch + 1] >> 32));
+      *reinterpret_cast<uint4 *>(sA + core_offset(tid, ch * 16, kTcCoeffs)) = v;
+    }
+  }
+  // 2. The constant B matrix, already in core-matrix order.
+  {
+    const int chunks = tc.rounds * kTcColumns * KB / 16;
+    const uint4 *src = reinterpret_cast<const uint4 *>(tc.b);
+    uint4 *dst = reinterpret_cast<uint4 *>(sB);
+    for (int i = tid; i < chunks; i += kTcThreads) dst[i] = src[i];
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(&tmem_base)),
+                 "r"(kTcColumns));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar)), "r"(1));
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base;
+  const uint32_t bar = smem_addr(&mbar);
+
+  // 3. One MMA round per 16 targets; each thread folds 8 targets of its coefficient.
+  constexpr uint32_t idesc = (2u << 4) | (static_cast<uint32_t>(kTcColumns >> 3) << 17) |
+                             (static_cast<uint32_t>(kTcCoeffs >> 4) << 24);
+  const int lane_base = (warp & 3) * 32;
+  const int row = lane_base + lane;
+  const int half = warp >> 2;
+  bool ok = true;
+  int round = 0;
+  for (; round < tc.rounds; round++) {
+    if (tid == 0) {
+#pragma unroll
+      for (int k = 0; k < KB / 32; k++) {
+        const uint64_t da = umma_desc(smem_addr(sA) + k * 2 * (kTcCoeffs / 8) * 128,
+                                      (kTcCoeffs / 8) * 128, 128);
+        const uint64_t db = umma_desc(smem_addr(sB) + round * kTcColumns * KB +
+                                          k * 2 * (kTcColumns / 8) * 128,
+                                      (kTcColumns / 8) * 128, 128);
+        mma_i8(tmem, da, db, idesc, k > 0 ? 1u : 0u);
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       bar)
+                   : "memory");
+    }
+    ok = __syncthreads_and(mbar_wait(bar, round & 1)) != 0;
+    if (!ok) break;
+    tc_fence_after();
+    for (int jl = half * 8; jl < half * 8 + 8; jl++) {
+      const int j = round * kTcTargets + jl;
+      if (j >= L) break;  // uniform across the warp
+      uint32_t d[16];
+      tmem_load16(tmem + (static_cast<uint32_t>(lane_base) << 16) + jl * 16, d);
+      const int prime = moduli_id + j;
+      const uint64_t q = t.q[prime], kq = t.k[prime];
+      const uint64_t c0 = fold5(d), c1 = fold5(d + 5), c2 = fold5(d + 10);
+      const int64_t xj = x[static_cast<long long>(j) * n + row];
+      const uint64_t v = c0 + static_cast<uint64_t>(mont_mult(static_cast<int64_t>(c1), tc.r40[j], q, kq)) +
+                         static_cast<uint64_t>(mont_mult(static_cast<int64_t>(c2), tc.r80[j], q, kq)) +
+                         static_cast<uint64_t>(mont_mult(xj, tc.c_r[j], q, kq));
+      const uint64_t est = static_cast<uint64_t>(static_cast<double>(v) * t.inv_q[prime]);
+      int64_t r = static_cast<int64_t>(v - est * q);
+      const int64_t qs = static_cast<int64_t>(q);
+      if (r < 0) r += qs;
+      if (r < 0) r += qs;
+      if (r >= qs) r -= qs;
+      if (r >= qs) r -= qs;
+      divided[j * kTcCoeffs + row] = r;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+  }
+  if (!ok) {
+    // The round's MMAs may still be running: wait for them (bounded) before the
+    // tensor memory is given back.
+    if (tid == 0) atomicExch(error, 1);
+    if (warp == 0) mbar_wait(bar, round & 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcColumns));
+  if (!ok) return;
+
+  // 4. The caller's operations on the divided limbs.
+  mod_down_store(t, ks, n, moduli_id, L, poly, coeff0, kTcCoeffs, ops, out, first_limb,
+                 [&](int j, int c) -> int64_t { return divided[j * kTcCoeffs + c]; });
+}
+
+size_t tc_smem_bytes(int K, int L) {
+  const int kb = row_bytes(K);
+  const int rounds = (L + kTcTargets - 1) / kTcTargets;
+  return static_cast<size_t>(kTcCoeffs) * kb + static_cast<size_t>(rounds) * kTcColumns * kb +
+         static_cast<size_t>(L) * kTcCoeffs * sizeof(int64_t);
+}
+
+using u128 = unsigned __int128;
+
+uint64_t mul_mod(uint64_t a, uint64_t b, uint64_t m) {
+  return static_cast<uint64_t>(static_cast<u128>(a) * b % m);
+}
+
+uint64_t pow_mod(uint64_t b, uint64_t e, uint64_t m) {
+  uint64_t r = 1 % m;
+  b %= m;
+  for (; e; e >>= 1, b = mul_mod(b, b, m))
+    if (e & 1) r = mul_mod(r, b, m);
+  return r;
+}
+
+}  // namespace
+
+bool mod_down_tc_supported(int special_count, int limbs, int n) {
+  return special_count >= 1 && special_count <= 16 && limbs >= 1 && n >= kTcCoeffs &&
+         n % kTcCoeffs == 0 && tc_smem_bytes(special_count, limbs) <= 200 * 1024;
+}
+
+ModDownTcHost make_mod_down_tc_tables(const std::vector<uint64_t> &q,
+                                      const std::vector<std::vector<int64_t>> &p_inverse_mult_r,
+                                      int moduli_id, int limbs, int special_count) {
+  const int K = special_count, L = limbs;
+  ModDownTcHost h;
+  h.kb = row_bytes(K);
+  h.rounds = (L + kTcTargets - 1) / kTcTargets;
+  h.b.assign(static_cast<size_t>(h.rounds) * kTcColumns * h.kb, 0);
+  h.c_r.resize(L);
+  h.r40.resize(L);
+  h.r80.resize(L);
+  for (int j = 0; j < L; j++) {
+    const int prime = moduli_id + j;
+    const uint64_t m = q[prime];
+    const uint64_t r = pow_mod(2, 62, m);
+    const uint64_t r_inv = pow_mod(r, m - 2, m);  // m is prime
+    std::vector<uint64_t> w(K);
+    uint64_t prod = 1 % m;
+    for (int s = K - 1; s >= 0; s--) {
+      const uint64_t pr = static_cast<uint64_t>(p_inverse_mult_r[s][prime]) % m;
+      prod = mul_mod(prod, mul_mod(pr, r_inv, m), m);  // times p_s^-1 mod q_j
+      w[s] = prod;
+    }
+    h.c_r[j] = static_cast<int64_t>(mul_mod(prod, r, m));
+    h.r40[j] = static_cast<int64_t>(pow_mod(2, 40 + 62, m));
+    h.r80[j] = static_cast<int64_t>(pow_mod(2, 80 + 62, m));
+    const uint64_t two64 = static_cast<uint64_t>((static_cast<u128>(1) << 64) % m);
+    const int round = j / kTcTargets, jl = j % kTcTargets;
+    uint8_t *b = h.b.data() + static_cast<size_t>(round) * kTcColumns * h.kb;
+    for (int s = 0; s < K; s++) {
+      const uint64_t wn = (m - w[s]) % m;
+      const uint64_t z = (m - mul_mod(two64, wn, m)) % m;
+      for (int sh = 0; sh < 15; sh++) {
+        const int col = jl * 16 + sh;
+        for (int u = 0; u < 8; u++) {
+          const int v = sh - u;
+          if (v < 0 || v >= 8) continue;
+          b[core_offset(col, s * 8 + u, kTcColumns)] = static_cast<uint8_t>(wn >> (8 * v));
+        }
+        if (sh < 8) b[core_offset(col, 8 * K + s, kTcColumns)] = static_cast<uint8_t>(z >> (8 * sh));
+      }
+    }
+  }
+  return h;
+}
+
+cudaError_t launch_mod_down_epilogue_tc(const PrimeTables &t, const KeySwitchTables &ks,
+                                        const ModDownTcTables &tc, int n, int moduli_id,
+                                        int limbs, const int64_t *acc, const EpilogueOps &ops,
+                                        int64_t *out, int *error, cudaStream_t s) {
+  const int K = ks.special_count;
+  if (!mod_down_tc_supported(K, limbs, n) || tc.b == nullptr || error == nullptr ||
+      tc.kb != row_bytes(K) || tc.rounds != (limbs + kTcTargets - 1) / kTcTargets ||
+      (ops.base_polys > 0 && ops.base == nullptr) || (ops.rescale && ops.signed_perm != nullptr) ||
+      ops.polys < 1 || ops.polys > 2 || ops.base_polys > ops.polys)
+    return cudaErrorInvalidValue;
+  const size_t smem = tc_smem_bytes(K, limbs);
+  const dim3 grid(n / kTcCoeffs, ops.polys);
+  cudaError_t e = cudaSuccess;
+  switch (K) {
+#define FHE_TC_CASE(KK)                                                                         \
+  case KK:                                                                                      \
+    e = cudaFuncSetAttribute(mod_down_tc_kernel<KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                             static_cast<int>(smem));                                           \
+    if (e != cudaSuccess) return e;                                                             \
+    note_launch();                                                                              \
+    mod_down_tc_kernel<KK><<<grid, kTcThreads, smem, s>>>(t, ks, tc, n, moduli_id, limbs, acc,  \
+                                                          ops, out, error);                     \
+    break;
+    FHE_TC_CASE(1) FHE_TC_CASE(2) FHE_TC_CASE(3) FHE_TC_CASE(4) FHE_TC_CASE(5) FHE_TC_CASE(6)
+    FHE_TC_CASE(7) FHE_TC_CASE(8) FHE_TC_CASE(9) FHE_TC_CASE(10) FHE_TC_CASE(11) FHE_TC_CASE(12)
+    FHE_TC_CASE(13) FHE_TC_CASE(14) FHE_TC_CASE(15) FHE_TC_CASE(16)
+#undef FHE_TC_CASE
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace fhe_b200

@@ -437,6 +437,10 @@ class Engine:
                                                          ctypes.byref(a), ctypes.byref(b)))
         return Data(self, a), Data(self, b)
 
+    def set_tensor_cores(self, enable: bool) -> None:
+        """INT8 tensor-core (default) or CUDA-core ModDown base conversion; same words."""
+        check(_lib.load().fhe_engine_set_tensor_cores(self._h, int(enable)))
+
     def create_bootstrap_key(self, secret_key: Data, stage_count: int = 3,
                              size: str = "medium") -> BootstrapKey:
         h = ctypes.c_void_p()

@@ -400,6 +400,14 @@ int fhe_relinearize_noalloc(fhe_engine *engine, const int64_t *ct_device, int mo
                             const int64_t *key_device, int key_moduli_id, int key_polys,
                             int64_t *out_device);
 
+/* ---- B200 options (no reference counterpart) ---------------------------------------- */
+
+/* Selects the form of the ModDown base conversion (the exact division by the special
+ * primes, core_key_switch.cpp:123-160): nonzero (the default) uses the INT8 tensor
+ * pipe (tcgen05.mma kind::i8) where the shape allows it, zero the CUDA cores.  Both
+ * give the same words. */
+int fhe_engine_set_tensor_cores(fhe_engine *engine, int enable);
+
 /* ---- processor-level kernels on device limbs (src/processor/single.h) --------------- */
 
 /* SingleProcessor::ntt / intt (single.cpp:420-454) on `polys` x `chains` device limbs
