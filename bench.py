@@ -146,6 +146,7 @@ def kernel_bytes(L: int, E: int, dnum: int, n: int) -> dict:
         "key_inner_product": (3 * dnum * E + 2 * E) * limb, # ext + 2 key polys, 2 out
         "mod_down_intt": 2 * 2 * E * limb,                  # 2 polys in and out
         "mod_down_epilogue": (2 * E + 2 * L + 2 * (L - 1)) * limb,
+        "mod_down_epilogue_tc": (2 * E + 2 * L + 2 * (L - 1)) * limb,
     }
 
 
@@ -505,6 +506,31 @@ def main(argv=None):
                     "share_of_timed_region": ms / elapsed,
                     "kernel_ms_per_step": {k: v[1] / args.steps for k, v in prof.items()}}
 
+    # ---- the same step with the ModDown on the CUDA cores (tensor cores are the default)
+    def timed_form(tensor_cores: bool):
+        eng.set_tensor_cores(tensor_cores)
+        step()
+        torch.cuda.synchronize()
+        eng.profile_reset()
+        eng.set_profiling(True)
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(args.steps):
+            step()
+        s1.record(stream)
+        torch.cuda.synchronize()
+        eng.set_profiling(False)
+        p = eng.profile()
+        eng.set_tensor_cores(2)
+        ms, u = aggregate(s0.elapsed_time(s1), float(B * args.steps), world, backend)
+        fam = "mod_down_epilogue_tc" if "mod_down_epilogue_tc" in p else "mod_down_epilogue"
+        cnt, fam_ms = p.get(fam, (0, 0.0))
+        return {"value": u / (ms / 1e3), "unit": "ct/s", "mod_down_kernel": fam,
+                "mod_down_avg_launch_ms": fam_ms / cnt if cnt else None,
+                "mod_down_ms_per_step": fam_ms / args.steps}
+
+    forms = {"tensor_core": timed_form(True), "cuda_core": timed_form(False)}
+
     # ---- end to end through the C ABI with pinned host buffers
     in_words = 2 * L0 * n
     out_words = 2 * (L - 1) * n
@@ -556,6 +582,7 @@ def main(argv=None):
                        "relinearize_limbs": L, "dnum": dnum, "parallelism": f"replicas{world}",
                        "l2": f"inputs larger than L2 ({B} pairs x {2 * 2 * L0 * n * 8 / 1e6:.1f} MB)"},
             "roofline": roofline,
+            "bconv_forms": forms,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "ct/s",
                     "h2d_bytes_per_step": B * 2 * in_words * 8,

@@ -686,9 +686,9 @@ static const fhe_b200::BootstrapKey &live_key(const fhe_engine *engine,
   return *key->impl;
 }
 
-int fhe_engine_set_tensor_cores(fhe_engine *engine, int enable) {
+int fhe_engine_set_tensor_cores(fhe_engine *engine, int mode) {
   REQUIRE_HANDLE(engine);
-  return guarded([&] { engine->impl->set_tensor_cores(enable != 0); });
+  return guarded([&] { engine->impl->set_tensor_cores(mode); });
 }
 
 int fhe_create_bootstrap_key(fhe_engine *engine, const fhe_data *secret_key, int stage_count,

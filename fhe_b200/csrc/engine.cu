@@ -157,9 +157,18 @@ const ModDownTcTables *Engine::mod_down_tc(int moduli_id) {
   return &mod_down_tc_cache_.emplace(moduli_id, tc).first->second;
 }
 
+void Engine::set_tensor_cores(int mode) {
+  if (mode != kTensorCoresOff && mode != kTensorCoresOn && mode != kTensorCoresAuto)
+    throw std::invalid_argument("the tensor core mode should be 0 (off), 1 (on) or 2 (auto).");
+  tensor_cores_ = mode;
+}
+
 cudaError_t Engine::mod_down_epilogue(int moduli_id, int limbs, const int64_t *acc,
                                       const EpilogueOps &ops, int64_t *out) {
-  const ModDownTcTables *tc = tensor_cores_ ? mod_down_tc(moduli_id) : nullptr;
+  const bool use = tensor_cores_ == kTensorCoresOn ||
+                   (tensor_cores_ == kTensorCoresAuto &&
+                    params.special_prime_count >= kTensorCoreMinSpecial);
+  const ModDownTcTables *tc = use ? mod_down_tc(moduli_id) : nullptr;
   if (tc)
     return timed("mod_down_epilogue_tc", [&] {
       return launch_mod_down_epilogue_tc(tables_, ks_, *tc, params.n, moduli_id, limbs, acc, ops,

@@ -251,10 +251,15 @@ class Engine {
   std::string profile_report();  // "name launches total_ms" lines; synchronizes
   void profile_reset();
 
-  // The ModDown base conversion on the INT8 tensor pipe (on by default where the
-  // shape allows it) or on the CUDA cores; both give the same words.
-  void set_tensor_cores(bool on) { tensor_cores_ = on; }
-  bool tensor_cores() const { return tensor_cores_; }
+  // Where the ModDown base conversion runs; every mode gives the same words.
+  //   kTensorCoresOff: CUDA cores; kTensorCoresOn: the INT8 tensor pipe wherever the
+  //   shape allows it; kTensorCoresAuto (default): the tensor pipe from
+  //   kTensorCoreMinSpecial special primes on, where it is the faster form (its cost
+  //   per output is fixed, the sequential division's grows with K).
+  enum TensorCoreMode : int { kTensorCoresOff = 0, kTensorCoresOn = 1, kTensorCoresAuto = 2 };
+  static constexpr int kTensorCoreMinSpecial = 6;
+  void set_tensor_cores(int mode);
+  int tensor_cores() const { return tensor_cores_; }
 
   const PrimeTables &tables() const { return tables_; }
   const KeySwitchTables &key_switch_tables() const { return ks_; }
@@ -267,7 +272,7 @@ class Engine {
   PrimeTables tables_{};
   KeySwitchTables ks_{};
   std::map<std::pair<int, int>, DevicePartitions> partition_cache_;
-  bool tensor_cores_ = true;
+  int tensor_cores_ = kTensorCoresAuto;
   std::map<int, ModDownTcTables> mod_down_tc_cache_;  // moduli id -> tables
   int *device_error_ = nullptr;  // set by a kernel whose bounded wait ran out
   const ModDownTcTables *mod_down_tc(int moduli_id);

@@ -437,9 +437,10 @@ class Engine:
                                                          ctypes.byref(a), ctypes.byref(b)))
         return Data(self, a), Data(self, b)
 
-    def set_tensor_cores(self, enable: bool) -> None:
-        """INT8 tensor-core (default) or CUDA-core ModDown base conversion; same words."""
-        check(_lib.load().fhe_engine_set_tensor_cores(self._h, int(enable)))
+    def set_tensor_cores(self, mode) -> None:
+        """Where the ModDown base conversion runs: False/0 CUDA cores, True/1 the INT8
+        tensor pipe, 2 (default) the tensor pipe from 6 special primes on; same words."""
+        check(_lib.load().fhe_engine_set_tensor_cores(self._h, int(mode)))
 
     def create_bootstrap_key(self, secret_key: Data, stage_count: int = 3,
                              size: str = "medium") -> BootstrapKey:

@@ -402,11 +402,17 @@ int fhe_relinearize_noalloc(fhe_engine *engine, const int64_t *ct_device, int mo
 
 /* ---- B200 options (no reference counterpart) ---------------------------------------- */
 
-/* Selects the form of the ModDown base conversion (the exact division by the special
- * primes, core_key_switch.cpp:123-160): nonzero (the default) uses the INT8 tensor
- * pipe (tcgen05.mma kind::i8) where the shape allows it, zero the CUDA cores.  Both
- * give the same words. */
-int fhe_engine_set_tensor_cores(fhe_engine *engine, int enable);
+/* Selects where the ModDown base conversion (the exact division by the special
+ * primes, core_key_switch.cpp:123-160) runs: FHE_TENSOR_CORES_OFF on the CUDA cores,
+ * FHE_TENSOR_CORES_ON on the INT8 tensor pipe (tcgen05.mma kind::i8) wherever the
+ * shape allows it, FHE_TENSOR_CORES_AUTO (the default) on the tensor pipe from 6
+ * special primes on, where it is the faster form.  Every mode gives the same words. */
+enum {
+  FHE_TENSOR_CORES_OFF = 0,
+  FHE_TENSOR_CORES_ON = 1,
+  FHE_TENSOR_CORES_AUTO = 2
+};
+int fhe_engine_set_tensor_cores(fhe_engine *engine, int mode);
 
 /* ---- processor-level kernels on device limbs (src/processor/single.h) --------------- */
 

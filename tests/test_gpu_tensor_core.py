@@ -33,7 +33,7 @@ def run_both(e, fn):
     try:
         plain = fn()
     finally:
-        e.set_tensor_cores(True)
+        e.set_tensor_cores(2)
         e.set_profiling(False)
     return tc, plain, families
 
