@@ -257,7 +257,7 @@ class Engine {
   //   kTensorCoreMinSpecial special primes on, where it is the faster form (its cost
   //   per output is fixed, the sequential division's grows with K).
   enum TensorCoreMode : int { kTensorCoresOff = 0, kTensorCoresOn = 1, kTensorCoresAuto = 2 };
-  static constexpr int kTensorCoreMinSpecial = 6;
+  static constexpr int kTensorCoreMinSpecial = 4;
   void set_tensor_cores(int mode);
   int tensor_cores() const { return tensor_cores_; }
 

@@ -14,7 +14,9 @@
 //     h - u of w'_sj = -prod_{t>=s} pinv_t mod q_j against byte u of d_s, and byte h
 //     of z_sj = -2^64 w'_sj mod q_j against the sign byte of d_s;
 //   * D (tensor memory, S32): 16 columns per target, column h = the exact partial
-//     sum at byte shift h (h < 15; each below 2^23).
+//     sum at byte shift h (h < 15; each below 2^23); one MMA round covers 8 targets,
+//     so a CTA holds 128 tensor-memory columns and the B of one round, and four
+//     CTAs fit on an SM.
 // The epilogue folds the partial sums into three words below 2^56 (shifts 0-4,
 // 5-9 and 10-14), scales the upper two by 2^40 and 2^80 and x_j by prod pinv with
 // one Montgomery product each, and reduces the total (below 2^63) to [0, q_j).
@@ -33,8 +35,8 @@ namespace {
 
 constexpr int kTcCoeffs = 128;   // MMA M = tensor memory lanes = coefficients per CTA
 constexpr int kTcThreads = 256;  // two warpgroups; warp w reads lanes 32 (w % 4) ...
-constexpr int kTcTargets = 16;   // target limbs per MMA round
-constexpr int kTcColumns = 256;  // 16 targets x 16 byte shifts = MMA N = TMEM columns
+constexpr int kTcTargets = 8;    // target limbs per MMA round
+constexpr int kTcColumns = 128;  // 8 targets x 16 byte shifts = MMA N = TMEM columns
 constexpr uint32_t kTcWaitLimit = 1u << 22;
 
 constexpr int row_bytes(int K) { return (9 * K + 31) / 32 * 32; }
@@ -108,16 +110,17 @@ __device__ __forceinline__ uint64_t fold5(const uint32_t *d) {
          (static_cast<uint64_t>(d[4]) << 32);
 }
 
+// Four CTAs per SM (64 registers) where that costs no spills, fewer otherwise.
 template <int K>
-__global__ void __launch_bounds__(kTcThreads)
+__global__ void __launch_bounds__(kTcThreads, K <= 10 && K != 7 ? 4 : (K <= 13 ? 3 : 1))
     mod_down_tc_kernel(PrimeTables t, KeySwitchTables ks, ModDownTcTables tc, int n,
                        int moduli_id, int L, const int64_t *acc, EpilogueOps ops, int64_t *out,
                        int *error) {
   constexpr int KB = row_bytes(K);
   extern __shared__ __align__(128) uint8_t smem[];
-  uint8_t *sA = smem;                                   // [128 rows][KB], core matrices
-  uint8_t *sB = smem + kTcCoeffs * KB;                  // [rounds][256 rows][KB]
-  int64_t *divided = reinterpret_cast<int64_t *>(sB + static_cast<size_t>(tc.rounds) * kTcColumns * KB);
+  uint8_t *sA = smem;                   // [128 rows][KB], core matrices
+  uint8_t *sB = smem + kTcCoeffs * KB;  // one round: [128 columns][KB]
+  int64_t *divided = reinterpret_cast<int64_t *>(sB + kTcColumns * KB);
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_base;
   __shared__ int64_t first_limb[kTcCoeffs];
@@ -158,13 +161,6 @@ __global__ void __launch_bounds__(kTcThreads)
       *reinterpret_cast<uint4 *>(sA + core_offset(tid, ch * 16, kTcCoeffs)) = v;
     }
   }
-  // 2. The constant B matrix, already in core-matrix order.
-  {
-    const int chunks = tc.rounds * kTcColumns * KB / 16;
-    const uint4 *src = reinterpret_cast<const uint4 *>(tc.b);
-    uint4 *dst = reinterpret_cast<uint4 *>(sB);
-    for (int i = tid; i < chunks; i += kTcThreads) dst[i] = src[i];
-  }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_addr(&tmem_base)),
@@ -179,7 +175,7 @@ __global__ void __launch_bounds__(kTcThreads)
   const uint32_t tmem = tmem_base;
   const uint32_t bar = smem_addr(&mbar);
 
-  // 3. One MMA round per 16 targets; each thread folds 8 targets of its coefficient.
+  // 3. One MMA round per 8 targets; each thread folds 4 targets of its coefficient.
   constexpr uint32_t idesc = (2u << 4) | (static_cast<uint32_t>(kTcColumns >> 3) << 17) |
                              (static_cast<uint32_t>(kTcCoeffs >> 4) << 24);
   const int lane_base = (warp & 3) * 32;
@@ -188,13 +184,22 @@ __global__ void __launch_bounds__(kTcThreads)
   bool ok = true;
   int round = 0;
   for (; round < tc.rounds; round++) {
+    {
+      // The round's slice of the constant B matrix, already in core-matrix order
+      // (the previous round's MMAs have completed: every thread passed its wait).
+      constexpr int chunks = kTcColumns * KB / 16;
+      const uint4 *src = reinterpret_cast<const uint4 *>(tc.b) + static_cast<size_t>(round) * chunks;
+      uint4 *dst = reinterpret_cast<uint4 *>(sB);
+      for (int i = tid; i < chunks; i += kTcThreads) dst[i] = src[i];
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();
+    }
     if (tid == 0) {
 #pragma unroll
       for (int k = 0; k < KB / 32; k++) {
         const uint64_t da = umma_desc(smem_addr(sA) + k * 2 * (kTcCoeffs / 8) * 128,
                                       (kTcCoeffs / 8) * 128, 128);
-        const uint64_t db = umma_desc(smem_addr(sB) + round * kTcColumns * KB +
-                                          k * 2 * (kTcColumns / 8) * 128,
+        const uint64_t db = umma_desc(smem_addr(sB) + k * 2 * (kTcColumns / 8) * 128,
                                       (kTcColumns / 8) * 128, 128);
         mma_i8(tmem, da, db, idesc, k > 0 ? 1u : 0u);
       }
@@ -205,7 +210,7 @@ __global__ void __launch_bounds__(kTcThreads)
     ok = __syncthreads_and(mbar_wait(bar, round & 1)) != 0;
     if (!ok) break;
     tc_fence_after();
-    for (int jl = half * 8; jl < half * 8 + 8; jl++) {
+    for (int jl = half * (kTcTargets / 2); jl < (half + 1) * (kTcTargets / 2); jl++) {
       const int j = round * kTcTargets + jl;
       if (j >= L) break;  // uniform across the warp
       uint32_t d[16];
@@ -250,8 +255,7 @@ __global__ void __launch_bounds__(kTcThreads)
 
 size_t tc_smem_bytes(int K, int L) {
   const int kb = row_bytes(K);
-  const int rounds = (L + kTcTargets - 1) / kTcTargets;
-  return static_cast<size_t>(kTcCoeffs) * kb + static_cast<size_t>(rounds) * kTcColumns * kb +
+  return static_cast<size_t>(kTcCoeffs) * kb + static_cast<size_t>(kTcColumns) * kb +
          static_cast<size_t>(L) * kTcCoeffs * sizeof(int64_t);
 }
 

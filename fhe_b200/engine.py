@@ -439,7 +439,7 @@ class Engine:
 
     def set_tensor_cores(self, mode) -> None:
         """Where the ModDown base conversion runs: False/0 CUDA cores, True/1 the INT8
-        tensor pipe, 2 (default) the tensor pipe from 6 special primes on; same words."""
+        tensor pipe, 2 (default) the tensor pipe from 4 special primes on; same words."""
         check(_lib.load().fhe_engine_set_tensor_cores(self._h, int(mode)))
 
     def create_bootstrap_key(self, secret_key: Data, stage_count: int = 3,

@@ -405,7 +405,7 @@ int fhe_relinearize_noalloc(fhe_engine *engine, const int64_t *ct_device, int mo
 /* Selects where the ModDown base conversion (the exact division by the special
  * primes, core_key_switch.cpp:123-160) runs: FHE_TENSOR_CORES_OFF on the CUDA cores,
  * FHE_TENSOR_CORES_ON on the INT8 tensor pipe (tcgen05.mma kind::i8) wherever the
- * shape allows it, FHE_TENSOR_CORES_AUTO (the default) on the tensor pipe from 6
+ * shape allows it, FHE_TENSOR_CORES_AUTO (the default) on the tensor pipe from 4
  * special primes on, where it is the faster form.  Every mode gives the same words. */
 enum {
   FHE_TENSOR_CORES_OFF = 0,
