@@ -378,6 +378,8 @@ def run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream):
                                     "key, 3)") + ", bootstrap preset, N=2^16, K=4, input level 3",
                        "ciphertexts_per_step": B, "precision_bits": bits,
                        "bootstrap_key_bytes": key_bytes,
+                       "cuda_graphs": {"captured": eng.graph_counts()[0],
+                                       "capture_failed": eng.graph_counts()[1]},
                        "kernel_ms_per_bootstrap": families},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_ms, "unit": "ms/bootstrap",

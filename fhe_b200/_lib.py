@@ -93,6 +93,8 @@ SIGNATURES = {
     "fhe_create_small_bootstrap_key": (_i, [_vp, _vp, _pp, _pp]),
     "fhe_bootstrap": (_i, [_vp, _vp, _vp, _vp, ctypes.POINTER(_vp), _i, _vp, _vp, _i, _pp]),
     "fhe_engine_set_tensor_cores": (_i, [_vp, _i]),
+    "fhe_engine_set_graphs": (_i, [_vp, _i]),
+    "fhe_engine_graph_counts": (_i, [_vp, _ip, _ip]),
     "fhe_create_bootstrap_key": (_i, [_vp, _vp, _i, ctypes.c_char_p, _pp]),
     "fhe_bootstrap_key_destroy": (_i, [_vp]),
     "fhe_bootstrap_key_info": (_i, [_vp, _ip, _ip, _ip, ctypes.POINTER(ctypes.c_uint64)]),

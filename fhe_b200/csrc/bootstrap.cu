@@ -630,6 +630,7 @@ std::unique_ptr<BootstrapKey> Engine::create_bootstrap_key(const Data &sk, int s
   require_bootstrap_stage_count(fn, stage_count, shift);
 
   auto bk = std::make_unique<BootstrapKey>();
+  bk->serial = ++serial_;
   bk->stage_count = stage_count;
   bk->inner_loop_shift = shift;
   // get_bootstrap_stage_levels (engine_bootstrap.cpp:121-130): nine levels for EvalRound.
@@ -874,27 +875,41 @@ std::unique_ptr<Data> Engine::apply_butterfly(const Data &ct, const BootstrapKey
   auto inner_text = [&](int i) -> const Data & { return i == 0 ? *inner0 : *rotated[i - 1]; };
   Owned outer_sum;
   for (const auto &[delta, outer_indices] : stage.process_order) {
+    // multiply_for_butterfly (CKKSCore::multiply(ct, pt), core.cpp:257-282) of every
+    // (text, diagonal) pair of the group, summed with add_inplace: one fused pass per
+    // kMaxMacTerms pairs.
     Owned inner_sum;
+    MacTerms terms;
+    bool continued = false;  // a previous pass already started the chain in inner_sum
+    auto flush = [&]() {
+      if (terms.count == 0) return;
+      const Data &x = *inner_sum;
+      check(timed("diagonal_mac", [&] {
+              return launch_diagonal_mac(tables_, params.log_n, x.chains, x.moduli_id, terms,
+                                         x.poly_stride(), continued, inner_sum->d,
+                                         x.poly_stride(), stream_);
+            }),
+            "diagonal products");
+      terms.count = 0;
+      continued = true;
+    };
     for (int o : outer_indices) {
       const auto &row = stage.diagonals.at(o);
       for (int i = (o == 0 ? 1 : 0); i < stage.inner; i++) {
-        // multiply_for_butterfly: CKKSCore::multiply(ct, pt) (core.cpp:257-282).
         const Data &x = inner_text(i);
         const Data &diagonal = *row.at(i);
-        if (diagonal.moduli_id != x.moduli_id || diagonal.chains != x.chains)
+        if (diagonal.moduli_id != x.moduli_id || diagonal.chains != x.chains || x.polys != 2)
           throw std::runtime_error("apply butterfly: the diagonal does not match the text.");
-        auto product = make_data(kUnitCiphertext, (x.flag | diagonal.flag) & ~kFlagRescaled,
-                                 x.moduli_id, x.polys, x.scale * diagonal.scale);
-        const long long ps = x.poly_stride();
-        for (int p = 0; p < x.polys; p++)
-          pointwise(kOpMult, x.chains, x.moduli_id, x.d + p * ps, diagonal.d, nullptr,
-                    product->d + p * ps);
         if (!inner_sum)
-          inner_sum = std::move(product);
-        else
-          add_inplace(*inner_sum, *product);
+          inner_sum = make_data(kUnitCiphertext, (x.flag | diagonal.flag) & ~kFlagRescaled,
+                                x.moduli_id, x.polys, x.scale * diagonal.scale);
+        if (terms.count == kMaxMacTerms) flush();
+        terms.x[terms.count] = x.d;
+        terms.d[terms.count] = diagonal.d;
+        terms.count++;
       }
     }
+    flush();
     Owned turned = std::move(inner_sum);
     if (delta != 0) {
       auto decomposed = mod_down_then_decompose(*turned);
@@ -910,6 +925,64 @@ std::unique_ptr<Data> Engine::apply_butterfly(const Data &ct, const BootstrapKey
 
 std::unique_ptr<Data> Engine::bootstrap(const Data &ct, const Data &rk, const Data &ck,
                                         const BootstrapKey &bk) {
+  if (!graphs_ || profiling_) return bootstrap_direct(ct, rk, ck, bk);
+  const double s_hi = static_cast<double>(ct.scale);
+  const GraphKey key{ct.moduli_id, ct.flag, ct.polys, s_hi,
+                     static_cast<double>(ct.scale - static_cast<long double>(s_hi)),
+                     rk.serial, ck.serial, bk.serial, stream_};
+  if (graph_failed_.count(key)) return bootstrap_direct(ct, rk, ck, bk);
+  auto seen = graph_seen_.find(key);
+  if (seen == graph_seen_.end()) {
+    // The direct run checks the inputs and fills every table a capture must not build.
+    auto out = bootstrap_direct(ct, rk, ck, bk);
+    graph_seen_[key] = {out->type, out->flag, out->moduli_id, out->polys, out->scale};
+    return out;
+  }
+  auto it = graph_cache_.find(key);
+  if (it == graph_cache_.end()) {
+    BootstrapGraph g;
+    g.in = make_data(ct.type, ct.flag, ct.moduli_id, ct.polys, ct.scale);
+    const GraphShape &shape = seen->second;
+    g.out = make_data(shape.type, shape.flag, shape.moduli_id, shape.polys, shape.scale);
+    synchronize();  // the graph's input and output exist before the capture starts
+    cudaGraph_t graph = nullptr;
+    check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+    const unsigned long long counted = kernel_launch_count();
+    cudaError_t e = cudaSuccess;
+    try {
+      auto r = bootstrap_direct(*g.in, rk, ck, bk);
+      e = cudaMemcpyAsync(g.out->d, r->d, r->words() * sizeof(int64_t), cudaMemcpyDeviceToDevice,
+                          stream_);
+    } catch (...) {
+      e = cudaErrorStreamCaptureInvalidated;
+    }
+    const cudaError_t end = cudaStreamEndCapture(stream_, &graph);
+    g.launches = kernel_launch_count() - counted;
+    unnote_launches(g.launches);
+    if (e == cudaSuccess && end == cudaSuccess)
+      e = cudaGraphInstantiate(&g.exec, graph, 0);
+    else if (e == cudaSuccess)
+      e = end;
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      // Something on the path cannot be captured: keep running it directly.
+      cudaGetLastError();
+      graph_failed_.insert(key);
+      return bootstrap_direct(ct, rk, ck, bk);
+    }
+    it = graph_cache_.emplace(key, std::move(g)).first;
+  }
+  BootstrapGraph &g = it->second;
+  check(cudaMemcpyAsync(g.in->d, ct.d, ct.words() * sizeof(int64_t), cudaMemcpyDeviceToDevice,
+                        stream_),
+        "graph input");
+  check(cudaGraphLaunch(g.exec, stream_), "graph launch");
+  note_launch(static_cast<unsigned>(g.launches));
+  return clone(*g.out);
+}
+
+std::unique_ptr<Data> Engine::bootstrap_direct(const Data &ct, const Data &rk, const Data &ck,
+                                               const BootstrapKey &bk) {
   // CKKSEngine::bootstrap(UnitCiphertext*, RelinearizationKey*, ConjugationKey*,
   // BootstrapKey*) (engine_bootstrap.cpp:804-838).
   const std::string fn = "Bootstrap Unit Ciphertext With Bootstrap Key";

@@ -691,6 +691,22 @@ int fhe_engine_set_tensor_cores(fhe_engine *engine, int mode) {
   return guarded([&] { engine->impl->set_tensor_cores(mode); });
 }
 
+int fhe_engine_set_graphs(fhe_engine *engine, int enable) {
+  REQUIRE_HANDLE(engine);
+  return guarded([&] { engine->impl->set_graphs(enable != 0); });
+}
+
+int fhe_engine_graph_counts(const fhe_engine *engine, int *captured, int *failed) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_OUT(captured);
+  REQUIRE_OUT(failed);
+  return guarded([&] {
+    const auto c = engine->impl->graph_counts();
+    *captured = c.first;
+    *failed = c.second;
+  });
+}
+
 int fhe_create_bootstrap_key(fhe_engine *engine, const fhe_data *secret_key, int stage_count,
                              const char *size, fhe_bootstrap_key **out) {
   REQUIRE_HANDLE(engine);

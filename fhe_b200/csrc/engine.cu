@@ -106,6 +106,8 @@ Engine::Engine(const Config &config) : params(config) {
 
 Engine::~Engine() {
   cudaStreamSynchronize(stream_);
+  for (auto &kv : graph_cache_)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
   // Objects still alive lose their device memory and their engine; the C ABI
   // rejects any later use of them.
   for (Data *d : live_) {
@@ -202,6 +204,7 @@ std::unique_ptr<Data> Engine::make_data(int type, int flag, int moduli_id, int p
   if (polys <= 0) throw std::invalid_argument("the polynomial count should be positive.");
   auto d = std::make_unique<Data>();
   d->engine = this;
+  d->serial = ++serial_;
   d->type = type;
   d->flag = flag;
   d->moduli_id = moduli_id;

@@ -79,6 +79,7 @@ struct Data {
   int delta = 0;
   long double scale = 1.0L;
   int64_t *d = nullptr;
+  uint64_t serial = 0;  // unique per engine, never reused (keys captured graphs)
 
   size_t words() const;
   long long poly_stride() const;
@@ -107,6 +108,7 @@ struct BootstrapStage {
 // (with their NTT-form permutation, made on use), the coefficients-to-slots and
 // slots-to-coefficients stages, and the small bootstrap key.
 struct BootstrapKey {
+  uint64_t serial = 0;  // unique per engine, never reused
   int stage_count = 0;
   int inner_loop_shift = 0;
   std::map<int, std::unique_ptr<Data>> rotation_keys;
@@ -227,6 +229,14 @@ class Engine {
                                                      const std::string &size);
   std::unique_ptr<Data> bootstrap(const Data &ct, const Data &rk, const Data &ck,
                                   const BootstrapKey &bk);
+  // After one direct run of an input shape, bootstrap(ct, rk, ck, bootstrap key) is
+  // captured once as a CUDA graph and replayed (one launch instead of ~10^4); on by
+  // default, off while profiling.  Same words either way.
+  void set_graphs(bool on) { graphs_ = on; }
+  // Captured graphs held, and input shapes whose capture failed (run directly).
+  std::pair<int, int> graph_counts() const {
+    return {static_cast<int>(graph_cache_.size()), static_cast<int>(graph_failed_.size())};
+  }
   // CKKSEngine::rotate(UnitCiphertext*, BootstrapKey*, delta, normalize)
   // (engine_rotate.cpp:192-206).
   std::unique_ptr<Data> rotate(const Data &ct, const BootstrapKey &bk, int delta,
@@ -273,6 +283,26 @@ class Engine {
   KeySwitchTables ks_{};
   std::map<std::pair<int, int>, DevicePartitions> partition_cache_;
   int tensor_cores_ = kTensorCoresAuto;
+  uint64_t serial_ = 0;
+  // Captured bootstraps: key = (input moduli id, flag, polys, scale, keys' serials,
+  // stream); the graph reads `in` and writes `out`, every temporary inside it.
+  using GraphKey =
+      std::tuple<int, int, int, double, double, uint64_t, uint64_t, uint64_t, cudaStream_t>;
+  struct GraphShape {
+    int type, flag, moduli_id, polys;
+    long double scale;
+  };
+  struct BootstrapGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::unique_ptr<Data> in, out;
+    unsigned long long launches = 0;
+  };
+  bool graphs_ = true;
+  std::map<GraphKey, GraphShape> graph_seen_;
+  std::map<GraphKey, BootstrapGraph> graph_cache_;
+  std::set<GraphKey> graph_failed_;
+  std::unique_ptr<Data> bootstrap_direct(const Data &ct, const Data &rk, const Data &ck,
+                                         const BootstrapKey &bk);
   std::map<int, ModDownTcTables> mod_down_tc_cache_;  // moduli id -> tables
   int *device_error_ = nullptr;  // set by a kernel whose bounded wait ran out
   const ModDownTcTables *mod_down_tc(int moduli_id);

@@ -14,6 +14,9 @@ std::atomic<unsigned long long> g_launches{0};
 
 void note_launch(unsigned count) { g_launches.fetch_add(count, std::memory_order_relaxed); }
 unsigned long long kernel_launch_count() { return g_launches.load(std::memory_order_relaxed); }
+void unnote_launches(unsigned long long count) {
+  g_launches.fetch_sub(count, std::memory_order_relaxed);
+}
 
 namespace {
 

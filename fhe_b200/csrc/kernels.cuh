@@ -31,6 +31,8 @@ struct DevicePartitions {
 // Process-wide count of kernel launches made by this library.
 void note_launch(unsigned count = 1);
 unsigned long long kernel_launch_count();
+// Takes back launches counted while a stream was being captured (nothing ran).
+void unnote_launches(unsigned long long count);
 
 struct KeySwitchTables {
   const int64_t *p_inverse_mult_r;  // [K][P] (entry for prime i at [s*P + i])
@@ -170,6 +172,21 @@ cudaError_t launch_permute_gather(int n, int polys, int limbs, const int64_t *x,
 cudaError_t launch_ntt_rotate_finish(const PrimeTables &t, int log_n, int limbs, int prime_base,
                                      const int64_t *x0, const int64_t *acc, const int32_t *perm,
                                      int64_t *y, cudaStream_t s);
+
+// The baby-step sums of the hoisted linear transform (apply_butterfly,
+// engine_bootstrap.cpp:248-262) in one pass: for both polynomials of extended
+// NTT-form texts, y = the reference's chain over t_i = mont_mult(x_i, d_i) (the
+// first term as is, each further one added as add_inplace does,
+// reduce(reduce(acc + t_i, 2q), q)); with `accumulate` the chain continues from y.
+constexpr int kMaxMacTerms = 32;
+struct MacTerms {
+  const int64_t *x[kMaxMacTerms];  // 2-polynomial texts, polynomial stride x_stride
+  const int64_t *d[kMaxMacTerms];  // 1-polynomial plaintexts
+  int count = 0;
+};
+cudaError_t launch_diagonal_mac(const PrimeTables &t, int log_n, int limbs, int prime_base,
+                                const MacTerms &terms, long long x_stride, bool accumulate,
+                                int64_t *y, long long y_stride, cudaStream_t s);
 
 // Per-limb Montgomery constants passed by value.
 constexpr int kMaxScalarLimbs = 128;

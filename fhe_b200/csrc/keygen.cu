@@ -269,10 +269,13 @@ void Engine::pointwise(int op, int limbs, int prime_base, const int64_t *a, cons
     if (limbs > kMaxScalarLimbs) throw std::invalid_argument("pointwise: too many limbs.");
     for (int j = 0; j < limbs; j++) c.v[j] = constants[j];
   }
-  note_launch();
-  pointwise_kernel<<<grid_for(static_cast<long long>(limbs) << params.log_n), kThreads, 0,
-                     stream_>>>(tables_, op, params.log_n, limbs, prime_base, a, b, c, y);
-  check(cudaGetLastError(), "pointwise");
+  check(timed("pointwise", [&] {
+          note_launch();
+          pointwise_kernel<<<grid_for(static_cast<long long>(limbs) << params.log_n), kThreads, 0,
+                             stream_>>>(tables_, op, params.log_n, limbs, prime_base, a, b, c, y);
+          return cudaGetLastError();
+        }),
+        "pointwise");
 }
 
 void Engine::ntt_in_place(int64_t *x, int limbs, int prime_base, long long stride, int polys) {

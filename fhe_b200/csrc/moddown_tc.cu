@@ -338,13 +338,22 @@ cudaError_t launch_mod_down_epilogue_tc(const PrimeTables &t, const KeySwitchTab
     return cudaErrorInvalidValue;
   const size_t smem = tc_smem_bytes(K, limbs);
   const dim3 grid(n / kTcCoeffs, ops.polys);
-  cudaError_t e = cudaSuccess;
+  // The shared-memory limit is raised once per instantiation and device to the most
+  // any supported shape needs, so no attribute call falls inside a graph capture.
+  static int raised[17] = {};
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return e;
+  const int bit = 1 << (device & 31);
   switch (K) {
 #define FHE_TC_CASE(KK)                                                                         \
   case KK:                                                                                      \
-    e = cudaFuncSetAttribute(mod_down_tc_kernel<KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                             static_cast<int>(smem));                                           \
-    if (e != cudaSuccess) return e;                                                             \
+    if (!(raised[KK] & bit)) {                                                                  \
+      e = cudaFuncSetAttribute(mod_down_tc_kernel<KK>,                                          \
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);        \
+      if (e != cudaSuccess) return e;                                                           \
+      raised[KK] |= bit;                                                                        \
+    }                                                                                           \
     note_launch();                                                                              \
     mod_down_tc_kernel<KK><<<grid, kTcThreads, smem, s>>>(t, ks, tc, n, moduli_id, limbs, acc,  \
                                                           ops, out, error);                     \

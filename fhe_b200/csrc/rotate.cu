@@ -111,6 +111,30 @@ __global__ void ntt_rotate_finish_kernel(PrimeTables t, int log_n, int limbs, in
   y[i] = v;
 }
 
+__global__ void diagonal_mac_kernel(PrimeTables t, int log_n, int limbs, int prime_base,
+                                    MacTerms terms, long long x_stride, bool accumulate,
+                                    int64_t *y, long long y_stride) {
+  const long long per_poly = static_cast<long long>(limbs) << log_n;
+  const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (i >= 2 * per_poly) return;
+  const int poly = i >= per_poly ? 1 : 0;
+  const long long r = i - poly * per_poly;
+  const int prime = prime_base + static_cast<int>(r >> log_n);
+  const uint64_t q = t.q[prime], k = t.k[prime];
+  const int64_t qs = static_cast<int64_t>(q), q2 = qs << 1;
+  int first = 0;
+  int64_t acc;
+  if (accumulate) {
+    acc = y[poly * y_stride + r];
+  } else {
+    acc = mont_mult(terms.x[0][poly * x_stride + r], terms.d[0][r], q, k);
+    first = 1;
+  }
+  for (int m = first; m < terms.count; m++)
+    acc = guard(guard(acc + mont_mult(terms.x[m][poly * x_stride + r], terms.d[m][r], q, k), q2), qs);
+  y[poly * y_stride + r] = acc;
+}
+
 }  // namespace
 
 cudaError_t launch_rotate_base(const PrimeTables &t, const KeySwitchTables &ks, int log_n,
@@ -163,6 +187,16 @@ cudaError_t launch_ntt_rotate_finish(const PrimeTables &t, int log_n, int limbs,
   note_launch();
   ntt_rotate_finish_kernel<<<grid_for((2LL * limbs) << log_n), kThreads, 0, s>>>(
       t, log_n, limbs, prime_base, x0, acc, perm, y);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_diagonal_mac(const PrimeTables &t, int log_n, int limbs, int prime_base,
+                                const MacTerms &terms, long long x_stride, bool accumulate,
+                                int64_t *y, long long y_stride, cudaStream_t s) {
+  if (terms.count < 1 || terms.count > kMaxMacTerms) return cudaErrorInvalidValue;
+  note_launch();
+  diagonal_mac_kernel<<<grid_for((2LL * limbs) << log_n), kThreads, 0, s>>>(
+      t, log_n, limbs, prime_base, terms, x_stride, accumulate, y, y_stride);
   return cudaGetLastError();
 }
 

@@ -442,6 +442,16 @@ class Engine:
         tensor pipe, 2 (default) the tensor pipe from 4 special primes on; same words."""
         check(_lib.load().fhe_engine_set_tensor_cores(self._h, int(mode)))
 
+    def set_graphs(self, enable: bool) -> None:
+        """CUDA-graph replay of bootstrap(ct, rk, ck, bootstrap_key) (default on)."""
+        check(_lib.load().fhe_engine_set_graphs(self._h, int(enable)))
+
+    def graph_counts(self) -> tuple:
+        """(captured bootstrap graphs held, input shapes whose capture failed)."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        check(_lib.load().fhe_engine_graph_counts(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def create_bootstrap_key(self, secret_key: Data, stage_count: int = 3,
                              size: str = "medium") -> BootstrapKey:
         h = ctypes.c_void_p()

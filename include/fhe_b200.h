@@ -413,6 +413,13 @@ enum {
   FHE_TENSOR_CORES_AUTO = 2
 };
 int fhe_engine_set_tensor_cores(fhe_engine *engine, int mode);
+/* CUDA graphs (default on): after one direct run of an input shape,
+ * fhe_bootstrap_with_key captures the whole bootstrap once and replays it.  Graphs
+ * are not used while profiling.  Same words either way. */
+int fhe_engine_set_graphs(fhe_engine *engine, int enable);
+/* The number of captured bootstrap graphs the engine holds, and of input shapes
+ * whose capture failed and which therefore run directly. */
+int fhe_engine_graph_counts(const fhe_engine *engine, int *captured, int *failed);
 
 /* ---- processor-level kernels on device limbs (src/processor/single.h) --------------- */
 

@@ -60,9 +60,19 @@ def test_bootstrap_key_matches_recorded_reference(engines, case):
     assert digest_doubles(slots) == case["decoded"]
     assert np.max(np.abs(slots - vals)) < 2.0 ** -16
 
-    # A second bootstrap with the same key gives the same words.
-    again = e.bootstrap(ct, rk, ck, bk)
-    assert digest(again.download()) == d["bootstrapped"]
+    # The second call captures the bootstrap as a CUDA graph, the third replays it;
+    # with graphs off the direct path runs again.  Same words every time.
+    before = e.kernel_launch_count()
+    for _ in range(2):
+        again = e.bootstrap(ct, rk, ck, bk)
+        assert digest(again.download()) == d["bootstrapped"]
+    assert e.kernel_launch_count() > before
+    assert e.graph_counts() == (1, 0)
+    e.set_graphs(False)
+    try:
+        assert digest(e.bootstrap(ct, rk, ck, bk).download()) == d["bootstrapped"]
+    finally:
+        e.set_graphs(True)
 
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: c["tier"])
