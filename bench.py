@@ -390,6 +390,127 @@ def run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream):
     return 0
 
 
+def run_batched_bench(args, torch, np, rank, world, local, backend, stream):
+    """The batched uneven serving step at N = 2^16, K = 10: `batch` ciphertext pairs at
+    levels uniform in 2..24, each multiplied, relinearized and rescaled, then rotated
+    by 2^k with k uniform in 0..14 (one fixed rotation key per k, 1.8 GB resident),
+    the whole batch replayed as one CUDA graph.  Per-operation latencies come from a
+    direct (unreplayed) pass that times every item with its own events."""
+    from fhe_b200 import Engine, NTT_FORM, INCLUDE_SPECIAL, RELINEARIZATION_KEY
+    from inputs import uniform_limbs
+
+    eng = Engine(log_coeff_count=LOG_N, special_prime_count=SPECIAL)
+    eng.set_stream(stream.cuda_stream)
+    n = eng.coeff_count
+    top = eng.moduli_id(eng.max_key_switching_level)
+    rng = np.random.default_rng(77 + rank)
+    parts = 2 * eng.partition_count(top)
+    rk = eng.upload(uniform_limbs(rng, eng.moduli[top:], parts, n), top,
+                    NTT_FORM | INCLUDE_SPECIAL, RELINEARIZATION_KEY)
+    rot = [eng.upload_fixed_rotation_key(uniform_limbs(rng, eng.moduli[top:], parts, n), top, 1 << k)
+           for k in range(15)]
+    B = args.batch
+    levels = rng.integers(2, 25, size=B)
+    steps_k = rng.integers(0, 15, size=B)
+    A, Bs, keys, host = [], [], [], []
+    for lv, k in zip(levels, steps_k):
+        mid = eng.moduli_id(int(lv))
+        q = eng.moduli[mid:eng.chain_count]
+        a, b = uniform_limbs(rng, q, 2, n), uniform_limbs(rng, q, 2, n)
+        A.append(eng.upload(a, mid))
+        Bs.append(eng.upload(b, mid))
+        keys.append(rot[int(k)])
+        host.append((mid, torch.from_numpy(a.reshape(-1)).pin_memory(),
+                     torch.from_numpy(b.reshape(-1)).pin_memory()))
+
+    def step():
+        for o in eng.multiply_rotate_batch(A, Bs, rk, keys):
+            o.free()
+
+    for _ in range(max(args.warmup, 2)):  # direct run, then the capture
+        step()
+    torch.cuda.synchronize()
+    if backend:
+        torch.distributed.barrier()
+    launches0 = Engine.kernel_launch_count()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        stop.record(stream)
+        torch.cuda.synchronize()
+    launches = Engine.kernel_launch_count() - launches0
+    elapsed_max, units = aggregate(start.elapsed_time(stop), float(B * args.steps), world, backend)
+    value = units / (elapsed_max / 1e3)
+
+    # Per-operation latency: every item alone, direct, event-timed.
+    eng.set_graphs(False)
+    lat = []
+    for a, b, k in zip(A, Bs, keys):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = eng.rotate(eng.multiply_relinearize_rescale(a, b, rk), k)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        lat.append(e0.elapsed_time(e1))
+        out.free()
+    eng.set_graphs(True)
+    lat.sort()
+    pct = lambda p: lat[min(len(lat) - 1, int(round(p / 100 * (len(lat) - 1))))]
+
+    # End to end: every pair from pinned host memory, the batch, every result back.
+    out_shapes = [o.download().size for o in eng.multiply_rotate_batch(A, Bs, rk, keys)]
+    pin_out = [torch.empty(sz, dtype=torch.int64).pin_memory() for sz in out_shapes]
+
+    def e2e_step():
+        ins = []
+        for mid, ha, hb in host:
+            ins.append((eng.upload_from_pointer(ha.data_ptr(), mid, 2),
+                        eng.upload_from_pointer(hb.data_ptr(), mid, 2)))
+        outs = eng.multiply_rotate_batch([x[0] for x in ins], [x[1] for x in ins], rk, keys)
+        for o, p in zip(outs, pin_out):
+            eng.download_to_pointer(o, p.data_ptr(), wait=False)
+        eng.synchronize()
+
+    e2e_step()
+    e2e_step()
+    torch.cuda.synchronize()
+    e_steps = max(1, min(args.steps, 3))
+    s2, t2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s2.record(stream)
+    for _ in range(e_steps):
+        e2e_step()
+    t2.record(stream)
+    torch.cuda.synchronize()
+    e_ms, e_units = aggregate(s2.elapsed_time(t2), float(B * e_steps), world, backend)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "batched uneven HMult+relin+rescale+rotate ct/s at N=2^16 (K=10)",
+            "value": value, "unit": "ct/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 2), "ms_per_step": elapsed_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic (seeded uniform residues, random relinearization and rotation keys)",
+            "config": {"workload": "engine.multiply_rotate_batch: per item multiply-relinearize-"
+                                   "rescale then rotate by 2^k, levels uniform in 2..24, k "
+                                   "uniform in 0..14, one CUDA graph per batch",
+                       "batch": B, "log_n": LOG_N, "special_prime_count": SPECIAL,
+                       "mean_input_limbs": float(np.mean(levels + 2)),
+                       "l2": "inputs larger than L2",
+                       "cuda_graphs": {"captured": eng.graph_counts()[0],
+                                       "capture_failed": eng.graph_counts()[1]},
+                       "latency_ms": {"p50": pct(50), "p99": pct(99), "mean": sum(lat) / len(lat),
+                                      "note": "one item alone, direct launches, event-timed"}},
+            "cpu_baseline": None,
+            "e2e": {"value": e_units / (e_ms / 1e3), "unit": "ct/s",
+                    "h2d_bytes_per_step": int(sum(h[1].numel() + h[2].numel() for h in host) * 8),
+                    "d2h_bytes_per_step": int(sum(out_shapes) * 8)},
+            "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
+    eng.close()
+    return 0
+
+
 # -------------------------------------------------------------------- main --
 
 def main(argv=None):
@@ -400,10 +521,11 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=16, help="ciphertext pairs per step")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="hmult",
-                    choices=["hmult", "ntt", "bootstrap", "bootstrap_rotation"],
+                    choices=["hmult", "ntt", "bootstrap", "bootstrap_rotation", "batched"],
                     help="hmult: the headline; ntt: forward NTT of --batch x 24 limbs at N=2^16; "
                          "bootstrap: --batch ciphertexts bootstrapped per step with a medium "
-                         "bootstrap key; bootstrap_rotation: the same with a rotation key")
+                         "bootstrap key; bootstrap_rotation: the same with a rotation key; "
+                         "batched: --batch uneven HMult+rotate items per step (use 256)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args(argv)
     rank, world, local = dist_env()
@@ -435,6 +557,8 @@ def main(argv=None):
     torch.cuda.set_stream(stream)
     if args.workload == "ntt":
         return run_ntt_microbench(args, torch, np, rank, world, local, backend, stream)
+    if args.workload == "batched":
+        return run_batched_bench(args, torch, np, rank, world, local, backend, stream)
     if args.workload in ("bootstrap", "bootstrap_rotation"):
         return run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream)
     eng = Engine(log_coeff_count=LOG_N, special_prime_count=SPECIAL)

@@ -95,6 +95,8 @@ SIGNATURES = {
     "fhe_engine_set_tensor_cores": (_i, [_vp, _i]),
     "fhe_engine_set_graphs": (_i, [_vp, _i]),
     "fhe_engine_graph_counts": (_i, [_vp, _ip, _ip]),
+    "fhe_multiply_rotate_batch": (_i, [_vp, _i, ctypes.POINTER(_vp), ctypes.POINTER(_vp), _vp,
+                                       ctypes.POINTER(_vp), _pp]),
     "fhe_create_bootstrap_key": (_i, [_vp, _vp, _i, ctypes.c_char_p, _pp]),
     "fhe_bootstrap_key_destroy": (_i, [_vp]),
     "fhe_bootstrap_key_info": (_i, [_vp, _ip, _ip, _ip, ctypes.POINTER(ctypes.c_uint64)]),

@@ -925,60 +925,13 @@ std::unique_ptr<Data> Engine::apply_butterfly(const Data &ct, const BootstrapKey
 
 std::unique_ptr<Data> Engine::bootstrap(const Data &ct, const Data &rk, const Data &ck,
                                         const BootstrapKey &bk) {
-  if (!graphs_ || profiling_) return bootstrap_direct(ct, rk, ck, bk);
-  const double s_hi = static_cast<double>(ct.scale);
-  const GraphKey key{ct.moduli_id, ct.flag, ct.polys, s_hi,
-                     static_cast<double>(ct.scale - static_cast<long double>(s_hi)),
-                     rk.serial, ck.serial, bk.serial, stream_};
-  if (graph_failed_.count(key)) return bootstrap_direct(ct, rk, ck, bk);
-  auto seen = graph_seen_.find(key);
-  if (seen == graph_seen_.end()) {
-    // The direct run checks the inputs and fills every table a capture must not build.
-    auto out = bootstrap_direct(ct, rk, ck, bk);
-    graph_seen_[key] = {out->type, out->flag, out->moduli_id, out->polys, out->scale};
-    return out;
-  }
-  auto it = graph_cache_.find(key);
-  if (it == graph_cache_.end()) {
-    BootstrapGraph g;
-    g.in = make_data(ct.type, ct.flag, ct.moduli_id, ct.polys, ct.scale);
-    const GraphShape &shape = seen->second;
-    g.out = make_data(shape.type, shape.flag, shape.moduli_id, shape.polys, shape.scale);
-    synchronize();  // the graph's input and output exist before the capture starts
-    cudaGraph_t graph = nullptr;
-    check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
-    const unsigned long long counted = kernel_launch_count();
-    cudaError_t e = cudaSuccess;
-    try {
-      auto r = bootstrap_direct(*g.in, rk, ck, bk);
-      e = cudaMemcpyAsync(g.out->d, r->d, r->words() * sizeof(int64_t), cudaMemcpyDeviceToDevice,
-                          stream_);
-    } catch (...) {
-      e = cudaErrorStreamCaptureInvalidated;
-    }
-    const cudaError_t end = cudaStreamEndCapture(stream_, &graph);
-    g.launches = kernel_launch_count() - counted;
-    unnote_launches(g.launches);
-    if (e == cudaSuccess && end == cudaSuccess)
-      e = cudaGraphInstantiate(&g.exec, graph, 0);
-    else if (e == cudaSuccess)
-      e = end;
-    if (graph) cudaGraphDestroy(graph);
-    if (e != cudaSuccess) {
-      // Something on the path cannot be captured: keep running it directly.
-      cudaGetLastError();
-      graph_failed_.insert(key);
-      return bootstrap_direct(ct, rk, ck, bk);
-    }
-    it = graph_cache_.emplace(key, std::move(g)).first;
-  }
-  BootstrapGraph &g = it->second;
-  check(cudaMemcpyAsync(g.in->d, ct.d, ct.words() * sizeof(int64_t), cudaMemcpyDeviceToDevice,
-                        stream_),
-        "graph input");
-  check(cudaGraphLaunch(g.exec, stream_), "graph launch");
-  note_launch(static_cast<unsigned>(g.launches));
-  return clone(*g.out);
+  auto out = run_captured({kGraphBootstrap, rk.serial, ck.serial, bk.serial}, {&ct},
+                          [&](const std::vector<const Data *> &in) {
+                            std::vector<Owned> r;
+                            r.push_back(bootstrap_direct(*in[0], rk, ck, bk));
+                            return r;
+                          });
+  return std::move(out[0]);
 }
 
 std::unique_ptr<Data> Engine::bootstrap_direct(const Data &ct, const Data &rk, const Data &ck,

@@ -696,6 +696,37 @@ int fhe_engine_set_graphs(fhe_engine *engine, int enable) {
   return guarded([&] { engine->impl->set_graphs(enable != 0); });
 }
 
+int fhe_multiply_rotate_batch(fhe_engine *engine, int count, const fhe_data *const *a,
+                              const fhe_data *const *b, const fhe_data *relinearization_key,
+                              const fhe_data *const *rotation_keys, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(relinearization_key);
+  REQUIRE_OUT(a);
+  REQUIRE_OUT(b);
+  REQUIRE_OUT(rotation_keys);
+  REQUIRE_OUT(out);
+  if (count < 1) {
+    fhe_b200::set_last_error("Multiply Rotate Batch: the batch is empty.");
+    return FHE_ERR_INVALID_ARGUMENT;
+  }
+  for (int i = 0; i < count; i++) {
+    REQUIRE_HANDLE(a[i]);
+    REQUIRE_HANDLE(b[i]);
+    REQUIRE_HANDLE(rotation_keys[i]);
+    out[i] = nullptr;
+  }
+  return guarded([&] {
+    std::vector<const Data *> va, vb, vk;
+    for (int i = 0; i < count; i++) {
+      va.push_back(&live(engine, a[i]));
+      vb.push_back(&live(engine, b[i]));
+      vk.push_back(&live(engine, rotation_keys[i]));
+    }
+    auto r = engine->impl->multiply_rotate_batch(va, vb, live(engine, relinearization_key), vk);
+    for (int i = 0; i < count; i++) out[i] = wrap(std::move(r[i]));
+  });
+}
+
 int fhe_engine_graph_counts(const fhe_engine *engine, int *captured, int *failed) {
   REQUIRE_HANDLE(engine);
   REQUIRE_OUT(captured);

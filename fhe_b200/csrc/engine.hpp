@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <complex>
+#include <functional>
 #include <map>
 #include <memory>
 #include <set>
@@ -63,6 +64,9 @@ enum PointwiseOp : int {
 
 // The ChaCha20 key and nonce of the engine's random stream (RandomNumberGenerator,
 // random_number_generator.cpp:9-55); the block counter is kept by the engine.
+// Operations replayed as CUDA graphs (the first element of a graph key).
+enum GraphOp : uint64_t { kGraphBootstrap = 1, kGraphMultiplyRotate = 2 };
+
 struct RngState {
   uint32_t seed[8];
   uint32_t nonce[2];
@@ -233,6 +237,12 @@ class Engine {
   // captured once as a CUDA graph and replayed (one launch instead of ~10^4); on by
   // default, off while profiling.  Same words either way.
   void set_graphs(bool on) { graphs_ = on; }
+  // Runs a batch of independent multiply-relinearize-rescale operations, each followed
+  // by a rotation with its own fixed key (the batched serving step; no reference
+  // counterpart), replayed as one CUDA graph after its first run.
+  std::vector<std::unique_ptr<Data>> multiply_rotate_batch(
+      const std::vector<const Data *> &a, const std::vector<const Data *> &b, const Data &rk,
+      const std::vector<const Data *> &rotation_keys);
   // Captured graphs held, and input shapes whose capture failed (run directly).
   std::pair<int, int> graph_counts() const {
     return {static_cast<int>(graph_cache_.size()), static_cast<int>(graph_failed_.size())};
@@ -284,23 +294,30 @@ class Engine {
   std::map<std::pair<int, int>, DevicePartitions> partition_cache_;
   int tensor_cores_ = kTensorCoresAuto;
   uint64_t serial_ = 0;
-  // Captured bootstraps: key = (input moduli id, flag, polys, scale, keys' serials,
-  // stream); the graph reads `in` and writes `out`, every temporary inside it.
-  using GraphKey =
-      std::tuple<int, int, int, double, double, uint64_t, uint64_t, uint64_t, cudaStream_t>;
+  // CUDA graphs of multi-kernel operations (graphs.cu): key = the operation, the
+  // serial numbers of its constant operands, the shapes of its inputs and the stream.
   struct GraphShape {
     int type, flag, moduli_id, polys;
     long double scale;
   };
-  struct BootstrapGraph {
+  struct CapturedGraph {
     cudaGraphExec_t exec = nullptr;
-    std::unique_ptr<Data> in, out;
+    std::vector<std::unique_ptr<Data>> in, out;  // the graph reads `in`, writes `out`
     unsigned long long launches = 0;
   };
   bool graphs_ = true;
-  std::map<GraphKey, GraphShape> graph_seen_;
-  std::map<GraphKey, BootstrapGraph> graph_cache_;
-  std::set<GraphKey> graph_failed_;
+  std::map<std::vector<uint64_t>, std::vector<GraphShape>> graph_seen_;
+  std::map<std::vector<uint64_t>, CapturedGraph> graph_cache_;
+  std::set<std::vector<uint64_t>> graph_failed_;
+  using GraphBody =
+      std::function<std::vector<std::unique_ptr<Data>>(const std::vector<const Data *> &)>;
+  // Runs `body` on `inputs` directly the first time its key is seen (checking the
+  // inputs and filling every table a capture must not build), captures it once as
+  // a CUDA graph over private copies of the inputs the second time, and replays the
+  // graph from then on.  A capture that fails leaves the key on the direct path.
+  std::vector<std::unique_ptr<Data>> run_captured(std::vector<uint64_t> key,
+                                                  const std::vector<const Data *> &inputs,
+                                                  const GraphBody &body);
   std::unique_ptr<Data> bootstrap_direct(const Data &ct, const Data &rk, const Data &ck,
                                          const BootstrapKey &bk);
   std::map<int, ModDownTcTables> mod_down_tc_cache_;  // moduli id -> tables

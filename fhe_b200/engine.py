@@ -446,6 +446,18 @@ class Engine:
         """CUDA-graph replay of bootstrap(ct, rk, ck, bootstrap_key) (default on)."""
         check(_lib.load().fhe_engine_set_graphs(self._h, int(enable)))
 
+    def multiply_rotate_batch(self, a: list, b: list, relinearization_key: Data,
+                              rotation_keys: list) -> list:
+        """[rotate(multiply_relinearize_rescale(a[i], b[i], rk), rotation_keys[i])]: one
+        serving step, replayed as a CUDA graph after its first run."""
+        n = len(a)
+        arr = lambda xs: (ctypes.c_void_p * n)(*[x.handle for x in xs])
+        out = (ctypes.c_void_p * n)()
+        check(_lib.load().fhe_multiply_rotate_batch(self._h, n, arr(a), arr(b),
+                                                    relinearization_key.handle,
+                                                    arr(rotation_keys), out))
+        return [Data(self, ctypes.c_void_p(out[i])) for i in range(n)]
+
     def graph_counts(self) -> tuple:
         """(captured bootstrap graphs held, input shapes whose capture failed)."""
         a, b = ctypes.c_int(), ctypes.c_int()

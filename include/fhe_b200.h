@@ -413,9 +413,17 @@ enum {
   FHE_TENSOR_CORES_AUTO = 2
 };
 int fhe_engine_set_tensor_cores(fhe_engine *engine, int mode);
+/* A serving step with no reference counterpart: for every i, multiply a[i] by b[i]
+ * with the relinearization key and rescale (fhe_multiply_relinearize_rescale), then
+ * rotate the product with rotation_keys[i] (fhe_rotate).  out receives count new
+ * handles.  After its first run a batch of the same shapes and keys is replayed as
+ * one CUDA graph. */
+int fhe_multiply_rotate_batch(fhe_engine *engine, int count, const fhe_data *const *a,
+                              const fhe_data *const *b, const fhe_data *relinearization_key,
+                              const fhe_data *const *rotation_keys, fhe_data **out);
 /* CUDA graphs (default on): after one direct run of an input shape,
- * fhe_bootstrap_with_key captures the whole bootstrap once and replays it.  Graphs
- * are not used while profiling.  Same words either way. */
+ * fhe_bootstrap_with_key and fhe_multiply_rotate_batch capture the whole operation
+ * once and replay it.  Graphs are not used while profiling.  Same words either way. */
 int fhe_engine_set_graphs(fhe_engine *engine, int enable);
 /* The number of captured bootstrap graphs the engine holds, and of input shapes
  * whose capture failed and which therefore run directly. */
