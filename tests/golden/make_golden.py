@@ -419,6 +419,50 @@ def bootstrap_key_cases():
                  max_error=float(np.max(np.abs(dec - vals))))]
 
 
+PIPELINE_SEED = (31, 41, 59, 26, 53, 58, 97, 93)
+PIPELINE_NONCE = (2, 7)
+
+
+def pipeline_cases():
+    """The plain CKKS pipeline of the reference's default engine (N = 2^14, one
+    special prime) and of the gold tier: after reseeding, secret, public and
+    relinearization keys; two complex vectors encoded at the top level and encrypted
+    with the public key; multiply with the relinearization key, rescale, decrypt,
+    decode.  Words of every ciphertext and the decoded slots, and the error against
+    the float64 product."""
+    from oracle import ref
+
+    cases = []
+    for tier in ("bronze", "gold"):
+        log_n, K, preset = TIERS[tier]
+        e = ref.Engine(log_n=log_n, special_prime_count=K, preset=preset, threads=os.cpu_count())
+        e.seed(PIPELINE_SEED, PIPELINE_NONCE)
+        out = {}
+        sk = e.create_secret_key()
+        pk = e.create_public_key(sk)
+        rk = e.create_relinearization_key(sk)
+        out["public_key"] = pk.limbs()
+        va = codec_values(11, e.slot_count, True)
+        vb = codec_values(12, e.slot_count, True)
+        a = e.encrypt(e.encode(va), pk)
+        b = e.encrypt(e.encode(vb), pk)
+        out["ct_a"], out["ct_b"] = a.limbs(), b.limbs()
+        product = e.multiply(a, b, rk)
+        out["product"] = product.limbs()
+        rescaled = e.rescale(product)
+        out["rescaled"] = rescaled.limbs()
+        info = rescaled.info()
+        slots = e.decode(e.decrypt(rescaled, sk))
+        cases.append(dict(tier=tier, log_n=log_n, special_prime_count=K, preset=preset,
+                          seed=list(PIPELINE_SEED), nonce=list(PIPELINE_NONCE), values_seeds=[11, 12],
+                          moduli=[int(v) for v in e.tables()["q"]],
+                          rescaled_moduli_id=info["moduli_id"], rescaled_level=info["level"],
+                          digests={k: digest(v) for k, v in out.items()},
+                          decoded=digest_doubles(slots),
+                          max_error=float(np.max(np.abs(slots - va * vb)))))
+    return cases
+
+
 def main():
     with open(os.path.join(HERE, "ntt_kat.json"), "w") as f:
         json.dump(parse_ntt_kats(), f, indent=1)
@@ -441,6 +485,9 @@ def main():
     boot_key = bootstrap_key_cases()
     with open(os.path.join(HERE, "bootstrap_key.json"), "w") as f:
         json.dump(boot_key, f, indent=1)
+    pipeline = pipeline_cases()
+    with open(os.path.join(HERE, "pipeline.json"), "w") as f:
+        json.dump(pipeline, f, indent=1)
     keygen = keygen_cases()
     with open(os.path.join(HERE, "keygen.json"), "w") as f:
         json.dump(keygen, f, indent=1)
