@@ -39,7 +39,7 @@ const char *Data::type_name() const {
 
 Data::~Data() {
   if (engine) {
-    if (d) engine->free_words(d);
+    if (d) engine->release(d, copy_pending);
     engine->forget(this);
   }
 }
@@ -60,6 +60,10 @@ Engine::Engine(const Config &config) : params(config) {
   check(cudaGetDevice(&device), "cudaGetDevice");
   check(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
   stream_ = own_stream_;
+  check(cudaStreamCreateWithFlags(&upload_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  check(cudaStreamCreateWithFlags(&download_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  check(cudaEventCreateWithFlags(&upload_done_, cudaEventDisableTiming), "cudaEventCreate");
+  check(cudaEventCreateWithFlags(&compute_done_, cudaEventDisableTiming), "cudaEventCreate");
   check(cudaMalloc(&device_error_, sizeof(int)), "cudaMalloc(error flag)");
   check(cudaMemset(device_error_, 0, sizeof(int)), "clear error flag");
   // Keep freed blocks in the stream-ordered pool: key switching allocates and frees
@@ -105,6 +109,8 @@ Engine::Engine(const Config &config) : params(config) {
 }
 
 Engine::~Engine() {
+  cudaStreamSynchronize(upload_stream_);
+  cudaStreamSynchronize(download_stream_);
   cudaStreamSynchronize(stream_);
   for (auto &kv : graph_cache_)
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
@@ -130,10 +136,16 @@ Engine::~Engine() {
   for (auto &kv : ntt_perm_cache_) cudaFree(kv.second);
   for (auto *b : table_buffers_) cudaFree(b);
   if (device_error_) cudaFree(device_error_);
+  cudaEventDestroy(upload_done_);
+  cudaEventDestroy(compute_done_);
+  cudaStreamDestroy(upload_stream_);
+  cudaStreamDestroy(download_stream_);
   if (own_stream_) cudaStreamDestroy(own_stream_);
 }
 
 void Engine::synchronize() {
+  check(cudaStreamSynchronize(upload_stream_), "cudaStreamSynchronize");
+  check(cudaStreamSynchronize(download_stream_), "cudaStreamSynchronize");
   check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
   int flag = 0;
   check(cudaMemcpy(&flag, device_error_, sizeof(int), cudaMemcpyDeviceToHost), "read error flag");
@@ -197,8 +209,29 @@ void Engine::free_words(int64_t *p) {
   if (p) cudaFreeAsync(p, stream_);
 }
 
+void Engine::release(int64_t *p, bool copy_pending) {
+  if (!p) return;
+  if (!copy_pending) {
+    cudaFreeAsync(p, stream_);
+    return;
+  }
+  // Behind the download and behind every kernel queued so far.
+  order_download_after_compute();
+  cudaFreeAsync(p, download_stream_);
+}
+
+void Engine::order_download_after_compute() {
+  check(cudaEventRecord(compute_done_, stream_), "cudaEventRecord");
+  check(cudaStreamWaitEvent(download_stream_, compute_done_, 0), "cudaStreamWaitEvent");
+}
+
+void Engine::order_compute_after_upload() {
+  check(cudaEventRecord(upload_done_, upload_stream_), "cudaEventRecord");
+  check(cudaStreamWaitEvent(stream_, upload_done_, 0), "cudaStreamWaitEvent");
+}
+
 std::unique_ptr<Data> Engine::make_data(int type, int flag, int moduli_id, int polys,
-                                        long double scale) {
+                                        long double scale, cudaStream_t alloc_stream) {
   if (moduli_id < 0 || moduli_id >= params.chain_count)
     throw std::invalid_argument("the moduli id is out of range.");
   if (polys <= 0) throw std::invalid_argument("the polynomial count should be positive.");
@@ -211,7 +244,14 @@ std::unique_ptr<Data> Engine::make_data(int type, int flag, int moduli_id, int p
   d->polys = polys;
   d->chains = params.chains(moduli_id, (flag & kFlagSpecial) != 0);
   d->scale = scale;
-  d->d = alloc_words(d->words());
+  if (alloc_stream) {
+    void *p = nullptr;
+    check(cudaMallocAsync(&p, std::max<size_t>(d->words(), 1) * sizeof(int64_t), alloc_stream),
+          "cudaMallocAsync");
+    d->d = static_cast<int64_t *>(p);
+  } else {
+    d->d = alloc_words(d->words());
+  }
   live_.insert(d.get());
   return d;
 }
@@ -221,9 +261,11 @@ void Engine::forget(Data *d) { live_.erase(d); }
 std::unique_ptr<Data> Engine::upload(int type, int flag, int moduli_id, int polys,
                                      long double scale, const int64_t *host) {
   if (!host) throw std::invalid_argument("the host limb pointer is null.");
-  auto d = make_data(type, flag, moduli_id, polys, scale);
-  check(cudaMemcpyAsync(d->d, host, d->words() * sizeof(int64_t), cudaMemcpyHostToDevice, stream_),
+  auto d = make_data(type, flag, moduli_id, polys, scale, upload_stream_);
+  check(cudaMemcpyAsync(d->d, host, d->words() * sizeof(int64_t), cudaMemcpyHostToDevice,
+                        upload_stream_),
         "upload limbs");
+  order_compute_after_upload();
   return d;
 }
 
@@ -234,8 +276,11 @@ void Engine::download(const Data &d, int64_t *host) {
 
 void Engine::download_async(const Data &d, int64_t *host) {
   if (!host) throw std::invalid_argument("the host limb pointer is null.");
-  check(cudaMemcpyAsync(host, d.d, d.words() * sizeof(int64_t), cudaMemcpyDeviceToHost, stream_),
+  order_download_after_compute();
+  check(cudaMemcpyAsync(host, d.d, d.words() * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                        download_stream_),
         "download limbs");
+  d.copy_pending = true;
 }
 
 std::unique_ptr<Data> Engine::clone(const Data &src) {
@@ -343,6 +388,21 @@ std::unique_ptr<Data> Engine::core_rescale(const Data &ct) {
   return out;
 }
 
+std::unique_ptr<Data> Engine::rescale_to_ntt(const Data &ct) {
+  // to_ntt(core_rescale(ct)) of a coefficient-form text in one pass.
+  if (ct.chains < 2) throw std::runtime_error("cannot rescale a single-limb text.");
+  if (ct.is_ntt()) throw std::invalid_argument("rescale to NTT: the text is in NTT form.");
+  auto out = make_data(ct.type, ct.flag | kFlagRescaled | kFlagNtt, ct.moduli_id + 1, ct.polys,
+                       params.rescaled_scale(ct.scale, ct.moduli_id));
+  check(timed("rescale_to_ntt", [&] {
+          return launch_rescale_to_ntt(tables_, ks_, params.log_n, ct.polys, out->chains,
+                                       ct.moduli_id, ct.d, ct.poly_stride(), out->d,
+                                       out->poly_stride(), stream_);
+        }),
+        "rescale to NTT");
+  return out;
+}
+
 std::unique_ptr<Data> Engine::rescale(const Data &ct) {
   const std::string fn = "Rescale Unit Ciphertext";
   const std::string prefix = fn + ": the input " + ct.type_name() + " ";
@@ -373,15 +433,13 @@ std::unique_ptr<Data> Engine::prepare_for_multiply(const Data &text, int level) 
     t = cur.get();
   }
   if (!t->is_rescaled()) {
-    std::unique_ptr<Data> r;
+    // rescale_, then the NTT form the product needs: one fused pass.
     if (t->is_ntt()) {
       auto intt = to_intt(*t);
-      auto rr = core_rescale(*intt);
-      r = to_ntt(*rr);
+      cur = rescale_to_ntt(*intt);
     } else {
-      r = core_rescale(*t);
+      cur = rescale_to_ntt(*t);
     }
-    cur = std::move(r);
     t = cur.get();
   }
   if (!t->is_ntt()) {

@@ -84,6 +84,7 @@ struct Data {
   long double scale = 1.0L;
   int64_t *d = nullptr;
   uint64_t serial = 0;  // unique per engine, never reused (keys captured graphs)
+  mutable bool copy_pending = false;  // a download may still read d
 
   size_t words() const;
   long long poly_stride() const;
@@ -145,8 +146,11 @@ class Engine {
   // Device memory from the stream-ordered pool.
   int64_t *alloc_words(size_t words);
   void free_words(int64_t *p);
+  // Frees an object's words; after a pending download, in order behind it.
+  void release(int64_t *p, bool copy_pending);
 
-  std::unique_ptr<Data> make_data(int type, int flag, int moduli_id, int polys, long double scale);
+  std::unique_ptr<Data> make_data(int type, int flag, int moduli_id, int polys, long double scale,
+                                  cudaStream_t alloc_stream = nullptr);
   std::unique_ptr<Data> upload(int type, int flag, int moduli_id, int polys, long double scale,
                                const int64_t *host);
   void download(const Data &d, int64_t *host);
@@ -288,6 +292,15 @@ class Engine {
  private:
   cudaStream_t own_stream_ = nullptr;
   cudaStream_t stream_ = nullptr;
+  // Host uploads and downloads run on streams of their own (one per direction),
+  // ordered against the compute stream by events, so the copies of one ciphertext
+  // overlap the kernels of its neighbours.
+  cudaStream_t upload_stream_ = nullptr;
+  cudaStream_t download_stream_ = nullptr;
+  cudaEvent_t upload_done_ = nullptr;
+  cudaEvent_t compute_done_ = nullptr;
+  void order_download_after_compute();  // the download stream waits for the compute so far
+  void order_compute_after_upload();    // the compute stream waits for the uploads so far
   std::vector<int64_t *> table_buffers_;
   PrimeTables tables_{};
   KeySwitchTables ks_{};
@@ -449,6 +462,7 @@ class Engine {
   // Core steps.
   std::unique_ptr<Data> core_rescale(const Data &ct);          // coefficient form
   std::unique_ptr<Data> prepare_for_multiply(const Data &text, int level);
+  std::unique_ptr<Data> rescale_to_ntt(const Data &text);  // to_ntt(core_rescale(text))
   // Hybrid key switch of the coefficient-form polynomial c1 at moduli_id (L limbs):
   // decompose, ModUp, key product, optional rotation term b * P (rotate_c0 = the
   // coefficient-form c0), ModDown and the epilogue operations `ops` into `out`.

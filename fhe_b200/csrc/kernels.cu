@@ -472,6 +472,17 @@ cudaError_t launch_to_ntt(const PrimeTables &t, int log_n, int polys, int limbs,
   return forward_ntt(log_n, polys, limbs, prime_base, t, ld, st, y, y_stride, s);
 }
 
+cudaError_t launch_rescale_to_ntt(const PrimeTables &t, const KeySwitchTables &ks, int log_n,
+                                  int polys, int limbs, int src_moduli_id, const int64_t *x,
+                                  long long x_stride, int64_t *y, long long y_stride,
+                                  cudaStream_t s) {
+  RescaleEnterLoad ld{x, x_stride,
+                      ks.rescale_scale + static_cast<long long>(src_moduli_id) * ks.prime_count,
+                      t.r_squared, t.q, t.k};
+  PlainStore st{y, y_stride};
+  return forward_ntt(log_n, polys, limbs, src_moduli_id + 1, t, ld, st, y, y_stride, s);
+}
+
 cudaError_t launch_to_intt(const PrimeTables &t, int log_n, int polys, int limbs, int prime_base,
                            const int64_t *x, long long x_stride, int64_t *y, long long y_stride,
                            cudaStream_t s) {

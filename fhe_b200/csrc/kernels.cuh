@@ -204,6 +204,12 @@ cudaError_t launch_scalar_enter(const PrimeTables &t, int n, int polys, int limb
 cudaError_t launch_to_ntt(const PrimeTables &t, int log_n, int polys, int limbs, int prime_base,
                           const int64_t *x, long long x_stride, int64_t *y, long long y_stride,
                           cudaStream_t s);
+// to_ntt_ of the rescale of a coefficient-form text in one pass: x is [polys][limbs +
+// 1][N] at src_moduli_id, y is [polys][limbs][N] at src_moduli_id + 1 (NTT form).
+cudaError_t launch_rescale_to_ntt(const PrimeTables &t, const KeySwitchTables &ks, int log_n,
+                                  int polys, int limbs, int src_moduli_id, const int64_t *x,
+                                  long long x_stride, int64_t *y, long long y_stride,
+                                  cudaStream_t s);
 // Inverse NTT with N^-1 enter-exit (to_intt_).
 cudaError_t launch_to_intt(const PrimeTables &t, int log_n, int polys, int limbs, int prime_base,
                            const int64_t *x, long long x_stride, int64_t *y, long long y_stride,

@@ -65,6 +65,27 @@ struct EnterLoad {
   }
 };
 
+// rescale_once_ (core_rescale.cpp:5-25) and to_ntt_'s enter on the way in: limb
+// `limb` of the rescaled text is made from limbs limb + 1 and 0 of the source, whose
+// first prime is prime - limb - 1 (the rounder compares unsigned, as get_rounder).
+struct RescaleEnterLoad {
+  const int64_t *src;             // [poly][limbs + 1][N]
+  long long poly_stride;
+  const int64_t *rescale_scale;   // the dropped prime's row, indexed by prime
+  const int64_t *r_squared;
+  const uint64_t *q;
+  const uint64_t *k;
+  __device__ __forceinline__ int64_t operator()(int poly, int limb, int prime, int gi, int n) const {
+    const int64_t *s = src + poly * poly_stride;
+    const int64_t x0 = s[gi];
+    const int64_t rounder = static_cast<uint64_t>(x0) > (q[prime - limb - 1] >> 1) ? 1 : 0;
+    const uint64_t qq = q[prime], kk = k[prime];
+    const int64_t v = rescale_word(s[static_cast<long long>(limb + 1) * n + gi], x0, rounder, qq, kk,
+                                   rescale_scale[prime]);
+    return mont_mult(v, r_squared[prime], qq, kk);
+  }
+};
+
 // mont_enter_exit by N^-1*R on the way out: to_intt_ (core_ntt.cpp:131-148),
 // optionally followed by reduce_2q_to_q (mod_down, core_key_switch.cpp:121).
 template <bool REDUCE>

@@ -162,13 +162,17 @@ int fhe_parameters_tables(const fhe_config *config, uint64_t *k, int64_t *r_squa
 
 /* Build an object from host limbs [polys][chains][N] (chains implied by
  * moduli_id and FHE_FLAG_INCLUDE_SPECIAL).  Replaces constructing Data
- * (src/data/data.cpp:9-48) around the reference's per-limb arrays. */
+ * (src/data/data.cpp:9-48) around the reference's per-limb arrays.  The copy runs on
+ * the engine's upload stream and later work waits for it; from pinned host memory the
+ * call returns at once and the copy overlaps kernels already queued. */
 int fhe_data_upload(fhe_engine *engine, int type, int flag, int moduli_id, int polys,
                     long double ckks_scale, const int64_t *host_limbs, fhe_data **out);
 /* Copy all limbs to host memory [polys][chains][N] (waits for queued work). */
 int fhe_data_download(const fhe_data *data, int64_t *host_limbs);
-/* Queue the same copy on the engine's stream without waiting (the host buffer
- * should be pinned; completion is observed with fhe_engine_synchronize). */
+/* Queue the same copy without waiting: it runs on the engine's download stream after
+ * the work queued so far, overlapping later kernels (the host buffer should be
+ * pinned; completion is observed with fhe_engine_synchronize).  Objects are never
+ * modified after they are made, so the copy reads the object's final words. */
 int fhe_data_download_async(const fhe_data *data, int64_t *host_limbs);
 int fhe_data_info_get(const fhe_data *data, fhe_data_info *info);
 /* Set the rotation step carried by a fixed rotation key (FixedRotationKey::delta_). */
