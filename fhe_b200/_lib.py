@@ -92,6 +92,7 @@ SIGNATURES = {
     "fhe_encode": (_i, [_vp, _f64p, _f64p, _i, _i, _i, _pp]),
     "fhe_create_small_bootstrap_key": (_i, [_vp, _vp, _pp, _pp]),
     "fhe_bootstrap": (_i, [_vp, _vp, _vp, _vp, ctypes.POINTER(_vp), _i, _vp, _vp, _i, _pp]),
+    "fhe_rotate_batch": (_i, [_vp, _vp, ctypes.POINTER(_vp), _i, _pp]),
     "fhe_engine_set_tensor_cores": (_i, [_vp, _i]),
     "fhe_engine_set_graphs": (_i, [_vp, _i]),
     "fhe_engine_graph_counts": (_i, [_vp, _ip, _ip]),

@@ -718,29 +718,23 @@ std::unique_ptr<Data> Engine::decompose(const Data &ct) {
   return out;
 }
 
-std::unique_ptr<Data> Engine::mod_down_then_decompose(const Data &ct) {
+std::unique_ptr<Data> Engine::mod_down_then_decompose(Data &ct) {
   // CKKSCore::mod_down_then_decompose (core_key_switch.cpp:468-508): polynomial 1 of
-  // an extended NTT-form text brought down to its chain, then decomposed.
+  // an extended NTT-form text brought down to its chain, then decomposed.  The
+  // ModDown works in place: polynomial 1 of `ct` is clobbered (its caller keeps only
+  // polynomial 0).
   const int m = ct.moduli_id, n = params.n;
   const DevicePartitions &dp = partitions(m, m);
   auto out = make_data(kDecomposed, ct.flag, m, dp.count, ct.scale);
-  int64_t *x = alloc_words(static_cast<size_t>(ct.chains) * n);
   int64_t *reduced = alloc_words(static_cast<size_t>(params.chains(m)) * n);
-  cudaError_t e = cudaMemcpyAsync(x, ct.d + ct.poly_stride(), ct.chains * n * sizeof(int64_t),
-                                  cudaMemcpyDeviceToDevice, stream_);
-  if (e == cudaSuccess) {
-    try {
-      mod_down_polys(x, m, 1, reduced);
-      decompose_into(reduced, m, out->d);
-    } catch (...) {
-      free_words(x);
-      free_words(reduced);
-      throw;
-    }
+  try {
+    mod_down_polys(ct.d + ct.poly_stride(), m, 1, reduced);
+    decompose_into(reduced, m, out->d);
+  } catch (...) {
+    free_words(reduced);
+    throw;
   }
-  free_words(x);
   free_words(reduced);
-  check(e, "copy");
   return out;
 }
 
@@ -749,42 +743,32 @@ std::unique_ptr<Data> Engine::attach_special_primes(const Data &text) {
   // special limbs, then to_ntt_ over the extended chain.
   if (text.flag & kFlagSpecial)
     throw std::invalid_argument("attach special primes: the text already has them.");
-  const int m = text.moduli_id, L = text.chains, n = params.n;
+  if (text.is_ntt()) throw std::invalid_argument("attach special primes: the text is in NTT form.");
+  const int m = text.moduli_id, L = text.chains;
   auto out = make_data(text.type, text.flag | kFlagNtt | kFlagSpecial, m, text.polys, text.scale);
-  std::vector<int64_t> p_product(L);
-  for (int j = 0; j < L; j++) p_product[j] = params.p_product_mult_r[m + j];
-  const long long ops = out->poly_stride();
-  for (int p = 0; p < text.polys; p++) {
-    pointwise(kOpEnter, L, m, text.d + p * text.poly_stride(), nullptr, p_product.data(),
-              out->d + p * ops);
-    check(cudaMemsetAsync(out->d + p * ops + static_cast<long long>(L) * n, 0,
-                          static_cast<size_t>(out->chains - L) * n * sizeof(int64_t), stream_),
-          "zero special limbs");
-  }
-  ntt_in_place(out->d, out->chains, m, ops, text.polys);
+  check(timed("attach_special_ntt", [&] {
+          return launch_attach_special_ntt(tables_, ks_, params.log_n, text.polys, L, m, text.d,
+                                           text.poly_stride(), out->d, out->poly_stride(),
+                                           stream_);
+        }),
+        "attach special primes");
   return out;
 }
 
 std::unique_ptr<Data> Engine::remove_special_primes(const Data &text) {
-  // remove_special_prime_chains_ (core.cpp:1165-1187): ModDown of every polynomial.
+  // remove_special_prime_chains_ (core.cpp:1165-1187): ModDown of every polynomial,
+  // on a copy (the ModDown works in place).
+  auto copy = clone(text);
+  return remove_special_primes_in_place(*copy);
+}
+
+std::unique_ptr<Data> Engine::remove_special_primes_in_place(Data &text) {
   if (!(text.flag & kFlagSpecial) || !text.is_ntt() || text.polys > 2)
     throw std::invalid_argument("remove special primes: the text has no special primes.");
   const int m = text.moduli_id;
   auto out = make_data(text.type, text.flag & ~(kFlagNtt | kFlagSpecial), m, text.polys,
                        text.scale);
-  int64_t *x = alloc_words(text.words());
-  cudaError_t e = cudaMemcpyAsync(x, text.d, text.words() * sizeof(int64_t),
-                                  cudaMemcpyDeviceToDevice, stream_);
-  if (e == cudaSuccess) {
-    try {
-      mod_down_polys(x, m, text.polys, out->d);
-    } catch (...) {
-      free_words(x);
-      throw;
-    }
-  }
-  free_words(x);
-  check(e, "copy");
+  mod_down_polys(text.d, m, text.polys, out->d);
   return out;
 }
 
@@ -920,7 +904,7 @@ std::unique_ptr<Data> Engine::apply_butterfly(const Data &ct, const BootstrapKey
     else
       add_inplace(*outer_sum, *turned);
   }
-  return remove_special_primes(*outer_sum);
+  return remove_special_primes_in_place(*outer_sum);
 }
 
 std::unique_ptr<Data> Engine::bootstrap(const Data &ct, const Data &rk, const Data &ck,

@@ -686,6 +686,28 @@ static const fhe_b200::BootstrapKey &live_key(const fhe_engine *engine,
   return *key->impl;
 }
 
+int fhe_rotate_batch(fhe_engine *engine, const fhe_data *ct, const fhe_data *const *keys,
+                     int key_count, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(ct);
+  REQUIRE_OUT(keys);
+  REQUIRE_OUT(out);
+  if (key_count < 1) {
+    fhe_b200::set_last_error("Batch Rotate Ciphertext With Fixed Rotation Keys: no keys.");
+    return FHE_ERR_INVALID_ARGUMENT;
+  }
+  for (int i = 0; i < key_count; i++) {
+    REQUIRE_HANDLE(keys[i]);
+    out[i] = nullptr;
+  }
+  return guarded([&] {
+    std::vector<const Data *> ks;
+    for (int i = 0; i < key_count; i++) ks.push_back(&live(engine, keys[i]));
+    auto r = engine->impl->rotate_batch(live(engine, ct), ks);
+    for (int i = 0; i < key_count; i++) out[i] = wrap(std::move(r[i]));
+  });
+}
+
 int fhe_engine_set_tensor_cores(fhe_engine *engine, int mode) {
   REQUIRE_HANDLE(engine);
   return guarded([&] { engine->impl->set_tensor_cores(mode); });

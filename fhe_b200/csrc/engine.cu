@@ -489,7 +489,8 @@ std::unique_ptr<Data> Engine::multiply(const Data &a, const Data &b) {
 }
 
 void Engine::key_switch_pipeline(const int64_t *c1, int moduli_id, const Data &key,
-                                 const int64_t *rotate_c0, const EpilogueOps &ops, int64_t *out) {
+                                 const int64_t *rotate_c0, const EpilogueOps &ops, int64_t *out,
+                                 const int64_t *decomposed) {
   const int n = params.n;
   const int L = params.chains(moduli_id);
   const int E = params.chains(moduli_id, true);
@@ -499,16 +500,22 @@ void Engine::key_switch_pipeline(const int64_t *c1, int moduli_id, const Data &k
   const DevicePartitions &dp = partitions(moduli_id, key.moduli_id);
   if (key.polys < 2 * (dp.max_key_index + 1))
     throw std::invalid_argument("the key switching key has too few polynomials.");
+  // A decomposition made earlier (hoisted rotations) replaces the ModUp: its partitions
+  // have the same starts and sizes, only the key index depends on the key's level.
   int64_t *digits = alloc_words(static_cast<size_t>(L) * n);
-  int64_t *ext = alloc_words(static_cast<size_t>(dp.count) * E * n);
+  int64_t *own_ext = decomposed ? nullptr : alloc_words(static_cast<size_t>(dp.count) * E * n);
+  const int64_t *ext = decomposed ? decomposed : own_ext;
   int64_t *acc = alloc_words(static_cast<size_t>(2) * E * n);
-  cudaError_t e = timed("mixed_radix", [&] {
-    return launch_mixed_radix(tables_, dp, n, moduli_id, c1, digits, stream_);
-  });
-  if (e == cudaSuccess)
-    e = timed("mod_up_ntt", [&] {
-      return launch_mod_up_ntt(tables_, dp, params.log_n, moduli_id, digits, ext, stream_);
+  cudaError_t e = cudaSuccess;
+  if (!decomposed) {
+    e = timed("mixed_radix", [&] {
+      return launch_mixed_radix(tables_, dp, n, moduli_id, c1, digits, stream_);
     });
+    if (e == cudaSuccess)
+      e = timed("mod_up_ntt", [&] {
+        return launch_mod_up_ntt(tables_, dp, params.log_n, moduli_id, digits, own_ext, stream_);
+      });
+  }
   if (e == cudaSuccess)
     e = timed("key_inner_product", [&] {
       return launch_key_inner_product(tables_, dp, n, moduli_id, ext, key.d, key.chains,
@@ -526,7 +533,7 @@ void Engine::key_switch_pipeline(const int64_t *c1, int moduli_id, const Data &k
     });
   if (e == cudaSuccess) e = mod_down_epilogue(moduli_id, L, acc, ops, out);
   free_words(digits);
-  free_words(ext);
+  free_words(own_ext);
   free_words(acc);
   check(e, "key switch");
 }
@@ -787,11 +794,41 @@ const int32_t *Engine::device_ntt_permutation(int delta) {
 
 // CKKSCore::rotate (core.cpp:939-963): key switch of c1 with the b * P term, ModDown,
 // then the key's signed coefficient permutation.
-std::unique_ptr<Data> Engine::core_rotate(const Data &ct, const Data &key) {
+std::unique_ptr<Data> Engine::core_rotate(const Data &ct, const Data &key, const Data *decomposed) {
   auto out = make_data(kUnitCiphertext, ct.flag, ct.moduli_id, 2, ct.scale);
   EpilogueOps ops;
   ops.signed_perm = device_signed_permutation(key.delta);
-  key_switch_pipeline(ct.d + ct.poly_stride(), ct.moduli_id, key, ct.d, ops, out->d);
+  key_switch_pipeline(ct.d + ct.poly_stride(), ct.moduli_id, key, ct.d, ops, out->d,
+                      decomposed ? decomposed->d : nullptr);
+  return out;
+}
+
+std::vector<std::unique_ptr<Data>> Engine::rotate_batch(const Data &ct,
+                                                        const std::vector<const Data *> &keys) {
+  // CKKSEngine::rotate_batch(ct, fixed rotation keys) (engine_rotate.cpp:262-300):
+  // the input is decomposed once (core_key_switch.cpp:434-466) and every key reuses
+  // the decomposition (core.cpp:939-952).
+  const std::string fn = "Batch Rotate Ciphertext With Fixed Rotation Keys";
+  require_text(fn, ct, 0, 1, 2, false);
+  for (const Data *k : keys) {
+    if (!k || k->type != kFixedRotationKey)
+      throw std::invalid_argument(fn + ": the key is not a fixed rotation key.");
+    require_key_level(fn, ct, *k, false, "fixed rotation key");
+  }
+  std::unique_ptr<Data> hold;
+  const Data *x = &ct;
+  if (params.preset.one_more_level && ct.moduli_id == 0) {
+    hold = level_down_any(ct, ct.level() - 1);
+    x = hold.get();
+  }
+  if (x->is_ntt()) {
+    hold = to_intt(*x);
+    x = hold.get();
+  }
+  std::vector<std::unique_ptr<Data>> out;
+  if (keys.empty()) return out;
+  auto decomposed = decompose(*x);
+  for (const Data *k : keys) out.push_back(core_rotate(*x, *k, decomposed.get()));
   return out;
 }
 

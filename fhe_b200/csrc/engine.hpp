@@ -172,6 +172,10 @@ class Engine {
   std::unique_ptr<Data> rotate(const Data &ct, const Data &fixed_rotation_key);
   std::unique_ptr<Data> rotate(const Data &ct, const std::vector<const Data *> &keys, int delta,
                                bool normalize_by_slot_count = true);
+  // Hoisted rotations of one ciphertext by several fixed keys (rotate_batch with fixed
+  // rotation keys, engine_rotate.cpp:262-300): one decomposition for all keys.
+  std::vector<std::unique_ptr<Data>> rotate_batch(const Data &ct,
+                                                  const std::vector<const Data *> &keys);
   // Plaintext rotation and conjugation (no key): engine_rotate.cpp:10-24.
   std::unique_ptr<Data> rotate_plain(const Data &pt, int delta);
   std::unique_ptr<Data> conjugate_plain(const Data &pt);
@@ -383,7 +387,8 @@ class Engine {
                             int rotate_count, int level, int inner_loop_shift);
   void require_bootstrap_stage_count(const std::string &fn, int stage_count,
                                      int inner_loop_shift) const;
-  std::unique_ptr<Data> mod_down_then_decompose(const Data &ct);
+  std::unique_ptr<Data> mod_down_then_decompose(Data &ct);  // clobbers polynomial 1
+  std::unique_ptr<Data> remove_special_primes_in_place(Data &text);  // clobbers text
   std::unique_ptr<Data> core_ntt_rotate(const Data &ct, const Data &decomposed, const Data &key,
                                         int delta);
   std::unique_ptr<Data> apply_butterfly(const Data &ct, const BootstrapKey &bk,
@@ -467,7 +472,8 @@ class Engine {
   // decompose, ModUp, key product, optional rotation term b * P (rotate_c0 = the
   // coefficient-form c0), ModDown and the epilogue operations `ops` into `out`.
   void key_switch_pipeline(const int64_t *c1, int moduli_id, const Data &key,
-                           const int64_t *rotate_c0, const EpilogueOps &ops, int64_t *out);
+                           const int64_t *rotate_c0, const EpilogueOps &ops, int64_t *out,
+                           const int64_t *decomposed = nullptr);
   // Key switch tail shared by relinearize variants; t3 is [3][L][N] coefficient
   // form at moduli_id (poly 2 is switched).
   void relinearize_tail(const int64_t *t3, int moduli_id, const Data &rk, int mode, int64_t *out);
@@ -475,7 +481,8 @@ class Engine {
                          bool for_multiply, const char *key_name = "relinearization key");
   std::unique_ptr<Data> core_level_down(const Data &text, int level);  // coefficient form
   std::unique_ptr<Data> level_down_any(const Data &text, int level);   // level_down_ (any form)
-  std::unique_ptr<Data> core_rotate(const Data &ct, const Data &key);   // coefficient form
+  std::unique_ptr<Data> core_rotate(const Data &ct, const Data &key,
+                                    const Data *decomposed = nullptr);   // coefficient form
 };
 
 // Thread-local last error of the C ABI.

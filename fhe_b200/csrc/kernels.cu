@@ -483,6 +483,21 @@ cudaError_t launch_rescale_to_ntt(const PrimeTables &t, const KeySwitchTables &k
   return forward_ntt(log_n, polys, limbs, src_moduli_id + 1, t, ld, st, y, y_stride, s);
 }
 
+cudaError_t launch_attach_special_ntt(const PrimeTables &t, const KeySwitchTables &ks, int log_n,
+                                      int polys, int limbs, int moduli_id, const int64_t *x,
+                                      long long x_stride, int64_t *y, long long y_stride,
+                                      cudaStream_t s) {
+  const long long n = 1LL << log_n;
+  const size_t special_bytes = static_cast<size_t>(ks.special_count) * n * sizeof(int64_t);
+  for (int p = 0; p < polys; p++) {
+    const cudaError_t e = cudaMemsetAsync(y + p * y_stride + limbs * n, 0, special_bytes, s);
+    if (e != cudaSuccess) return e;
+  }
+  ProductEnterLoad ld{x, x_stride, ks.p_product_mult_r, t.r_squared, t.q, t.k};
+  PlainStore st{y, y_stride};
+  return forward_ntt(log_n, polys, limbs, moduli_id, t, ld, st, y, y_stride, s);
+}
+
 cudaError_t launch_to_intt(const PrimeTables &t, int log_n, int polys, int limbs, int prime_base,
                            const int64_t *x, long long x_stride, int64_t *y, long long y_stride,
                            cudaStream_t s) {

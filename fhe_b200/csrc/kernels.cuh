@@ -210,6 +210,13 @@ cudaError_t launch_rescale_to_ntt(const PrimeTables &t, const KeySwitchTables &k
                                   int polys, int limbs, int src_moduli_id, const int64_t *x,
                                   long long x_stride, int64_t *y, long long y_stride,
                                   cudaStream_t s);
+// attach_special_prime_chains_ of a coefficient-form text: y [polys][limbs + K][N]
+// = to_ntt_ of (x * P on the limbs, zero special limbs); the zero limbs are written
+// as zeros (their transform), the others go through one fused NTT.
+cudaError_t launch_attach_special_ntt(const PrimeTables &t, const KeySwitchTables &ks, int log_n,
+                                      int polys, int limbs, int moduli_id, const int64_t *x,
+                                      long long x_stride, int64_t *y, long long y_stride,
+                                      cudaStream_t s);
 // Inverse NTT with N^-1 enter-exit (to_intt_).
 cudaError_t launch_to_intt(const PrimeTables &t, int log_n, int polys, int limbs, int prime_base,
                            const int64_t *x, long long x_stride, int64_t *y, long long y_stride,

@@ -86,6 +86,22 @@ struct RescaleEnterLoad {
   }
 };
 
+// attach_special_prime_chains_ (core.cpp:1127-1155) on the way in: x * P R^-1
+// (mont_enter_scalar_ by P * R mod q) then to_ntt_'s enter.
+struct ProductEnterLoad {
+  const int64_t *src;
+  long long poly_stride;
+  const int64_t *p_product;  // P * R mod q, indexed by prime
+  const int64_t *r_squared;
+  const uint64_t *q;
+  const uint64_t *k;
+  __device__ __forceinline__ int64_t operator()(int poly, int limb, int prime, int gi, int n) const {
+    const uint64_t qq = q[prime], kk = k[prime];
+    const int64_t x = src[poly * poly_stride + (long long)limb * n + gi];
+    return mont_mult(mont_mult(x, p_product[prime], qq, kk), r_squared[prime], qq, kk);
+  }
+};
+
 // mont_enter_exit by N^-1*R on the way out: to_intt_ (core_ntt.cpp:131-148),
 // optionally followed by reduce_2q_to_q (mod_down, core_key_switch.cpp:121).
 template <bool REDUCE>

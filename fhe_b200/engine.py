@@ -304,6 +304,14 @@ class Engine:
             return Data(self, h)
         return self._call("fhe_rotate", ct, key)
 
+    def rotate_batch(self, ct: Data, fixed_rotation_keys: list) -> list:
+        """Hoisted rotations: one decomposition of ct for every fixed key."""
+        n = len(fixed_rotation_keys)
+        keys = (ctypes.c_void_p * n)(*[k.handle for k in fixed_rotation_keys])
+        out = (ctypes.c_void_p * n)()
+        check(_lib.load().fhe_rotate_batch(self._h, ct.handle, keys, n, out))
+        return [Data(self, ctypes.c_void_p(out[i])) for i in range(n)]
+
     def rotate_plaintext(self, pt: Data, delta: int) -> Data:
         h = ctypes.c_void_p()
         check(_lib.load().fhe_rotate_plaintext(self._h, pt.handle, delta, ctypes.byref(h)))

@@ -326,6 +326,12 @@ int fhe_decrypt(fhe_engine *engine, const fhe_data *ciphertext, const fhe_data *
  * key-switching level.  Needs a bootstrapping preset. */
 int fhe_create_small_bootstrap_key(fhe_engine *engine, const fhe_data *secret_key,
                                    fhe_data **to_sparse, fhe_data **to_dense);
+/* CKKSEngine::rotate_batch(Ciphertext*, std::vector<FixedRotationKey*>)
+ * (engine_rotate.cpp:262-300), per unit ciphertext: the input is decomposed once and
+ * every fixed key reuses the decomposition (hoisted rotations).  out receives
+ * key_count new handles, out[i] rotated by keys[i]. */
+int fhe_rotate_batch(fhe_engine *engine, const fhe_data *ct, const fhe_data *const *keys,
+                     int key_count, fhe_data **out);
 /* CKKSEngine::bootstrap(UnitCiphertext*, RelinearizationKey*, ConjugationKey*,
  * RotationKey*, SmallBootstrapKey*, int stage_count) (engine_bootstrap.cpp:712-754):
  * level down to 0, mod raise, coefficients-to-slots, EvalRound, slots-to-coefficients

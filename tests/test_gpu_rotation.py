@@ -121,3 +121,19 @@ def test_rotation_errors_mirror_reference(config_c):
         e.rotate(a, fk)
     with pytest.raises(FheError, match="target level cannot be reached"):
         e.level_down(a, 40)
+
+
+@pytest.mark.parametrize("mid,key_mid", [(1, 1), (6, 1), (12, 3)])
+def test_hoisted_rotate_batch_matches_single_rotations(config_c, mid, key_mid):
+    """rotate_batch with fixed keys (one decomposition, engine_rotate.cpp:262-300)
+    gives the words of one rotation per key, for keys at the text's level or above."""
+    e, _ = config_c
+    rng = np.random.default_rng(7300 + mid)
+    a = e.upload(uniform_limbs(rng, e.moduli[mid:e.chain_count], 2, e.coeff_count), mid)
+    keys = [e.upload_fixed_rotation_key(
+        uniform_limbs(rng, e.moduli[key_mid:], 2 * e.partition_count(key_mid), e.coeff_count),
+        key_mid, d) for d in (1, 3, 1 << 10)]
+    hoisted = e.rotate_batch(a, keys)
+    for k, h in zip(keys, hoisted):
+        assert np.array_equal(h.download(), e.rotate(a, k).download())
+
