@@ -133,7 +133,7 @@ __device__ __forceinline__ int tile_index(int c, int i) {
 }
 
 template <int S, bool INVERSE, class Loader, class Storer>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
     ntt_pass_kernel(NttPass a, PrimeTables t, Loader load, Storer store) {
   constexpr int M = 1 << S;
   constexpr int R = (S + 2) / 3;
