@@ -311,16 +311,16 @@ std::unique_ptr<Data> Engine::multiply_scalar(const Data &ct, double value) {
   const int mid = x->moduli_id;
   const int L = x->chains;
   const auto mult = mult_multiplier(value, level);
-  int64_t *entered = alloc_words(static_cast<size_t>(x->polys) * x->poly_stride());
-  const long long ps = x->poly_stride();
-  for (int q = 0; q < x->polys; q++)
-    pointwise(kOpEnterReduce, L, mid, x->d + q * ps, nullptr, mult.data(), entered + q * ps);
+  if (L > kMaxScalarLimbs) throw std::invalid_argument(fn + ": too many limbs.");
+  LimbScalars c{};
+  for (int j = 0; j < L; j++) c.v[j] = mult[j];
   const long double rs = params.rescaled_scale(x->scale, mid);
   auto out = make_data(kUnitCiphertext, x->flag, params.moduli_id(level - 1), x->polys, rs * rs);
-  const cudaError_t e = launch_rescale(tables_, ks_, params.n, x->polys, L, mid, entered, ps,
-                                       out->d, out->poly_stride(), stream_);
-  free_words(entered);
-  check(e, "rescale");
+  check(timed("scalar_rescale", [&] {
+          return launch_scalar_rescale(tables_, ks_, params.n, x->polys, L, mid, c, x->d,
+                                       x->poly_stride(), out->d, out->poly_stride(), stream_);
+        }),
+        "multiply scalar");
   return out;
 }
 

@@ -200,6 +200,13 @@ cudaError_t launch_scalar_enter(const PrimeTables &t, int n, int polys, int limb
                                 int x_limb_offset, const LimbScalars &s, int64_t *y,
                                 long long y_stride, cudaStream_t st);
 
+// CKKSCore::multiply(ct, double) (core.cpp:196-229): y [polys][limbs - 1][N] at
+// moduli_id + 1 = rescale_once_ of reduce(mont_enter(x, c[limb])) of coefficient-form x.
+cudaError_t launch_scalar_rescale(const PrimeTables &t, const KeySwitchTables &ks, int n,
+                                  int polys, int limbs, int moduli_id, const LimbScalars &c,
+                                  const int64_t *x, long long x_stride, int64_t *y,
+                                  long long y_stride, cudaStream_t s);
+
 // Forward NTT with Montgomery enter (to_ntt_) of polys x limbs, in place or not.
 cudaError_t launch_to_ntt(const PrimeTables &t, int log_n, int polys, int limbs, int prime_base,
                           const int64_t *x, long long x_stride, int64_t *y, long long y_stride,
