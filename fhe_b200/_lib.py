@@ -93,6 +93,8 @@ SIGNATURES = {
     "fhe_create_small_bootstrap_key": (_i, [_vp, _vp, _pp, _pp]),
     "fhe_bootstrap": (_i, [_vp, _vp, _vp, _vp, ctypes.POINTER(_vp), _i, _vp, _vp, _i, _pp]),
     "fhe_rotate_batch": (_i, [_vp, _vp, ctypes.POINTER(_vp), _i, _pp]),
+    "fhe_ntt_tuning_set": (_i, [_i, _i, _i, _i]),
+    "fhe_ntt_tuning_get": (_i, [_i, _ip, _ip, _ip]),
     "fhe_engine_set_tensor_cores": (_i, [_vp, _i]),
     "fhe_engine_set_graphs": (_i, [_vp, _i]),
     "fhe_engine_graph_counts": (_i, [_vp, _ip, _ip]),
@@ -153,7 +155,28 @@ def load():
             f.restype = res
             f.argtypes = args
         _lib = lib
+        install_ntt_tuning(lib)
     return _lib
+
+
+TUNING_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ntt_tuning.json")
+
+
+def install_ntt_tuning(lib, path: str = TUNING_PATH) -> int:
+    """Installs the NTT shapes measured by fhe_b200.autotune (if the file exists);
+    returns how many transform sizes were set."""
+    if not os.path.exists(path):
+        return 0
+    import json
+
+    with open(path) as f:
+        table = json.load(f)
+    count = 0
+    for log_n, t in table.get("ntt", {}).items():
+        if lib.fhe_ntt_tuning_set(int(log_n), t["s_second"], t["first_columns_log"],
+                                  t["second_tile_log"]) == 0:
+            count += 1
+    return count
 
 
 class FheError(RuntimeError):

@@ -708,6 +708,30 @@ int fhe_rotate_batch(fhe_engine *engine, const fhe_data *ct, const fhe_data *con
   });
 }
 
+int fhe_ntt_tuning_set(int log_n, int s_second, int first_columns_log, int second_tile_log) {
+  fhe_b200::NttTuning t;
+  t.s_second = s_second;
+  t.first_columns_log = first_columns_log;
+  t.second_tile_log = second_tile_log;
+  if (!fhe_b200::set_ntt_tuning(log_n, t)) {
+    fhe_b200::set_last_error("NTT tuning: the shape is not valid for this transform size.");
+    return FHE_ERR_INVALID_ARGUMENT;
+  }
+  fhe_b200::set_last_error("");
+  return FHE_OK;
+}
+
+int fhe_ntt_tuning_get(int log_n, int *s_second, int *first_columns_log, int *second_tile_log) {
+  REQUIRE_OUT(s_second);
+  REQUIRE_OUT(first_columns_log);
+  REQUIRE_OUT(second_tile_log);
+  const fhe_b200::NttTuning t = fhe_b200::ntt_tuning(log_n);
+  *s_second = t.s_second;
+  *first_columns_log = t.first_columns_log;
+  *second_tile_log = t.second_tile_log;
+  return FHE_OK;
+}
+
 int fhe_engine_set_tensor_cores(fhe_engine *engine, int mode) {
   REQUIRE_HANDLE(engine);
   return guarded([&] { engine->impl->set_tensor_cores(mode); });

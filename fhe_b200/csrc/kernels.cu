@@ -14,6 +14,37 @@ std::atomic<unsigned long long> g_launches{0};
 
 void note_launch(unsigned count) { g_launches.fetch_add(count, std::memory_order_relaxed); }
 unsigned long long kernel_launch_count() { return g_launches.load(std::memory_order_relaxed); }
+namespace {
+NttTuning g_ntt_tuning[18];  // zero: the default
+}
+
+NttTuning ntt_default_tuning(int log_n) {
+  NttTuning t;
+  t.s_second = log_n >= 15 ? 8 : (log_n >= 13 ? 7 : 6);
+  t.first_columns_log = log_n - t.s_second >= 9 ? 3 : 4;
+  t.second_tile_log = 12;
+  return t;
+}
+
+NttTuning ntt_tuning(int log_n) {
+  if (log_n >= 0 && log_n < 18 && g_ntt_tuning[log_n].s_second > 0) return g_ntt_tuning[log_n];
+  return ntt_default_tuning(log_n);
+}
+
+bool set_ntt_tuning(int log_n, const NttTuning &tu) {
+  if (log_n < 12 || log_n > 17) return false;
+  const int s1 = log_n - tu.s_second;
+  const int c2 = tu.second_tile_log - tu.s_second;
+  if (tu.s_second < 1 || tu.s_second > 11 || s1 < 1 || s1 > 11) return false;
+  if (tu.first_columns_log < 0 || tu.first_columns_log > tu.s_second) return false;
+  if (c2 < 0 || c2 > s1) return false;
+  if ((sizeof(int64_t) << (tu.first_columns_log + s1)) > static_cast<size_t>(kNttMaxSmem) ||
+      (sizeof(int64_t) << tu.second_tile_log) > static_cast<size_t>(kNttMaxSmem))
+    return false;
+  g_ntt_tuning[log_n] = tu;
+  return true;
+}
+
 void unnote_launches(unsigned long long count) {
   g_launches.fetch_sub(count, std::memory_order_relaxed);
 }

@@ -188,6 +188,22 @@ cudaError_t launch_diagonal_mac(const PrimeTables &t, int log_n, int limbs, int 
                                 const MacTerms &terms, long long x_stride, bool accumulate,
                                 int64_t *y, long long y_stride, cudaStream_t s);
 
+// Shapes of the two-pass NTT of 2^log_n words (12 <= log_n <= 17): the inner pass
+// covers s_second stages, the outer (strided) pass the others; first_columns_log
+// sub-transforms share a CTA in the outer pass, 2^second_tile_log words make a CTA
+// tile in the inner pass.  The defaults are hand-chosen; fhe_b200/autotune.py
+// measures the candidates on the device and the package installs the fastest.
+struct NttTuning {
+  int s_second = 0;
+  int first_columns_log = 0;
+  int second_tile_log = 0;
+};
+constexpr int kNttMaxSmem = 128 * 1024;
+NttTuning ntt_tuning(int log_n);
+NttTuning ntt_default_tuning(int log_n);
+// Installs a tuning for log_n; false (and nothing changes) when it is not valid.
+bool set_ntt_tuning(int log_n, const NttTuning &tuning);
+
 // Per-limb Montgomery constants passed by value.
 constexpr int kMaxScalarLimbs = 128;
 struct LimbScalars {

@@ -19,6 +19,7 @@
 
 #include <cuda_runtime.h>
 
+#include "kernels.cuh"
 #include "modarith.cuh"
 
 namespace fhe_b200 {
@@ -256,20 +257,24 @@ __global__ void __launch_bounds__(256, 4)
   }
 }
 
-// Pass plan of a transform of 2^log_n words.
+// Pass plan of a transform of 2^log_n words: for two passes, the tuned or default
+// split and tile shapes (ntt_tuning, kernels.cuh).  Every plan performs the same
+// butterflies, so every plan gives the same words.
 struct NttPlan {
-  int passes;     // 1 or 2
-  int s_first;    // S of the strided (outer) pass, or log_n for a single pass
-  int s_second;   // S of the contiguous (inner) pass
+  int passes;             // 1 or 2
+  int s_first;            // S of the strided (outer) pass, or log_n for a single pass
+  int s_second;           // S of the contiguous (inner) pass
+  int first_columns_log;  // sub-transforms per CTA of the strided pass
+  int second_columns_log; // sub-transforms per CTA of the contiguous pass
 };
 
 inline NttPlan ntt_plan(int log_n) {
-  if (log_n <= 11) return {1, log_n, 0};
-  const int s2 = log_n >= 15 ? 8 : (log_n >= 13 ? 7 : 6);
-  return {2, log_n - s2, s2};
+  if (log_n <= 11) return {1, log_n, 0, 0, 0};
+  const NttTuning tu = ntt_tuning(log_n);
+  return {2, log_n - tu.s_second, tu.s_second, tu.first_columns_log,
+          tu.second_tile_log - tu.s_second};
 }
 
-constexpr int kNttTileLog = 12;  // 4096 words per tile
 constexpr int kNttThreads = 256;
 
 template <int S, bool INVERSE, class Loader, class Storer>
@@ -279,11 +284,16 @@ cudaError_t launch_ntt_pass(const NttPass &a, const PrimeTables &t, const Loader
   const dim3 grid(subs >> a.columns_log, a.polys * a.limbs);
   const size_t smem = sizeof(int64_t) << (a.columns_log + S);
   auto kernel = ntt_pass_kernel<S, INVERSE, Loader, Storer>;
-  if (smem > 48 * 1024) {
+  // Raised once per instantiation to the most any valid plan uses, so no attribute
+  // call lands inside a graph capture.
+  static bool raised = false;
+  if (!raised) {
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
+                                         kNttMaxSmem);
     if (e != cudaSuccess) return e;
+    raised = true;
   }
+  if (smem > static_cast<size_t>(kNttMaxSmem)) return cudaErrorInvalidValue;
   note_launch(1);
   kernel<<<grid, kNttThreads, smem, stream>>>(a, t, ld, st);
   return cudaGetLastError();
@@ -327,12 +337,12 @@ cudaError_t forward_ntt(int log_n, int polys, int limbs, int prime_base, const P
   PlainLoad mid_load{work, work_stride};
   a.stride_log = plan.s_second;
   a.first = 0;
-  a.columns_log = plan.s_first >= 9 ? 3 : 4;
+  a.columns_log = plan.first_columns_log;
   cudaError_t e = dispatch_ntt_pass<false>(plan.s_first, a, t, ld, mid_store, stream);
   if (e != cudaSuccess) return e;
   a.stride_log = 0;
   a.first = plan.s_first;
-  a.columns_log = kNttTileLog - plan.s_second;
+  a.columns_log = plan.second_columns_log;
   return dispatch_ntt_pass<false>(plan.s_second, a, t, mid_load, st, stream);
 }
 
@@ -352,12 +362,12 @@ cudaError_t inverse_ntt(int log_n, int polys, int limbs, int prime_base, const P
   PlainLoad mid_load{work, work_stride};
   a.stride_log = 0;
   a.first = 0;
-  a.columns_log = kNttTileLog - plan.s_second;
+  a.columns_log = plan.second_columns_log;
   cudaError_t e = dispatch_ntt_pass<true>(plan.s_second, a, t, ld, mid_store, stream);
   if (e != cudaSuccess) return e;
   a.stride_log = plan.s_second;
   a.first = plan.s_second;
-  a.columns_log = plan.s_first >= 9 ? 3 : 4;
+  a.columns_log = plan.first_columns_log;
   return dispatch_ntt_pass<true>(plan.s_first, a, t, mid_load, st, stream);
 }
 

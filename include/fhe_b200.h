@@ -439,6 +439,16 @@ int fhe_engine_set_graphs(fhe_engine *engine, int enable);
  * whose capture failed and which therefore run directly. */
 int fhe_engine_graph_counts(const fhe_engine *engine, int *captured, int *failed);
 
+/* Shapes of the two-pass NTT of 2^log_n words (12 <= log_n <= 17, process-wide): the
+ * contiguous pass covers s_second stages, the strided pass log_n - s_second;
+ * 2^first_columns_log sub-transforms share a CTA in the strided pass and
+ * 2^second_tile_log words make a CTA tile in the contiguous one.  Every shape gives
+ * the same words; fhe_b200/autotune.py measures them on the device and writes the
+ * fastest to fhe_b200/ntt_tuning.json, which the Python package installs on load.
+ * set returns FHE_ERR_INVALID_ARGUMENT for a shape the kernels cannot run. */
+int fhe_ntt_tuning_set(int log_n, int s_second, int first_columns_log, int second_tile_log);
+int fhe_ntt_tuning_get(int log_n, int *s_second, int *first_columns_log, int *second_tile_log);
+
 /* ---- processor-level kernels on device limbs (src/processor/single.h) --------------- */
 
 /* SingleProcessor::ntt / intt (single.cpp:420-454) on `polys` x `chains` device limbs
