@@ -93,6 +93,9 @@ SIGNATURES = {
     "fhe_create_small_bootstrap_key": (_i, [_vp, _vp, _pp, _pp]),
     "fhe_bootstrap": (_i, [_vp, _vp, _vp, _vp, ctypes.POINTER(_vp), _i, _vp, _vp, _i, _pp]),
     "fhe_rotate_batch": (_i, [_vp, _vp, ctypes.POINTER(_vp), _i, _pp]),
+    "fhe_data_serialized_size": (_i, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
+    "fhe_data_serialize": (_i, [_vp, _vp, ctypes.c_uint64]),
+    "fhe_data_deserialize": (_i, [_vp, _vp, ctypes.c_uint64, _pp]),
     "fhe_ntt_tuning_set": (_i, [_i, _i, _i, _i]),
     "fhe_ntt_tuning_get": (_i, [_i, _ip, _ip, _ip]),
     "fhe_engine_set_tensor_cores": (_i, [_vp, _i]),

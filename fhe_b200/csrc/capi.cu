@@ -246,6 +246,28 @@ int fhe_data_download_async(const fhe_data *data, int64_t *host_limbs) {
   return guarded([&] { live(nullptr, data).engine->download_async(*data->impl, host_limbs); });
 }
 
+int fhe_data_serialized_size(const fhe_data *data, uint64_t *size) {
+  REQUIRE_HANDLE(data);
+  REQUIRE_OUT(size);
+  return guarded([&] { *size = live(nullptr, data).engine->serialized_size(*data->impl); });
+}
+
+int fhe_data_serialize(const fhe_data *data, void *buffer, uint64_t capacity) {
+  REQUIRE_HANDLE(data);
+  REQUIRE_OUT(buffer);
+  return guarded([&] {
+    live(nullptr, data).engine->serialize(*data->impl, buffer, static_cast<size_t>(capacity));
+  });
+}
+
+int fhe_data_deserialize(fhe_engine *engine, const void *buffer, uint64_t size, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_OUT(buffer);
+  REQUIRE_OUT(out);
+  *out = nullptr;
+  return guarded([&] { *out = wrap(engine->impl->deserialize(buffer, static_cast<size_t>(size))); });
+}
+
 int fhe_data_info_get(const fhe_data *data, fhe_data_info *info) {
   REQUIRE_HANDLE(data);
   REQUIRE_OUT(info);

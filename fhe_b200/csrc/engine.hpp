@@ -153,6 +153,10 @@ class Engine {
                                   cudaStream_t alloc_stream = nullptr);
   std::unique_ptr<Data> upload(int type, int flag, int moduli_id, int polys, long double scale,
                                const int64_t *host);
+  // The wire format of serialize.cu: header (parameters, shape, scale) and limbs.
+  size_t serialized_size(const Data &d) const;
+  void serialize(const Data &d, void *buffer, size_t capacity);
+  std::unique_ptr<Data> deserialize(const void *buffer, size_t size);
   void download(const Data &d, int64_t *host);
   void download_async(const Data &d, int64_t *host);
   std::unique_ptr<Data> clone(const Data &d);

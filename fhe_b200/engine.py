@@ -51,6 +51,14 @@ class Data:
         check(_lib.load().fhe_data_download(self._h, out.ctypes.data_as(_lib._i64p)))
         return out
 
+    def serialize(self) -> bytes:
+        """The object in the engine's wire format (header and limbs)."""
+        size = ctypes.c_uint64()
+        check(_lib.load().fhe_data_serialized_size(self._h, ctypes.byref(size)))
+        buf = ctypes.create_string_buffer(size.value)
+        check(_lib.load().fhe_data_serialize(self._h, buf, size.value))
+        return buf.raw
+
     def set_delta(self, delta: int) -> None:
         check(_lib.load().fhe_data_set_delta(self._h, delta))
 
@@ -444,6 +452,12 @@ class Engine:
         check(_lib.load().fhe_create_small_bootstrap_key(self._h, secret_key.handle,
                                                          ctypes.byref(a), ctypes.byref(b)))
         return Data(self, a), Data(self, b)
+
+    def deserialize(self, blob: bytes) -> Data:
+        """An object from Data.serialize of an engine with the same parameters."""
+        h = ctypes.c_void_p()
+        check(_lib.load().fhe_data_deserialize(self._h, blob, len(blob), ctypes.byref(h)))
+        return Data(self, h)
 
     def set_tensor_cores(self, mode) -> None:
         """Where the ModDown base conversion runs: False/0 CUDA cores, True/1 the INT8

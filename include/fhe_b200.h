@@ -175,6 +175,16 @@ int fhe_data_download(const fhe_data *data, int64_t *host_limbs);
  * modified after they are made, so the copy reads the object's final words. */
 int fhe_data_download_async(const fhe_data *data, int64_t *host_limbs);
 int fhe_data_info_get(const fhe_data *data, fhe_data_info *info);
+/* A wire format for any object (the reference declares Data::write and Bytearray,
+ * data/data.h:66 and data/bytearray.h, but defines no format): an 80-byte
+ * little-endian header (magic "FHEB200D", format version, the reference's
+ * DATA_VERSION, the engine's N, prime counts and a hash of its prime chain, the
+ * object's type, flags, moduli id, shape, delta and scale) followed by the limbs
+ * [polys][chains][N].  serialize waits for queued work; deserialize rejects objects
+ * of an engine with other parameters. */
+int fhe_data_serialized_size(const fhe_data *data, uint64_t *size);
+int fhe_data_serialize(const fhe_data *data, void *buffer, uint64_t capacity);
+int fhe_data_deserialize(fhe_engine *engine, const void *buffer, uint64_t size, fhe_data **out);
 /* Set the rotation step carried by a fixed rotation key (FixedRotationKey::delta_). */
 int fhe_data_set_delta(fhe_data *data, int delta);
 /* Device address of the limbs (valid until fhe_data_destroy). */

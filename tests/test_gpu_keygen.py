@@ -63,3 +63,26 @@ def test_encrypt_multiply_decrypt_round_trip(engines):
     out = e.decode(e.decrypt(prod, sk), complex_output=True)
     err = np.max(np.abs(out - a * b))
     assert err < 2.0 ** -20, err
+
+
+def test_serialized_objects_round_trip(engines):
+    """Keys and ciphertexts survive the wire format word for word, with their
+    metadata; an engine with other parameters or a damaged header rejects them."""
+    from fhe_b200._lib import FheError
+
+    e = engines(14, 1, 1)
+    sk = e.create_secret_key()
+    rk = e.create_relinearization_key(sk)
+    ct = e.encrypt(e.encode(np.linspace(-1, 1, e.slot_count)), sk)
+    for obj in (sk, rk, ct):
+        blob = obj.serialize()
+        back = e.deserialize(blob)
+        assert back.info() == obj.info()
+        assert np.array_equal(back.download(), obj.download())
+    blob = bytearray(ct.serialize())
+    with pytest.raises(FheError, match="deserialize"):
+        engines(15, 2, 1).deserialize(bytes(blob))
+    blob[0:8] = b"NOTADATA"
+    with pytest.raises(FheError, match="not a serialized engine object"):
+        e.deserialize(bytes(blob))
+
