@@ -144,6 +144,7 @@ def kernel_bytes(L: int, E: int, dnum: int, n: int) -> dict:
         "tensor_to_intt": (4 * L + 3 * L) * limb,           # 4 NTT polys in, 3 out
         "mixed_radix": 2 * L * limb,                        # digits of poly 2
         "mod_up_ntt": (L + dnum * E) * limb,                # digits in, extended out
+        "mod_up_ntt_tc": (L + dnum * E) * limb,
         "key_inner_product": (3 * dnum * E + 2 * E) * limb, # ext + 2 key polys, 2 out
         "mod_down_intt": 2 * 2 * E * limb,                  # 2 polys in and out
         "mod_down_epilogue": (2 * E + 2 * L + 2 * (L - 1)) * limb,
@@ -656,9 +657,13 @@ def main(argv=None):
         ms, u = aggregate(s0.elapsed_time(s1), float(B * args.steps), world, backend)
         fam = "mod_down_epilogue_tc" if "mod_down_epilogue_tc" in p else "mod_down_epilogue"
         cnt, fam_ms = p.get(fam, (0, 0.0))
+        up = "mod_up_ntt_tc" if "mod_up_ntt_tc" in p else "mod_up_ntt"
+        up_cnt, up_ms = p.get(up, (0, 0.0))
         return {"value": u / (ms / 1e3), "unit": "ct/s", "mod_down_kernel": fam,
                 "mod_down_avg_launch_ms": fam_ms / cnt if cnt else None,
-                "mod_down_ms_per_step": fam_ms / args.steps}
+                "mod_down_ms_per_step": fam_ms / args.steps,
+                "mod_up_family": up, "mod_up_avg_launch_ms": up_ms / up_cnt if up_cnt else None,
+                "mod_up_ms_per_step": up_ms / args.steps}
 
     forms = {"tensor_core": timed_form(True), "cuda_core": timed_form(False)}
 

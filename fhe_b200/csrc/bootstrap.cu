@@ -685,10 +685,7 @@ void Engine::decompose_into(const int64_t *x, int moduli_id, int64_t *out) {
   cudaError_t e = timed("mixed_radix", [&] {
     return launch_mixed_radix(tables_, dp, n, moduli_id, x, digits, stream_);
   });
-  if (e == cudaSuccess)
-    e = timed("mod_up_ntt", [&] {
-      return launch_mod_up_ntt(tables_, dp, params.log_n, moduli_id, digits, out, stream_);
-    });
+  if (e == cudaSuccess) e = mod_up(dp, moduli_id, digits, out);
   free_words(digits);
   check(e, "decompose");
 }

@@ -177,12 +177,48 @@ void Engine::set_tensor_cores(int mode) {
   tensor_cores_ = mode;
 }
 
+bool Engine::use_tensor_cores() const {
+  return tensor_cores_ == kTensorCoresOn ||
+         (tensor_cores_ == kTensorCoresAuto && params.special_prime_count >= kTensorCoreMinSpecial);
+}
+
+const ModUpTcTables *Engine::mod_up_tc(int moduli_id) {
+  const auto parts = params.partitions(moduli_id, moduli_id);
+  int max_size = 0;
+  for (const auto &pt : parts) max_size = std::max(max_size, pt.size);
+  if (!mod_up_tc_supported(max_size, params.n)) return nullptr;
+  auto it = mod_up_tc_cache_.find(moduli_id);
+  if (it != mod_up_tc_cache_.end()) return &it->second;
+  std::vector<PartitionConstants> constants;
+  for (const auto &pt : parts) constants.push_back(params.partition_constants(moduli_id, pt));
+  const ModUpTcHost h = make_mod_up_tc_tables(params.k, params.r_squared, moduli_id,
+                                              params.chains(moduli_id, true), parts, constants);
+  ModUpTcTables tc;
+  tc.b = upload_table(h.b);
+  tc.b_offset = upload_table(h.b_offset);
+  tc.c_k = upload_table(h.c_k);
+  tc.rounds = h.rounds;
+  return &mod_up_tc_cache_.emplace(moduli_id, tc).first->second;
+}
+
+cudaError_t Engine::mod_up(const DevicePartitions &dp, int moduli_id, const int64_t *digits,
+                           int64_t *ext) {
+  const ModUpTcTables *tc = use_tensor_cores() ? mod_up_tc(moduli_id) : nullptr;
+  if (!tc)
+    return timed("mod_up_ntt", [&] {
+      return launch_mod_up_ntt(tables_, dp, params.log_n, moduli_id, digits, ext, stream_);
+    });
+  return timed("mod_up_ntt_tc", [&] {
+    const cudaError_t e = launch_mod_up_contract_tc(tables_, dp, *tc, params.n, moduli_id, digits,
+                                                    ext, device_error_, stream_);
+    if (e != cudaSuccess) return e;
+    return launch_extended_ntt(tables_, dp, params.log_n, moduli_id, ext, stream_);
+  });
+}
+
 cudaError_t Engine::mod_down_epilogue(int moduli_id, int limbs, const int64_t *acc,
                                       const EpilogueOps &ops, int64_t *out) {
-  const bool use = tensor_cores_ == kTensorCoresOn ||
-                   (tensor_cores_ == kTensorCoresAuto &&
-                    params.special_prime_count >= kTensorCoreMinSpecial);
-  const ModDownTcTables *tc = use ? mod_down_tc(moduli_id) : nullptr;
+  const ModDownTcTables *tc = use_tensor_cores() ? mod_down_tc(moduli_id) : nullptr;
   if (tc)
     return timed("mod_down_epilogue_tc", [&] {
       return launch_mod_down_epilogue_tc(tables_, ks_, *tc, params.n, moduli_id, limbs, acc, ops,
@@ -511,10 +547,7 @@ void Engine::key_switch_pipeline(const int64_t *c1, int moduli_id, const Data &k
     e = timed("mixed_radix", [&] {
       return launch_mixed_radix(tables_, dp, n, moduli_id, c1, digits, stream_);
     });
-    if (e == cudaSuccess)
-      e = timed("mod_up_ntt", [&] {
-        return launch_mod_up_ntt(tables_, dp, params.log_n, moduli_id, digits, own_ext, stream_);
-      });
+    if (e == cudaSuccess) e = mod_up(dp, moduli_id, digits, own_ext);
   }
   if (e == cudaSuccess)
     e = timed("key_inner_product", [&] {

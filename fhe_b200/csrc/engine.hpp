@@ -342,6 +342,12 @@ class Engine {
   std::unique_ptr<Data> bootstrap_direct(const Data &ct, const Data &rk, const Data &ck,
                                          const BootstrapKey &bk);
   std::map<int, ModDownTcTables> mod_down_tc_cache_;  // moduli id -> tables
+  std::map<int, ModUpTcTables> mod_up_tc_cache_;      // moduli id -> tables
+  const ModUpTcTables *mod_up_tc(int moduli_id);
+  bool use_tensor_cores() const;
+  // ModUp of every partition's digits into NTT-form extended limbs, in the selected form.
+  cudaError_t mod_up(const DevicePartitions &dp, int moduli_id, const int64_t *digits,
+                     int64_t *ext);
   int *device_error_ = nullptr;  // set by a kernel whose bounded wait ran out
   const ModDownTcTables *mod_down_tc(int moduli_id);
   // The ModDown epilogue in the selected form.

@@ -476,7 +476,12 @@ cudaError_t launch_mod_up_ntt(const PrimeTables &t, const DevicePartitions &dp, 
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  const long long stride = static_cast<long long>(dp.extended) * n;
+  return launch_extended_ntt(t, dp, log_n, moduli_id, ext, s);
+}
+
+cudaError_t launch_extended_ntt(const PrimeTables &t, const DevicePartitions &dp, int log_n,
+                                int moduli_id, int64_t *ext, cudaStream_t s) {
+  const long long stride = static_cast<long long>(dp.extended) << log_n;
   PlainLoad ld{ext, stride};
   PlainStore st{ext, stride};
   return forward_ntt(log_n, dp.count, dp.extended, moduli_id, t, ld, st, ext, stride, s);

@@ -148,6 +148,39 @@ ModDownTcHost make_mod_down_tc_tables(const std::vector<uint64_t> &q,
                                       const std::vector<std::vector<int64_t>> &p_inverse_mult_r,
                                       int moduli_id, int limbs, int special_count);
 
+// Constants of the tensor-core ModUp contraction at one moduli id (modup_tc.cu): per
+// partition, the bytes of its constants C_ij (i < alpha, j < extended limbs) as the
+// UMMA B operand, and C_ij * k_j mod 2^62 for the per-term Montgomery quotients.
+struct ModUpTcTables {
+  const uint8_t *b = nullptr;           // per partition: [rounds][128 columns][kb bytes]
+  const long long *b_offset = nullptr;  // [partitions] byte offset of each partition's B
+  const int64_t *c_k = nullptr;         // [partitions][16][extended]
+  int rounds = 0;                       // ceil(extended / 8)
+};
+struct ModUpTcHost {
+  std::vector<uint8_t> b;
+  std::vector<long long> b_offset;
+  std::vector<int64_t> c_k;
+  int rounds = 0;
+};
+struct Partition;
+struct PartitionConstants;
+bool mod_up_tc_supported(int max_size, int n);
+ModUpTcHost make_mod_up_tc_tables(const std::vector<uint64_t> &k,
+                                  const std::vector<int64_t> &r_squared, int moduli_id,
+                                  int extended, const std::vector<Partition> &parts,
+                                  const std::vector<PartitionConstants> &constants);
+// ModUp's contraction (core_key_switch.cpp:92-108) of every partition into ext
+// [count][extended][N] (coefficient form, before the NTT) with the digit products on
+// the INT8 tensor pipe; same words as the CUDA-core contraction.
+cudaError_t launch_mod_up_contract_tc(const PrimeTables &t, const DevicePartitions &dp,
+                                      const ModUpTcTables &tc, int n, int moduli_id,
+                                      const int64_t *digits, int64_t *ext, int *error,
+                                      cudaStream_t s);
+// The forward NTT that completes ModUp, over every partition's extended limbs.
+cudaError_t launch_extended_ntt(const PrimeTables &t, const DevicePartitions &dp, int log_n,
+                                int moduli_id, int64_t *ext, cudaStream_t s);
+
 // Rotation's b * P term (create_key_switcher_for_rotate, core_key_switch.cpp:550-576):
 // acc0[j] = reduce(acc0[j] + NTT(mont(mont(c0[j], P mod q * R), R^2))) for the L
 // limbs of the ciphertext; `work` holds L limbs of intermediate data.

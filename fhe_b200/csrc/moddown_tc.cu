@@ -28,87 +28,15 @@
 #include "epilogue.cuh"
 #include "kernels.cuh"
 #include "modarith.cuh"
+#include "umma.cuh"
 
 namespace fhe_b200 {
 
 namespace {
 
-constexpr int kTcCoeffs = 128;   // MMA M = tensor memory lanes = coefficients per CTA
-constexpr int kTcThreads = 256;  // two warpgroups; warp w reads lanes 32 (w % 4) ...
-constexpr int kTcTargets = 8;    // target limbs per MMA round
-constexpr int kTcColumns = 128;  // 8 targets x 16 byte shifts = MMA N = TMEM columns
-constexpr uint32_t kTcWaitLimit = 1u << 22;
+using namespace umma;
 
-constexpr int row_bytes(int K) { return (9 * K + 31) / 32 * 32; }
-
-// Byte offset of element (row, k) of a K-major operand of `rows` rows stored as
-// UMMA core matrices (8 rows x 16 bytes): [k / 16][row / 8][row % 8][k % 16].
-__host__ __device__ inline int core_offset(int row, int k, int rows) {
-  return ((k / 16) * (rows / 8) + row / 8) * 128 + (row % 8) * 16 + (k % 16);
-}
-
-__device__ __forceinline__ uint32_t smem_addr(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// Shared-memory matrix descriptor: K-major without swizzle; lbo = bytes between the
-// two 16-byte halves of a 32-byte K step, sbo = bytes between 8-row groups.
-__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-  return static_cast<uint64_t>((addr >> 4) & 0x3FFF) |
-         (static_cast<uint64_t>((lbo >> 4) & 0x3FFF) << 16) |
-         (static_cast<uint64_t>((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(done)
-      : "r"(addr), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-
-__device__ bool mbar_wait(uint32_t addr, uint32_t parity) {
-  for (uint32_t i = 0; i < kTcWaitLimit; i++)
-    if (mbar_try_wait(addr, parity)) return true;
-  return false;
-}
-
-__device__ __forceinline__ void mma_i8(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc,
-                                       uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-      "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
-}
-
-__device__ __forceinline__ void tmem_load16(uint32_t addr, uint32_t (&d)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-      : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]),
-        "=r"(d[7]), "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]),
-        "=r"(d[14]), "=r"(d[15])
-      : "r"(addr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-
-// Five partial sums (each below 2^23) at byte shifts 0, 8, ..., 32: below 2^56.
-__device__ __forceinline__ uint64_t fold5(const uint32_t *d) {
-  return static_cast<uint64_t>(d[0]) + (static_cast<uint64_t>(d[1]) << 8) +
-         (static_cast<uint64_t>(d[2]) << 16) + (static_cast<uint64_t>(d[3]) << 24) +
-         (static_cast<uint64_t>(d[4]) << 32);
-}
+constexpr int row_bytes(int K) { return (9 * K + 31) / 32 * 32; }  // d_s bytes + sign bytes
 
 // Four CTAs per SM (64 registers) where that costs no spills, fewer otherwise.
 template <int K>
@@ -161,14 +89,9 @@ __global__ void __launch_bounds__(kTcThreads, K <= 10 && K != 7 ? 4 : (K <= 13 ?
       *reinterpret_cast<uint4 *>(sA + core_offset(tid, ch * 16, kTcCoeffs)) = v;
     }
   }
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                     smem_addr(&tmem_base)),
-                 "r"(kTcColumns));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-  }
-  if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar)), "r"(1));
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (warp == 0) tmem_alloc(&tmem_base);
+  if (tid == 0) mbar_init(&mbar);
+  fence_async_smem();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -176,8 +99,6 @@ __global__ void __launch_bounds__(kTcThreads, K <= 10 && K != 7 ? 4 : (K <= 13 ?
   const uint32_t bar = smem_addr(&mbar);
 
   // 3. One MMA round per 8 targets; each thread folds 4 targets of its coefficient.
-  constexpr uint32_t idesc = (2u << 4) | (static_cast<uint32_t>(kTcColumns >> 3) << 17) |
-                             (static_cast<uint32_t>(kTcCoeffs >> 4) << 24);
   const int lane_base = (warp & 3) * 32;
   const int row = lane_base + lane;
   const int half = warp >> 2;
@@ -191,21 +112,12 @@ __global__ void __launch_bounds__(kTcThreads, K <= 10 && K != 7 ? 4 : (K <= 13 ?
       const uint4 *src = reinterpret_cast<const uint4 *>(tc.b) + static_cast<size_t>(round) * chunks;
       uint4 *dst = reinterpret_cast<uint4 *>(sB);
       for (int i = tid; i < chunks; i += kTcThreads) dst[i] = src[i];
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      fence_async_smem();
       __syncthreads();
     }
     if (tid == 0) {
-#pragma unroll
-      for (int k = 0; k < KB / 32; k++) {
-        const uint64_t da = umma_desc(smem_addr(sA) + k * 2 * (kTcCoeffs / 8) * 128,
-                                      (kTcCoeffs / 8) * 128, 128);
-        const uint64_t db = umma_desc(smem_addr(sB) + k * 2 * (kTcColumns / 8) * 128,
-                                      (kTcColumns / 8) * 128, 128);
-        mma_i8(tmem, da, db, idesc, k > 0 ? 1u : 0u);
-      }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       bar)
-                   : "memory");
+      mma_round(tmem, sA, sB, KB);
+      mma_commit(bar);
     }
     ok = __syncthreads_and(mbar_wait(bar, round & 1)) != 0;
     if (!ok) break;
@@ -244,8 +156,7 @@ __global__ void __launch_bounds__(kTcThreads, K <= 10 && K != 7 ? 4 : (K <= 13 ?
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcColumns));
+  if (warp == 0) tmem_dealloc(tmem);
   if (!ok) return;
 
   // 4. The caller's operations on the divided limbs.

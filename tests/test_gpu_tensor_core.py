@@ -1,6 +1,6 @@
-"""The two forms of the ModDown base conversion give the same words: the INT8
-tensor-core form (tcgen05.mma kind::i8, the default where the shape allows it) and
-the CUDA-core form (the reference's sequential division by the special primes),
+"""The two forms of the base conversions give the same words: the INT8 tensor-core
+forms (tcgen05.mma kind::i8; ModDown's division by the special primes and ModUp's
+digit contraction) and the CUDA-core forms (the reference's operation order),
 on every key-switching operation, several levels and three parameter sets.  The
 recorded-reference and oracle parity suites run the tensor-core form too."""
 import numpy as np
@@ -64,5 +64,7 @@ def test_tensor_core_mod_down_matches_cuda_core(engines, log_n, K, preset, mids)
         tc, plain, families = run_both(e, ops)
         assert "mod_down_epilogue_tc" in families, families
         assert "mod_down_epilogue" not in families, families
+        assert "mod_up_ntt_tc" in families, families
+        assert "mod_up_ntt" not in families, families
         for got, want in zip(tc, plain):
             assert np.array_equal(got, want)
