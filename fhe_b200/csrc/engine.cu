@@ -177,9 +177,9 @@ void Engine::set_tensor_cores(int mode) {
   tensor_cores_ = mode;
 }
 
-bool Engine::use_tensor_cores() const {
+bool Engine::use_tensor_cores(int min_special) const {
   return tensor_cores_ == kTensorCoresOn ||
-         (tensor_cores_ == kTensorCoresAuto && params.special_prime_count >= kTensorCoreMinSpecial);
+         (tensor_cores_ == kTensorCoresAuto && params.special_prime_count >= min_special);
 }
 
 const ModUpTcTables *Engine::mod_up_tc(int moduli_id) {
@@ -203,7 +203,8 @@ const ModUpTcTables *Engine::mod_up_tc(int moduli_id) {
 
 cudaError_t Engine::mod_up(const DevicePartitions &dp, int moduli_id, const int64_t *digits,
                            int64_t *ext) {
-  const ModUpTcTables *tc = use_tensor_cores() ? mod_up_tc(moduli_id) : nullptr;
+  const ModUpTcTables *tc =
+      use_tensor_cores(kTensorCoreModUpMinSpecial) ? mod_up_tc(moduli_id) : nullptr;
   if (!tc)
     return timed("mod_up_ntt", [&] {
       return launch_mod_up_ntt(tables_, dp, params.log_n, moduli_id, digits, ext, stream_);
@@ -218,7 +219,8 @@ cudaError_t Engine::mod_up(const DevicePartitions &dp, int moduli_id, const int6
 
 cudaError_t Engine::mod_down_epilogue(int moduli_id, int limbs, const int64_t *acc,
                                       const EpilogueOps &ops, int64_t *out) {
-  const ModDownTcTables *tc = use_tensor_cores() ? mod_down_tc(moduli_id) : nullptr;
+  const ModDownTcTables *tc =
+      use_tensor_cores(kTensorCoreMinSpecial) ? mod_down_tc(moduli_id) : nullptr;
   if (tc)
     return timed("mod_down_epilogue_tc", [&] {
       return launch_mod_down_epilogue_tc(tables_, ks_, *tc, params.n, moduli_id, limbs, acc, ops,

@@ -285,11 +285,13 @@ class Engine {
 
   // Where the ModDown base conversion runs; every mode gives the same words.
   //   kTensorCoresOff: CUDA cores; kTensorCoresOn: the INT8 tensor pipe wherever the
-  //   shape allows it; kTensorCoresAuto (default): the tensor pipe from
-  //   kTensorCoreMinSpecial special primes on, where it is the faster form (its cost
-  //   per output is fixed, the sequential division's grows with K).
+  //   shape allows it; kTensorCoresAuto (default): each conversion on the tensor pipe
+  //   from the number of special primes where it measured faster (ModDown from 4,
+  //   ModUp from 8: the tensor form's cost per output is mostly fixed, the CUDA-core
+  //   form's grows with K).
   enum TensorCoreMode : int { kTensorCoresOff = 0, kTensorCoresOn = 1, kTensorCoresAuto = 2 };
   static constexpr int kTensorCoreMinSpecial = 4;
+  static constexpr int kTensorCoreModUpMinSpecial = 8;
   void set_tensor_cores(int mode);
   int tensor_cores() const { return tensor_cores_; }
 
@@ -344,7 +346,7 @@ class Engine {
   std::map<int, ModDownTcTables> mod_down_tc_cache_;  // moduli id -> tables
   std::map<int, ModUpTcTables> mod_up_tc_cache_;      // moduli id -> tables
   const ModUpTcTables *mod_up_tc(int moduli_id);
-  bool use_tensor_cores() const;
+  bool use_tensor_cores(int min_special) const;
   // ModUp of every partition's digits into NTT-form extended limbs, in the selected form.
   cudaError_t mod_up(const DevicePartitions &dp, int moduli_id, const int64_t *digits,
                      int64_t *ext);

@@ -460,8 +460,9 @@ class Engine:
         return Data(self, h)
 
     def set_tensor_cores(self, mode) -> None:
-        """Where the ModDown base conversion runs: False/0 CUDA cores, True/1 the INT8
-        tensor pipe, 2 (default) the tensor pipe from 4 special primes on; same words."""
+        """Where the base conversions run: False/0 CUDA cores, True/1 the INT8 tensor
+        pipe, 2 (default) the tensor pipe where it measured faster (ModDown from 4
+        special primes, ModUp from 8); same words."""
         check(_lib.load().fhe_engine_set_tensor_cores(self._h, int(mode)))
 
     def set_graphs(self, enable: bool) -> None:

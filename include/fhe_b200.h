@@ -422,11 +422,12 @@ int fhe_relinearize_noalloc(fhe_engine *engine, const int64_t *ct_device, int mo
 
 /* ---- B200 options (no reference counterpart) ---------------------------------------- */
 
-/* Selects where the ModDown base conversion (the exact division by the special
- * primes, core_key_switch.cpp:123-160) runs: FHE_TENSOR_CORES_OFF on the CUDA cores,
- * FHE_TENSOR_CORES_ON on the INT8 tensor pipe (tcgen05.mma kind::i8) wherever the
- * shape allows it, FHE_TENSOR_CORES_AUTO (the default) on the tensor pipe from 4
- * special primes on, where it is the faster form.  Every mode gives the same words. */
+/* Selects where the base conversions run (ModUp's digit contraction,
+ * core_key_switch.cpp:92-108, and ModDown's exact division by the special primes,
+ * :123-160): FHE_TENSOR_CORES_OFF on the CUDA cores, FHE_TENSOR_CORES_ON on the INT8
+ * tensor pipe (tcgen05.mma kind::i8) wherever the shape allows it,
+ * FHE_TENSOR_CORES_AUTO (the default) on the tensor pipe where it measured faster
+ * (ModDown from 4 special primes, ModUp from 8).  Every mode gives the same words. */
 enum {
   FHE_TENSOR_CORES_OFF = 0,
   FHE_TENSOR_CORES_ON = 1,
