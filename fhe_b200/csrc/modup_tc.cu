@@ -29,7 +29,7 @@ using namespace umma;
 constexpr int digit_row_bytes(int A) { return (8 * A + 31) / 32 * 32; }
 
 template <int A>
-__global__ void __launch_bounds__(kTcThreads, 3)
+__global__ void __launch_bounds__(kTcThreads, 4)
     mod_up_tc_kernel(PrimeTables t, DevicePartitions dp, ModUpTcTables tc, int n, int moduli_id,
                      const int64_t *digits, int64_t *ext, int *error) {
   constexpr int KB = digit_row_bytes(A);
