@@ -517,6 +517,69 @@ def run_batched_bench(args, torch, np, rank, world, local, backend, stream):
     return 0
 
 
+def run_plain_bench(args, torch, np, rank, world, local, backend, stream):
+    """The plain CKKS pipeline of the reference's default engine (N = 2^14, one
+    special prime, scale 2^40): per pair, encode two vectors of 2^13 complex slots,
+    encrypt them with the public key, multiply and relinearize, rescale, decrypt and
+    decode; every stage runs on the device.  Slot values come from host memory and
+    the decoded slots go back to it inside the timed region."""
+    from fhe_b200 import Engine
+    from inputs import codec_values
+
+    eng = Engine(log_coeff_count=14, special_prime_count=1)
+    eng.set_stream(stream.cuda_stream)
+    eng.seed([5 + rank, 6, 7, 8, 9, 10, 11, 12], [3, 4])
+    sk = eng.create_secret_key()
+    pk = eng.create_public_key(sk)
+    rk = eng.create_relinearization_key(sk)
+    B = args.batch
+    va = [codec_values(300 + i, eng.slot_count, True) for i in range(B)]
+    vb = [codec_values(600 + i, eng.slot_count, True) for i in range(B)]
+
+    def step():
+        outs = []
+        for a, b in zip(va, vb):
+            ca, cb = eng.encrypt(eng.encode(a), pk), eng.encrypt(eng.encode(b), pk)
+            prod = eng.rescale(eng.multiply(ca, cb, rk))
+            outs.append(eng.decode(eng.decrypt(prod, sk), complex_output=True))
+        return outs
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches0 = Engine.kernel_launch_count()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            outs = step()
+        stop.record(stream)
+        torch.cuda.synchronize()
+    launches = Engine.kernel_launch_count() - launches0
+    elapsed_max, units = aggregate(start.elapsed_time(stop), float(B * args.steps), world, backend)
+    err = max(float(np.max(np.abs(o - a * b))) for o, a, b in zip(outs, va, vb))
+    if rank == 0:
+        print(json.dumps({
+            "metric": "plain CKKS pipeline pairs/s at N=2^14 (encode, encrypt, multiply, "
+                      "relinearize, rescale, decrypt, decode)",
+            "value": units / (elapsed_max / 1e3), "unit": "pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64+f64",
+            "data": "synthetic (seeded complex slots uniform in [-1, 1], keys made on the device)",
+            "config": {"workload": "the reference's default engine (N=2^14, K=1, scale 2^40)",
+                       "pairs_per_step": B, "max_error_vs_float64_product": err,
+                       "precision_bits": float(-np.log2(err)) if err > 0 else 64.0},
+            "cpu_baseline": None,
+            "e2e": {"value": units / (elapsed_max / 1e3), "unit": "pairs/s",
+                    "h2d_bytes_per_step": int(B * 2 * eng.slot_count * 16),
+                    "d2h_bytes_per_step": int(B * eng.slot_count * 16),
+                    "note": "slot values from host memory, decoded slots back to it, every "
+                            "stage between on the device"},
+            "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
+    eng.close()
+    return 0
+
+
 # -------------------------------------------------------------------- main --
 
 def main(argv=None):
@@ -527,11 +590,13 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=16, help="ciphertext pairs per step")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="hmult",
-                    choices=["hmult", "ntt", "bootstrap", "bootstrap_rotation", "batched"],
+                    choices=["hmult", "ntt", "bootstrap", "bootstrap_rotation", "batched",
+                             "plain"],
                     help="hmult: the headline; ntt: forward NTT of --batch x 24 limbs at N=2^16; "
                          "bootstrap: --batch ciphertexts bootstrapped per step with a medium "
                          "bootstrap key; bootstrap_rotation: the same with a rotation key; "
-                         "batched: --batch uneven HMult+rotate items per step (use 256)")
+                         "batched: --batch uneven HMult+rotate items per step (use 256); "
+                         "plain: the N=2^14 pipeline from slot values to decoded slots")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args(argv)
     rank, world, local = dist_env()
@@ -563,6 +628,8 @@ def main(argv=None):
     torch.cuda.set_stream(stream)
     if args.workload == "ntt":
         return run_ntt_microbench(args, torch, np, rank, world, local, backend, stream)
+    if args.workload == "plain":
+        return run_plain_bench(args, torch, np, rank, world, local, backend, stream)
     if args.workload == "batched":
         return run_batched_bench(args, torch, np, rank, world, local, backend, stream)
     if args.workload in ("bootstrap", "bootstrap_rotation"):
