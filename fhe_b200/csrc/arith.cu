@@ -380,6 +380,9 @@ std::unique_ptr<Data> Engine::square(const Data &ct, const Data *rk) {
   if (rk) require_key_level(fn, ct, *rk, true);
   auto r = rescale_any(ct);
   auto x = r->is_ntt() ? std::move(r) : to_ntt(*r);
+  // The square's tensor (d1 = x0 x1 doubled with add_reduce) is the product's tensor
+  // of x with itself, so with a key the fused tensor-iNTT relinearization serves.
+  if (rk) return relinearized_product(*x, *x, *rk);
   auto out = make_data(kUnitCiphertext, x->flag & ~kFlagRescaled, x->moduli_id, 3,
                        x->scale * x->scale);
   const long long ps = x->poly_stride();
@@ -388,8 +391,7 @@ std::unique_ptr<Data> Engine::square(const Data &ct, const Data *rk) {
   pointwise(kOpMult, L, mid, x->d, x->d + ps, nullptr, out->d + ps);
   pointwise(kOpAddReduce, L, mid, out->d + ps, out->d + ps, nullptr, out->d + ps);
   pointwise(kOpMult, L, mid, x->d + ps, x->d + ps, nullptr, out->d + 2 * ps);
-  if (!rk) return out;
-  return relinearize(*out, *rk);
+  return out;
 }
 
 }  // namespace fhe_b200

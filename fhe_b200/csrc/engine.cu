@@ -623,8 +623,36 @@ std::unique_ptr<Data> Engine::multiply_relinearize(const Data &a, const Data &b,
   require_text(fn, b, 1, 2, 2, true);
   require_key_level(fn, a, rk, true);
   require_key_level(fn, b, rk, true);
-  auto m = multiply(a, b);
-  return relinearize(*m, rk);
+  const int level = std::min(a.level(), b.level());
+  auto pa = prepare_for_multiply(a, level);
+  auto pb = prepare_for_multiply(b, level);
+  return relinearized_product(*pa, *pb, rk);
+}
+
+std::unique_ptr<Data> Engine::relinearized_product(const Data &pa, const Data &pb, const Data &rk) {
+  // multiply (core.cpp:284-314) then relinearize (core.cpp:713-741) of prepared
+  // NTT-form inputs: the tensor is formed inside the inverse NTT's load, so its three
+  // NTT-form polynomials are never written.
+  const int m = pa.moduli_id;
+  const int L = pa.chains;
+  int64_t *t3 = alloc_words(static_cast<size_t>(3) * L * params.n);
+  cudaError_t e = timed("tensor_to_intt", [&] {
+    return launch_tensor_to_intt(tables_, params.log_n, L, m, pa.d, pb.d, t3, stream_);
+  });
+  if (e != cudaSuccess) {
+    free_words(t3);
+    check(e, "tensor");
+  }
+  const int flag = (pa.flag | pb.flag) & ~kFlagRescaled & ~kFlagNtt;
+  auto out = make_data(kUnitCiphertext, flag, m, 2, pa.scale * pb.scale);
+  try {
+    relinearize_tail(t3, m, rk, 1, out->d);
+  } catch (...) {
+    free_words(t3);
+    throw;
+  }
+  free_words(t3);
+  return out;
 }
 
 std::unique_ptr<Data> Engine::multiply_relinearize_rescale(const Data &a, const Data &b,

@@ -480,6 +480,7 @@ class Engine {
   std::unique_ptr<Data> core_rescale(const Data &ct);          // coefficient form
   std::unique_ptr<Data> prepare_for_multiply(const Data &text, int level);
   std::unique_ptr<Data> rescale_to_ntt(const Data &text);  // to_ntt(core_rescale(text))
+  std::unique_ptr<Data> relinearized_product(const Data &pa, const Data &pb, const Data &rk);
   // Hybrid key switch of the coefficient-form polynomial c1 at moduli_id (L limbs):
   // decompose, ModUp, key product, optional rotation term b * P (rotate_c0 = the
   // coefficient-form c0), ModDown and the epilogue operations `ops` into `out`.
