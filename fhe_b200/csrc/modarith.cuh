@@ -73,6 +73,28 @@ FHE_HD int64_t mont_mult_const(int64_t a, int64_t b, uint64_t q, uint64_t k) {
   return redc_wide(lo, hi, q, k);
 }
 
+// mont_mult_const for operands known to lie in range: 0 <= w, b < 2^62 and odd
+// q < 2^61, with k = -q^-1 mod 2^62.  Same word, fewer carries: with 32-bit
+// halves, Z = w b + s q = c0 + c1 2^32 + c2 2^64 where
+//   c0 = w0 b0 + s0 q0,  c1 = w0 b1 + w1 b0 + s0 q1 + s1 q0,  c2 = w1 b1 + s1 q1.
+// Z is a multiple of 2^62, so the low words of w0 b0 and s0 q0 sum to 0 or 2^32 and
+// c0 / 2^32 = hi(w0 b0) + hi(s0 q0 + lo(w0 b0)); Y = c1 + c0 / 2^32 is below 2^64
+// and a multiple of 2^30, and Z / 2^62 = Y / 2^30 + 4 c2.  Every partial sum below
+// stays under 2^64 for these bounds (w1, b1, s1 < 2^30; q1 < 2^29).
+FHE_HD int64_t mont_mult_small(uint64_t w, uint64_t b, uint64_t q, uint64_t k) {
+  const uint32_t w0 = static_cast<uint32_t>(w), w1 = static_cast<uint32_t>(w >> 32);
+  const uint32_t b0 = static_cast<uint32_t>(b), b1 = static_cast<uint32_t>(b >> 32);
+  const uint32_t q0 = static_cast<uint32_t>(q), q1 = static_cast<uint32_t>(q >> 32);
+  const uint64_t p = mad32(w0, b0, 0);
+  uint64_t y = mad32(w1, b0, mad32(w0, b1, p >> 32));
+  const uint64_t lo = static_cast<uint32_t>(p) | (y << 32);  // w b mod 2^64
+  const uint64_t s = (lo * k) & kMontMask;
+  const uint32_t s0 = static_cast<uint32_t>(s), s1 = static_cast<uint32_t>(s >> 32);
+  const uint64_t u = mad32(s0, q0, static_cast<uint32_t>(p));
+  y = mad32(s1, q0, mad32(s0, q1, y)) + (u >> 32);
+  return static_cast<int64_t>(mad32(s1 << 2, q1, mad32(w1 << 2, b1, y >> 30)));
+}
+
 // Montgomery exit (unit.h:25-31): REDC of a single (sign-extended) word.
 FHE_HD int64_t mont_exit(int64_t x, uint64_t q, uint64_t k) {
   return redc_wide(static_cast<uint64_t>(x), x < 0 ? ~uint64_t(0) : 0, q, k);

@@ -19,6 +19,8 @@
 
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "kernels.cuh"
 #include "modarith.cuh"
 
@@ -133,6 +135,14 @@ __device__ __forceinline__ int tile_index(int c, int i) {
   return c * M + (i ^ (((i >> 4) ^ ((i >> 5) << 2) ^ c) & kMask));
 }
 
+// The swizzle is linear over XOR: tile_index(c, i ^ v) = tile_index(c, i) ^
+// tile_xor(v) for i, v < M.  The elements of a radix-8 group are base ^ (e << dlog),
+// so each costs one XOR with a constant.
+template <int M>
+__device__ __forceinline__ constexpr int tile_xor(int v) {
+  return v ^ (((v >> 4) ^ ((v >> 5) << 2)) & (M >= 16 ? 15 : M - 1));
+}
+
 template <int S, bool INVERSE, class Loader, class Storer>
 __global__ void __launch_bounds__(256, 4)
     ntt_pass_kernel(NttPass a, PrimeTables t, Loader load, Storer store) {
@@ -176,15 +186,15 @@ __global__ void __launch_bounds__(256, 4)
       const int base = ((g >> dlog) << (dlog + r)) | (g & (D - 1));
       const int u = u0 + c;
       const int gbase = (u >> a.stride_log) * (M << a.stride_log) + (u & (T - 1));
+      const int tb = tile_index<M>(c, base);
       int64_t x[8];
 #pragma unroll
       for (int e = 0; e < 8; e++) {
         if (e < E) {
-          const int i = base + e * D;
           if (round == 0) {
-            x[e] = load(poly, limb, prime, gbase + i * T, n);
+            x[e] = load(poly, limb, prime, gbase + (base + e * D) * T, n);
           } else {
-            x[e] = tile_smem[tile_index<M>(c, i)];
+            x[e] = tile_smem[tb ^ tile_xor<M>(e << dlog)];
           }
         }
       }
@@ -193,62 +203,96 @@ __global__ void __launch_bounds__(256, 4)
       // elements, and the blocks' twiddles are consecutive table entries, so each
       // stage needs a single index computation.
       const int gi0 = gbase + base * T;
+      // For q < 2^60, words in [0, 2q) stay there through every butterfly (the
+      // reference's lazy range; twiddles are below 2q), and for them the
+      // butterfly's signed compares and sign-extended product reduce to the short
+      // forms below (same words); any other word takes the reference's forms.
+      bool in_range = q < (uint64_t(1) << 60);
 #pragma unroll
-      for (int j = 0; j < 3; j++) {
-        if (j < r) {
-          if (!INVERSE) {
-            // stage s: twiddle root[2^s - 1 + (gi >> (log_n - s))]; the block of
-            // element e is e >> (r - j) (ntt.cpp:46-134)
-            const int s = a.first + first_local + j;
-            const int half = E >> (j + 1);
-            const int64_t *wp = tw + ((1 << s) - 1 + (gi0 >> (a.log_n - s)));
+      for (int e = 0; e < 8; e++)
+        if (e < E) in_range = in_range && static_cast<uint64_t>(x[e]) < static_cast<uint64_t>(q2);
+      auto stages = [&](auto lazy) {
+        constexpr bool kLazy = decltype(lazy)::value;
+        // guard(a + b, q2) and guard(a + q2 - b, q2) (unit.h:13)
+        auto add_guard = [&](int64_t a1, int64_t b1) -> int64_t {
+          if (kLazy) {
+            const int64_t y = a1 + b1 - q2;
+            return y < 0 ? y + q2 : y;
+          }
+          return guard(a1 + b1, q2);
+        };
+        auto sub_guard = [&](int64_t a1, int64_t b1) -> int64_t {
+          if (kLazy) {
+            const int64_t y = a1 - b1;
+            return y < 0 ? y + q2 : y;
+          }
+          return guard(a1 + q2 - b1, q2);
+        };
+        auto product = [&](int64_t w, int64_t v) -> int64_t {
+          if (kLazy) return mont_mult_small(static_cast<uint64_t>(w), static_cast<uint64_t>(v), q, k);
+          return mont_mult_const(w, v, q, k);
+        };
 #pragma unroll
-            for (int h = 0; h < (1 << j); h++) {
-              const int64_t w = __ldg(wp + h);
+        for (int j = 0; j < 3; j++) {
+          if (j < r) {
+            if (!INVERSE) {
+              // stage s: twiddle root[2^s - 1 + (gi >> (log_n - s))]; the block of
+              // element e is e >> (r - j) (ntt.cpp:46-134)
+              const int s = a.first + first_local + j;
+              const int half = E >> (j + 1);
+              const int64_t *wp = tw + ((1 << s) - 1 + (gi0 >> (a.log_n - s)));
 #pragma unroll
-              for (int e2 = 0; e2 < 4; e2++) {
-                if (e2 < half) {
-                  const int e = h * 2 * half + e2;
-                  const int64_t uu = x[e];
-                  const int64_t p = mont_mult_const(w, x[e + half], q, k);
-                  x[e] = guard(uu + p, q2);
-                  x[e + half] = guard(uu + q2 - p, q2);
-                }
-              }
-            }
-          } else {
-            // distance 2^dg: twiddle root_inverse[N - N/2^dg + (gi >> (dg + 1))]
-            // (ntt.cpp:177-272); the block of element e is e >> (j + 1)
-            const int dg = a.first + first_local + j;
-            const int half = 1 << j;
-            const int64_t *wp = tw + (n - (n >> dg) + (gi0 >> (dg + 1)));
-#pragma unroll
-            for (int h = 0; h < 4; h++) {
-              if (h < (E >> (j + 1))) {
+              for (int h = 0; h < (1 << j); h++) {
                 const int64_t w = __ldg(wp + h);
 #pragma unroll
                 for (int e2 = 0; e2 < 4; e2++) {
                   if (e2 < half) {
                     const int e = h * 2 * half + e2;
                     const int64_t uu = x[e];
-                    const int64_t vv = x[e + half];
-                    x[e] = guard(uu + vv, q2);
-                    x[e + half] = mont_mult_const(w, guard(uu + q2 - vv, q2), q, k);
+                    const int64_t p = product(w, x[e + half]);
+                    x[e] = add_guard(uu, p);
+                    x[e + half] = sub_guard(uu, p);
+                  }
+                }
+              }
+            } else {
+              // distance 2^dg: twiddle root_inverse[N - N/2^dg + (gi >> (dg + 1))]
+              // (ntt.cpp:177-272); the block of element e is e >> (j + 1)
+              const int dg = a.first + first_local + j;
+              const int half = 1 << j;
+              const int64_t *wp = tw + (n - (n >> dg) + (gi0 >> (dg + 1)));
+#pragma unroll
+              for (int h = 0; h < 4; h++) {
+                if (h < (E >> (j + 1))) {
+                  const int64_t w = __ldg(wp + h);
+#pragma unroll
+                  for (int e2 = 0; e2 < 4; e2++) {
+                    if (e2 < half) {
+                      const int e = h * 2 * half + e2;
+                      const int64_t uu = x[e];
+                      const int64_t vv = x[e + half];
+                      x[e] = add_guard(uu, vv);
+                      x[e + half] = product(w, sub_guard(uu, vv));
+                    }
                   }
                 }
               }
             }
           }
         }
+      };
+      if (in_range) {
+        stages(std::true_type{});
+      } else {
+        stages(std::false_type{});
       }
 #pragma unroll
       for (int e = 0; e < 8; e++) {
         if (e < E) {
-          const int i = base + e * D;
           if (round == R - 1) {
-            store(poly, limb, prime, gbase + i * T, n, x[e]);
+            store(poly, limb, prime, gbase + (base + e * D) * T, n, x[e]);
           } else {
-            tile_smem[tile_index<M>(c, i)] = x[e];
+            tile_smem[tb ^ tile_xor<M>(e << dlog)] = x[e];
           }
         }
       }

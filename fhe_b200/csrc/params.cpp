@@ -240,7 +240,10 @@ Parameters::Parameters(const Config &cfg)
     q.insert(q.begin(), large[1]);
   }
   for (auto prime : q) {
-    if (!is_prime_u64(prime) || (prime - 1) % (2 * static_cast<uint64_t>(n)) != 0)
+    // Below 2^61: the lazy [0, 2q) words fit the R = 2^62 Montgomery form (the
+    // device's short product, mont_mult_small, relies on it).
+    if (!is_prime_u64(prime) || (prime - 1) % (2 * static_cast<uint64_t>(n)) != 0 ||
+        prime >= (uint64_t(1) << 61))
       throw std::runtime_error("CKKS Parameters: corrupt prime table.");
   }
   prime_count = static_cast<int>(q.size());
