@@ -277,6 +277,9 @@ def run_ntt_microbench(args, torch, np, rank, world, local, backend, stream):
 
 # -------------------------------------------------------------- bootstrap --
 
+CONCURRENCY = 4  # the engine's default worker streams for batch calls
+
+
 def run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream):
     """Bootstrapping at N = 2^16 (bootstrap preset, 4 special primes, 2^15 complex
     slots uniform in [-1, 1], 3 stages): each step bootstraps `batch` ciphertexts
@@ -310,6 +313,8 @@ def run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream):
         return eng.bootstrap(c, rk, ck, rot, sbk, 3)
 
     def step(inputs):
+        if with_key:  # one batch call: the bootstraps share the engine's worker streams
+            return eng.bootstrap_batch(inputs, rk, ck, bk)
         return [boot(c) for c in inputs]
 
     for _ in range(args.warmup):
@@ -346,10 +351,9 @@ def run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        for h in host_ct:
-            c = eng.upload_from_pointer(h.data_ptr(), info["moduli_id"], 2, info["flag"],
-                                        scale=float(info["scale"]))
-            o = boot(c)
+        ins = [eng.upload_from_pointer(h.data_ptr(), info["moduli_id"], 2, info["flag"],
+                                       scale=float(info["scale"])) for h in host_ct]
+        for o in step(ins):
             eng.download_to_pointer(o, out_host.data_ptr(), wait=False)
     eng.synchronize()  # the last results are in host memory
     e2e_ms = (time.perf_counter() - t0) * 1e3 / (args.steps * B)
@@ -380,6 +384,8 @@ def run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream):
                                     "engine.bootstrap(ct, rk, ck, rotation key, small bootstrap "
                                     "key, 3)") + ", bootstrap preset, N=2^16, K=4, input level 3",
                        "ciphertexts_per_step": B, "precision_bits": bits,
+                       "api": "fhe_bootstrap_batch" if with_key else "fhe_bootstrap",
+                       "streams": CONCURRENCY if with_key else 1,
                        "bootstrap_key_bytes": key_bytes,
                        "cuda_graphs": {"captured": eng.graph_counts()[0],
                                        "capture_failed": eng.graph_counts()[1]},
@@ -655,7 +661,15 @@ def main(argv=None):
         b = eng.upload(uniform_limbs(rng, q_in, 2, n), mid)
         pairs.append((a, b))
 
+    pa, pb = [p[0] for p in pairs], [p[1] for p in pairs]
+
     def step():
+        # One batch call: the pairs run concurrently on the engine's worker streams.
+        outs = eng.multiply_relinearize_rescale_batch(pa, pb, rk)
+        for o in outs:
+            o.free()
+
+    def per_call_step():
         outs = [eng.multiply_relinearize_rescale(a, b, rk) for a, b in pairs]
         for o in outs:
             o.free()
@@ -665,8 +679,6 @@ def main(argv=None):
     torch.cuda.synchronize()
     if backend:
         torch.distributed.barrier()
-    eng.profile_reset()
-    eng.set_profiling(True)
     launches0 = Engine.kernel_launch_count()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
@@ -677,13 +689,38 @@ def main(argv=None):
         stop.record(stream)
         torch.cuda.synchronize()
     launches = Engine.kernel_launch_count() - launches0
-    eng.set_profiling(False)
-    prof = eng.profile()
     elapsed = start.elapsed_time(stop)
     if backend:
         torch.distributed.barrier()
     elapsed_max, units = aggregate(elapsed, float(B * args.steps), world, backend)
     value = units / (elapsed_max / 1e3)
+
+    def timed_steps(fn, profile: bool):
+        """Device ms of args.steps calls of fn; with profile, per-family event times
+        too (one stream, so each kernel's time is its own)."""
+        fn()
+        torch.cuda.synchronize()
+        if profile:
+            eng.set_concurrency(1)
+            eng.profile_reset()
+            eng.set_profiling(True)
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        s1.record(stream)
+        torch.cuda.synchronize()
+        p = None
+        if profile:
+            eng.set_profiling(False)
+            eng.set_concurrency(CONCURRENCY)
+            p = eng.profile()
+        ms, u = aggregate(s0.elapsed_time(s1), float(B * args.steps), world, backend)
+        return u / (ms / 1e3), p
+
+    # The same pairs one call each (no batch), and the per-kernel profile.
+    per_call_value, _ = timed_steps(per_call_step, False)
+    _, prof = timed_steps(step, True)
 
     # ---- roofline of the dominant kernel family (event-timed in the region above)
     bytes_per = kernel_bytes(L, E, dnum, n)
@@ -708,25 +745,14 @@ def main(argv=None):
     # ---- the same step with the ModDown on the CUDA cores (tensor cores are the default)
     def timed_form(tensor_cores: bool):
         eng.set_tensor_cores(tensor_cores)
-        step()
-        torch.cuda.synchronize()
-        eng.profile_reset()
-        eng.set_profiling(True)
-        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s0.record(stream)
-        for _ in range(args.steps):
-            step()
-        s1.record(stream)
-        torch.cuda.synchronize()
-        eng.set_profiling(False)
-        p = eng.profile()
+        form_value, _ = timed_steps(step, False)
+        _, p = timed_steps(step, True)
         eng.set_tensor_cores(2)
-        ms, u = aggregate(s0.elapsed_time(s1), float(B * args.steps), world, backend)
         fam = "mod_down_epilogue_tc" if "mod_down_epilogue_tc" in p else "mod_down_epilogue"
         cnt, fam_ms = p.get(fam, (0, 0.0))
         up = "mod_up_ntt_tc" if "mod_up_ntt_tc" in p else "mod_up_ntt"
         up_cnt, up_ms = p.get(up, (0, 0.0))
-        return {"value": u / (ms / 1e3), "unit": "ct/s", "mod_down_kernel": fam,
+        return {"value": form_value, "unit": "ct/s", "mod_down_kernel": fam,
                 "mod_down_avg_launch_ms": fam_ms / cnt if cnt else None,
                 "mod_down_ms_per_step": fam_ms / args.steps,
                 "mod_up_family": up, "mod_up_avg_launch_ms": up_ms / up_cnt if up_cnt else None,
@@ -744,17 +770,17 @@ def main(argv=None):
         pin_in[i, 1].copy_(torch.from_numpy(uniform_limbs(rng, q_in, 2, n).reshape(-1)))
 
     def e2e_step():
-        outs = []
-        for i in range(B):
-            a = eng.upload_from_pointer(pin_in[i, 0].data_ptr(), mid, 2)
-            b = eng.upload_from_pointer(pin_in[i, 1].data_ptr(), mid, 2)
-            o = eng.multiply_relinearize_rescale(a, b, rk)
-            eng.download_to_pointer(o, pin_out[i].data_ptr(), wait=False)
-            outs.append((a, b, o))
-        # No wait: copies overlap neighbouring kernels, also across steps; every
-        # object is freed behind the work that reads it.
-        for t in outs:
-            for d in t:
+        # Batch calls of CONCURRENCY pairs: a chunk's kernels start once its own
+        # uploads land, so copies and kernels of neighbouring chunks overlap.
+        for c0 in range(0, B, CONCURRENCY):
+            idx = range(c0, min(B, c0 + CONCURRENCY))
+            ins_a = [eng.upload_from_pointer(pin_in[i, 0].data_ptr(), mid, 2) for i in idx]
+            ins_b = [eng.upload_from_pointer(pin_in[i, 1].data_ptr(), mid, 2) for i in idx]
+            outs = eng.multiply_relinearize_rescale_batch(ins_a, ins_b, rk)
+            for i, o in zip(idx, outs):
+                eng.download_to_pointer(o, pin_out[i].data_ptr(), wait=False)
+            # No wait: every object is freed behind the work that reads it.
+            for d in ins_a + ins_b + outs:
                 d.free()
 
     e2e_step()
@@ -783,6 +809,8 @@ def main(argv=None):
             "scaling": "weak", "vs_baseline": None, "dtype": "int64",
             "data": "synthetic (seeded uniform residues, random relinearization key)",
             "config": {"workload": WORKLOAD, "pairs_per_step": B, "log_n": LOG_N,
+                       "api": "fhe_multiply_relinearize_rescale_batch", "streams": CONCURRENCY,
+                       "per_call_ct_s": per_call_value,
                        "special_prime_count": SPECIAL, "input_limbs": L0,
                        "relinearize_limbs": L, "dnum": dnum, "parallelism": f"replicas{world}",
                        "l2": f"inputs larger than L2 ({B} pairs x {2 * 2 * L0 * n * 8 / 1e6:.1f} MB)"},

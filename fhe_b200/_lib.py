@@ -100,6 +100,11 @@ SIGNATURES = {
     "fhe_ntt_tuning_get": (_i, [_i, _ip, _ip, _ip]),
     "fhe_engine_set_tensor_cores": (_i, [_vp, _i]),
     "fhe_engine_set_graphs": (_i, [_vp, _i]),
+    "fhe_engine_set_concurrency": (_i, [_vp, _i]),
+    "fhe_multiply_relinearize_rescale_batch": (_i, [_vp, _i, ctypes.POINTER(_vp),
+                                                   ctypes.POINTER(_vp), _vp, ctypes.POINTER(_vp)]),
+    "fhe_bootstrap_batch": (_i, [_vp, _i, ctypes.POINTER(_vp), _vp, _vp, _vp,
+                                ctypes.POINTER(_vp)]),
     "fhe_engine_graph_counts": (_i, [_vp, _ip, _ip]),
     "fhe_multiply_rotate_batch": (_i, [_vp, _i, ctypes.POINTER(_vp), ctypes.POINTER(_vp), _vp,
                                        ctypes.POINTER(_vp), _pp]),

@@ -795,6 +795,67 @@ int fhe_multiply_rotate_batch(fhe_engine *engine, int count, const fhe_data *con
   });
 }
 
+int fhe_multiply_relinearize_rescale_batch(fhe_engine *engine, int count,
+                                           const fhe_data *const *a, const fhe_data *const *b,
+                                           const fhe_data *relinearization_key, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(relinearization_key);
+  REQUIRE_OUT(a);
+  REQUIRE_OUT(b);
+  REQUIRE_OUT(out);
+  if (count < 1) {
+    fhe_b200::set_last_error("Multiply Relinearize Rescale Batch: the batch is empty.");
+    return FHE_ERR_INVALID_ARGUMENT;
+  }
+  for (int i = 0; i < count; i++) {
+    REQUIRE_HANDLE(a[i]);
+    REQUIRE_HANDLE(b[i]);
+    out[i] = nullptr;
+  }
+  return guarded([&] {
+    std::vector<const Data *> va, vb;
+    for (int i = 0; i < count; i++) {
+      va.push_back(&live(engine, a[i]));
+      vb.push_back(&live(engine, b[i]));
+    }
+    auto r = engine->impl->multiply_relinearize_rescale_batch(va, vb,
+                                                              live(engine, relinearization_key));
+    for (int i = 0; i < count; i++) out[i] = wrap(std::move(r[i]));
+  });
+}
+
+int fhe_bootstrap_batch(fhe_engine *engine, int count, const fhe_data *const *cts,
+                        const fhe_data *relinearization_key, const fhe_data *conjugation_key,
+                        const fhe_bootstrap_key *bootstrap_key, fhe_data **out) {
+  REQUIRE_HANDLE(engine);
+  REQUIRE_HANDLE(relinearization_key);
+  REQUIRE_HANDLE(conjugation_key);
+  REQUIRE_HANDLE(bootstrap_key);
+  REQUIRE_OUT(cts);
+  REQUIRE_OUT(out);
+  if (count < 1) {
+    fhe_b200::set_last_error("Bootstrap Batch: the batch is empty.");
+    return FHE_ERR_INVALID_ARGUMENT;
+  }
+  for (int i = 0; i < count; i++) {
+    REQUIRE_HANDLE(cts[i]);
+    out[i] = nullptr;
+  }
+  return guarded([&] {
+    std::vector<const Data *> v;
+    for (int i = 0; i < count; i++) v.push_back(&live(engine, cts[i]));
+    auto r = engine->impl->bootstrap_batch(v, live(engine, relinearization_key),
+                                           live(engine, conjugation_key),
+                                           live_key(engine, bootstrap_key));
+    for (int i = 0; i < count; i++) out[i] = wrap(std::move(r[i]));
+  });
+}
+
+int fhe_engine_set_concurrency(fhe_engine *engine, int streams) {
+  REQUIRE_HANDLE(engine);
+  return guarded([&] { engine->impl->set_concurrency(streams); });
+}
+
 int fhe_engine_graph_counts(const fhe_engine *engine, int *captured, int *failed) {
   REQUIRE_HANDLE(engine);
   REQUIRE_OUT(captured);

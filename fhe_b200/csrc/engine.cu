@@ -64,6 +64,7 @@ Engine::Engine(const Config &config) : params(config) {
   check(cudaStreamCreateWithFlags(&download_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
   check(cudaEventCreateWithFlags(&upload_done_, cudaEventDisableTiming), "cudaEventCreate");
   check(cudaEventCreateWithFlags(&compute_done_, cudaEventDisableTiming), "cudaEventCreate");
+  set_concurrency(concurrency_);
   check(cudaMalloc(&device_error_, sizeof(int)), "cudaMalloc(error flag)");
   check(cudaMemset(device_error_, 0, sizeof(int)), "clear error flag");
   // Keep freed blocks in the stream-ordered pool: key switching allocates and frees
@@ -136,6 +137,12 @@ Engine::~Engine() {
   for (auto &kv : ntt_perm_cache_) cudaFree(kv.second);
   for (auto *b : table_buffers_) cudaFree(b);
   if (device_error_) cudaFree(device_error_);
+  for (auto w : workers_) {
+    cudaStreamSynchronize(w);
+    cudaStreamDestroy(w);
+  }
+  for (auto ev : worker_done_) cudaEventDestroy(ev);
+  if (fork_) cudaEventDestroy(fork_);
   cudaEventDestroy(upload_done_);
   cudaEventDestroy(compute_done_);
   cudaStreamDestroy(upload_stream_);

@@ -255,6 +255,20 @@ class Engine {
   std::vector<std::unique_ptr<Data>> multiply_rotate_batch(
       const std::vector<const Data *> &a, const std::vector<const Data *> &b, const Data &rk,
       const std::vector<const Data *> &rotation_keys);
+  // The independent operations of a batch run on up to this many streams at once
+  // (1 to kMaxConcurrency; default 4; 1 runs them in order on the engine's stream).
+  // Each operation's kernels stay in order on its stream, so the words are the same;
+  // the streams fill the SMs left idle by one operation's last wave of CTAs.
+  static constexpr int kMaxConcurrency = 8;
+  void set_concurrency(int streams);
+  int concurrency() const { return concurrency_; }
+  // multiply_relinearize_rescale of every pair (a[i], b[i]), concurrently.
+  std::vector<std::unique_ptr<Data>> multiply_relinearize_rescale_batch(
+      const std::vector<const Data *> &a, const std::vector<const Data *> &b, const Data &rk);
+  // bootstrap(ct, rk, ck, bk) of every ciphertext, concurrently.
+  std::vector<std::unique_ptr<Data>> bootstrap_batch(const std::vector<const Data *> &cts,
+                                                     const Data &rk, const Data &ck,
+                                                     const BootstrapKey &bk);
   // Captured graphs held, and input shapes whose capture failed (run directly).
   std::pair<int, int> graph_counts() const {
     return {static_cast<int>(graph_cache_.size()), static_cast<int>(graph_failed_.size())};
@@ -329,6 +343,13 @@ class Engine {
     unsigned long long launches = 0;
   };
   bool graphs_ = true;
+  // Streams of batch items (graphs.cu): item i of a batch runs on worker i % count,
+  // forked from and joined back into the engine's stream by events.
+  int concurrency_ = 4;
+  std::vector<cudaStream_t> workers_;
+  std::vector<cudaEvent_t> worker_done_;
+  cudaEvent_t fork_ = nullptr;
+  void run_concurrent(int count, const std::function<void(int)> &item);
   std::map<std::vector<uint64_t>, std::vector<GraphShape>> graph_seen_;
   std::map<std::vector<uint64_t>, CapturedGraph> graph_cache_;
   std::set<std::vector<uint64_t>> graph_failed_;

@@ -3,7 +3,11 @@
 // operation's shape has run directly (which checks its inputs and builds every
 // table it needs), it is captured once on the engine's stream, temporaries
 // allocated and freed inside the graph, and replayed from then on: one launch per
-// call, the same kernels and the same words.
+// call, the same kernels and the same words.  The items of a batch run on several
+// streams (forked from and joined into the engine's stream), so one item's kernels
+// fill the SMs that another's last wave of CTAs leaves idle; captured, the items
+// become parallel branches of the graph.
+#include <algorithm>
 #include <cstring>
 
 #include "engine.hpp"
@@ -100,6 +104,77 @@ std::vector<std::unique_ptr<Data>> Engine::run_captured(std::vector<uint64_t> ke
   return out;
 }
 
+void Engine::set_concurrency(int streams) {
+  if (streams < 1 || streams > kMaxConcurrency)
+    throw std::invalid_argument("set_concurrency: the stream count should be between 1 and 8.");
+  if (!fork_) check(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "cudaEventCreate");
+  while (static_cast<int>(workers_.size()) < streams) {
+    cudaStream_t w = nullptr;
+    check(cudaStreamCreateWithFlags(&w, cudaStreamNonBlocking), "cudaStreamCreate");
+    workers_.push_back(w);
+    cudaEvent_t ev = nullptr;
+    check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+    worker_done_.push_back(ev);
+  }
+  concurrency_ = streams;
+}
+
+void Engine::run_concurrent(int count, const std::function<void(int)> &item) {
+  const int streams = std::min(count, concurrency_);
+  if (streams <= 1) {
+    for (int i = 0; i < count; i++) item(i);
+    return;
+  }
+  // Inside a capture of the engine's stream the fork and join events make the
+  // workers part of the same graph, as parallel branches.
+  const cudaStream_t home = stream_;
+  check(cudaEventRecord(fork_, home), "fork");
+  for (int w = 0; w < streams; w++) check(cudaStreamWaitEvent(workers_[w], fork_, 0), "fork");
+  auto join = [&] {
+    stream_ = home;
+    cudaError_t e = cudaSuccess;
+    for (int w = 0; w < streams; w++) {
+      if (e == cudaSuccess) e = cudaEventRecord(worker_done_[w], workers_[w]);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(home, worker_done_[w], 0);
+    }
+    return e;
+  };
+  try {
+    for (int i = 0; i < count; i++) {
+      stream_ = workers_[i % streams];
+      item(i);
+    }
+  } catch (...) {
+    join();
+    throw;
+  }
+  check(join(), "join");
+}
+
+std::vector<std::unique_ptr<Data>> Engine::multiply_relinearize_rescale_batch(
+    const std::vector<const Data *> &a, const std::vector<const Data *> &b, const Data &rk) {
+  const std::string fn = "Multiply Relinearize Rescale Batch";
+  if (a.size() != b.size() || a.empty())
+    throw std::invalid_argument(fn + ": the batch lists should have one entry each per item.");
+  for (size_t i = 0; i < a.size(); i++)
+    if (!a[i] || !b[i]) throw std::invalid_argument(fn + ": a batch entry is null.");
+  std::vector<std::unique_ptr<Data>> out(a.size());
+  run_concurrent(static_cast<int>(a.size()),
+                 [&](int i) { out[i] = multiply_relinearize_rescale(*a[i], *b[i], rk); });
+  return out;
+}
+
+std::vector<std::unique_ptr<Data>> Engine::bootstrap_batch(const std::vector<const Data *> &cts,
+                                                           const Data &rk, const Data &ck,
+                                                           const BootstrapKey &bk) {
+  if (cts.empty()) throw std::invalid_argument("Bootstrap Batch: the batch is empty.");
+  for (const Data *c : cts)
+    if (!c) throw std::invalid_argument("Bootstrap Batch: a batch entry is null.");
+  std::vector<std::unique_ptr<Data>> out(cts.size());
+  run_concurrent(static_cast<int>(cts.size()), [&](int i) { out[i] = bootstrap(*cts[i], rk, ck, bk); });
+  return out;
+}
+
 std::vector<std::unique_ptr<Data>> Engine::multiply_rotate_batch(
     const std::vector<const Data *> &a, const std::vector<const Data *> &b, const Data &rk,
     const std::vector<const Data *> &rotation_keys) {
@@ -115,12 +190,13 @@ std::vector<std::unique_ptr<Data>> Engine::multiply_rotate_batch(
     inputs.push_back(a[i]);
     inputs.push_back(b[i]);
   }
+  key.push_back(static_cast<uint64_t>(concurrency_));
   return run_captured(std::move(key), inputs, [&](const std::vector<const Data *> &in) {
-    std::vector<std::unique_ptr<Data>> out;
-    for (size_t i = 0; i < rotation_keys.size(); i++) {
+    std::vector<std::unique_ptr<Data>> out(rotation_keys.size());
+    run_concurrent(static_cast<int>(rotation_keys.size()), [&](int i) {
       auto product = multiply_relinearize_rescale(*in[2 * i], *in[2 * i + 1], rk);
-      out.push_back(rotate(*product, *rotation_keys[i]));
-    }
+      out[i] = rotate(*product, *rotation_keys[i]);
+    });
     return out;
   });
 }

@@ -382,11 +382,11 @@ struct TensorLoad {
   __device__ __forceinline__ int64_t operator()(int poly, int limb, int prime, int gi, int n) const {
     const long long i = static_cast<long long>(limb) * n + gi;
     const uint64_t qq = q[prime], kk = k[prime];
-    if (poly == 0) return mont_mult(a[i], b[i], qq, kk);
-    if (poly == 2) return mont_mult(a[poly_stride + i], b[poly_stride + i], qq, kk);
+    if (poly == 0) return mont_mult_lazy(a[i], b[i], qq, kk);
+    if (poly == 2) return mont_mult_lazy(a[poly_stride + i], b[poly_stride + i], qq, kk);
     const int64_t qs = static_cast<int64_t>(qq);
-    return guard(guard(mont_mult(a[i], b[poly_stride + i], qq, kk) +
-                           mont_mult(a[poly_stride + i], b[i], qq, kk),
+    return guard(guard(mont_mult_lazy(a[i], b[poly_stride + i], qq, kk) +
+                           mont_mult_lazy(a[poly_stride + i], b[i], qq, kk),
                        qs << 1),
                  qs);
   }

@@ -64,7 +64,7 @@ struct EnterLoad {
   const uint64_t *k;
   __device__ __forceinline__ int64_t operator()(int poly, int limb, int prime, int gi, int n) const {
     const int64_t x = src[poly * poly_stride + (long long)limb * n + gi];
-    return mont_mult(x, constant[prime], q[prime], k[prime]);
+    return mont_mult_lazy(x, constant[prime], q[prime], k[prime]);
   }
 };
 
@@ -83,9 +83,9 @@ struct RescaleEnterLoad {
     const int64_t x0 = s[gi];
     const int64_t rounder = static_cast<uint64_t>(x0) > (q[prime - limb - 1] >> 1) ? 1 : 0;
     const uint64_t qq = q[prime], kk = k[prime];
-    const int64_t v = rescale_word(s[static_cast<long long>(limb + 1) * n + gi], x0, rounder, qq, kk,
-                                   rescale_scale[prime]);
-    return mont_mult(v, r_squared[prime], qq, kk);
+    const int64_t v = rescale_word<true>(s[static_cast<long long>(limb + 1) * n + gi], x0, rounder,
+                                         qq, kk, rescale_scale[prime]);
+    return mont_mult_lazy(v, r_squared[prime], qq, kk);
   }
 };
 
@@ -101,7 +101,7 @@ struct ProductEnterLoad {
   __device__ __forceinline__ int64_t operator()(int poly, int limb, int prime, int gi, int n) const {
     const uint64_t qq = q[prime], kk = k[prime];
     const int64_t x = src[poly * poly_stride + (long long)limb * n + gi];
-    return mont_mult(mont_mult(x, p_product[prime], qq, kk), r_squared[prime], qq, kk);
+    return mont_mult_lazy(mont_mult_lazy(x, p_product[prime], qq, kk), r_squared[prime], qq, kk);
   }
 };
 
@@ -116,7 +116,7 @@ struct EnterExitStore {
   const uint64_t *k;
   __device__ __forceinline__ void operator()(int poly, int limb, int prime, int gi, int n, int64_t v) const {
     const uint64_t qq = q[prime], kk = k[prime];
-    int64_t y = mont_exit(mont_mult(v, n_inverse[prime], qq, kk), qq, kk);
+    int64_t y = mont_exit(mont_mult_lazy(v, n_inverse[prime], qq, kk), qq, kk);
     if (REDUCE) y = guard(y, static_cast<int64_t>(qq));
     dst[poly * poly_stride + (long long)limb * n + gi] = y;
   }
@@ -143,11 +143,27 @@ __device__ __forceinline__ constexpr int tile_xor(int v) {
   return v ^ (((v >> 4) ^ ((v >> 5) << 2)) & (M >= 16 ? 15 : M - 1));
 }
 
+// A pass of S stages runs in R = ceil(S / 3) rounds of as equal a size as possible
+// (S = 8: 3 + 3 + 2; S = 10: 3 + 3 + 2 + 2), each round a radix-2^r group of up to 8
+// words per thread held in registers.  (Radix-16 rounds measured slower: at 80
+// registers they spill and fewer CTAs fit an SM.)
+constexpr int kNttMaxRoundLog = 3;
+__host__ __device__ constexpr int ntt_rounds(int S) {
+  return (S + kNttMaxRoundLog - 1) / kNttMaxRoundLog;
+}
+__host__ __device__ constexpr int ntt_round_log(int S, int round) {
+  return S / ntt_rounds(S) + (round < S % ntt_rounds(S) ? 1 : 0);
+}
+__host__ __device__ constexpr int ntt_round_first(int S, int round) {
+  return round * (S / ntt_rounds(S)) + (round < S % ntt_rounds(S) ? round : S % ntt_rounds(S));
+}
+
 template <int S, bool INVERSE, class Loader, class Storer>
 __global__ void __launch_bounds__(256, 4)
     ntt_pass_kernel(NttPass a, PrimeTables t, Loader load, Storer store) {
   constexpr int M = 1 << S;
-  constexpr int R = (S + 2) / 3;
+  constexpr int R = ntt_rounds(S);
+  constexpr int kMaxE = 1 << kNttMaxRoundLog;
   extern __shared__ int64_t tile_smem[];
 
   const int pl = blockIdx.y;
@@ -166,10 +182,9 @@ __global__ void __launch_bounds__(256, 4)
 
 #pragma unroll
   for (int round = 0; round < R; round++) {
-    constexpr int kLastR = S - 3 * (R - 1);
-    const int r = (round < R - 1) ? 3 : kLastR;
+    const int r = ntt_round_log(S, round);
     const int E = 1 << r;
-    const int first_local = 3 * round;
+    const int first_local = ntt_round_first(S, round);
     const int dlog = INVERSE ? first_local : (S - first_local - r);
     const int D = 1 << dlog;
     const int groups_per_col = M >> r;
@@ -187,9 +202,9 @@ __global__ void __launch_bounds__(256, 4)
       const int u = u0 + c;
       const int gbase = (u >> a.stride_log) * (M << a.stride_log) + (u & (T - 1));
       const int tb = tile_index<M>(c, base);
-      int64_t x[8];
+      int64_t x[kMaxE];
 #pragma unroll
-      for (int e = 0; e < 8; e++) {
+      for (int e = 0; e < kMaxE; e++) {
         if (e < E) {
           if (round == 0) {
             x[e] = load(poly, limb, prime, gbase + (base + e * D) * T, n);
@@ -209,7 +224,7 @@ __global__ void __launch_bounds__(256, 4)
       // forms below (same words); any other word takes the reference's forms.
       bool in_range = q < (uint64_t(1) << 60);
 #pragma unroll
-      for (int e = 0; e < 8; e++)
+      for (int e = 0; e < kMaxE; e++)
         if (e < E) in_range = in_range && static_cast<uint64_t>(x[e]) < static_cast<uint64_t>(q2);
       auto stages = [&](auto lazy) {
         constexpr bool kLazy = decltype(lazy)::value;
@@ -233,7 +248,7 @@ __global__ void __launch_bounds__(256, 4)
           return mont_mult_const(w, v, q, k);
         };
 #pragma unroll
-        for (int j = 0; j < 3; j++) {
+        for (int j = 0; j < kNttMaxRoundLog; j++) {
           if (j < r) {
             if (!INVERSE) {
               // stage s: twiddle root[2^s - 1 + (gi >> (log_n - s))]; the block of
@@ -245,7 +260,7 @@ __global__ void __launch_bounds__(256, 4)
               for (int h = 0; h < (1 << j); h++) {
                 const int64_t w = __ldg(wp + h);
 #pragma unroll
-                for (int e2 = 0; e2 < 4; e2++) {
+                for (int e2 = 0; e2 < kMaxE / 2; e2++) {
                   if (e2 < half) {
                     const int e = h * 2 * half + e2;
                     const int64_t uu = x[e];
@@ -262,11 +277,11 @@ __global__ void __launch_bounds__(256, 4)
               const int half = 1 << j;
               const int64_t *wp = tw + (n - (n >> dg) + (gi0 >> (dg + 1)));
 #pragma unroll
-              for (int h = 0; h < 4; h++) {
+              for (int h = 0; h < kMaxE / 2; h++) {
                 if (h < (E >> (j + 1))) {
                   const int64_t w = __ldg(wp + h);
 #pragma unroll
-                  for (int e2 = 0; e2 < 4; e2++) {
+                  for (int e2 = 0; e2 < kMaxE / 2; e2++) {
                     if (e2 < half) {
                       const int e = h * 2 * half + e2;
                       const int64_t uu = x[e];
@@ -287,7 +302,7 @@ __global__ void __launch_bounds__(256, 4)
         stages(std::false_type{});
       }
 #pragma unroll
-      for (int e = 0; e < 8; e++) {
+      for (int e = 0; e < kMaxE; e++) {
         if (e < E) {
           if (round == R - 1) {
             store(poly, limb, prime, gbase + (base + e * D) * T, n, x[e]);

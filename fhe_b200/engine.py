@@ -481,6 +481,31 @@ class Engine:
                                                     arr(rotation_keys), out))
         return [Data(self, ctypes.c_void_p(out[i])) for i in range(n)]
 
+    def multiply_relinearize_rescale_batch(self, a: list, b: list,
+                                           relinearization_key: Data) -> list:
+        """[multiply_relinearize_rescale(a[i], b[i], rk)], the items run concurrently
+        on the engine's worker streams; the same words."""
+        n = len(a)
+        arr = lambda xs: (ctypes.c_void_p * n)(*[x.handle for x in xs])
+        out = (ctypes.c_void_p * n)()
+        check(_lib.load().fhe_multiply_relinearize_rescale_batch(
+            self._h, n, arr(a), arr(b), relinearization_key.handle, out))
+        return [Data(self, ctypes.c_void_p(out[i])) for i in range(n)]
+
+    def bootstrap_batch(self, cts: list, relinearization_key: Data, conjugation_key: Data,
+                        bootstrap_key: "BootstrapKey") -> list:
+        """[bootstrap(ct, rk, ck, bootstrap_key) for ct in cts], concurrently."""
+        n = len(cts)
+        arr = (ctypes.c_void_p * n)(*[c.handle for c in cts])
+        out = (ctypes.c_void_p * n)()
+        check(_lib.load().fhe_bootstrap_batch(self._h, n, arr, relinearization_key.handle,
+                                              conjugation_key.handle, bootstrap_key.handle, out))
+        return [Data(self, ctypes.c_void_p(out[i])) for i in range(n)]
+
+    def set_concurrency(self, streams: int) -> None:
+        """Streams the items of a batch share (1 to 8, default 4); same words."""
+        check(_lib.load().fhe_engine_set_concurrency(self._h, int(streams)))
+
     def graph_counts(self) -> tuple:
         """(captured bootstrap graphs held, input shapes whose capture failed)."""
         a, b = ctypes.c_int(), ctypes.c_int()

@@ -442,6 +442,19 @@ int fhe_engine_set_tensor_cores(fhe_engine *engine, int mode);
 int fhe_multiply_rotate_batch(fhe_engine *engine, int count, const fhe_data *const *a,
                               const fhe_data *const *b, const fhe_data *relinearization_key,
                               const fhe_data *const *rotation_keys, fhe_data **out);
+/* Batches with no reference counterpart: the same words as one call per item
+ * (fhe_multiply_relinearize_rescale for every pair a[i], b[i]; fhe_bootstrap_with_key
+ * for every cts[i]), the items run concurrently on the engine's worker streams.  out
+ * receives count new handles. */
+int fhe_multiply_relinearize_rescale_batch(fhe_engine *engine, int count,
+                                           const fhe_data *const *a, const fhe_data *const *b,
+                                           const fhe_data *relinearization_key, fhe_data **out);
+int fhe_bootstrap_batch(fhe_engine *engine, int count, const fhe_data *const *cts,
+                        const fhe_data *relinearization_key, const fhe_data *conjugation_key,
+                        const fhe_bootstrap_key *bootstrap_key, fhe_data **out);
+/* How many streams the items of a batch share (1 to 8, default 4; 1 runs them in
+ * order on the engine's stream).  Same words for every count. */
+int fhe_engine_set_concurrency(fhe_engine *engine, int streams);
 /* CUDA graphs (default on): after one direct run of an input shape,
  * fhe_bootstrap_with_key and fhe_multiply_rotate_batch capture the whole operation
  * once and replay it.  Graphs are not used while profiling.  Same words either way. */

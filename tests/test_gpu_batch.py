@@ -40,3 +40,37 @@ def test_multiply_rotate_batch_matches_single_operations(engines):
         for g, w in zip(got, want):
             assert np.array_equal(g.download(), w), run
     assert e.graph_counts() == (captured_before + 1, 0)
+
+
+@pytest.mark.parametrize("streams", [1, 3, 8])
+def test_multiply_relinearize_rescale_batch_matches_single_operations(engines, streams):
+    e = engines(16, 10, 1)
+    n = e.coeff_count
+    top = e.moduli_id(e.max_key_switching_level)
+    rng = np.random.default_rng(99 + streams)
+    key = uniform_limbs(rng, e.moduli[top:], 2 * e.partition_count(top), n)
+    rk = e.upload(key, top, NTT | SPECIAL, RELIN)
+    pairs = []
+    for level in [24, 3, 24, 11, 17, 24, 5]:
+        mid = e.moduli_id(level)
+        q = e.moduli[mid:e.chain_count]
+        pairs.append((e.upload(uniform_limbs(rng, q, 2, n), mid),
+                      e.upload(uniform_limbs(rng, q, 2, n), mid)))
+    want = [e.multiply_relinearize_rescale(a, b, rk).download() for a, b in pairs]
+    e.set_concurrency(streams)
+    try:
+        for run in range(2):
+            got = e.multiply_relinearize_rescale_batch([p[0] for p in pairs],
+                                                       [p[1] for p in pairs], rk)
+            for g, w in zip(got, want):
+                assert np.array_equal(g.download(), w), run
+    finally:
+        e.set_concurrency(4)
+
+
+def test_concurrency_bounds(engines):
+    e = engines(16, 10, 1)
+    for bad in (0, 9):
+        with pytest.raises(Exception):
+            e.set_concurrency(bad)
+    e.set_concurrency(4)

@@ -74,6 +74,16 @@ def test_bootstrap_key_matches_recorded_reference(engines, case):
     finally:
         e.set_graphs(True)
 
+    # A batch runs its bootstraps on several streams (each stream with graphs of its
+    # own after its first direct run): the words of the single calls.
+    ct2 = e.encrypt(e.encode(codec_values(case["values_seed"] + 1, e.slot_count, True),
+                             case["encrypt_level"]), sk)
+    want2 = digest(e.bootstrap(ct2, rk, ck, bk).download())
+    batch = [ct, ct2, ct]
+    for run in range(3):
+        got = [digest(o.download()) for o in e.bootstrap_batch(batch, rk, ck, bk)]
+        assert got == [d["bootstrapped"], want2, d["bootstrapped"]], run
+
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: c["tier"])
 def test_bootstrap_key_rejects_bad_arguments(engines, case):
