@@ -235,6 +235,7 @@ def run_ntt_microbench(args, torch, np, rank, world, local, backend, stream):
 
     eng = Engine(log_coeff_count=16, special_prime_count=4)
     eng.set_stream(stream.cuda_stream)
+    eng.set_concurrency(CONCURRENCY)
     n, limbs, B = eng.coeff_count, 24, args.batch
     rng = np.random.default_rng(5 + rank)
     buf = eng.upload(uniform_limbs(rng, eng.moduli[:limbs], B, n), eng.chain_count - limbs,
@@ -277,7 +278,7 @@ def run_ntt_microbench(args, torch, np, rank, world, local, backend, stream):
 
 # -------------------------------------------------------------- bootstrap --
 
-CONCURRENCY = 4  # the engine's default worker streams for batch calls
+CONCURRENCY = 4  # worker streams of batch calls (the engine's default; --streams)
 
 
 def run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream):
@@ -292,6 +293,7 @@ def run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream):
     with_key = args.workload == "bootstrap"
     eng = Engine(log_coeff_count=16, special_prime_count=4, scheme_preset=2)
     eng.set_stream(stream.cuda_stream)
+    eng.set_concurrency(CONCURRENCY)
     B = args.batch
     eng.seed([11 + rank, 22, 33, 44, 55, 66, 77, 88], [1, 2])
     sk = eng.create_secret_key()
@@ -410,6 +412,7 @@ def run_batched_bench(args, torch, np, rank, world, local, backend, stream):
 
     eng = Engine(log_coeff_count=LOG_N, special_prime_count=SPECIAL)
     eng.set_stream(stream.cuda_stream)
+    eng.set_concurrency(CONCURRENCY)
     n = eng.coeff_count
     top = eng.moduli_id(eng.max_key_switching_level)
     rng = np.random.default_rng(77 + rank)
@@ -534,6 +537,7 @@ def run_plain_bench(args, torch, np, rank, world, local, backend, stream):
 
     eng = Engine(log_coeff_count=14, special_prime_count=1)
     eng.set_stream(stream.cuda_stream)
+    eng.set_concurrency(CONCURRENCY)
     eng.seed([5 + rank, 6, 7, 8, 9, 10, 11, 12], [3, 4])
     sk = eng.create_secret_key()
     pk = eng.create_public_key(sk)
@@ -604,7 +608,12 @@ def main(argv=None):
                          "batched: --batch uneven HMult+rotate items per step (use 256); "
                          "plain: the N=2^14 pipeline from slot values to decoded slots")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--streams", type=int, default=None,
+                    help="worker streams of batch calls (1-8; default: the engine's 4)")
     args = ap.parse_args(argv)
+    global CONCURRENCY
+    if args.streams is not None:
+        CONCURRENCY = args.streams
     rank, world, local = dist_env()
 
     if args.impl == "reference":
@@ -642,6 +651,7 @@ def main(argv=None):
         return run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream)
     eng = Engine(log_coeff_count=LOG_N, special_prime_count=SPECIAL)
     eng.set_stream(stream.cuda_stream)
+    eng.set_concurrency(CONCURRENCY)
     n = eng.coeff_count
     level = eng.max_key_switching_level
     mid = eng.moduli_id(level)
