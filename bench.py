@@ -749,7 +749,9 @@ def main(argv=None):
                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                     "peak_source": peak_kind, "avg_launch_ms": avg_ms,
                     "algorithmic_bytes_per_launch": bytes_per.get(dominant),
-                    "share_of_timed_region": ms / elapsed,
+                    # of the kernel time of one stream (the profiled pass runs the
+                    # batch on one stream, as ncu's serialised launch list does)
+                    "share_of_kernel_time": ms / sum(v[1] for v in prof.values()),
                     "kernel_ms_per_step": {k: v[1] / args.steps for k, v in prof.items()}}
 
     # ---- the same step with the ModDown on the CUDA cores (tensor cores are the default)
