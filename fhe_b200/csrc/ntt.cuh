@@ -179,6 +179,10 @@ __global__ void __launch_bounds__(256, 4)
   const bool strided = T > 1;
   const int C = 1 << a.columns_log;
   const int u0 = blockIdx.x * C;
+  // Round 0 checks the words it loads; if every group of the CTA was in range, the
+  // tile stays in range through the later rounds, which then skip the check.
+  bool slow = false;
+  bool tile_lazy = false;
 
 #pragma unroll
   for (int round = 0; round < R; round++) {
@@ -222,10 +226,14 @@ __global__ void __launch_bounds__(256, 4)
       // reference's lazy range; twiddles are below 2q), and for them the
       // butterfly's signed compares and sign-extended product reduce to the short
       // forms below (same words); any other word takes the reference's forms.
-      bool in_range = q < (uint64_t(1) << 60);
+      bool in_range = tile_lazy;
+      if (round == 0) {
+        in_range = q < (uint64_t(1) << 60);
 #pragma unroll
-      for (int e = 0; e < kMaxE; e++)
-        if (e < E) in_range = in_range && static_cast<uint64_t>(x[e]) < static_cast<uint64_t>(q2);
+        for (int e = 0; e < kMaxE; e++)
+          if (e < E) in_range = in_range && static_cast<uint64_t>(x[e]) < static_cast<uint64_t>(q2);
+        slow = slow || !in_range;
+      }
       auto stages = [&](auto lazy) {
         constexpr bool kLazy = decltype(lazy)::value;
         // guard(a + b, q2) and guard(a + q2 - b, q2) (unit.h:13)
@@ -312,7 +320,11 @@ __global__ void __launch_bounds__(256, 4)
         }
       }
     }
-    if (round < R - 1) __syncthreads();
+    if (round == 0 && R > 1) {
+      tile_lazy = __syncthreads_or(slow) == 0;
+    } else if (round < R - 1) {
+      __syncthreads();
+    }
   }
 }
 
