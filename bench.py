@@ -261,13 +261,44 @@ def run_ntt_microbench(args, torch, np, rank, world, local, backend, stream):
     bytes_per_step = 2 * B * limbs * n * 8
     gbs = bytes_per_step * args.steps * world / (elapsed_max / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
+
+    def timed_op(fn, nbytes):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        s1.record(stream)
+        torch.cuda.synchronize()
+        ms, u = aggregate(s0.elapsed_time(s1), float(B * args.steps), world, backend)
+        return {"polys_per_s": u / (ms / 1e3),
+                "achieved_gbs": nbytes * args.steps / (ms / 1e3) / 1e9,
+                "frac_of_peak": nbytes * args.steps / (ms / 1e3) / 1e9 / peak}
+
+    # The inverse transform, and SingleProcessor::mont_mult of two batches (config B's
+    # pointwise product: reads a and b, writes y).
+    other = eng.upload(uniform_limbs(rng, eng.moduli[:limbs], B, n), eng.chain_count - limbs,
+                       kind=UNIT_PLAINTEXT)
+    optr = other.device_pointer()
+    extra = {
+        "inverse_ntt": timed_op(lambda: eng.ntt_limbs(ptr, 0, limbs, B, stride, inverse=True),
+                                bytes_per_step),
+        "pointwise_mont_mult": timed_op(
+            lambda: eng.mont_mult_limbs(optr, ptr, optr, 0, limbs, B, stride),
+            3 * B * limbs * n * 8),
+    }
+    other.free()
     if rank == 0:
         print(json.dumps({
             "metric": "forward NTT polys/s (24 limbs, N=2^16)", "value": units / (elapsed_max / 1e3),
             "unit": "polys/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": elapsed_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int64", "data": "synthetic uniform residues",
-            "config": {"workload": "ntt 24 limbs x batch", "batch": B},
+            "config": {"workload": "ntt 24 limbs x batch", "batch": B,
+                       "l2": f"limbs larger than L2 for batch >= 11 ({B * limbs * n * 8 / 1e6:.0f} MB)"},
+            "other_kernels": extra,
             "roofline": {"bound": "hbm", "achieved": gbs / world, "peak": peak, "unit": "GB/s",
                          "frac": gbs / world / peak, "traffic": None, "peak_source": peak_kind},
             "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)

@@ -143,6 +143,8 @@ SIGNATURES = {
     "fhe_encrypt": (_i, [_vp, _vp, _vp, _pp]),
     "fhe_decrypt": (_i, [_vp, _vp, _vp, _pp]),
     "fhe_decode": (_i, [_vp, _vp, _f64p, _f64p]),
+    "fhe_mont_mult_limbs": (_i, [_vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _i, _i, _i,
+                                 ctypes.c_longlong]),
     "fhe_ntt_limbs": (_i, [_vp, _i64p, _i, _i, _i, ctypes.c_longlong, _i]),
     "fhe_relinearize_noalloc": (_i, [_vp, _i64p, _i, _i64p, _i, _i, _i64p]),
 }

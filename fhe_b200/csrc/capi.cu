@@ -368,6 +368,14 @@ int fhe_ntt_limbs(fhe_engine *engine, int64_t *device_limbs, int moduli_id, int 
   });
 }
 
+int fhe_mont_mult_limbs(fhe_engine *engine, const int64_t *a, const int64_t *b, int64_t *y,
+                        int moduli_id, int chains, int polys, long long poly_stride) {
+  REQUIRE_HANDLE(engine);
+  return guarded([&] {
+    engine->impl->mont_mult_limbs(a, b, y, moduli_id, chains, polys, poly_stride);
+  });
+}
+
 }  // extern "C"
 
 extern "C" {

@@ -419,6 +419,20 @@ void Engine::ntt_limbs(int64_t *limbs, int moduli_id, int chains, int polys, lon
         "ntt_limbs");
 }
 
+void Engine::mont_mult_limbs(const int64_t *a, const int64_t *b, int64_t *y, int moduli_id, int chains,
+                             int polys, long long stride) {
+  if (!a || !b || !y) throw std::invalid_argument("a device limb pointer is null.");
+  if (moduli_id < 0 || chains <= 0 || moduli_id + chains > params.prime_count || polys <= 0 ||
+      stride < static_cast<long long>(chains) * params.n)
+    throw std::invalid_argument("the limb range is out of the moduli chain.");
+  if (stride == static_cast<long long>(chains) * params.n) {
+    pointwise(kOpMult, polys * chains, moduli_id, a, b, nullptr, y, chains);  // one launch
+    return;
+  }
+  for (int p = 0; p < polys; p++)
+    pointwise(kOpMult, chains, moduli_id, a + p * stride, b + p * stride, nullptr, y + p * stride);
+}
+
 // ------------------------------------------------------------------ rescale --
 
 std::unique_ptr<Data> Engine::core_rescale(const Data &ct) {

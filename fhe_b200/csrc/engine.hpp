@@ -290,6 +290,10 @@ class Engine {
 
   void ntt_limbs(int64_t *limbs, int moduli_id, int chains, int polys, long long stride,
                  bool inverse);
+  // SingleProcessor::mont_mult (single.h:27) on device limbs: y = REDC(a b) per word,
+  // `polys` x `chains` limbs at moduli_id, [poly][chain][N] with the given stride.
+  void mont_mult_limbs(const int64_t *a, const int64_t *b, int64_t *y, int moduli_id, int chains,
+                       int polys, long long stride);
 
   // Per-kernel-family device time, measured with CUDA events on the engine's
   // stream around each launch while profiling is on.
@@ -384,9 +388,10 @@ class Engine {
                     int64_t shift);
   void draw_gaussian(int64_t *out);
   void tile(const int64_t *chain, int limbs, int prime_base, int64_t *y, long long y_stride);
-  // constants: host array of `limbs` per-limb values (or null), passed by value.
+  // constants: host array of `limbs` per-limb values (or null), passed by value;
+  // limb j runs modulo prime prime_base + j % period (period 0: limbs).
   void pointwise(int op, int limbs, int prime_base, const int64_t *a, const int64_t *b,
-                 const int64_t *constants, int64_t *y);
+                 const int64_t *constants, int64_t *y, int period = 0);
   void ntt_in_place(int64_t *x, int limbs, int prime_base, long long stride, int polys);
   void intt_in_place(int64_t *x, int limbs, int prime_base, long long stride, int polys);
   std::unique_ptr<Data> create_key_switching_key(const Data &from, const Data &to, int level,

@@ -172,33 +172,74 @@ __global__ void signed_tile_kernel(PrimeTables t, int log_n, int limbs, int prim
   y[j * y_stride + c] = s < 0 ? s + q : guard(s, q);
 }
 
-// y[j] = op(a[j], b[j]) over `limbs` limbs of N words; a, b, y are [limbs][N]
-// views (any may alias).
-__global__ void pointwise_kernel(PrimeTables t, int op, int log_n, int limbs, int prime_base,
-                                 const int64_t *a, const int64_t *b, LimbScalars c, int64_t *y) {
-  const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-  if (i >= (static_cast<long long>(limbs) << log_n)) return;
-  const int j = static_cast<int>(i >> log_n);
-  const int prime = prime_base + j;
-  const uint64_t q = t.q[prime], k = t.k[prime];
+// One word of y[j] = op(a[j], b[j]): word i (global index over the limbs) of limb j.
+__device__ __forceinline__ int64_t pointwise_word(int op, long long i, int log_n, int j, int64_t ai,
+                                                  int64_t bi, const LimbScalars &c, uint64_t q,
+                                                  uint64_t k) {
   const int64_t qs = static_cast<int64_t>(q), q2 = qs << 1;
   int64_t v = 0;
   switch (op) {
-    case kOpMult: v = mont_mult(a[i], b[i], q, k); break;
-    case kOpAddReduce: v = guard(guard(a[i] + b[i], q2), qs); break;
-    case kOpSubReduce: v = guard(guard(a[i] + q2 - b[i], q2), qs); break;
-    case kOpReduce: v = guard(a[i], qs); break;
-    case kOpEnter: v = mont_mult(a[i], c.v[j], q, k); break;
-    case kOpNegate: v = qs - a[i]; break;
-    case kOpAddScalarFirst: v = guard(a[i] + ((i & ((1LL << log_n) - 1)) == 0 ? c.v[j] : 0), qs); break;
-    case kOpEnterReduce: v = guard(mont_mult(a[i], c.v[j], q, k), qs); break;
+    case kOpMult: v = mont_mult(ai, bi, q, k); break;
+    case kOpAddReduce: v = guard(guard(ai + bi, q2), qs); break;
+    case kOpSubReduce: v = guard(guard(ai + q2 - bi, q2), qs); break;
+    case kOpReduce: v = guard(ai, qs); break;
+    case kOpEnter: v = mont_mult(ai, c.v[j], q, k); break;
+    case kOpNegate: v = qs - ai; break;
+    case kOpAddScalarFirst: v = guard(ai + ((i & ((1LL << log_n) - 1)) == 0 ? c.v[j] : 0), qs); break;
+    case kOpEnterReduce: v = guard(mont_mult(ai, c.v[j], q, k), qs); break;
     case kOpMonomial: {
       const int64_t m = c.v[j];
       v = (i & ((1LL << log_n) - 1)) == (1LL << (log_n - 1)) ? (m < 0 ? m + qs : guard(m, qs)) : 0;
       break;
     }
   }
-  y[i] = v;
+  return v;
+}
+
+__device__ __forceinline__ bool pointwise_reads_a(int op) { return op != kOpMonomial; }
+__device__ __forceinline__ bool pointwise_reads_b(int op) {
+  return op == kOpMult || op == kOpAddReduce || op == kOpSubReduce;
+}
+
+// y[j] = op(a[j], b[j]) over `limbs` limbs of N words; a, b, y are [limbs][N]
+// views (any may alias).  W consecutive words per thread: W = 4 moves them as
+// 16-byte vectors (every pointer 16-byte aligned), which keeps enough loads in
+// flight to stream at HBM speed; W = 1 serves unaligned views.
+// Limb j runs modulo prime prime_base + j % period (period = limbs but for batches of
+// polynomials laid out back to back).
+template <int W>
+__global__ void pointwise_kernel(PrimeTables t, int op, int log_n, int limbs, int period,
+                                 int prime_base, const int64_t *a, const int64_t *b, LimbScalars c,
+                                 int64_t *y) {
+  const long long i0 = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) * W;
+  if (i0 >= (static_cast<long long>(limbs) << log_n)) return;
+  const int j = static_cast<int>(i0 >> log_n) % period;  // W <= N: the words share a limb
+  const int prime = prime_base + j;
+  const uint64_t q = t.q[prime], k = t.k[prime];
+  int64_t av[W] = {}, bv[W] = {}, yv[W];
+  if (W == 4) {
+    if (pointwise_reads_a(op)) {
+      const longlong2 x0 = reinterpret_cast<const longlong2 *>(a + i0)[0];
+      const longlong2 x1 = reinterpret_cast<const longlong2 *>(a + i0)[1];
+      av[0] = x0.x; av[1] = x0.y; av[2 % W] = x1.x; av[3 % W] = x1.y;
+    }
+    if (pointwise_reads_b(op)) {
+      const longlong2 x0 = reinterpret_cast<const longlong2 *>(b + i0)[0];
+      const longlong2 x1 = reinterpret_cast<const longlong2 *>(b + i0)[1];
+      bv[0] = x0.x; bv[1] = x0.y; bv[2 % W] = x1.x; bv[3 % W] = x1.y;
+    }
+  } else {
+    if (pointwise_reads_a(op)) av[0] = a[i0];
+    if (pointwise_reads_b(op)) bv[0] = b[i0];
+  }
+#pragma unroll
+  for (int w = 0; w < W; w++) yv[w] = pointwise_word(op, i0 + w, log_n, j, av[w], bv[w], c, q, k);
+  if (W == 4) {
+    reinterpret_cast<longlong2 *>(y + i0)[0] = make_longlong2(yv[0], yv[1 % W]);
+    reinterpret_cast<longlong2 *>(y + i0)[1] = make_longlong2(yv[2 % W], yv[3 % W]);
+  } else {
+    y[i0] = yv[0];
+  }
 }
 
 }  // namespace
@@ -262,17 +303,26 @@ void Engine::signed_tile(const int64_t *chain, int64_t q_src, int limbs, int pri
 }
 
 void Engine::pointwise(int op, int limbs, int prime_base, const int64_t *a, const int64_t *b,
-                       const int64_t *constants, int64_t *y) {
-  // The per-limb constants travel by value in the launch (no copy, no wait).
+                       const int64_t *constants, int64_t *y, int period) {
+  if (period <= 0 || period > limbs) period = limbs;
+  // The per-limb constants (one per prime of the period) travel by value in the
+  // launch (no copy, no wait).
   LimbScalars c{};
   if (constants) {
-    if (limbs > kMaxScalarLimbs) throw std::invalid_argument("pointwise: too many limbs.");
-    for (int j = 0; j < limbs; j++) c.v[j] = constants[j];
+    if (period > kMaxScalarLimbs) throw std::invalid_argument("pointwise: too many limbs.");
+    for (int j = 0; j < period; j++) c.v[j] = constants[j];
   }
+  const long long words = static_cast<long long>(limbs) << params.log_n;
+  const bool aligned = ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b) |
+                         reinterpret_cast<uintptr_t>(y)) & 15) == 0;
   check(timed("pointwise", [&] {
           note_launch();
-          pointwise_kernel<<<grid_for(static_cast<long long>(limbs) << params.log_n), kThreads, 0,
-                             stream_>>>(tables_, op, params.log_n, limbs, prime_base, a, b, c, y);
+          if (aligned && params.n >= 4)
+            pointwise_kernel<4><<<grid_for(words / 4), kThreads, 0, stream_>>>(
+                tables_, op, params.log_n, limbs, period, prime_base, a, b, c, y);
+          else
+            pointwise_kernel<1><<<grid_for(words), kThreads, 0, stream_>>>(
+                tables_, op, params.log_n, limbs, period, prime_base, a, b, c, y);
           return cudaGetLastError();
         }),
         "pointwise");

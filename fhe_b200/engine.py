@@ -546,3 +546,9 @@ class Engine:
         """Plain per-limb NTT/iNTT (SingleProcessor::ntt/intt) on device memory, in place."""
         check(_lib.load().fhe_ntt_limbs(self._h, ctypes.cast(device_ptr, _lib._i64p), moduli_id,
                                         chains, polys, poly_stride, int(inverse)))
+
+    def mont_mult_limbs(self, a_ptr: int, b_ptr: int, y_ptr: int, moduli_id: int, chains: int,
+                        polys: int, poly_stride: int) -> None:
+        """SingleProcessor::mont_mult on device memory: y = REDC(a * b) per word."""
+        check(_lib.load().fhe_mont_mult_limbs(self._h, a_ptr, b_ptr, y_ptr, moduli_id, chains,
+                                              polys, poly_stride))

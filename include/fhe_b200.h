@@ -479,6 +479,11 @@ int fhe_ntt_tuning_get(int log_n, int *s_second, int *first_columns_log, int *se
  * at moduli_id, in place, [poly][chain][N] with the given poly stride (words). */
 int fhe_ntt_limbs(fhe_engine *engine, int64_t *device_limbs, int moduli_id, int chains,
                   int polys, long long poly_stride, int inverse);
+/* SingleProcessor::mont_mult (single.h:27, unit.cpp): y = REDC(a * b) word by word on
+ * `polys` x `chains` device limbs at moduli_id ([poly][chain][N], the given stride);
+ * y may alias a or b. */
+int fhe_mont_mult_limbs(fhe_engine *engine, const int64_t *a, const int64_t *b, int64_t *y,
+                        int moduli_id, int chains, int polys, long long poly_stride);
 
 #ifdef __cplusplus
 }

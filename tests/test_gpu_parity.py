@@ -135,3 +135,35 @@ def test_errors_mirror_reference_messages(engines):
     with pytest.raises(FheError, match="should have 3 polynomials"):
         key = uniform_limbs(np.random.default_rng(3), e.moduli[3:], 2 * e.partition_count(3), e.coeff_count)
         e.relinearize(e.upload(y, 3, NTT), e.upload(key, 3, NTT | SPECIAL, RELINEARIZATION_KEY))
+
+
+def test_mont_mult_limbs_matches_redc(engines):
+    """SingleProcessor::mont_mult on device limbs (unit.h:15-23): y = (a b + s q) / 2^62
+    with s = (a b mod 2^64) k mod 2^62, k = -q^-1 mod 2^62, in [0, 2q)."""
+    import torch
+
+    e = engines(14, 1, 1)
+    n, chains, polys = e.coeff_count, 5, 2
+    mid = 1
+    rng = np.random.default_rng(77)
+    qs = [int(q) for q in e.moduli[mid:mid + chains]]
+    a = np.stack([np.stack([rng.integers(0, 2 * q, size=n, dtype=np.int64) for q in qs])
+                  for _ in range(polys)])
+    b = np.stack([np.stack([rng.integers(0, 2 * q, size=n, dtype=np.int64) for q in qs])
+                  for _ in range(polys)])
+    da = torch.from_numpy(a).cuda()
+    db = torch.from_numpy(b).cuda()
+    dy = torch.empty_like(da)
+    e.synchronize()
+    torch.cuda.synchronize()
+    e.mont_mult_limbs(da.data_ptr(), db.data_ptr(), dy.data_ptr(), mid, chains, polys, chains * n)
+    e.synchronize()
+    got = dy.cpu().numpy()
+    R = 1 << 62
+    for j, q in enumerate(qs):
+        k = (-pow(q, -1, R)) % R
+        for p in range(polys):
+            for c in range(0, n, 97):
+                x = int(a[p, j, c]) * int(b[p, j, c])
+                s = ((x % (1 << 64)) * k) % R
+                assert int(got[p, j, c]) == (x + s * q) >> 62
