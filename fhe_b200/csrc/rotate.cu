@@ -111,28 +111,66 @@ __global__ void ntt_rotate_finish_kernel(PrimeTables t, int log_n, int limbs, in
   y[i] = v;
 }
 
+// W consecutive words per thread (W = 2: 16-byte accesses, every pointer and stride
+// 16-byte aligned), the terms' loads issued four at a time ahead of their products,
+// so the diagonal streams keep enough loads in flight.
+template <int W>
 __global__ void diagonal_mac_kernel(PrimeTables t, int log_n, int limbs, int prime_base,
                                     MacTerms terms, long long x_stride, bool accumulate,
                                     int64_t *y, long long y_stride) {
   const long long per_poly = static_cast<long long>(limbs) << log_n;
-  const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  const long long i = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) * W;
   if (i >= 2 * per_poly) return;
-  const int poly = i >= per_poly ? 1 : 0;
+  const int poly = i >= per_poly ? 1 : 0;  // W <= N: the words share a polynomial and limb
   const long long r = i - poly * per_poly;
   const int prime = prime_base + static_cast<int>(r >> log_n);
   const uint64_t q = t.q[prime], k = t.k[prime];
   const int64_t qs = static_cast<int64_t>(q), q2 = qs << 1;
+  auto load = [&](const int64_t *p, int64_t (&v)[W]) {
+    if (W == 2) {
+      const longlong2 x = *reinterpret_cast<const longlong2 *>(p);
+      v[0] = x.x;
+      v[1 % W] = x.y;
+    } else {
+      v[0] = *p;
+    }
+  };
   int first = 0;
-  int64_t acc;
+  int64_t acc[W];
   if (accumulate) {
-    acc = y[poly * y_stride + r];
+    load(y + poly * y_stride + r, acc);
   } else {
-    acc = mont_mult(terms.x[0][poly * x_stride + r], terms.d[0][r], q, k);
+    int64_t x[W], d[W];
+    load(terms.x[0] + poly * x_stride + r, x);
+    load(terms.d[0] + r, d);
+#pragma unroll
+    for (int w = 0; w < W; w++) acc[w] = mont_mult_lazy(x[w], d[w], q, k);
     first = 1;
   }
-  for (int m = first; m < terms.count; m++)
-    acc = guard(guard(acc + mont_mult(terms.x[m][poly * x_stride + r], terms.d[m][r], q, k), q2), qs);
-  y[poly * y_stride + r] = acc;
+  constexpr int kAhead = 4;
+  for (int m0 = first; m0 < terms.count; m0 += kAhead) {
+    int64_t x[kAhead][W], d[kAhead][W];
+#pragma unroll
+    for (int u = 0; u < kAhead; u++) {
+      if (m0 + u < terms.count) {
+        load(terms.x[m0 + u] + poly * x_stride + r, x[u]);
+        load(terms.d[m0 + u] + r, d[u]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kAhead; u++) {
+      if (m0 + u < terms.count) {
+#pragma unroll
+        for (int w = 0; w < W; w++)
+          acc[w] = guard(guard(acc[w] + mont_mult_lazy(x[u][w], d[u][w], q, k), q2), qs);
+      }
+    }
+  }
+  if (W == 2) {
+    *reinterpret_cast<longlong2 *>(y + poly * y_stride + r) = make_longlong2(acc[0], acc[1 % W]);
+  } else {
+    y[poly * y_stride + r] = acc[0];
+  }
 }
 
 }  // namespace
@@ -194,9 +232,17 @@ cudaError_t launch_diagonal_mac(const PrimeTables &t, int log_n, int limbs, int 
                                 const MacTerms &terms, long long x_stride, bool accumulate,
                                 int64_t *y, long long y_stride, cudaStream_t s) {
   if (terms.count < 1 || terms.count > kMaxMacTerms) return cudaErrorInvalidValue;
+  uintptr_t bits = reinterpret_cast<uintptr_t>(y) | static_cast<uintptr_t>(x_stride * 8) |
+                   static_cast<uintptr_t>(y_stride * 8);
+  for (int m = 0; m < terms.count; m++)
+    bits |= reinterpret_cast<uintptr_t>(terms.x[m]) | reinterpret_cast<uintptr_t>(terms.d[m]);
   note_launch();
-  diagonal_mac_kernel<<<grid_for((2LL * limbs) << log_n), kThreads, 0, s>>>(
-      t, log_n, limbs, prime_base, terms, x_stride, accumulate, y, y_stride);
+  if ((bits & 15) == 0 && log_n >= 1)
+    diagonal_mac_kernel<2><<<grid_for(((2LL * limbs) << log_n) / 2), kThreads, 0, s>>>(
+        t, log_n, limbs, prime_base, terms, x_stride, accumulate, y, y_stride);
+  else
+    diagonal_mac_kernel<1><<<grid_for((2LL * limbs) << log_n), kThreads, 0, s>>>(
+        t, log_n, limbs, prime_base, terms, x_stride, accumulate, y, y_stride);
   return cudaGetLastError();
 }
 
