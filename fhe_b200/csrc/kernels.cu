@@ -113,27 +113,34 @@ __global__ void rescale_kernel(PrimeTables t, KeySwitchTables ks, int n, int lim
 // CKKSCore::multiply(ct, double) (core.cpp:196-229) in one pass: every limb entered by
 // its scaled constant and reduced (mont_enter + reduce_2q_to_q), then rescale_once_
 // by limb 0; limb 0's entered word is recomputed per output instead of stored.
+// Each thread serves one coefficient of kScalarLimbsPerThread consecutive output
+// limbs, so the dropped limb's entered word e0 is formed once for all of them.
+constexpr int kScalarLimbsPerThread = 4;
+
 __global__ void scalar_rescale_kernel(PrimeTables t, KeySwitchTables ks, int log_n, int limbs,
                                       int moduli_id, LimbScalars c, const int64_t *x,
                                       long long xs, int64_t *y, long long ys) {
-  const int poly = blockIdx.y;
-  const long long per_poly = static_cast<long long>(limbs - 1) << log_n;
+  const int poly = blockIdx.z;
+  const long long cidx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (cidx >= (1LL << log_n)) return;
   const uint64_t q0 = t.q[moduli_id], k0 = t.k[moduli_id];
   const int64_t *xp = x + poly * xs;
   int64_t *yp = y + poly * ys;
-  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < per_poly;
-       i += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const int j = static_cast<int>(i >> log_n);
-    const long long cidx = i & ((1LL << log_n) - 1);
+  const int64_t e0 = guard(mont_mult_lazy(xp[cidx], c.v[0], q0, k0), static_cast<int64_t>(q0));
+  const int64_t rounder = static_cast<uint64_t>(e0) > (q0 >> 1) ? 1 : 0;  // get_rounder
+  const int j0 = blockIdx.y * kScalarLimbsPerThread;
+#pragma unroll
+  for (int u = 0; u < kScalarLimbsPerThread; u++) {
+    const int j = j0 + u;
+    if (j >= limbs - 1) break;
     const int prime = moduli_id + 1 + j;
     const uint64_t q = t.q[prime], k = t.k[prime];
-    const int64_t e0 = guard(mont_mult(xp[cidx], c.v[0], q0, k0), static_cast<int64_t>(q0));
-    const int64_t ej = guard(mont_mult(xp[(static_cast<long long>(j + 1) << log_n) + cidx], c.v[j + 1],
-                                       q, k),
+    const int64_t ej = guard(mont_mult_lazy(xp[(static_cast<long long>(j + 1) << log_n) + cidx],
+                                            c.v[j + 1], q, k),
                              static_cast<int64_t>(q));
-    const int64_t rounder = static_cast<uint64_t>(e0) > (q0 >> 1) ? 1 : 0;  // get_rounder
-    yp[i] = rescale_word(ej, e0, rounder, q, k,
-                         ks.rescale_scale[static_cast<long long>(moduli_id) * ks.prime_count + prime]);
+    yp[(static_cast<long long>(j) << log_n) + cidx] =
+        rescale_word<true>(ej, e0, rounder, q, k,
+                           ks.rescale_scale[static_cast<long long>(moduli_id) * ks.prime_count + prime]);
   }
 }
 
@@ -427,7 +434,8 @@ cudaError_t launch_scalar_rescale(const PrimeTables &t, const KeySwitchTables &k
                                   long long y_stride, cudaStream_t s) {
   if (limbs < 2 || limbs > kMaxScalarLimbs) return cudaErrorInvalidValue;
   const int log_n = __builtin_ctz(static_cast<unsigned>(n));
-  const dim3 grid(blocks_for(static_cast<long long>(limbs - 1) * n), polys);
+  const dim3 grid(blocks_for(n), (limbs - 1 + kScalarLimbsPerThread - 1) / kScalarLimbsPerThread,
+                  polys);
   note_launch();
   scalar_rescale_kernel<<<grid, kThreads, 0, s>>>(t, ks, log_n, limbs, moduli_id, c, x, x_stride,
                                                   y, y_stride);
