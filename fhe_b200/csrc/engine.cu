@@ -83,6 +83,21 @@ Engine::Engine(const Config &config) : params(config) {
   tables_.n_inverse = upload_table(p.n_inverse);
   tables_.root = upload_table(p.root);
   tables_.root_inverse = upload_table(p.root_inverse);
+  {
+    // The same twiddles reduced to [0, q), for the transforms whose result only
+    // matters modulo q (ntt.cuh, kValueOnly).
+    const size_t per = static_cast<size_t>(p.n) - 1;
+    std::vector<int64_t> rc(p.root), ric(p.root_inverse);
+    for (int i = 0; i < P; i++) {
+      const int64_t qi = static_cast<int64_t>(p.q[i]);
+      for (size_t j = 0; j < per; j++) {
+        rc[i * per + j] = guard(rc[i * per + j], qi);
+        ric[i * per + j] = guard(ric[i * per + j], qi);
+      }
+    }
+    tables_.root_reduced = upload_table(rc);
+    tables_.root_inverse_reduced = upload_table(ric);
+  }
   std::vector<double> inv_q(P), inv_2q(P);
   for (int i = 0; i < P; i++) {
     inv_q[i] = 1.0 / static_cast<double>(p.q[i]);

@@ -492,7 +492,10 @@ cudaError_t launch_extended_ntt(const PrimeTables &t, const DevicePartitions &dp
   const long long stride = static_cast<long long>(dp.extended) << log_n;
   PlainLoad ld{ext, stride};
   PlainStore st{ext, stride};
-  return forward_ntt(log_n, dp.count, dp.extended, moduli_id, t, ld, st, ext, stride, s);
+  // Value-only: the extended polynomial reaches the output only through the key
+  // inner product's reduction to [0, q) and ModDown's reduced inverse transform.
+  return forward_ntt<PlainLoad, PlainStore, true>(log_n, dp.count, dp.extended, moduli_id, t, ld, st,
+                                                  ext, stride, s);
 }
 
 cudaError_t launch_key_inner_product(const PrimeTables &t, const DevicePartitions &dp, int n,
@@ -510,7 +513,9 @@ cudaError_t launch_mod_down_intt(const PrimeTables &t, int log_n, int moduli_id,
   const long long stride = static_cast<long long>(extended) << log_n;
   PlainLoad ld{acc, stride};
   EnterExitStore<true> st{acc, stride, t.n_inverse, t.q, t.k};
-  return inverse_ntt(log_n, polys, extended, moduli_id, t, ld, st, acc, stride, s);
+  // Value-only: the store reduces every word to [0, q).
+  return inverse_ntt<PlainLoad, EnterExitStore<true>, true>(log_n, polys, extended, moduli_id, t, ld,
+                                                            st, acc, stride, s);
 }
 
 cudaError_t launch_mod_down_epilogue_ops(const PrimeTables &t, const KeySwitchTables &ks, int n,

@@ -177,6 +177,8 @@ struct PrimeTables {
   const int64_t *n_inverse;
   const int64_t *root;          // [prime][N-1]
   const int64_t *root_inverse;  // [prime][N-1]
+  const int64_t *root_reduced;          // root, each word reduced to [0, q)
+  const int64_t *root_inverse_reduced;  // root_inverse, each word reduced to [0, q)
   const double *inv_q;          // 1 / q
   const double *inv_2q;         // 1 / (2q)
   int log_n;

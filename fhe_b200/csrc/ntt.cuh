@@ -158,7 +158,7 @@ __host__ __device__ constexpr int ntt_round_first(int S, int round) {
   return round * (S / ntt_rounds(S)) + (round < S % ntt_rounds(S) ? round : S % ntt_rounds(S));
 }
 
-template <int S, bool INVERSE, class Loader, class Storer>
+template <int S, bool INVERSE, class Loader, class Storer, bool VALUE_ONLY = false>
 __global__ void __launch_bounds__(256, 4)
     ntt_pass_kernel(NttPass a, PrimeTables t, Loader load, Storer store) {
   constexpr int M = 1 << S;
@@ -174,7 +174,12 @@ __global__ void __launch_bounds__(256, 4)
   const uint64_t k = t.k[prime];
   const int64_t q2 = static_cast<int64_t>(q << 1);
   const int n = 1 << a.log_n;
-  const int64_t *tw = (INVERSE ? t.root_inverse : t.root) + static_cast<size_t>(prime) * (n - 1);
+  const int64_t *tw = (VALUE_ONLY ? (INVERSE ? t.root_inverse_reduced : t.root_reduced)
+                                  : (INVERSE ? t.root_inverse : t.root)) +
+                     static_cast<size_t>(prime) * (n - 1);
+  // A forward value-only pass after the first reads words in [0, 4q).
+  const uint64_t in_bound = (VALUE_ONLY && !INVERSE && a.first > 0) ? (q << 2) : (q << 1);
+  const bool last_pass = !INVERSE && a.first + S == a.log_n;
   const int T = 1 << a.stride_log;
   const bool strided = T > 1;
   const int C = 1 << a.columns_log;
@@ -231,7 +236,7 @@ __global__ void __launch_bounds__(256, 4)
         in_range = q < (uint64_t(1) << 60);
 #pragma unroll
         for (int e = 0; e < kMaxE; e++)
-          if (e < E) in_range = in_range && static_cast<uint64_t>(x[e]) < static_cast<uint64_t>(q2);
+          if (e < E) in_range = in_range && static_cast<uint64_t>(x[e]) < in_bound;
         slow = slow || !in_range;
       }
       auto stages = [&](auto lazy) {
@@ -271,6 +276,16 @@ __global__ void __launch_bounds__(256, 4)
                 for (int e2 = 0; e2 < kMaxE / 2; e2++) {
                   if (e2 < half) {
                     const int e = h * 2 * half + e2;
+                    if (kLazy && VALUE_ONLY) {
+                      // Harvey's form: words in [0, 4q), one guard per butterfly;
+                      // twiddles below q keep the product below 2q (q < 2^60).
+                      int64_t uu = x[e] - q2;
+                      uu = uu < 0 ? uu + q2 : uu;
+                      const int64_t p = product(w, x[e + half]);
+                      x[e] = uu + p;
+                      x[e + half] = uu - p + q2;
+                      continue;
+                    }
                     const int64_t uu = x[e];
                     const int64_t p = product(w, x[e + half]);
                     x[e] = add_guard(uu, p);
@@ -295,7 +310,9 @@ __global__ void __launch_bounds__(256, 4)
                       const int64_t uu = x[e];
                       const int64_t vv = x[e + half];
                       x[e] = add_guard(uu, vv);
-                      x[e + half] = product(w, sub_guard(uu, vv));
+                      // Harvey's form: the product's operand in (0, 4q) needs no guard.
+                      x[e + half] = (kLazy && VALUE_ONLY) ? product(w, uu - vv + q2)
+                                                          : product(w, sub_guard(uu, vv));
                     }
                   }
                 }
@@ -313,6 +330,10 @@ __global__ void __launch_bounds__(256, 4)
       for (int e = 0; e < kMaxE; e++) {
         if (e < E) {
           if (round == R - 1) {
+            if (VALUE_ONLY && !INVERSE && last_pass && in_range) {
+              const int64_t y = x[e] - q2;  // [0, 4q) -> [0, 2q)
+              x[e] = y < 0 ? x[e] : y;
+            }
             store(poly, limb, prime, gbase + (base + e * D) * T, n, x[e]);
           } else {
             tile_smem[tb ^ tile_xor<M>(e << dlog)] = x[e];
@@ -348,13 +369,13 @@ inline NttPlan ntt_plan(int log_n) {
 
 constexpr int kNttThreads = 256;
 
-template <int S, bool INVERSE, class Loader, class Storer>
+template <int S, bool INVERSE, class Loader, class Storer, bool VALUE_ONLY = false>
 cudaError_t launch_ntt_pass(const NttPass &a, const PrimeTables &t, const Loader &ld,
                             const Storer &st, cudaStream_t stream) {
   const int subs = (1 << a.log_n) >> S;
   const dim3 grid(subs >> a.columns_log, a.polys * a.limbs);
   const size_t smem = sizeof(int64_t) << (a.columns_log + S);
-  auto kernel = ntt_pass_kernel<S, INVERSE, Loader, Storer>;
+  auto kernel = ntt_pass_kernel<S, INVERSE, Loader, Storer, VALUE_ONLY>;
   // Raised once per instantiation to the most any valid plan uses, so no attribute
   // call lands inside a graph capture.
   static bool raised = false;
@@ -370,21 +391,21 @@ cudaError_t launch_ntt_pass(const NttPass &a, const PrimeTables &t, const Loader
   return cudaGetLastError();
 }
 
-template <bool INVERSE, class Loader, class Storer>
+template <bool INVERSE, class Loader, class Storer, bool VALUE_ONLY = false>
 cudaError_t dispatch_ntt_pass(int S, const NttPass &a, const PrimeTables &t, const Loader &ld,
                               const Storer &st, cudaStream_t stream) {
   switch (S) {
-    case 1: return launch_ntt_pass<1, INVERSE>(a, t, ld, st, stream);
-    case 2: return launch_ntt_pass<2, INVERSE>(a, t, ld, st, stream);
-    case 3: return launch_ntt_pass<3, INVERSE>(a, t, ld, st, stream);
-    case 4: return launch_ntt_pass<4, INVERSE>(a, t, ld, st, stream);
-    case 5: return launch_ntt_pass<5, INVERSE>(a, t, ld, st, stream);
-    case 6: return launch_ntt_pass<6, INVERSE>(a, t, ld, st, stream);
-    case 7: return launch_ntt_pass<7, INVERSE>(a, t, ld, st, stream);
-    case 8: return launch_ntt_pass<8, INVERSE>(a, t, ld, st, stream);
-    case 9: return launch_ntt_pass<9, INVERSE>(a, t, ld, st, stream);
-    case 10: return launch_ntt_pass<10, INVERSE>(a, t, ld, st, stream);
-    case 11: return launch_ntt_pass<11, INVERSE>(a, t, ld, st, stream);
+    case 1: return launch_ntt_pass<1, INVERSE, Loader, Storer, VALUE_ONLY>(a, t, ld, st, stream);
+    case 2: return launch_ntt_pass<2, INVERSE, Loader, Storer, VALUE_ONLY>(a, t, ld, st, stream);
+    case 3: return launch_ntt_pass<3, INVERSE, Loader, Storer, VALUE_ONLY>(a, t, ld, st, stream);
+    case 4: return launch_ntt_pass<4, INVERSE, Loader, Storer, VALUE_ONLY>(a, t, ld, st, stream);
+    case 5: return launch_ntt_pass<5, INVERSE, Loader, Storer, VALUE_ONLY>(a, t, ld, st, stream);
+    case 6: return launch_ntt_pass<6, INVERSE, Loader, Storer, VALUE_ONLY>(a, t, ld, st, stream);
+    case 7: return launch_ntt_pass<7, INVERSE, Loader, Storer, VALUE_ONLY>(a, t, ld, st, stream);
+    case 8: return launch_ntt_pass<8, INVERSE, Loader, Storer, VALUE_ONLY>(a, t, ld, st, stream);
+    case 9: return launch_ntt_pass<9, INVERSE, Loader, Storer, VALUE_ONLY>(a, t, ld, st, stream);
+    case 10: return launch_ntt_pass<10, INVERSE, Loader, Storer, VALUE_ONLY>(a, t, ld, st, stream);
+    case 11: return launch_ntt_pass<11, INVERSE, Loader, Storer, VALUE_ONLY>(a, t, ld, st, stream);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -392,7 +413,7 @@ cudaError_t dispatch_ntt_pass(int S, const NttPass &a, const PrimeTables &t, con
 // Batched forward NTT of `polys` x `limbs` limbs.  The first pass reads through
 // `ld`, the last pass writes through `st`; intermediate data lives in `work`
 // ([poly][limb][N], stride work_stride), which may alias the final destination.
-template <class Loader, class Storer>
+template <class Loader, class Storer, bool VALUE_ONLY = false>
 cudaError_t forward_ntt(int log_n, int polys, int limbs, int prime_base, const PrimeTables &t,
                         const Loader &ld, const Storer &st, int64_t *work, long long work_stride,
                         cudaStream_t stream) {
@@ -402,22 +423,24 @@ cudaError_t forward_ntt(int log_n, int polys, int limbs, int prime_base, const P
     a.stride_log = 0;
     a.first = 0;
     a.columns_log = 0;
-    return dispatch_ntt_pass<false>(plan.s_first, a, t, ld, st, stream);
+    return dispatch_ntt_pass<false, Loader, Storer, VALUE_ONLY>(plan.s_first, a, t, ld, st, stream);
   }
   PlainStore mid_store{work, work_stride};
   PlainLoad mid_load{work, work_stride};
   a.stride_log = plan.s_second;
   a.first = 0;
   a.columns_log = plan.first_columns_log;
-  cudaError_t e = dispatch_ntt_pass<false>(plan.s_first, a, t, ld, mid_store, stream);
+  cudaError_t e = dispatch_ntt_pass<false, Loader, PlainStore, VALUE_ONLY>(plan.s_first, a, t, ld,
+                                                                          mid_store, stream);
   if (e != cudaSuccess) return e;
   a.stride_log = 0;
   a.first = plan.s_first;
   a.columns_log = plan.second_columns_log;
-  return dispatch_ntt_pass<false>(plan.s_second, a, t, mid_load, st, stream);
+  return dispatch_ntt_pass<false, PlainLoad, Storer, VALUE_ONLY>(plan.s_second, a, t, mid_load, st,
+                                                                 stream);
 }
 
-template <class Loader, class Storer>
+template <class Loader, class Storer, bool VALUE_ONLY = false>
 cudaError_t inverse_ntt(int log_n, int polys, int limbs, int prime_base, const PrimeTables &t,
                         const Loader &ld, const Storer &st, int64_t *work, long long work_stride,
                         cudaStream_t stream) {
@@ -427,19 +450,21 @@ cudaError_t inverse_ntt(int log_n, int polys, int limbs, int prime_base, const P
     a.stride_log = 0;
     a.first = 0;
     a.columns_log = 0;
-    return dispatch_ntt_pass<true>(plan.s_first, a, t, ld, st, stream);
+    return dispatch_ntt_pass<true, Loader, Storer, VALUE_ONLY>(plan.s_first, a, t, ld, st, stream);
   }
   PlainStore mid_store{work, work_stride};
   PlainLoad mid_load{work, work_stride};
   a.stride_log = 0;
   a.first = 0;
   a.columns_log = plan.second_columns_log;
-  cudaError_t e = dispatch_ntt_pass<true>(plan.s_second, a, t, ld, mid_store, stream);
+  cudaError_t e = dispatch_ntt_pass<true, Loader, PlainStore, VALUE_ONLY>(plan.s_second, a, t, ld,
+                                                                         mid_store, stream);
   if (e != cudaSuccess) return e;
   a.stride_log = plan.s_second;
   a.first = plan.s_second;
   a.columns_log = plan.first_columns_log;
-  return dispatch_ntt_pass<true>(plan.s_first, a, t, mid_load, st, stream);
+  return dispatch_ntt_pass<true, PlainLoad, Storer, VALUE_ONLY>(plan.s_first, a, t, mid_load, st,
+                                                                stream);
 }
 
 }  // namespace fhe_b200
