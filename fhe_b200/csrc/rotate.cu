@@ -180,8 +180,10 @@ cudaError_t launch_rotate_base(const PrimeTables &t, const KeySwitchTables &ks, 
                                int64_t *acc0, cudaStream_t s) {
   ScaledEnterLoad ld{c0, ks.p_product_mult_r, t.r_squared, t.q, t.k};
   AccumulateStore st{acc0, t.q};
-  return forward_ntt(log_n, 1, limbs, moduli_id, t, ld, st, work,
-                     static_cast<long long>(limbs) << log_n, s);
+  // Value-only: the accumulated key product reaches the output through ModDown.
+  return forward_ntt<ScaledEnterLoad, AccumulateStore, true>(log_n, 1, limbs, moduli_id, t, ld, st,
+                                                             work,
+                                                             static_cast<long long>(limbs) << log_n, s);
 }
 
 cudaError_t launch_permute_signed(const PrimeTables &t, int n, int polys, int limbs,
