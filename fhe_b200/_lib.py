@@ -99,6 +99,7 @@ SIGNATURES = {
     "fhe_ntt_tuning_set": (_i, [_i, _i, _i, _i]),
     "fhe_ntt_tuning_get": (_i, [_i, _ip, _ip, _ip]),
     "fhe_engine_set_tensor_cores": (_i, [_vp, _i]),
+    "fhe_engine_set_tensor_core_wait_limit": (_i, [_vp, ctypes.c_longlong]),
     "fhe_engine_set_graphs": (_i, [_vp, _i]),
     "fhe_engine_set_concurrency": (_i, [_vp, _i]),
     "fhe_multiply_relinearize_rescale_batch": (_i, [_vp, _i, ctypes.POINTER(_vp),

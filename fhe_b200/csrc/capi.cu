@@ -767,6 +767,11 @@ int fhe_engine_set_tensor_cores(fhe_engine *engine, int mode) {
   return guarded([&] { engine->impl->set_tensor_cores(mode); });
 }
 
+int fhe_engine_set_tensor_core_wait_limit(fhe_engine *engine, long long limit) {
+  REQUIRE_HANDLE(engine);
+  return guarded([&] { engine->impl->set_tensor_core_wait_limit(limit); });
+}
+
 int fhe_engine_set_graphs(fhe_engine *engine, int enable) {
   REQUIRE_HANDLE(engine);
   return guarded([&] { engine->impl->set_graphs(enable != 0); });

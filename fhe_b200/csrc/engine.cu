@@ -199,6 +199,12 @@ void Engine::set_tensor_cores(int mode) {
   tensor_cores_ = mode;
 }
 
+void Engine::set_tensor_core_wait_limit(long long limit) {
+  if (limit > static_cast<long long>(UINT32_MAX))
+    throw std::invalid_argument("the tensor core wait limit should be below 2^32.");
+  tc_wait_limit_ = limit < 0 ? kTcDefaultWaitLimit : static_cast<uint32_t>(limit);
+}
+
 bool Engine::use_tensor_cores(int min_special) const {
   return tensor_cores_ == kTensorCoresOn ||
          (tensor_cores_ == kTensorCoresAuto && params.special_prime_count >= min_special);
@@ -233,7 +239,7 @@ cudaError_t Engine::mod_up(const DevicePartitions &dp, int moduli_id, const int6
     });
   return timed("mod_up_ntt_tc", [&] {
     const cudaError_t e = launch_mod_up_contract_tc(tables_, dp, *tc, params.n, moduli_id, digits,
-                                                    ext, device_error_, stream_);
+                                                    ext, tc_status(), stream_);
     if (e != cudaSuccess) return e;
     return launch_extended_ntt(tables_, dp, params.log_n, moduli_id, ext, stream_);
   });
@@ -246,7 +252,7 @@ cudaError_t Engine::mod_down_epilogue(int moduli_id, int limbs, const int64_t *a
   if (tc)
     return timed("mod_down_epilogue_tc", [&] {
       return launch_mod_down_epilogue_tc(tables_, ks_, *tc, params.n, moduli_id, limbs, acc, ops,
-                                         out, device_error_, stream_);
+                                         out, tc_status(), stream_);
     });
   return timed("mod_down_epilogue", [&] {
     return launch_mod_down_epilogue_ops(tables_, ks_, params.n, moduli_id, limbs, acc, ops, out,

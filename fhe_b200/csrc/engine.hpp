@@ -312,6 +312,11 @@ class Engine {
   static constexpr int kTensorCoreModUpMinSpecial = 8;
   void set_tensor_cores(int mode);
   int tensor_cores() const { return tensor_cores_; }
+  // Diagnostics: how many times the tensor-core kernels poll for each MMA round
+  // before they give up, set the error flag that synchronize() reports, drain their
+  // MMAs and return (0: give up at once; negative: the default).  Applies to
+  // kernels launched afterwards.
+  void set_tensor_core_wait_limit(long long limit);
 
   const PrimeTables &tables() const { return tables_; }
   const KeySwitchTables &key_switch_tables() const { return ks_; }
@@ -376,6 +381,13 @@ class Engine {
   cudaError_t mod_up(const DevicePartitions &dp, int moduli_id, const int64_t *digits,
                      int64_t *ext);
   int *device_error_ = nullptr;  // set by a kernel whose bounded wait ran out
+  uint32_t tc_wait_limit_ = kTcDefaultWaitLimit;
+  TcStatus tc_status() const {
+    TcStatus st;
+    st.error = device_error_;
+    st.wait_limit = tc_wait_limit_;
+    return st;
+  }
   const ModDownTcTables *mod_down_tc(int moduli_id);
   // The ModDown epilogue in the selected form.
   cudaError_t mod_down_epilogue(int moduli_id, int limbs, const int64_t *acc,

@@ -126,6 +126,15 @@ struct ModDownTcTables {
   int kb = 0;                   // A row bytes: 9 K rounded up to 32
 };
 
+// Where the tensor-core kernels report a bounded wait that ran out, and how long
+// their first wait on each MMA round may poll (the wait that drains the MMAs before
+// tensor memory is freed always polls for the full limit).
+constexpr uint32_t kTcDefaultWaitLimit = 1u << 22;
+struct TcStatus {
+  int *error = nullptr;                     // set to 1 when a wait ran out (outputs unspecified)
+  uint32_t wait_limit = kTcDefaultWaitLimit;  // polls of the mbarrier per MMA round
+};
+
 // The epilogue of launch_mod_down_epilogue_ops with the division as an INT8
 // tensor-core contraction (tcgen05.mma kind::i8, accumulator in tensor memory).
 // Same words as the CUDA-core form.  n must be a multiple of 128; error receives 1
@@ -133,7 +142,7 @@ struct ModDownTcTables {
 cudaError_t launch_mod_down_epilogue_tc(const PrimeTables &t, const KeySwitchTables &ks,
                                         const ModDownTcTables &tc, int n, int moduli_id,
                                         int limbs, const int64_t *acc, const EpilogueOps &ops,
-                                        int64_t *out, int *error, cudaStream_t s);
+                                        int64_t *out, const TcStatus &status, cudaStream_t s);
 // Whether the tensor-core epilogue serves this shape (special primes, limbs, n).
 bool mod_down_tc_supported(int special_count, int limbs, int n);
 // Host copies of the tables of ModDownTcTables at one moduli id, from the prime
@@ -175,7 +184,7 @@ ModUpTcHost make_mod_up_tc_tables(const std::vector<uint64_t> &k,
 // the INT8 tensor pipe; same words as the CUDA-core contraction.
 cudaError_t launch_mod_up_contract_tc(const PrimeTables &t, const DevicePartitions &dp,
                                       const ModUpTcTables &tc, int n, int moduli_id,
-                                      const int64_t *digits, int64_t *ext, int *error,
+                                      const int64_t *digits, int64_t *ext, const TcStatus &status,
                                       cudaStream_t s);
 // The forward NTT that completes ModUp, over every partition's extended limbs.
 cudaError_t launch_extended_ntt(const PrimeTables &t, const DevicePartitions &dp, int log_n,

@@ -43,7 +43,7 @@ template <int K>
 __global__ void __launch_bounds__(kTcThreads, K <= 10 && K != 7 ? 4 : (K <= 13 ? 3 : 1))
     mod_down_tc_kernel(PrimeTables t, KeySwitchTables ks, ModDownTcTables tc, int n,
                        int moduli_id, int L, const int64_t *acc, EpilogueOps ops, int64_t *out,
-                       int *error) {
+                       TcStatus status) {
   constexpr int KB = row_bytes(K);
   extern __shared__ __align__(128) uint8_t smem[];
   uint8_t *sA = smem;                   // [128 rows][KB], core matrices
@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(kTcThreads, K <= 10 && K != 7 ? 4 : (K <= 13 ?
       mma_round(tmem, sA, sB, KB);
       mma_commit(bar);
     }
-    ok = __syncthreads_and(mbar_wait(bar, round & 1)) != 0;
+    ok = __syncthreads_and(mbar_wait(bar, round & 1, status.wait_limit)) != 0;
     if (!ok) break;
     tc_fence_after();
     for (int jl = half * (kTcTargets / 2); jl < (half + 1) * (kTcTargets / 2); jl++) {
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(kTcThreads, K <= 10 && K != 7 ? 4 : (K <= 13 ?
   if (!ok) {
     // The round's MMAs may still be running: wait for them (bounded) before the
     // tensor memory is given back.
-    if (tid == 0) atomicExch(error, 1);
+    if (tid == 0) atomicExch(status.error, 1);
     if (warp == 0) mbar_wait(bar, round & 1);
   }
   tc_fence_before();
@@ -240,9 +240,9 @@ ModDownTcHost make_mod_down_tc_tables(const std::vector<uint64_t> &q,
 cudaError_t launch_mod_down_epilogue_tc(const PrimeTables &t, const KeySwitchTables &ks,
                                         const ModDownTcTables &tc, int n, int moduli_id,
                                         int limbs, const int64_t *acc, const EpilogueOps &ops,
-                                        int64_t *out, int *error, cudaStream_t s) {
+                                        int64_t *out, const TcStatus &status, cudaStream_t s) {
   const int K = ks.special_count;
-  if (!mod_down_tc_supported(K, limbs, n) || tc.b == nullptr || error == nullptr ||
+  if (!mod_down_tc_supported(K, limbs, n) || tc.b == nullptr || status.error == nullptr ||
       tc.kb != row_bytes(K) || tc.rounds != (limbs + kTcTargets - 1) / kTcTargets ||
       (ops.base_polys > 0 && ops.base == nullptr) || (ops.rescale && ops.signed_perm != nullptr) ||
       ops.polys < 1 || ops.polys > 2 || ops.base_polys > ops.polys)
@@ -267,7 +267,7 @@ cudaError_t launch_mod_down_epilogue_tc(const PrimeTables &t, const KeySwitchTab
     }                                                                                           \
     note_launch();                                                                              \
     mod_down_tc_kernel<KK><<<grid, kTcThreads, smem, s>>>(t, ks, tc, n, moduli_id, limbs, acc,  \
-                                                          ops, out, error);                     \
+                                                          ops, out, status);                     \
     break;
     FHE_TC_CASE(1) FHE_TC_CASE(2) FHE_TC_CASE(3) FHE_TC_CASE(4) FHE_TC_CASE(5) FHE_TC_CASE(6)
     FHE_TC_CASE(7) FHE_TC_CASE(8) FHE_TC_CASE(9) FHE_TC_CASE(10) FHE_TC_CASE(11) FHE_TC_CASE(12)

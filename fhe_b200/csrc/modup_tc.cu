@@ -31,7 +31,7 @@ constexpr int digit_row_bytes(int A) { return (8 * A + 31) / 32 * 32; }
 template <int A>
 __global__ void __launch_bounds__(kTcThreads, 4)
     mod_up_tc_kernel(PrimeTables t, DevicePartitions dp, ModUpTcTables tc, int n, int moduli_id,
-                     const int64_t *digits, int64_t *ext, int *error) {
+                     const int64_t *digits, int64_t *ext, TcStatus status) {
   constexpr int KB = digit_row_bytes(A);
   const int p = blockIdx.y;
   if (dp.size[p] != A) return;  // uniform per CTA, before any barrier
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(kTcThreads, 4)
       mma_round(tmem, sA, sB, KB);
       mma_commit(bar);
     }
-    ok = __syncthreads_and(mbar_wait(bar, round & 1)) != 0;
+    ok = __syncthreads_and(mbar_wait(bar, round & 1, status.wait_limit)) != 0;
     if (!ok) break;
     tc_fence_after();
     for (int jl = half * (kTcTargets / 2); jl < (half + 1) * (kTcTargets / 2); jl++) {
@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(kTcThreads, 4)
     tc_fence_after();
   }
   if (!ok) {
-    if (tid == 0) atomicExch(error, 1);
+    if (tid == 0) atomicExch(status.error, 1);
     if (warp == 0) mbar_wait(bar, round & 1);
   }
   tc_fence_before();
@@ -198,9 +198,9 @@ ModUpTcHost make_mod_up_tc_tables(const std::vector<uint64_t> &k,
 
 cudaError_t launch_mod_up_contract_tc(const PrimeTables &t, const DevicePartitions &dp,
                                       const ModUpTcTables &tc, int n, int moduli_id,
-                                      const int64_t *digits, int64_t *ext, int *error,
+                                      const int64_t *digits, int64_t *ext, const TcStatus &status,
                                       cudaStream_t s) {
-  if (!mod_up_tc_supported(dp.max_size, n) || tc.b == nullptr || error == nullptr ||
+  if (!mod_up_tc_supported(dp.max_size, n) || tc.b == nullptr || status.error == nullptr ||
       tc.rounds != (dp.extended + kTcTargets - 1) / kTcTargets)
     return cudaErrorInvalidValue;
   static int raised[17] = {};
@@ -222,7 +222,7 @@ cudaError_t launch_mod_up_contract_tc(const PrimeTables &t, const DevicePartitio
     }                                                                                             \
     note_launch();                                                                                \
     mod_up_tc_kernel<AA><<<grid, kTcThreads, mod_up_tc_smem(AA), s>>>(t, dp, tc, n, moduli_id,    \
-                                                                      digits, ext, error);        \
+                                                                      digits, ext, status);        \
     break;
       FHE_UP_CASE(1) FHE_UP_CASE(2) FHE_UP_CASE(3) FHE_UP_CASE(4) FHE_UP_CASE(5) FHE_UP_CASE(6)
       FHE_UP_CASE(7) FHE_UP_CASE(8) FHE_UP_CASE(9) FHE_UP_CASE(10) FHE_UP_CASE(11) FHE_UP_CASE(12)

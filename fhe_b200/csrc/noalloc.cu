@@ -1,25 +1,28 @@
 // Relinearization that allocates nothing per call.
 //
 // Some callers of this library cannot allocate device memory while they work:
-// code running inside a CUDA graph capture, real-time pipelines with a fixed
-// memory budget, or hosts whose allocator policy forbids cudaMalloc after
-// start-up.  For them, fhe_relinearize_noalloc runs the same key-switching kernels
-// as fhe_relinearize but takes its temporaries (the iNTT'd ciphertext, the
-// mixed-radix digits, the extended partitions, the key-product accumulators and the
-// partition constants) from one file-scope device array of kNoAllocScratchWords
-// words instead of the stream-ordered pool.  Inputs and outputs are caller-owned
-// device buffers.
+// applications whose own allocator reserves the GPU's memory up front and hands
+// libraries a fixed budget, real-time loops where the implicit device
+// synchronisation of cudaMalloc/cudaFree (or an out-of-memory failure in mid-run)
+// is not acceptable, and code running where CUDA allocation calls are not allowed,
+// such as stream callbacks.  For them, fhe_relinearize_noalloc runs the same
+// key-switching kernels as fhe_relinearize but takes its temporaries (the iNTT'd
+// ciphertext, the mixed-radix digits, the extended partitions, the key-product
+// accumulators and the partition constants) from one file-scope device array of
+// kNoAllocScratchWords words instead of the stream-ordered pool.  Inputs and
+// outputs are caller-owned device buffers.
 //
 // Set-up: the first call on each device resolves the device address of the array
 // with cudaGetSymbolAddress while that device is current; that first call should
 // therefore come before any stream capture.  Every later call on the device reuses
 // the address.  All calls share the one array and it keeps the last call's
-// contents; everything a call reads is written by the same call first.  Calls that
-// overlap on the GPU (different streams, or different host threads on one device)
-// race on the array and must be serialised by the caller.
+// contents; everything a call reads is written by the same call first (the
+// partition constants are computed on the device from the call's own arguments,
+// so no host buffer is read after the call returns).  Calls that overlap on the
+// GPU (different streams, or different host threads on one device) race on the
+// array and must be serialised by the caller.
 #include <cuda_runtime.h>
 
-#include <cstring>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -36,16 +39,14 @@ namespace {
 
 // 4 Mi words = 32 MiB of scratch, held by every GPU that loads the library.
 constexpr size_t kNoAllocScratchWords = size_t(1) << 22;
-// Partition constants staged on the host: dnum <= 64 partitions.
+// dnum <= 64 partitions.
 constexpr int kMaxPartitions = 64;
-constexpr size_t kConstantWords = 1 << 17;
 
 __device__ __align__(256) int64_t g_noalloc_scratch[kNoAllocScratchWords];
 
 constexpr int kMaxDevices = 64;
 int64_t *g_scratch_address[kMaxDevices] = {};
 std::mutex g_setup_mutex;
-int64_t g_host_constants[kConstantWords];  // host staging, no heap
 
 int64_t *scratch_address() {
   int device = 0;
@@ -65,15 +66,105 @@ int64_t *scratch_address() {
   return g_scratch_address[device];
 }
 
-// Partition constants of (moduli_id, key_moduli_id) written into the host staging
-// buffer in the DevicePartitions layout (ints, then inverse_r, product_r,
-// product_r_squared), following ckks/parameters.cpp:334-360 and
-// ckks/precomputed.cpp:326-382 without any heap allocation.
-size_t stage_partitions(const Parameters &p, int moduli_id, int key_moduli_id,
-                        DevicePartitions &dp, int starts[], int sizes[], int indices[]) {
+// The partition ranges of (moduli_id, key_moduli_id), passed to the device by value
+// (ckks/parameters.cpp:334-360: partitions of K limbs counted from the top, the
+// lowest one cut short; the key's partition index counts from its own top).
+struct PartitionLayout {
+  int count;
+  int extended;
+  int moduli_id;
+  int start[kMaxPartitions];
+  int size[kMaxPartitions];
+  int key_index[kMaxPartitions];
+};
+
+// a * b mod m on the signed 128-bit product (arithmetic.cpp:33-38).
+__device__ int64_t device_mod_mul(int64_t a, int64_t b, int64_t m) {
+  return static_cast<int64_t>((static_cast<__int128>(a) * b) % m);
+}
+
+// Extended Euclid on signed 64-bit values; 0 when no inverse exists
+// (arithmetic.cpp:9-31).
+__device__ int64_t device_mod_invert(int64_t x, int64_t modulus) {
+  int64_t a = x, b = modulus, ra = 1, rb = 0;
+  while (b > 0) {
+    const int64_t quotient = a / b;
+    int64_t t = a;
+    a = b;
+    b = t - quotient * b;
+    t = ra;
+    ra = rb;
+    rb = t - quotient * rb;
+  }
+  if (a != 1) return 0;
+  return ra >= 0 ? ra : ra + modulus;
+}
+
+// Garner constants of one partition per CTA, in the DevicePartitions layout (ints,
+// then inverse_r [16], product_r [16][16], product_r_squared [16][E] per partition),
+// following ckks/precomputed.cpp:326-382; unused entries are written as zero.  The
+// product of the partition's leading primes is carried as residues modulo each
+// prime that needs it.
+__global__ void noalloc_partition_constants_kernel(PartitionLayout lay, const uint64_t *q,
+                                                   const int64_t *r_squared, int *ints,
+                                                   int64_t *inverse_r, int64_t *product_r,
+                                                   int64_t *product_r_squared) {
+  constexpr int64_t kR = int64_t(1) << 62;
+  const int part = blockIdx.x;
+  const int E = lay.extended;
+  const uint64_t *qq = q + lay.moduli_id;
+  const int64_t *r2 = r_squared + lay.moduli_id;
+  const int st = lay.start[part], sz = lay.size[part];
+  if (threadIdx.x == 0) {
+    ints[part] = st;
+    ints[lay.count + part] = sz;
+    ints[2 * lay.count + part] = lay.key_index[part];
+  }
+  auto product_mod = [&](int cnt, int64_t m) {
+    int64_t acc = 1;
+    for (int z = 0; z < cnt; z++)
+      acc = device_mod_mul(acc, static_cast<int64_t>(qq[st + z] % static_cast<uint64_t>(m)), m);
+    return acc;
+  };
+  const int entries = 16 + 256 + 16 * E;
+  for (int idx = threadIdx.x; idx < entries; idx += blockDim.x) {
+    int64_t value = 0;
+    if (idx < 16) {
+      const int ci = idx + 1;
+      if (ci < sz) {
+        const int64_t chain_q = static_cast<int64_t>(qq[st + ci]);
+        const int64_t inverse = device_mod_invert(product_mod(ci, chain_q), chain_q);
+        value = (chain_q & 1) == 0 ? inverse : device_mod_mul(inverse, kR, chain_q);
+      }
+      inverse_r[part * 16 + idx] = value;
+    } else if (idx < 16 + 256) {
+      const int r = idx - 16;
+      const int ci = r / 16 + 1, mi = ci + 1 + r % 16;
+      if (mi < sz) {
+        const int64_t mq = static_cast<int64_t>(qq[st + mi]);
+        const int64_t v = product_mod(ci, mq);
+        value = (mq & 1) == 0 ? v : device_mod_mul(v, kR, mq);
+      }
+      product_r[part * 256 + r] = value;
+    } else {
+      const int r = idx - 16 - 256;
+      const int ci = r / E + 1, mi = r % E;
+      if (ci < sz) {
+        const int64_t mq = static_cast<int64_t>(qq[mi]);
+        const int64_t v = product_mod(ci, mq);
+        value = (mq & 1) == 0 ? v : device_mod_mul(v, r2[mi], mq);
+      }
+      product_r_squared[static_cast<size_t>(part) * 16 * E + r] = value;
+    }
+  }
+}
+
+// Partition ranges of (moduli_id, key_moduli_id) and the host-side fields of
+// DevicePartitions, without any heap allocation.
+void plan_partitions(const Parameters &p, int moduli_id, int key_moduli_id, PartitionLayout &lay,
+                     DevicePartitions &dp) {
   const int K = p.special_prime_count;
   const int L = p.chains(moduli_id);
-  const int E = p.chains(moduli_id, true);
   const int pc = p.partition_count(moduli_id);
   if (pc > kMaxPartitions) throw std::invalid_argument("too many partitions for the no-alloc path.");
   int index = p.partition_count(key_moduli_id) - pc;
@@ -83,59 +174,24 @@ size_t stage_partitions(const Parameters &p, int moduli_id, int key_moduli_id,
     const int hi = start + K < L ? start + K : L;
     if (index < 0) throw std::invalid_argument("the key was created at a lower level than the text.");
     if (hi - lo > 16) throw std::invalid_argument("partition larger than 16 limbs.");
-    starts[count] = lo;
-    sizes[count] = hi - lo;
-    indices[count] = index;
+    lay.start[count] = lo;
+    lay.size[count] = hi - lo;
+    lay.key_index[count] = index;
     count++;
   }
-  const size_t int_words = (3 * static_cast<size_t>(count) * sizeof(int) + 7) / 8;
-  const size_t words = int_words + static_cast<size_t>(count) * (16 + 256 + 16 * static_cast<size_t>(E));
-  if (words > kConstantWords) throw std::invalid_argument("partition constants exceed the no-alloc staging.");
-  std::memset(g_host_constants, 0, words * sizeof(int64_t));
-  int *ints = reinterpret_cast<int *>(g_host_constants);
-  int64_t *inv = g_host_constants + int_words;
-  int64_t *prod = inv + static_cast<size_t>(count) * 16;
-  int64_t *prod2 = prod + static_cast<size_t>(count) * 256;
-  const uint64_t *qq = p.q.data() + moduli_id;
-  const int64_t *r2 = p.r_squared.data() + moduli_id;
-  constexpr int64_t kR = int64_t(1) << 62;
+  lay.count = count;
+  lay.extended = p.chains(moduli_id, true);
+  lay.moduli_id = moduli_id;
   dp.count = count;
-  dp.extended = E;
+  dp.extended = lay.extended;
   dp.max_size = 0;
   dp.size_mask = 0;
   dp.max_key_index = 0;
   for (int part = 0; part < count; part++) {
-    const int st = starts[part], sz = sizes[part];
-    ints[part] = st;
-    ints[count + part] = sz;
-    ints[2 * count + part] = indices[part];
-    dp.max_size = dp.max_size > sz ? dp.max_size : sz;
-    dp.size_mask |= 1u << sz;
-    dp.max_key_index = dp.max_key_index > indices[part] ? dp.max_key_index : indices[part];
-    auto product_mod = [&](int cnt, int64_t m) {
-      int64_t acc = 1;
-      for (int z = 0; z < cnt; z++)
-        acc = mod_mul(acc, static_cast<int64_t>(qq[st + z] % static_cast<uint64_t>(m)), m);
-      return acc;
-    };
-    for (int ci = 1; ci < sz; ci++) {
-      const int64_t chain_q = static_cast<int64_t>(qq[st + ci]);
-      const int64_t inverse = mod_invert(product_mod(ci, chain_q), chain_q);
-      inv[part * 16 + ci - 1] = (chain_q & 1) == 0 ? inverse : mod_mul(inverse, kR, chain_q);
-      for (int mi = ci + 1; mi < sz; mi++) {
-        const int64_t mq = static_cast<int64_t>(qq[st + mi]);
-        const int64_t v = product_mod(ci, mq);
-        prod[(part * 16 + ci - 1) * 16 + (mi - ci - 1)] = (mq & 1) == 0 ? v : mod_mul(v, kR, mq);
-      }
-      for (int mi = 0; mi < E; mi++) {
-        const int64_t mq = static_cast<int64_t>(qq[mi]);
-        const int64_t v = product_mod(ci, mq);
-        prod2[(static_cast<size_t>(part) * 16 + ci - 1) * E + mi] =
-            (mq & 1) == 0 ? v : mod_mul(v, r2[mi], mq);
-      }
-    }
+    dp.max_size = dp.max_size > lay.size[part] ? dp.max_size : lay.size[part];
+    dp.size_mask |= 1u << lay.size[part];
+    dp.max_key_index = dp.max_key_index > lay.key_index[part] ? dp.max_key_index : lay.key_index[part];
   }
-  return words;
 }
 
 }  // namespace
@@ -165,16 +221,13 @@ extern "C" int fhe_relinearize_noalloc(fhe_engine *engine, const int64_t *ct_dev
     const int n = p.n;
     const int L = p.chains(moduli_id);
     const int E = p.chains(moduli_id, true);
-    int starts[kMaxPartitions], sizes[kMaxPartitions], indices[kMaxPartitions];
+    PartitionLayout lay;
     DevicePartitions dp;
-    // The host staging buffer is shared: stage and copy under the lock (a copy from
-    // pageable memory returns once the buffer may be reused).
-    std::unique_lock<std::mutex> staging(g_setup_mutex, std::defer_lock);
-    int64_t *scratch = scratch_address();
-    staging.lock();
-    const size_t const_words = stage_partitions(p, moduli_id, key_moduli_id, dp, starts, sizes, indices);
+    plan_partitions(p, moduli_id, key_moduli_id, lay, dp);
     if (key_polys < 2 * (dp.max_key_index + 1))
       throw std::invalid_argument(std::string(fn) + ": the key switching key has too few polynomials.");
+    const size_t int_words = (3 * static_cast<size_t>(dp.count) * sizeof(int) + 7) / 8;
+    const size_t const_words = int_words + static_cast<size_t>(dp.count) * (16 + 256 + 16 * static_cast<size_t>(E));
     const size_t const_region = (const_words + 31) & ~size_t(31);  // keep 256-byte alignment
     const size_t t3_words = static_cast<size_t>(3) * L * n;
     const size_t digit_words = static_cast<size_t>(L) * n;
@@ -185,11 +238,8 @@ extern "C" int fhe_relinearize_noalloc(fhe_engine *engine, const int64_t *ct_dev
       throw std::invalid_argument(std::string(fn) + ": needs " + std::to_string(need) +
                                   " scratch words, more than the fixed " +
                                   std::to_string(kNoAllocScratchWords) + " (N x limbs too large).");
+    int64_t *scratch = scratch_address();
     cudaStream_t s = e.stream();
-    cudaError_t rc = cudaMemcpyAsync(scratch, g_host_constants, const_words * sizeof(int64_t),
-                                     cudaMemcpyHostToDevice, s);
-    staging.unlock();
-    const size_t int_words = (3 * static_cast<size_t>(dp.count) * sizeof(int) + 7) / 8;
     int *dints = reinterpret_cast<int *>(scratch);
     dp.start = dints;
     dp.size = dints + dp.count;
@@ -197,11 +247,16 @@ extern "C" int fhe_relinearize_noalloc(fhe_engine *engine, const int64_t *ct_dev
     dp.inverse_r = scratch + int_words;
     dp.product_r = dp.inverse_r + static_cast<size_t>(dp.count) * 16;
     dp.product_r_squared = dp.product_r + static_cast<size_t>(dp.count) * 256;
+    const PrimeTables &t = e.tables();
+    note_launch();
+    noalloc_partition_constants_kernel<<<dp.count, 256, 0, s>>>(lay, t.q, t.r_squared, dints,
+                                                                dp.inverse_r, dp.product_r,
+                                                                dp.product_r_squared);
+    cudaError_t rc = cudaGetLastError();
     int64_t *t3 = scratch + const_region;
     int64_t *digits = t3 + t3_words;
     int64_t *ext = digits + digit_words;
     int64_t *acc = ext + ext_words;
-    const PrimeTables &t = e.tables();
     const long long ps = static_cast<long long>(L) * n;
     if (rc == cudaSuccess) rc = launch_to_intt(t, p.log_n, 3, L, moduli_id, ct_device, ps, t3, ps, s);
     if (rc == cudaSuccess) rc = launch_mixed_radix(t, dp, n, moduli_id, t3 + 2 * ps, digits, s);

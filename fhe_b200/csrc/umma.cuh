@@ -54,8 +54,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t parity) {
   return done != 0;
 }
 
-__device__ inline bool mbar_wait(uint32_t addr, uint32_t parity) {
-  for (uint32_t i = 0; i < kTcWaitLimit; i++)
+// Polls the mbarrier phase at most `limit` times (0: gives up at once).
+__device__ inline bool mbar_wait(uint32_t addr, uint32_t parity, uint32_t limit = kTcWaitLimit) {
+  for (uint32_t i = 0; i < limit; i++)
     if (mbar_try_wait(addr, parity)) return true;
   return false;
 }

@@ -465,6 +465,11 @@ class Engine:
         special primes, ModUp from 8); same words."""
         check(_lib.load().fhe_engine_set_tensor_cores(self._h, int(mode)))
 
+    def set_tensor_core_wait_limit(self, limit: int) -> None:
+        """Diagnostics: polls per tensor-core MMA round before a kernel gives up and
+        flags an error for the next synchronize (0: at once; negative: default)."""
+        check(_lib.load().fhe_engine_set_tensor_core_wait_limit(self._h, int(limit)))
+
     def set_graphs(self, enable: bool) -> None:
         """CUDA-graph replay of bootstrap(ct, rk, ck, bootstrap_key) (default on)."""
         check(_lib.load().fhe_engine_set_graphs(self._h, int(enable)))

@@ -404,18 +404,21 @@ int fhe_switch_key(fhe_engine *engine, const fhe_data *ct, const fhe_data *key_s
                    fhe_data **out);
 
 /* Relinearize without allocating (no counterpart in the reference, which has no
- * device memory).  For callers that cannot call cudaMalloc while they run -- code
- * inside a CUDA graph capture, real-time loops with a fixed memory budget, hosts
- * whose allocator policy forbids device allocation after start-up.  Same words as
+ * device memory).  For callers that cannot call cudaMalloc while they run: an
+ * application whose own allocator owns the GPU's memory and gives libraries a fixed
+ * budget, a real-time loop that cannot take cudaMalloc's implicit device
+ * synchronisation or an out-of-memory failure in mid-run, or code running where
+ * CUDA allocation calls are not allowed (stream callbacks).  Same words as
  * fhe_relinearize; inputs and output are caller-owned device buffers on the
  * engine's device: ct [3][L][N] in NTT form at moduli_id, the key switching key
  * [key_polys][prime_count(key_moduli_id)][N] at key_moduli_id, out [2][L][N].
- * All temporaries come from one fixed 32 MiB device array per GPU, held until the
- * process exits; a call whose temporaries would not fit is rejected with
+ * All temporaries, the partition constants included (computed on the device), come
+ * from one fixed 32 MiB device array per GPU, held until the process exits; a call
+ * whose temporaries would not fit (N = 2^16 with many limbs) is rejected with
  * FHE_ERR_INVALID_ARGUMENT.  The first call on a device resolves that array's
  * address (cudaGetSymbolAddress) and should come before any stream capture.  All
- * calls share the array: calls that overlap on the GPU race and must be
- * serialised by the caller. */
+ * calls share the array and it keeps the last call's contents: calls that overlap
+ * on the GPU race and must be serialised by the caller. */
 int fhe_relinearize_noalloc(fhe_engine *engine, const int64_t *ct_device, int moduli_id,
                             const int64_t *key_device, int key_moduli_id, int key_polys,
                             int64_t *out_device);
@@ -434,6 +437,14 @@ enum {
   FHE_TENSOR_CORES_AUTO = 2
 };
 int fhe_engine_set_tensor_cores(fhe_engine *engine, int mode);
+/* Diagnostics (no reference counterpart): how many times each tensor-core kernel
+ * polls for an MMA round to complete before it gives up (0: at once; negative: the
+ * default, about 4 M polls).  A kernel that gives up still waits, with the default
+ * limit, for its MMAs to finish before it frees its tensor memory, leaves its
+ * outputs unspecified and sets the engine's error flag, which the next
+ * fhe_engine_synchronize reports as FHE_ERR_CUDA.  Applies to kernels launched
+ * afterwards (a CUDA graph captured earlier keeps its limit). */
+int fhe_engine_set_tensor_core_wait_limit(fhe_engine *engine, long long limit);
 /* A serving step with no reference counterpart: for every i, multiply a[i] by b[i]
  * with the relinearization key and rescale (fhe_multiply_relinearize_rescale), then
  * rotate the product with rotation_keys[i] (fhe_rotate).  out receives count new

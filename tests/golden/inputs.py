@@ -19,6 +19,7 @@ TIERS = {
     "bronze": (14, 1, 1),
     "silver": (15, 2, 1),
     "gold": (16, 4, 1),
+    "c10": (16, 10, 1),  # the headline key-switching set: 10 special primes, dnum = 3
     "platinum": (17, 6, 1),
     "bootstrap_gold": (16, 4, 2),
 }

@@ -8,8 +8,11 @@
    iNTT, tensor, relinearize, rescale and engine multiply+relinearize+rescale,
    stored as SHA-256 digests of the int64 limbs (full arrays for N <= 16).
 
-Needs the reference tree (default /root/reference, or $FHE_REFERENCE); the tests
-read only the committed JSON.  Usage: python tests/golden/make_golden.py
+Needs the reference tree ($FHE_REFERENCE, else the ``reference`` directory beside
+the repository); the tests read only the committed JSON.  Usage:
+``python tests/golden/make_golden.py`` (every fixture) or
+``python tests/golden/make_golden.py --headline`` (ref_ops_c10.json only: the
+reference_ops digests at N = 2^16 with 10 special primes).
 """
 from __future__ import annotations
 
@@ -27,7 +30,7 @@ sys.path.insert(0, HERE)
 
 from inputs import ROTATION_KEY_DELTAS, arith_inputs, codec_values, digest_doubles, digest_list, key_switch_inputs, TIERS, case_inputs, digest  # noqa: E402
 
-REF = os.environ.get("FHE_REFERENCE", "/root/reference")
+REF = os.environ.get("FHE_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference"))
 
 
 def _tests(text: str):
@@ -140,16 +143,21 @@ def key_switch_ops(e, seed, q, n, mid, K, a, rk):
     return res
 
 
-def reference_ops():
+REFERENCE_OPS_PLAN = [("pebble", [0, 1, 5]), ("sand", [2]), ("iron", [1]), ("bronze", [1, 3]),
+                      ("silver", [1]), ("gold", [5]), ("bootstrap_gold", [1])]
+# The headline key-switching configuration: N = 2^16 with 10 special primes.  Moduli
+# id 1 is the key-switching level (28 limbs, partitions [8, 10, 10]); id 2 has a
+# 7-limb first partition; id 5 has 24 limbs and partitions [4, 10, 10].
+HEADLINE_OPS_PLAN = [("c10", [1, 2, 5])]
+
+
+def reference_ops(plan=REFERENCE_OPS_PLAN, seed=1000, threads=1):
     from oracle import ref
 
     cases = []
-    plan = [("pebble", [0, 1, 5]), ("sand", [2]), ("iron", [1]), ("bronze", [1, 3]),
-            ("silver", [1]), ("gold", [5]), ("bootstrap_gold", [1])]
-    seed = 1000
     for tier, moduli_ids in plan:
         log_n, K, preset = TIERS[tier]
-        e = ref.Engine(log_n=log_n, special_prime_count=K, preset=preset)
+        e = ref.Engine(log_n=log_n, special_prime_count=K, preset=preset, threads=threads)
         q = e.tables()["q"]
         n = e.n
         for mid in moduli_ids:
@@ -463,7 +471,18 @@ def pipeline_cases():
     return cases
 
 
+def headline_ops():
+    """ref_ops_c10.json: the reference_ops digests at N = 2^16 with 10 special primes
+    (the benchmarked parameter set), on the reference's worker pool."""
+    return reference_ops(HEADLINE_OPS_PLAN, seed=3000, threads=os.cpu_count())
+
+
 def main():
+    if sys.argv[1:] == ["--headline"]:
+        cases = headline_ops()
+        with open(os.path.join(HERE, "ref_ops_c10.json"), "w") as f:
+            json.dump(cases, f, indent=1)
+        return
     with open(os.path.join(HERE, "ntt_kat.json"), "w") as f:
         json.dump(parse_ntt_kats(), f, indent=1)
     with open(os.path.join(HERE, "precomputed_kat.json"), "w") as f:

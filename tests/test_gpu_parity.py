@@ -15,11 +15,31 @@ NTT, RESCALED, SPECIAL = 2, 4, 16
 CASES = load_golden("ref_ops.json")
 
 
+HEADLINE_CASES = load_golden("ref_ops_c10.json")
+
+
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c['tier']}-m{c['moduli_id']}")
 def test_ops_match_recorded_reference(engines, case):
+    check_core_ops(engines(case["log_n"], case["special_prime_count"], case["preset"]), case)
+
+
+@pytest.mark.parametrize("mode", [1, 0], ids=["tensor-cores", "cuda-cores"])
+@pytest.mark.parametrize("case", HEADLINE_CASES, ids=lambda c: f"{c['tier']}-m{c['moduli_id']}")
+def test_headline_ops_match_recorded_reference(engines, case, mode):
+    """N = 2^16 with 10 special primes (dnum = 3, up to 10-limb partitions), against
+    the reference's own words, with both base conversions forced onto the INT8
+    tensor pipe and then onto the CUDA cores."""
+    e = engines(case["log_n"], case["special_prime_count"], case["preset"])
+    e.set_tensor_cores(mode)
+    try:
+        check_core_ops(e, case)
+    finally:
+        e.set_tensor_cores(2)
+
+
+def check_core_ops(e, case):
     from fhe_b200 import RELINEARIZATION_KEY
 
-    e = engines(case["log_n"], case["special_prime_count"], case["preset"])
     q = np.array(case["moduli"], dtype=np.uint64)
     assert e.moduli.tolist() == case["moduli"]
     mid = case["moduli_id"]

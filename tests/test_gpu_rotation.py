@@ -16,11 +16,31 @@ SCALE = 2.0 ** 40
 CASES = [c for c in load_golden("ref_ops.json") if "rotate_1" in c["digests"]]
 
 
+HEADLINE_CASES = load_golden("ref_ops_c10.json")
+
+
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c['tier']}-m{c['moduli_id']}")
 def test_key_switch_ops_match_recorded_reference(engines, case):
+    check_key_switch_ops(engines(case["log_n"], case["special_prime_count"], case["preset"]), case)
+
+
+@pytest.mark.parametrize("mode", [1, 0], ids=["tensor-cores", "cuda-cores"])
+@pytest.mark.parametrize("case", HEADLINE_CASES, ids=lambda c: f"{c['tier']}-m{c['moduli_id']}")
+def test_headline_key_switch_ops_match_recorded_reference(engines, case, mode):
+    """Rotations, conjugation, key switching, level down and the mixed-level multiply
+    at N = 2^16 with 10 special primes, against the reference's own words, with the
+    base conversions on the tensor pipe and then on the CUDA cores."""
+    e = engines(case["log_n"], case["special_prime_count"], case["preset"])
+    e.set_tensor_cores(mode)
+    try:
+        check_key_switch_ops(e, case)
+    finally:
+        e.set_tensor_cores(2)
+
+
+def check_key_switch_ops(e, case):
     from fhe_b200 import RELINEARIZATION_KEY, UNIT_PLAINTEXT
 
-    e = engines(case["log_n"], case["special_prime_count"], case["preset"])
     q = np.array(case["moduli"], dtype=np.uint64)
     assert e.moduli.tolist() == case["moduli"]
     mid, K, n = case["moduli_id"], case["special_prime_count"], e.coeff_count

@@ -82,6 +82,18 @@ def test_oracle_matches_recorded_reference_outputs(case):
         assert digest(arr) == case["digests"][name], name
 
 
+@pytest.mark.parametrize("case", load_golden("ref_ops_c10.json"), ids=lambda c: f"c10-m{c['moduli_id']}")
+def test_oracle_matches_reference_at_headline_config(case):
+    """Oracle vs the compiled reference at N = 2^16 with 10 special primes (dnum = 3,
+    partitions of up to 10 limbs): relinearization and the fused multiply chain."""
+    q = _chain(case)
+    ctx = oracle.Context(case["log_n"], q, case["special_prime_count"])
+    mid = case["moduli_id"]
+    a, b, ct3, key = case_inputs(case["seed"], q, ctx.n, mid, case["special_prime_count"])
+    assert digest(ctx.relinearize(mid, ct3, mid, key)) == case["digests"]["relinearize"]
+    assert digest(ctx.mult_relin_rescale(mid, a, b, mid, key)) == case["digests"]["mult_relin_rescale"]
+
+
 def _chain(case):
     return np.array(case["moduli"], dtype=np.uint64)
 
