@@ -17,6 +17,10 @@ relinearization key (operation time does not depend on the values).
           HBM copy bandwidth (MEASURED_PEAKS.json).
   cpu_baseline : the reference's own CPU implementation (oracle/_ref, all host
           threads) on a bounded sample of the same operation.
+  bootstrap : the other half of the headline metric, in the same run: ms per
+          bootstrap at N = 2^16 (bootstrap preset, 2^15 slots, medium 3-stage
+          bootstrap key, 8 ciphertexts per step), with precision bits, its own
+          e2e, per-family kernel ms, clock record and reference CPU baseline.
 
 Multi-GPU: replicas -- every rank runs the same per-GPU workload on its own GPU
 with no data exchange ("scaling": "weak"); torch.distributed is used only for the
@@ -144,7 +148,8 @@ def kernel_bytes(L: int, E: int, dnum: int, n: int) -> dict:
         "tensor_to_intt": (4 * L + 3 * L) * limb,           # 4 NTT polys in, 3 out
         "mixed_radix": 2 * L * limb,                        # digits of poly 2
         "mod_up_ntt": (L + dnum * E) * limb,                # digits in, extended out
-        "mod_up_ntt_tc": (L + dnum * E) * limb,
+        "mod_up_contract_tc": (L + dnum * E) * limb,        # digits in, extended out
+        "mod_up_ntt_tc": 2 * dnum * E * limb,               # extended limbs in and out
         "key_inner_product": (3 * dnum * E + 2 * E) * limb, # ext + 2 key polys, 2 out
         "mod_down_intt": 2 * 2 * E * limb,                  # 2 polys in and out
         "mod_down_epilogue": (2 * E + 2 * L + 2 * (L - 1)) * limb,
@@ -153,6 +158,59 @@ def kernel_bytes(L: int, E: int, dnum: int, n: int) -> dict:
 
 
 # ------------------------------------------------------------- reference arm --
+
+INT8_NOMINAL_OPS = 4.5e15  # B200 dense INT8 tensor throughput, nominal (no measured figure)
+
+
+def partition_sizes(L: int, K: int) -> list:
+    """Limbs of each key-switching partition at L limbs (ckks/parameters.cpp:334-360)."""
+    pc = (L + K - 1) // K
+    return [min(L, s + K) - max(0, s) for s in range(L - pc * K, L, K)]
+
+
+def pipe_figures(prof: dict, steps: int, pairs: int, n: int, L: int, K: int, sm_mhz, sms: int):
+    """What bounds the headline step: butterflies per SM per clock of the transform
+    families (their loaders and storers included) from the event-timed launches and
+    the SM clock sampled during the run, and the INT8 operations the two tensor-core
+    kernels issue per second against the nominal dense INT8 peak."""
+    E = L + K
+    dnum = (L + K - 1) // K
+    hz = (sm_mhz or 1965.0) * 1e6
+    log_n = n.bit_length() - 1
+    bfly_per_limb = (n // 2) * log_n
+    transforms = {"rescale_to_ntt": 4 * L, "tensor_to_intt": 3 * L, "mod_up_ntt_tc": dnum * E,
+                  "mod_down_intt": 2 * E}
+    integer = {}
+    for fam, limbs in transforms.items():
+        if fam in prof:
+            sec = prof[fam][1] / 1e3
+            integer[fam] = {"limb_transforms_per_pair": limbs,
+                            "butterflies_per_sm_per_clock":
+                                pairs * steps * limbs * bfly_per_limb / (sec * sms * hz)}
+    tiles = n // 128
+    kb_down = (9 * K + 31) // 32 * 32
+    issued = {
+        # 2 polys x ceil(L/8) rounds of 128 x 128 x kb per 128 coefficients
+        "mod_down_epilogue_tc": 2 * tiles * -(-L // 8) * 2 * 128 * 128 * kb_down,
+        "mod_up_contract_tc": sum(tiles * -(-E // 8) * 2 * 128 * 128 * ((8 * a + 31) // 32 * 32)
+                                  for a in partition_sizes(L, K)),
+    }
+    useful = {  # 64 byte-pair products per 64-bit multiply-accumulate
+        "mod_down_epilogue_tc": 2 * 64 * 2 * n * K * L,
+        "mod_up_contract_tc": 2 * 64 * n * sum(a * E for a in partition_sizes(L, K)),
+    }
+    tensor = {}
+    for fam, ops in issued.items():
+        if fam in prof:
+            cnt, ms = prof[fam]
+            sec = ms / cnt / 1e3
+            tensor[fam] = {"issued_int8_ops_per_launch": ops,
+                           "algorithmic_int8_ops_per_launch": useful[fam],
+                           "avg_launch_ms": ms / cnt, "issued_ops_per_s": ops / sec,
+                           "peak_ops_per_s": INT8_NOMINAL_OPS, "peak_source": "nominal",
+                           "frac": ops / sec / INT8_NOMINAL_OPS}
+    return integer, tensor
+
 
 def run_reference(args, rank: int):
     """The reference's own CPU implementation of the path (oracle/_ref), all host
@@ -212,10 +270,10 @@ def cpu_baseline_sample():
 
         if ref.available():
             threads = os.cpu_count() or 1
-            _, times = ref.bench_mult_relin_rescale(LOG_N, SPECIAL, -1, threads, 1, 3)
+            _, times = ref.bench_mult_relin_rescale(LOG_N, SPECIAL, -1, threads, 2, 10)
             ms = sum(times) / len(times)
             return {"value": 1000.0 / ms, "unit": "ct/s", "cores": threads, "kind": "reference",
-                    "sample": "3 HMult+relin+rescale ops (after 1 warm-up) through the reference "
+                    "sample": "10 HMult+relin+rescale ops (after 2 warm-up) through the reference "
                               "CKKSEngine with CPU_PARALLEL, keygen excluded"}
     except Exception as exc:  # the baseline must not sink the GPU line
         return {"value": None, "unit": "ct/s", "cores": 0, "kind": "reference",
@@ -312,20 +370,30 @@ def run_ntt_microbench(args, torch, np, rank, world, local, backend, stream):
 CONCURRENCY = 4  # worker streams of batch calls (the engine's default; --streams)
 
 
+BOOTSTRAP_BATCH = 8  # ciphertexts per step of the bootstrap measurement
+
+
 def run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream):
+    """The bootstrap workloads as their own bench line."""
+    line = bootstrap_measure(args, torch, np, rank, world, local, backend, stream,
+                             args.workload == "bootstrap", args.batch)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def bootstrap_measure(args, torch, np, rank, world, local, backend, stream, with_key, B):
     """Bootstrapping at N = 2^16 (bootstrap preset, 4 special primes, 2^15 complex
-    slots uniform in [-1, 1], 3 stages): each step bootstraps `batch` ciphertexts
-    encrypted at level 3.  Keys are made on the device before timing.  Workload
-    "bootstrap" uses a "medium" bootstrap key (hoisted baby-step giant-step
-    transforms); "bootstrap_rotation" the rotation key and small bootstrap key."""
+    slots uniform in [-1, 1], 3 stages): each step bootstraps B ciphertexts
+    encrypted at level 3.  Keys are made on the device before timing.  with_key: a
+    "medium" bootstrap key (hoisted baby-step giant-step transforms); otherwise the
+    rotation key and small bootstrap key.  Returns the bench line (every rank)."""
     from fhe_b200 import Engine
     from inputs import codec_values
 
-    with_key = args.workload == "bootstrap"
     eng = Engine(log_coeff_count=16, special_prime_count=4, scheme_preset=2)
     eng.set_stream(stream.cuda_stream)
     eng.set_concurrency(CONCURRENCY)
-    B = args.batch
     eng.seed([11 + rank, 22, 33, 44, 55, 66, 77, 88], [1, 2])
     sk = eng.create_secret_key()
     rk = eng.create_relinearization_key(sk)
@@ -382,14 +450,17 @@ def run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream):
     out_host = torch.empty(tuple(outs[0].download().shape), dtype=torch.int64).pin_memory()
     info = cts[0].info()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
     for _ in range(args.steps):
         ins = [eng.upload_from_pointer(h.data_ptr(), info["moduli_id"], 2, info["flag"],
                                        scale=float(info["scale"])) for h in host_ct]
         for o in step(ins):
             eng.download_to_pointer(o, out_host.data_ptr(), wait=False)
     eng.synchronize()  # the last results are in host memory
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / (args.steps * B)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = aggregate(e0.elapsed_time(e1), 0.0, world, backend)[0] / (args.steps * B)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -405,8 +476,7 @@ def run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream):
         except Exception as exc:
             cpu = {"value": None, "unit": "ms/bootstrap", "cores": 0, "kind": "reference",
                    "sample": f"failed: {exc}"}
-    if rank == 0:
-        print(json.dumps({
+    line = {
             "metric": "bootstrap ms at N=2^16 (2^15 slots, 3 stages)", "value": ms_per_bootstrap,
             "unit": "ms/bootstrap", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": elapsed_max / args.steps, "higher_is_better": False, "scaling": "weak",
@@ -427,9 +497,10 @@ def run_bootstrap_bench(args, torch, np, rank, world, local, backend, stream):
             "e2e": {"value": e2e_ms, "unit": "ms/bootstrap",
                     "h2d_bytes_per_step": int(sum(h.numel() * 8 for h in host_ct)),
                     "d2h_bytes_per_step": int(out_host.numel() * 8 * B)},
-            "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
+            "gpu_launches": launches, "clocks": clocks.summary()}
+    del outs, cts
     eng.close()
-    return 0
+    return line
 
 
 def run_batched_bench(args, torch, np, rank, world, local, backend, stream):
@@ -639,6 +710,8 @@ def main(argv=None):
                          "batched: --batch uneven HMult+rotate items per step (use 256); "
                          "plain: the N=2^14 pipeline from slot values to decoded slots")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-bootstrap", action="store_true",
+                    help="hmult: leave out the bootstrap measurement of the headline line")
     ap.add_argument("--streams", type=int, default=None,
                     help="worker streams of batch calls (1-8; default: the engine's 4)")
     args = ap.parse_args(argv)
@@ -776,7 +849,14 @@ def main(argv=None):
         tpath = os.path.join(HERE, "profiles", "traffic.json")
         if os.path.exists(tpath):
             traffic = json.load(open(tpath)).get(dominant)
+        integer, tensor = pipe_figures(prof, args.steps, B, n, L, SPECIAL, clocks.summary()["sm_mhz"],
+                                       torch.cuda.get_device_properties(0).multi_processor_count)
         roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
+                    "limiter": "integer instruction issue: every transform and Montgomery product "
+                               "is 64-bit integer arithmetic on the CUDA cores (integer_pipe); the "
+                               "HBM fraction and the INT8 tensor-pipe fraction (tensor_pipe) are "
+                               "both small",
+                    "integer_pipe": integer, "tensor_pipe": tensor,
                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                     "peak_source": peak_kind, "avg_launch_ms": avg_ms,
                     "algorithmic_bytes_per_launch": bytes_per.get(dominant),
@@ -795,6 +875,8 @@ def main(argv=None):
         cnt, fam_ms = p.get(fam, (0, 0.0))
         up = "mod_up_ntt_tc" if "mod_up_ntt_tc" in p else "mod_up_ntt"
         up_cnt, up_ms = p.get(up, (0, 0.0))
+        if up == "mod_up_ntt_tc":  # the tensor-pipe contraction and the NTT that follows it
+            up_ms += p.get("mod_up_contract_tc", (0, 0.0))[1]
         return {"value": form_value, "unit": "ct/s", "mod_down_kernel": fam,
                 "mod_down_avg_launch_ms": fam_ms / cnt if cnt else None,
                 "mod_down_ms_per_step": fam_ms / args.steps,
@@ -830,7 +912,7 @@ def main(argv=None):
     torch.cuda.synchronize()
     if backend:
         torch.distributed.barrier()
-    e_steps = max(1, min(args.steps, 5))
+    e_steps = args.steps
     s2, t2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s2.record(stream)
     for _ in range(e_steps):
@@ -841,6 +923,7 @@ def main(argv=None):
     e_elapsed, e_units = aggregate(s2.elapsed_time(t2), float(B * e_steps), world, backend)
     e2e_value = e_units / (e_elapsed / 1e3)
 
+    line = None
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -866,9 +949,17 @@ def main(argv=None):
             "gpu_launches": launches,
             "clocks": clocks.summary(),
         }
-        print(json.dumps(line), flush=True)
-    del pairs, rk
+    del pairs, pa, pb, rk
     eng.close()
+    # The other half of the headline metric: bootstrap ms (medium bootstrap key, 8
+    # ciphertexts per step), measured in the same run under its own clock record.
+    boot = None
+    if not args.no_bootstrap:
+        boot = bootstrap_measure(args, torch, np, rank, world, local, backend, stream, True,
+                                 BOOTSTRAP_BATCH)
+    if rank == 0:
+        line["bootstrap"] = boot
+        print(json.dumps(line), flush=True)
     if backend:
         torch.distributed.destroy_process_group()
     return 0

@@ -237,10 +237,13 @@ cudaError_t Engine::mod_up(const DevicePartitions &dp, int moduli_id, const int6
     return timed("mod_up_ntt", [&] {
       return launch_mod_up_ntt(tables_, dp, params.log_n, moduli_id, digits, ext, stream_);
     });
+  // Profiled as two families, so the tensor-pipe contraction's time is its own.
+  const cudaError_t e = timed("mod_up_contract_tc", [&] {
+    return launch_mod_up_contract_tc(tables_, dp, *tc, params.n, moduli_id, digits, ext,
+                                     tc_status(), stream_);
+  });
+  if (e != cudaSuccess) return e;
   return timed("mod_up_ntt_tc", [&] {
-    const cudaError_t e = launch_mod_up_contract_tc(tables_, dp, *tc, params.n, moduli_id, digits,
-                                                    ext, tc_status(), stream_);
-    if (e != cudaSuccess) return e;
     return launch_extended_ntt(tables_, dp, params.log_n, moduli_id, ext, stream_);
   });
 }
