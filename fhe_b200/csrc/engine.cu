@@ -186,8 +186,6 @@ const ModDownTcTables *Engine::mod_down_tc(int moduli_id) {
   ModDownTcTables tc;
   tc.b = upload_table(h.b);
   tc.c_r = upload_table(h.c_r);
-  tc.r40 = upload_table(h.r40);
-  tc.r80 = upload_table(h.r80);
   tc.rounds = h.rounds;
   tc.kb = h.kb;
   return &mod_down_tc_cache_.emplace(moduli_id, tc).first->second;
@@ -219,12 +217,11 @@ const ModUpTcTables *Engine::mod_up_tc(int moduli_id) {
   if (it != mod_up_tc_cache_.end()) return &it->second;
   std::vector<PartitionConstants> constants;
   for (const auto &pt : parts) constants.push_back(params.partition_constants(moduli_id, pt));
-  const ModUpTcHost h = make_mod_up_tc_tables(params.k, params.r_squared, moduli_id,
+  const ModUpTcHost h = make_mod_up_tc_tables(params.q, params.r_squared, moduli_id,
                                               params.chains(moduli_id, true), parts, constants);
   ModUpTcTables tc;
   tc.b = upload_table(h.b);
   tc.b_offset = upload_table(h.b_offset);
-  tc.c_k = upload_table(h.c_k);
   tc.rounds = h.rounds;
   return &mod_up_tc_cache_.emplace(moduli_id, tc).first->second;
 }

@@ -187,10 +187,12 @@ __global__ void mixed_radix_kernel(PrimeTables t, DevicePartitions dp, int n, in
 // ModUp contraction (core_key_switch.cpp:92-106): extended limb j of partition p
 // is the chain acc = guard(REDC(d_i c_ij) + acc, 2q) over the partition's digits
 // (c_0j = R^2 mod q_j).  A thread owns one coefficient of one partition, keeps its
-// alpha digits in registers and walks all extended limbs.  The chain is evaluated as
-// one lazy sum (RedcSum) when every digit is in [0, 2^61), which holds for all
-// digits produced from canonical inputs, and term by term otherwise; both give the
-// same word.
+// alpha digits in registers and walks all extended limbs.  The extended limbs feed
+// only value-only consumers (the forward NTT in Harvey's form, the key inner
+// product, ModDown's reduced inverse transform), so only the chain's value modulo
+// q_j matters: when every digit is in [0, 2^61), which holds for all digits produced
+// from canonical inputs, sum_i d_i c_ij is accumulated exactly and reduced by one
+// REDC (WideSum) to a word in [0, 2q); otherwise the chain runs term by term.
 constexpr int kContractChunk = 8;  // extended limbs per thread
 
 template <int A>
@@ -220,28 +222,25 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int j0 = j_begin; j0 < j_begin + kContractChunk; j0 += kLanes) {
       if (j0 >= E) break;
-      RedcSum sum[kLanes];
-      uint64_t kl[kLanes];
+      WideSum sum[kLanes];
       int jl[kLanes];
 #pragma unroll
       for (int l = 0; l < kLanes; l++) {
         jl[l] = j0 + l < E ? j0 + l : E - 1;
-        kl[l] = t.k[moduli_id + jl[l]];
-        sum[l].add(static_cast<uint64_t>(d[0]), static_cast<uint64_t>(t.r_squared[moduli_id + jl[l]]),
-                   kl[l]);
+        sum[l].add(static_cast<uint64_t>(d[0]), static_cast<uint64_t>(t.r_squared[moduli_id + jl[l]]));
       }
 #pragma unroll
       for (int i = 1; i < A; i++) {
 #pragma unroll
         for (int l = 0; l < kLanes; l++)
-          sum[l].add(static_cast<uint64_t>(d[i]), static_cast<uint64_t>(cst[(i - 1) * E + jl[l]]), kl[l]);
+          sum[l].add(static_cast<uint64_t>(d[i]), static_cast<uint64_t>(cst[(i - 1) * E + jl[l]]));
       }
 #pragma unroll
       for (int l = 0; l < kLanes; l++) {
         if (j0 + l < E) {
           const int prime = moduli_id + jl[l];
           const uint64_t q = t.q[prime];
-          out[static_cast<long long>(jl[l]) * n] = sum[l].reduce(q, q << 1, t.inv_2q[prime]);
+          out[static_cast<long long>(jl[l]) * n] = sum[l].reduce(q, t.k[prime], q << 1, t.inv_2q[prime]);
         }
       }
     }
@@ -260,9 +259,12 @@ __global__ void __launch_bounds__(256)
 
 // ------------------------------------------------------ key inner product --
 
-// With two or more partitions the reference chain (mont_mult, then mont_mult_add
-// and reduce_2q_to_q per further partition) equals (sum t_p) mod q; it is evaluated
-// as a lazy sum when every operand is in [0, 2^61) and term by term otherwise.
+// The reference chain (mont_mult, then mont_mult_add and reduce_2q_to_q per further
+// partition) has the value sum_p REDC(e_p k_p) modulo q.  Its consumers are
+// value-only (ModDown's inverse transform reduces every word; the rotation's b*P
+// term and the bootstrap's NTT-form rotations and diagonal sums end in ModDown), so
+// with every operand in [0, 2^61) the sum is evaluated exactly and reduced to a word
+// in [0, q); otherwise the chain runs term by term.
 __global__ void key_inner_product_kernel(PrimeTables t, DevicePartitions dp, int n, int moduli_id,
                                          const int64_t *ext, const int64_t *key, int key_primes,
                                          int view_offset, int64_t *acc) {
@@ -275,8 +277,12 @@ __global__ void key_inner_product_kernel(PrimeTables t, DevicePartitions dp, int
     const int prime = moduli_id + j;
     const uint64_t q = t.q[prime], k = t.k[prime];
     const int64_t qs = static_cast<int64_t>(q), q2 = qs << 1;
-    bool fast = dp.count >= 2;
-    RedcSum s0, s1;
+    // Up to 16 partitions: one REDC of the exact sum; more: the lazy sum of the terms'
+    // own REDCs (RedcSum), whose 128-bit accumulators cannot overflow.
+    const bool wide = dp.count <= 16;
+    bool fast = true;
+    WideSum w0, w1;
+    RedcSum r0, r1;
     for (int p = 0; p < dp.count && fast; p++) {
       const int64_t e = ext[static_cast<long long>(p) * total + i];
       const int kidx = dp.key_index[p];
@@ -286,12 +292,17 @@ __global__ void key_inner_product_kernel(PrimeTables t, DevicePartitions dp, int
         fast = false;
         break;
       }
-      s0.add(static_cast<uint64_t>(e), static_cast<uint64_t>(k0), k);
-      s1.add(static_cast<uint64_t>(e), static_cast<uint64_t>(k1), k);
+      if (wide) {
+        w0.add(static_cast<uint64_t>(e), static_cast<uint64_t>(k0));
+        w1.add(static_cast<uint64_t>(e), static_cast<uint64_t>(k1));
+      } else {
+        r0.add(static_cast<uint64_t>(e), static_cast<uint64_t>(k0), k);
+        r1.add(static_cast<uint64_t>(e), static_cast<uint64_t>(k1), k);
+      }
     }
     if (fast) {
-      acc[i] = s0.reduce(q, q, t.inv_q[prime]);
-      acc[total + i] = s1.reduce(q, q, t.inv_q[prime]);
+      acc[i] = wide ? w0.reduce(q, k, q, t.inv_q[prime]) : r0.reduce(q, q, t.inv_q[prime]);
+      acc[total + i] = wide ? w1.reduce(q, k, q, t.inv_q[prime]) : r1.reduce(q, q, t.inv_q[prime]);
       continue;
     }
     int64_t x0 = 0, x1 = 0;

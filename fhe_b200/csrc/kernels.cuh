@@ -118,10 +118,8 @@ cudaError_t launch_mod_down_epilogue_ops(const PrimeTables &t, const KeySwitchTa
 // of the divisor sequence d_s, whose sum runs on the INT8 tensor pipe with 8-bit
 // limbs of d_s and of the constants (S32 accumulation, exact).
 struct ModDownTcTables {
-  const uint8_t *b = nullptr;   // [rounds][256 columns][kb bytes], UMMA K-major core matrices
+  const uint8_t *b = nullptr;   // [rounds][128 columns][kb bytes], UMMA K-major core matrices
   const int64_t *c_r = nullptr; // [L] prod_s pinv_s * R mod q_j (x_j's Montgomery factor)
-  const int64_t *r40 = nullptr; // [L] 2^40 * R mod q_j
-  const int64_t *r80 = nullptr; // [L] 2^80 * R mod q_j
   int rounds = 0;               // ceil(L / 16) MMA rounds of 16 target limbs
   int kb = 0;                   // A row bytes: 9 K rounded up to 32
 };
@@ -149,7 +147,7 @@ bool mod_down_tc_supported(int special_count, int limbs, int n);
 // chain and the p^-1 R constants per division step ([K][prime]).
 struct ModDownTcHost {
   std::vector<uint8_t> b;
-  std::vector<int64_t> c_r, r40, r80;
+  std::vector<int64_t> c_r;
   int rounds = 0;
   int kb = 0;
 };
@@ -158,24 +156,22 @@ ModDownTcHost make_mod_down_tc_tables(const std::vector<uint64_t> &q,
                                       int moduli_id, int limbs, int special_count);
 
 // Constants of the tensor-core ModUp contraction at one moduli id (modup_tc.cu): per
-// partition, the bytes of its constants C_ij (i < alpha, j < extended limbs) as the
-// UMMA B operand, and C_ij * k_j mod 2^62 for the per-term Montgomery quotients.
+// partition, the bytes of C_ij 2^(8a) mod q_j (i < alpha, byte a < 8, j < extended
+// limbs) as the UMMA B operand, 16 targets per MMA round.
 struct ModUpTcTables {
   const uint8_t *b = nullptr;           // per partition: [rounds][128 columns][kb bytes]
   const long long *b_offset = nullptr;  // [partitions] byte offset of each partition's B
-  const int64_t *c_k = nullptr;         // [partitions][16][extended]
-  int rounds = 0;                       // ceil(extended / 8)
+  int rounds = 0;                       // ceil(extended / 16)
 };
 struct ModUpTcHost {
   std::vector<uint8_t> b;
   std::vector<long long> b_offset;
-  std::vector<int64_t> c_k;
   int rounds = 0;
 };
 struct Partition;
 struct PartitionConstants;
 bool mod_up_tc_supported(int max_size, int n);
-ModUpTcHost make_mod_up_tc_tables(const std::vector<uint64_t> &k,
+ModUpTcHost make_mod_up_tc_tables(const std::vector<uint64_t> &q,
                                   const std::vector<int64_t> &r_squared, int moduli_id,
                                   int extended, const std::vector<Partition> &parts,
                                   const std::vector<PartitionConstants> &constants);

@@ -151,6 +151,30 @@ struct RedcSum {
   }
 };
 
+// sum_i a_i b_i accumulated exactly in 128 bits and reduced by one REDC of the whole
+// sum: the value is that of the chain of REDC(a_i b_i) terms modulo q, but not its
+// representative.  For sums whose consumers only use the value modulo q (ModUp's
+// extended limbs feed value-only transforms).  Valid for a_i, b_i < 2^61 and at most
+// 16 terms: the sum is below 2^126 and its REDC below (terms / 2 + 1) q.
+struct WideSum {
+  uint64_t lo = 0, hi = 0;
+  FHE_HD void add(uint64_t a, uint64_t b) {
+    uint64_t l, h;
+    mul_wide(a, b, l, h);
+    const uint64_t nl = lo + l;
+    hi += h + (nl < lo ? 1 : 0);
+    lo = nl;
+  }
+  // REDC(sum) reduced modulo m (q or 2q); inv_m ~ 1/m.
+  FHE_HD int64_t reduce(uint64_t q, uint64_t k, uint64_t m, double inv_m) const {
+    RedcSum r;
+    r.p_lo = lo;
+    r.p_hi = hi;
+    r.s_lo = (lo * k) & kMontMask;
+    return r.reduce(q, m, inv_m);
+  }
+};
+
 // One word of rescale_once_ (core_rescale.cpp:5-25): (x_j - x_0) reduced, times
 // q_0^-1 R, plus the rounder of x_0, reduced to [0, q).
 template <bool LAZY = false>

@@ -10,16 +10,18 @@
 //   * A (128 coefficients x kb bytes): the 8 little-endian bytes of every d_s as an
 //     unsigned word, then one byte [d_s < 0] per divisor (a negative d_s read as
 //     unsigned is d_s + 2^64, which the sign byte takes back);
-//   * B (per moduli id, built on the host): for target j and byte shift h, the byte
-//     h - u of w'_sj = -prod_{t>=s} pinv_t mod q_j against byte u of d_s, and byte h
-//     of z_sj = -2^64 w'_sj mod q_j against the sign byte of d_s;
-//   * D (tensor memory, S32): 16 columns per target, column h = the exact partial
-//     sum at byte shift h (h < 15; each below 2^23); one MMA round covers 8 targets,
-//     so a CTA holds 128 tensor-memory columns and the B of one round, and four
-//     CTAs fit on an SM.
-// The epilogue folds the partial sums into three words below 2^56 (shifts 0-4,
-// 5-9 and 10-14), scales the upper two by 2^40 and 2^80 and x_j by prod pinv with
-// one Montgomery product each, and reduces the total (below 2^63) to [0, q_j).
+//   * B (per moduli id, built on the host): for target j, the 8 bytes of
+//     e_saj = w'_sj 2^(8a) R mod q_j against byte a of d_s, where
+//     w'_sj = -prod_{t>=s} pinv_t mod q_j, and of z_sj = -2^64 w'_sj R mod q_j
+//     against the sign byte of d_s;
+//   * D (tensor memory, S32): 8 columns per target, column b = the exact partial sum
+//     of byte b of the constants (each below 2^24), so X_j = sum_b D_b 2^(8b) is
+//     congruent to R sum_s d_s w'_sj and below 2^81; one MMA round covers 16
+//     targets, so a CTA holds 128 tensor-memory columns and the B of one round, and
+//     four CTAs fit on an SM.
+// The epilogue folds the 8 partial sums into a 128-bit word, takes one REDC of it
+// (a word below q_j + 2^19), adds x_j prod pinv (one Montgomery product) and
+// reduces the total (below 4 q_j) to [0, q_j).
 // The divisor triangle (K(K-1)/2 divisions per coefficient) stays on the CUDA
 // cores, as in the CUDA-core form.
 #include <cstring>
@@ -98,7 +100,7 @@ __global__ void __launch_bounds__(kTcThreads, K <= 10 && K != 7 ? 4 : (K <= 13 ?
   const uint32_t tmem = tmem_base;
   const uint32_t bar = smem_addr(&mbar);
 
-  // 3. One MMA round per 8 targets; each thread folds 4 targets of its coefficient.
+  // 3. One MMA round per 16 targets; each thread folds 8 targets of its coefficient.
   const int lane_base = (warp & 3) * 32;
   const int row = lane_base + lane;
   const int half = warp >> 2;
@@ -122,26 +124,29 @@ __global__ void __launch_bounds__(kTcThreads, K <= 10 && K != 7 ? 4 : (K <= 13 ?
     ok = __syncthreads_and(mbar_wait(bar, round & 1, status.wait_limit)) != 0;
     if (!ok) break;
     tc_fence_after();
-    for (int jl = half * (kTcTargets / 2); jl < (half + 1) * (kTcTargets / 2); jl++) {
-      const int j = round * kTcTargets + jl;
-      if (j >= L) break;  // uniform across the warp
+    // Each warpgroup folds 8 of the round's 16 targets, two per tensor-memory load.
+    for (int jp = half * (kTcTargets / 2); jp < (half + 1) * (kTcTargets / 2); jp += 2) {
+      const int j0 = round * kTcTargets + jp;
+      if (j0 >= L) break;  // uniform across the warp
       uint32_t d[16];
-      tmem_load16(tmem + (static_cast<uint32_t>(lane_base) << 16) + jl * 16, d);
-      const int prime = moduli_id + j;
-      const uint64_t q = t.q[prime], kq = t.k[prime];
-      const uint64_t c0 = fold5(d), c1 = fold5(d + 5), c2 = fold5(d + 10);
-      const int64_t xj = x[static_cast<long long>(j) * n + row];
-      const uint64_t v = c0 + static_cast<uint64_t>(mont_mult(static_cast<int64_t>(c1), tc.r40[j], q, kq)) +
-                         static_cast<uint64_t>(mont_mult(static_cast<int64_t>(c2), tc.r80[j], q, kq)) +
-                         static_cast<uint64_t>(mont_mult(xj, tc.c_r[j], q, kq));
-      const uint64_t est = static_cast<uint64_t>(static_cast<double>(v) * t.inv_q[prime]);
-      int64_t r = static_cast<int64_t>(v - est * q);
-      const int64_t qs = static_cast<int64_t>(q);
-      if (r < 0) r += qs;
-      if (r < 0) r += qs;
-      if (r >= qs) r -= qs;
-      if (r >= qs) r -= qs;
-      divided[j * kTcCoeffs + row] = r;
+      tmem_load16(tmem + (static_cast<uint32_t>(lane_base) << 16) + jp * 8, d);
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int j = j0 + h;
+        if (j >= L) break;  // uniform across the warp
+        const int prime = moduli_id + j;
+        const uint64_t q = t.q[prime], kq = t.k[prime];
+        uint64_t lo, hi;
+        fold8(d + 8 * h, lo, hi);
+        const int64_t xj = x[static_cast<long long>(j) * n + row];
+        // REDC(X) < q + 2^19; x_j is the reduced inverse transform's word in [0, q).
+        const uint64_t v = static_cast<uint64_t>(redc_wide(lo, hi, q, kq)) +
+                           static_cast<uint64_t>(mont_mult_small(static_cast<uint64_t>(xj),
+                                                                 static_cast<uint64_t>(tc.c_r[j]), q, kq));
+        uint64_t r = v >= (q << 1) ? v - (q << 1) : v;
+        r = r >= q ? r - q : r;
+        divided[j * kTcCoeffs + row] = static_cast<int64_t>(r);
+      }
     }
     tc_fence_before();
     __syncthreads();
@@ -200,8 +205,6 @@ ModDownTcHost make_mod_down_tc_tables(const std::vector<uint64_t> &q,
   h.rounds = (L + kTcTargets - 1) / kTcTargets;
   h.b.assign(static_cast<size_t>(h.rounds) * kTcColumns * h.kb, 0);
   h.c_r.resize(L);
-  h.r40.resize(L);
-  h.r80.resize(L);
   for (int j = 0; j < L; j++) {
     const int prime = moduli_id + j;
     const uint64_t m = q[prime];
@@ -215,23 +218,20 @@ ModDownTcHost make_mod_down_tc_tables(const std::vector<uint64_t> &q,
       w[s] = prod;
     }
     h.c_r[j] = static_cast<int64_t>(mul_mod(prod, r, m));
-    h.r40[j] = static_cast<int64_t>(pow_mod(2, 40 + 62, m));
-    h.r80[j] = static_cast<int64_t>(pow_mod(2, 80 + 62, m));
     const uint64_t two64 = static_cast<uint64_t>((static_cast<u128>(1) << 64) % m);
     const int round = j / kTcTargets, jl = j % kTcTargets;
     uint8_t *b = h.b.data() + static_cast<size_t>(round) * kTcColumns * h.kb;
     for (int s = 0; s < K; s++) {
-      const uint64_t wn = (m - w[s]) % m;
-      const uint64_t z = (m - mul_mod(two64, wn, m)) % m;
-      for (int sh = 0; sh < 15; sh++) {
-        const int col = jl * 16 + sh;
-        for (int u = 0; u < 8; u++) {
-          const int v = sh - u;
-          if (v < 0 || v >= 8) continue;
-          b[core_offset(col, s * 8 + u, kTcColumns)] = static_cast<uint8_t>(wn >> (8 * v));
-        }
-        if (sh < 8) b[core_offset(col, 8 * K + s, kTcColumns)] = static_cast<uint8_t>(z >> (8 * sh));
+      const uint64_t wn = mul_mod((m - w[s]) % m, r, m);  // w'_sj R
+      const uint64_t z = (m - mul_mod(two64, wn, m)) % m;  // -2^64 w'_sj R
+      uint64_t e = wn;  // w'_sj 2^(8a) R for a = 0, 1, ...
+      for (int a = 0; a < 8; a++) {
+        for (int bb = 0; bb < 8; bb++)
+          b[core_offset(jl * 8 + bb, s * 8 + a, kTcColumns)] = static_cast<uint8_t>(e >> (8 * bb));
+        e = static_cast<uint64_t>((static_cast<u128>(e) << 8) % m);
       }
+      for (int bb = 0; bb < 8; bb++)
+        b[core_offset(jl * 8 + bb, 8 * K + s, kTcColumns)] = static_cast<uint8_t>(z >> (8 * bb));
     }
   }
   return h;

@@ -1,20 +1,21 @@
 // Tensor-core ModUp contraction (tcgen05.mma kind::i8 on sm_100a).
 //
 // ModUp raises each partition's mixed-radix digits d_0 .. d_{a-1} to every limb j of
-// the extended chain (core_key_switch.cpp:92-108):
-//   t_j = sum_i REDC(d_i * C_ij)  chained with guard(., 2q),
-// C_0j = R^2 and C_ij the partition's product constants.  With every d_i below 2^61
-// the chain equals (sum_i d_i C_ij + q_j sum_i s_ij) / 2^62 mod 2q_j, where s_ij =
-// d_i C_ij k_j mod 2^62 is the term's own Montgomery quotient; the result feeds the
-// lazy NTT, so this exact representative is what must be reproduced.  Here:
-//   * sum_i d_i C_ij runs on the INT8 tensor pipe: A holds the 8 little-endian bytes
-//     of every digit, B (per moduli id and partition, built on the host) the bytes
-//     of C_ij at every byte shift, D the 15 exact partial sums per (coefficient,
-//     target) (each below 2^23), folded into a 128-bit word;
-//   * each s_ij is one low 64-bit product with C_ij k_j mod 2^62 (precomputed) on
-//     the CUDA cores, and the sum is reduced exactly as the CUDA-core form does.
+// the extended chain (core_key_switch.cpp:92-108): the reference's chain of
+// REDC(d_i * C_ij) terms (C_0j = R^2, C_ij the partition's product constants) has
+// the value sum_i d_i C_ij R^-1 modulo q_j.  The extended limbs feed only
+// value-only consumers (the forward NTT in Harvey's form, the key inner product,
+// ModDown's reduced inverse transform), so any representative in [0, 2q_j) of that
+// value gives the reference's final words.  Here:
+//   * A holds the 8 little-endian bytes d_i[a] of every digit (K = 8a bytes);
+//   * B (per moduli id and partition, built on the host) holds, for 16 targets per
+//     MMA round, the 8 bytes of e_iaj = C_ij 2^(8a) mod q_j, so the 8 exact partial
+//     sums D_b = sum_(i,a) d_i[a] e_iaj[b] (each below 2^23) give
+//     X_j = sum_b D_b 2^(8b) = sum_(i,a) d_i[a] e_iaj == sum_i d_i C_ij (mod q_j),
+//     with X_j below 2^80;
+//   * one REDC of X_j on the CUDA cores leaves a word below q_j + 2^18 < 2 q_j.
 // A coefficient with a digit of 2^61 or more takes the reference's chain term by
-// term.  Same words as mod_up_contract_kernel.
+// term.  The values equal mod_up_contract_kernel's.
 #include "kernels.cuh"
 #include "modarith.cuh"
 #include "params.hpp"
@@ -27,7 +28,6 @@ namespace {
 using namespace umma;
 
 constexpr int digit_row_bytes(int A) { return (8 * A + 31) / 32 * 32; }
-
 template <int A>
 __global__ void __launch_bounds__(kTcThreads, 4)
     mod_up_tc_kernel(PrimeTables t, DevicePartitions dp, ModUpTcTables tc, int n, int moduli_id,
@@ -83,7 +83,6 @@ __global__ void __launch_bounds__(kTcThreads, 4)
   const int row = lane_base + lane;
   const int half = warp >> 2;
   const int64_t *cst = dp.product_r_squared + static_cast<long long>(p) * 16 * E;
-  const int64_t *ck = tc.c_k + static_cast<long long>(p) * 16 * E;
   const uint8_t *bp = tc.b + tc.b_offset[p];
   int64_t *out = ext + static_cast<long long>(p) * E * n + coeff0 + row;
   bool ok = true;
@@ -104,36 +103,31 @@ __global__ void __launch_bounds__(kTcThreads, 4)
     ok = __syncthreads_and(mbar_wait(bar, round & 1, status.wait_limit)) != 0;
     if (!ok) break;
     tc_fence_after();
-    for (int jl = half * (kTcTargets / 2); jl < (half + 1) * (kTcTargets / 2); jl++) {
-      const int j = round * kTcTargets + jl;
-      if (j >= E) break;  // uniform across the warp
+    // Each warpgroup folds 8 of the round's 16 targets, two per tensor-memory load.
+    for (int jp = half * (kTcTargets / 2); jp < (half + 1) * (kTcTargets / 2); jp += 2) {
+      const int j0 = round * kTcTargets + jp;
+      if (j0 >= E) break;  // uniform across the warp
       uint32_t d[16];
-      tmem_load16(tmem + (static_cast<uint32_t>(lane_base) << 16) + jl * 16, d);
-      const int prime = moduli_id + j;
-      const uint64_t q = t.q[prime], kq = t.k[prime];
-      if (fast[row]) {
-        const uint64_t c0 = fold5(d), c1 = fold5(d + 5), c2 = fold5(d + 10);
-        RedcSum sum;
-        sum.p_lo = c0 + (c1 << 40);
-        sum.p_hi = (c1 >> 24) + (c2 << 16) + (sum.p_lo < c0 ? 1 : 0);
+      tmem_load16(tmem + (static_cast<uint32_t>(lane_base) << 16) + jp * 8, d);
 #pragma unroll
-        for (int i = 0; i < A; i++) {
-          const uint64_t s = (static_cast<uint64_t>(sd[i * kTcCoeffs + row]) *
-                              static_cast<uint64_t>(ck[i * E + j])) &
-                             kMontMask;
-          const uint64_t ns = sum.s_lo + s;
-          sum.s_hi += ns < sum.s_lo ? 1 : 0;
-          sum.s_lo = ns;
+      for (int h = 0; h < 2; h++) {
+        const int j = j0 + h;
+        if (j >= E) break;  // uniform across the warp
+        const int prime = moduli_id + j;
+        const uint64_t q = t.q[prime], kq = t.k[prime];
+        if (fast[row]) {
+          uint64_t lo, hi;
+          fold8(d + 8 * h, lo, hi);
+          out[static_cast<long long>(j) * n] = redc_wide(lo, hi, q, kq);
+        } else {
+          // The reference's chain term by term (mod_up_contract_kernel's slow path).
+          const int64_t q2 = static_cast<int64_t>(q << 1);
+          int64_t v = mont_mult(sd[row], t.r_squared[prime], q, kq);
+#pragma unroll
+          for (int i = 1; i < A; i++)
+            v = guard(mont_mult(sd[i * kTcCoeffs + row], cst[(i - 1) * E + j], q, kq) + v, q2);
+          out[static_cast<long long>(j) * n] = v;
         }
-        out[static_cast<long long>(j) * n] = sum.reduce(q, q << 1, t.inv_2q[prime]);
-      } else {
-        // The reference's chain term by term (mod_up_contract_kernel's slow path).
-        const int64_t q2 = static_cast<int64_t>(q << 1);
-        int64_t v = mont_mult(sd[row], t.r_squared[prime], q, kq);
-#pragma unroll
-        for (int i = 1; i < A; i++)
-          v = guard(mont_mult(sd[i * kTcCoeffs + row], cst[(i - 1) * E + j], q, kq) + v, q2);
-        out[static_cast<long long>(j) * n] = v;
       }
     }
     tc_fence_before();
@@ -161,14 +155,14 @@ bool mod_up_tc_supported(int max_size, int n) {
   return max_size >= 1 && max_size <= 16 && n >= kTcCoeffs && n % kTcCoeffs == 0;
 }
 
-ModUpTcHost make_mod_up_tc_tables(const std::vector<uint64_t> &k,
+ModUpTcHost make_mod_up_tc_tables(const std::vector<uint64_t> &q,
                                   const std::vector<int64_t> &r_squared, int moduli_id,
                                   int extended, const std::vector<Partition> &parts,
                                   const std::vector<PartitionConstants> &constants) {
+  using u128 = unsigned __int128;
   ModUpTcHost h;
   const int E = extended;
   h.rounds = (E + kTcTargets - 1) / kTcTargets;
-  h.c_k.assign(parts.size() * 16 * static_cast<size_t>(E), 0);
   for (size_t p = 0; p < parts.size(); p++) {
     const int A = parts[p].size;
     const int kb = digit_row_bytes(A);
@@ -176,20 +170,19 @@ ModUpTcHost make_mod_up_tc_tables(const std::vector<uint64_t> &k,
     h.b.resize(h.b.size() + static_cast<size_t>(h.rounds) * kTcColumns * kb, 0);
     uint8_t *b = h.b.data() + h.b_offset.back();
     for (int j = 0; j < E; j++) {
-      const int prime = moduli_id + j;
+      const uint64_t qj = q[moduli_id + j];
       uint8_t *round = b + static_cast<size_t>(j / kTcTargets) * kTcColumns * kb;
       const int jl = j % kTcTargets;
       for (int i = 0; i < A; i++) {
-        const uint64_t c = i == 0 ? static_cast<uint64_t>(r_squared[prime])
+        const uint64_t c = i == 0 ? static_cast<uint64_t>(r_squared[moduli_id + j])
                                   : static_cast<uint64_t>(
                                         constants[p].product_r_squared[static_cast<size_t>(i - 1) * E + j]);
-        h.c_k[(p * 16 + i) * static_cast<size_t>(E) + j] = static_cast<int64_t>((c * k[prime]) & kMontMask);
-        for (int sh = 0; sh < 15; sh++)
-          for (int u = 0; u < 8; u++) {
-            const int v = sh - u;
-            if (v < 0 || v >= 8) continue;
-            round[core_offset(jl * 16 + sh, i * 8 + u, kTcColumns)] = static_cast<uint8_t>(c >> (8 * v));
-          }
+        uint64_t e = c % qj;  // C_ij 2^(8a) mod q_j for a = 0, 1, ...
+        for (int a = 0; a < 8; a++) {
+          for (int bb = 0; bb < 8; bb++)
+            round[core_offset(jl * 8 + bb, i * 8 + a, kTcColumns)] = static_cast<uint8_t>(e >> (8 * bb));
+          e = static_cast<uint64_t>((static_cast<u128>(e) << 8) % qj);
+        }
       }
     }
   }

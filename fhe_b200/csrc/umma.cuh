@@ -13,11 +13,11 @@ namespace fhe_b200 {
 namespace umma {
 
 // The shape both contractions use: a CTA owns 128 coefficients (the MMA's M and the
-// tensor-memory lanes) with two warpgroups; one MMA round covers 8 target limbs x 16
-// byte shifts = 128 columns (the MMA's N and the tensor-memory columns).
+// tensor-memory lanes) with two warpgroups; one MMA round covers 16 target limbs x 8
+// byte columns = 128 columns (the MMA's N and the tensor-memory columns).
 constexpr int kTcCoeffs = 128;
 constexpr int kTcThreads = 256;  // warp w reads tensor-memory lanes 32 (w % 4) ...
-constexpr int kTcTargets = 8;
+constexpr int kTcTargets = 16;
 constexpr int kTcColumns = 128;
 constexpr uint32_t kTcWaitLimit = 1u << 22;
 // Instruction descriptor of tcgen05.mma kind::i8: U8 x U8 -> S32, both K-major.
@@ -128,11 +128,22 @@ __device__ __forceinline__ void mma_round(uint32_t tmem, const uint8_t *a, const
   }
 }
 
-// Five partial sums (each below 2^23) at byte shifts 0, 8, ..., 32: below 2^56.
-__device__ __forceinline__ uint64_t fold5(const uint32_t *d) {
-  return static_cast<uint64_t>(d[0]) + (static_cast<uint64_t>(d[1]) << 8) +
-         (static_cast<uint64_t>(d[2]) << 16) + (static_cast<uint64_t>(d[3]) << 24) +
-         (static_cast<uint64_t>(d[4]) << 32);
+// X = sum_b D_b 2^(8b) of 8 partial sums below 2^24 (byte columns 0-7), as a
+// 128-bit word below 2^81.
+__device__ __forceinline__ void fold8(const uint32_t *dv, uint64_t &lo, uint64_t &hi) {
+  const uint64_t low = static_cast<uint64_t>(dv[0]) + (static_cast<uint64_t>(dv[1]) << 8) +
+                       (static_cast<uint64_t>(dv[2]) << 16) + (static_cast<uint64_t>(dv[3]) << 24) +
+                       (static_cast<uint64_t>(dv[4]) << 32);  // below 2^57
+  const uint64_t a5 = static_cast<uint64_t>(dv[5]) << 40;     // below 2^64
+  const uint64_t a6 = static_cast<uint64_t>(dv[6]) << 48, a7 = static_cast<uint64_t>(dv[7]) << 56;
+  uint64_t l = low + a5;
+  uint64_t carry = l < low ? 1 : 0;
+  uint64_t l2 = l + a6;
+  carry += l2 < l ? 1 : 0;
+  l = l2 + a7;
+  carry += l < l2 ? 1 : 0;
+  lo = l;
+  hi = (static_cast<uint64_t>(dv[6]) >> 16) + (static_cast<uint64_t>(dv[7]) >> 8) + carry;
 }
 
 }  // namespace umma

@@ -789,6 +789,7 @@ class GpuCKKSEngine : public AbstractEngine {
   // ---- long texts, unit by unit
 
   Plaintext *encode_values(const double *re, const double *im, int count, int level) {
+    if (level < 0) level = info_.max_level;  // the reference's get_max_level() default
     std::vector<UnitPlaintext *> units;
     try {
       for (int start = 0; start < count || (count == 0 && units.empty()); start += info_.slot_count) {
