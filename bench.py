@@ -394,6 +394,7 @@ def bootstrap_measure(args, torch, np, rank, world, local, backend, stream, with
     eng = Engine(log_coeff_count=16, special_prime_count=4, scheme_preset=2)
     eng.set_stream(stream.cuda_stream)
     eng.set_concurrency(CONCURRENCY)
+    eng.set_tensor_cores(args.tensor_cores)
     eng.seed([11 + rank, 22, 33, 44, 55, 66, 77, 88], [1, 2])
     sk = eng.create_secret_key()
     rk = eng.create_relinearization_key(sk)
@@ -487,6 +488,7 @@ def bootstrap_measure(args, torch, np, rank, world, local, backend, stream, with
                                     "engine.bootstrap(ct, rk, ck, rotation key, small bootstrap "
                                     "key, 3)") + ", bootstrap preset, N=2^16, K=4, input level 3",
                        "ciphertexts_per_step": B, "precision_bits": bits,
+                       "tensor_cores": ["off", "on", "auto"][args.tensor_cores],
                        "api": "fhe_bootstrap_batch" if with_key else "fhe_bootstrap",
                        "streams": CONCURRENCY if with_key else 1,
                        "bootstrap_key_bytes": key_bytes,
@@ -710,6 +712,9 @@ def main(argv=None):
                          "batched: --batch uneven HMult+rotate items per step (use 256); "
                          "plain: the N=2^14 pipeline from slot values to decoded slots")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tensor-cores", type=int, default=2, choices=[0, 1, 2],
+                    help="base conversions: 0 CUDA cores, 1 INT8 tensor pipe, 2 the engine's "
+                         "default (tensor pipe where it measured faster); same words")
     ap.add_argument("--no-bootstrap", action="store_true",
                     help="hmult: leave out the bootstrap measurement of the headline line")
     ap.add_argument("--streams", type=int, default=None,
@@ -865,9 +870,11 @@ def main(argv=None):
                     "share_of_kernel_time": ms / sum(v[1] for v in prof.values()),
                     "kernel_ms_per_step": {k: v[1] / args.steps for k, v in prof.items()}}
 
-    # ---- the same step with the ModDown on the CUDA cores (tensor cores are the default)
-    def timed_form(tensor_cores: bool):
-        eng.set_tensor_cores(tensor_cores)
+    # ---- the same step with the base conversions on the CUDA cores (OFF), on the
+    # tensor pipe (AUTO, the default at 10 special primes) and with ModUp's and
+    # ModDown's NTTs on the tensor pipe as well (ON); every form gives the same words.
+    def timed_form(mode: int):
+        eng.set_tensor_cores(mode)
         form_value, _ = timed_steps(step, False)
         _, p = timed_steps(step, True)
         eng.set_tensor_cores(2)
@@ -877,13 +884,17 @@ def main(argv=None):
         up_cnt, up_ms = p.get(up, (0, 0.0))
         if up == "mod_up_ntt_tc":  # the tensor-pipe contraction and the NTT that follows it
             up_ms += p.get("mod_up_contract_tc", (0, 0.0))[1]
-        return {"value": form_value, "unit": "ct/s", "mod_down_kernel": fam,
+        down = "mod_down_intt_tc" if "mod_down_intt_tc" in p else "mod_down_intt"
+        return {"value": form_value, "unit": "ct/s", "mode": ["off", "on", "auto"][mode],
+                "mod_down_kernel": fam,
                 "mod_down_avg_launch_ms": fam_ms / cnt if cnt else None,
                 "mod_down_ms_per_step": fam_ms / args.steps,
                 "mod_up_family": up, "mod_up_avg_launch_ms": up_ms / up_cnt if up_cnt else None,
-                "mod_up_ms_per_step": up_ms / args.steps}
+                "mod_up_ms_per_step": up_ms / args.steps,
+                "mod_down_ntt_family": down, "mod_down_ntt_ms_per_step": p.get(down, (0, 0.0))[1] / args.steps}
 
-    forms = {"tensor_core": timed_form(True), "cuda_core": timed_form(False)}
+    forms = {"tensor_core": timed_form(2), "tensor_core_with_ntt": timed_form(1),
+             "cuda_core": timed_form(0)}
 
     # ---- end to end through the C ABI with pinned host buffers
     in_words = 2 * L0 * n
@@ -923,6 +934,21 @@ def main(argv=None):
     e_elapsed, e_units = aggregate(s2.elapsed_time(t2), float(B * e_steps), world, backend)
     e2e_value = e_units / (e_elapsed / 1e3)
 
+    # ---- the host link alone: the step's input bytes from the same pinned buffer to
+    # the device in one copy, the ceiling of the end-to-end rate
+    dev_in = torch.empty(pin_in.shape, dtype=torch.int64, device="cuda")
+    dev_in.copy_(pin_in, non_blocking=True)
+    torch.cuda.synchronize()
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h0.record(stream)
+    for _ in range(3):
+        dev_in.copy_(pin_in, non_blocking=True)
+    h1.record(stream)
+    torch.cuda.synchronize()
+    h2d_bytes = B * 2 * in_words * 8
+    h2d_gbs = 3 * h2d_bytes / (h0.elapsed_time(h1) / 1e3) / 1e9
+    del dev_in
+
     line = None
     if rank == 0:
         cpu = None
@@ -945,7 +971,9 @@ def main(argv=None):
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "ct/s",
                     "h2d_bytes_per_step": B * 2 * in_words * 8,
-                    "d2h_bytes_per_step": B * out_words * 8},
+                    "d2h_bytes_per_step": B * out_words * 8,
+                    "h2d_gbs_measured": h2d_gbs,
+                    "h2d_ceiling_ct_s": B / (h2d_bytes / (h2d_gbs * 1e9))},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
         }

@@ -692,9 +692,7 @@ void Engine::decompose_into(const int64_t *x, int moduli_id, int64_t *out) {
 
 void Engine::mod_down_polys(int64_t *extended, int moduli_id, int polys, int64_t *out) {
   const int L = params.chains(moduli_id), E = params.chains(moduli_id, true);
-  cudaError_t e = timed("mod_down_intt", [&] {
-    return launch_mod_down_intt(tables_, params.log_n, moduli_id, E, extended, stream_, polys);
-  });
+  cudaError_t e = mod_down_transform(moduli_id, E, extended, polys);
   if (e == cudaSuccess) {
     EpilogueOps ops;
     ops.polys = polys;

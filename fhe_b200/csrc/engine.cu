@@ -106,6 +106,11 @@ Engine::Engine(const Config &config) : params(config) {
   tables_.inv_q = upload_table(inv_q);
   tables_.inv_2q = upload_table(inv_2q);
   tables_.log_n = p.log_n;
+  if (tc_ntt_supported(p.log_n)) {
+    const TcNttHost h = make_tc_ntt_tables(p);
+    tc_ntt_.bmat = upload_table(h.bmat);
+    tc_ntt_.psi_pow = upload_table(h.psi_pow);
+  }
 
   std::vector<int64_t> pinv(static_cast<size_t>(std::max(p.special_prime_count, 1)) * P, 0);
   for (int s = 0; s < p.special_prime_count; s++)
@@ -241,7 +246,21 @@ cudaError_t Engine::mod_up(const DevicePartitions &dp, int moduli_id, const int6
   });
   if (e != cudaSuccess) return e;
   return timed("mod_up_ntt_tc", [&] {
+    if (use_tc_ntt())  // the extended limbs only matter modulo q: the tensor-core NTT
+      return launch_tc_ntt(tc_ntt_, tables_, false, dp.count, dp.extended, moduli_id, ext,
+                           static_cast<long long>(dp.extended) * params.n, tc_status(), stream_);
     return launch_extended_ntt(tables_, dp, params.log_n, moduli_id, ext, stream_);
+  });
+}
+
+cudaError_t Engine::mod_down_transform(int moduli_id, int extended, int64_t *acc, int polys) {
+  if (use_tc_ntt())
+    return timed("mod_down_intt_tc", [&] {
+      return launch_tc_ntt(tc_ntt_, tables_, true, polys, extended, moduli_id, acc,
+                           static_cast<long long>(extended) * params.n, tc_status(), stream_);
+    });
+  return timed("mod_down_intt", [&] {
+    return launch_mod_down_intt(tables_, params.log_n, moduli_id, extended, acc, stream_, polys);
   });
 }
 
@@ -604,10 +623,7 @@ void Engine::key_switch_pipeline(const int64_t *c1, int moduli_id, const Data &k
       return launch_rotate_base(tables_, ks_, params.log_n, moduli_id, L, rotate_c0, digits, acc,
                                 stream_);
     });
-  if (e == cudaSuccess)
-    e = timed("mod_down_intt", [&] {
-      return launch_mod_down_intt(tables_, params.log_n, moduli_id, E, acc, stream_);
-    });
+  if (e == cudaSuccess) e = mod_down_transform(moduli_id, E, acc, 2);
   if (e == cudaSuccess) e = mod_down_epilogue(moduli_id, L, acc, ops, out);
   free_words(digits);
   free_words(own_ext);

@@ -304,12 +304,12 @@ class Engine {
   // Where the ModDown base conversion runs; every mode gives the same words.
   //   kTensorCoresOff: CUDA cores; kTensorCoresOn: the INT8 tensor pipe wherever the
   //   shape allows it; kTensorCoresAuto (default): each conversion on the tensor pipe
-  //   from the number of special primes where it measured faster (ModDown from 4,
-  //   ModUp from 8: the tensor form's cost per output is mostly fixed, the CUDA-core
-  //   form's grows with K).
+  //   from the number of special primes where it measured faster (ModDown and ModUp
+  //   from 4: the tensor form's cost per output is mostly fixed, the CUDA-core form's
+  //   grows with K).
   enum TensorCoreMode : int { kTensorCoresOff = 0, kTensorCoresOn = 1, kTensorCoresAuto = 2 };
   static constexpr int kTensorCoreMinSpecial = 4;
-  static constexpr int kTensorCoreModUpMinSpecial = 8;
+  static constexpr int kTensorCoreModUpMinSpecial = 4;
   void set_tensor_cores(int mode);
   int tensor_cores() const { return tensor_cores_; }
   // Diagnostics: how many times the tensor-core kernels poll for each MMA round
@@ -382,6 +382,14 @@ class Engine {
                      int64_t *ext);
   int *device_error_ = nullptr;  // set by a kernel whose bounded wait ran out
   uint32_t tc_wait_limit_ = kTcDefaultWaitLimit;
+  TcNttTables tc_ntt_{};  // set when the ring degree has a tensor-core NTT
+  // The value-only transforms run on the tensor pipe only when the tensor cores are
+  // forced on: the CUDA-core form measured faster (see ntt_tc.cu), so AUTO keeps it.
+  bool use_tc_ntt() const { return tc_ntt_.bmat != nullptr && tensor_cores_ == kTensorCoresOn; }
+  // ModDown's inverse transform of `polys` extended polynomials at moduli_id, in
+  // place, reduced to [0, q): on the tensor pipe when the tensor cores are in use and
+  // the ring degree has a tensor-core NTT, else on the CUDA cores (same words).
+  cudaError_t mod_down_transform(int moduli_id, int extended, int64_t *acc, int polys);
   TcStatus tc_status() const {
     TcStatus st;
     st.error = device_error_;

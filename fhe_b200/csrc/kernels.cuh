@@ -182,6 +182,28 @@ cudaError_t launch_mod_up_contract_tc(const PrimeTables &t, const DevicePartitio
                                       const ModUpTcTables &tc, int n, int moduli_id,
                                       const int64_t *digits, int64_t *ext, const TcStatus &status,
                                       cudaStream_t s);
+// Tensor-core NTT of the value-only transforms (ntt_tc.cu, N = 2^16): per prime, the
+// four byte-split 16 x 16 transform matrices as UMMA B operands and the powers
+// psi^e R mod q for e < N in natural order.
+struct TcNttTables {
+  const uint8_t *bmat = nullptr;     // [P][4][128 columns][128 bytes], core-matrix order
+  const int64_t *psi_pow = nullptr;  // [P][N]
+};
+struct TcNttHost {
+  std::vector<uint8_t> bmat;
+  std::vector<int64_t> psi_pow;
+};
+struct Parameters;
+bool tc_ntt_supported(int log_n);
+TcNttHost make_tc_ntt_tables(const Parameters &p);
+// In-place forward (ModUp's) or inverse (ModDown's, with its enter-exit scaling and
+// a reduction to [0, q)) transform of polys x limbs limbs ([poly][limb][N], poly
+// stride poly_stride) on the INT8 tensor pipe; the values modulo q equal the
+// reference's transforms' (forward outputs in [0, 2q)).
+cudaError_t launch_tc_ntt(const TcNttTables &tt, const PrimeTables &t, bool inverse, int polys,
+                          int limbs, int prime_base, int64_t *data, long long poly_stride,
+                          const TcStatus &status, cudaStream_t s);
+
 // The forward NTT that completes ModUp, over every partition's extended limbs.
 cudaError_t launch_extended_ntt(const PrimeTables &t, const DevicePartitions &dp, int log_n,
                                 int moduli_id, int64_t *ext, cudaStream_t s);

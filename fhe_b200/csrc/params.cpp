@@ -278,6 +278,7 @@ Parameters::Parameters(const Config &cfg)
   n_inverse.resize(prime_count);
   root.resize(static_cast<size_t>(prime_count) * (n - 1));
   root_inverse.resize(static_cast<size_t>(prime_count) * (n - 1));
+  psi.resize(prime_count);
   std::map<uint64_t, int> derived;
   for (int i = 0; i < prime_count; i++) {
     const uint64_t qi = q[i];
@@ -287,6 +288,7 @@ Parameters::Parameters(const Config &cfg)
       k[i] = k[j];
       r_squared[i] = r_squared[j];
       n_inverse[i] = n_inverse[j];
+      psi[i] = psi[j];
       std::copy_n(&root[size_t(j) * (n - 1)], n - 1, &root[size_t(i) * (n - 1)]);
       std::copy_n(&root_inverse[size_t(j) * (n - 1)], n - 1, &root_inverse[size_t(i) * (n - 1)]);
       continue;
@@ -303,6 +305,7 @@ Parameters::Parameters(const Config &cfg)
       psi = mod_pow(base, unit_power, qs);
       if (mod_pow(psi, n, qs) != 1) break;
     }
+    this->psi[i] = psi;
     const int64_t psi_inv = mod_invert(psi, qs);
     std::vector<int64_t> fwd(n), inv(n);
     int64_t a = 1, b = 1;

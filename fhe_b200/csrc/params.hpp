@@ -104,6 +104,7 @@ class Parameters {
   std::vector<int64_t> n_inverse;    // [P]  N^-1 * 2^62 mod q
   std::vector<int64_t> root;         // [P][N-1] bit-reversed psi powers, Montgomery form
   std::vector<int64_t> root_inverse; // [P][N-1] backward-paint inverse powers
+  std::vector<int64_t> psi;          // [P]  the primitive 2N-th root the tables are built from
   std::vector<int64_t> p_product_mult_r;               // [C]
   std::vector<std::vector<int64_t>> p_inverse_mult_r;  // [K][p_index]
   std::vector<std::vector<int64_t>> rescale_scale;     // [P-1][P-from-1]

@@ -462,7 +462,8 @@ class Engine:
     def set_tensor_cores(self, mode) -> None:
         """Where the base conversions run: False/0 CUDA cores, True/1 the INT8 tensor
         pipe, 2 (default) the tensor pipe where it measured faster (ModDown from 4
-        special primes, ModUp from 8); same words."""
+        special primes, ModUp from 4; with 1 also ModUp's and ModDown's NTTs at N = 2^16);
+        same words."""
         check(_lib.load().fhe_engine_set_tensor_cores(self._h, int(mode)))
 
     def set_tensor_core_wait_limit(self, limit: int) -> None:

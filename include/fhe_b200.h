@@ -428,9 +428,11 @@ int fhe_relinearize_noalloc(fhe_engine *engine, const int64_t *ct_device, int mo
 /* Selects where the base conversions run (ModUp's digit contraction,
  * core_key_switch.cpp:92-108, and ModDown's exact division by the special primes,
  * :123-160): FHE_TENSOR_CORES_OFF on the CUDA cores, FHE_TENSOR_CORES_ON on the INT8
- * tensor pipe (tcgen05.mma kind::i8) wherever the shape allows it,
- * FHE_TENSOR_CORES_AUTO (the default) on the tensor pipe where it measured faster
- * (ModDown from 4 special primes, ModUp from 8).  Every mode gives the same words. */
+ * tensor pipe (tcgen05.mma kind::i8) wherever the shape allows it, together with
+ * ModUp's forward and ModDown's inverse NTT at N = 2^16 (a radix-16 four-step
+ * transform as INT8 contractions), FHE_TENSOR_CORES_AUTO (the default) on the
+ * tensor pipe where it measured faster (both base conversions from 4 special
+ * primes; the NTTs stay on the CUDA cores).  Every mode gives the same words. */
 enum {
   FHE_TENSOR_CORES_OFF = 0,
   FHE_TENSOR_CORES_ON = 1,

@@ -36,7 +36,9 @@ def _numbers(text):
 def test_reference_example_runs_unchanged_on_the_gpu(example):
     cpu, gpu = _run(f"{example}_cpu"), _run(f"{example}_gpu")
     cpu_lines, gpu_lines = cpu.strip().splitlines(), gpu.strip().splitlines()
-    assert [l.split(":")[0] for l in gpu_lines] == [l.split(":")[0] for l in cpu_lines]
+    labels = [l.strip() for l in gpu_lines if l.rstrip().endswith(":")]
+    assert labels == [l.strip() for l in cpu_lines if l.rstrip().endswith(":")]
+    assert labels == ["message:", "decrypted:"]
     message = _numbers(gpu_lines[1])
     decrypted = _numbers(gpu_lines[3])
     assert message == _numbers(cpu_lines[1])
