@@ -232,25 +232,33 @@ const ModUpTcTables *Engine::mod_up_tc(int moduli_id) {
 }
 
 cudaError_t Engine::mod_up(const DevicePartitions &dp, int moduli_id, const int64_t *digits,
-                           int64_t *ext) {
+                           int64_t *ext, bool skip_own) {
+  if (skip_own && use_tc_ntt()) return cudaErrorInvalidValue;
   const ModUpTcTables *tc =
       use_tensor_cores(kTensorCoreModUpMinSpecial) ? mod_up_tc(moduli_id) : nullptr;
   if (!tc)
     return timed("mod_up_ntt", [&] {
-      return launch_mod_up_ntt(tables_, dp, params.log_n, moduli_id, digits, ext, stream_);
+      return launch_mod_up_ntt(tables_, dp, params.log_n, moduli_id, digits, ext, stream_,
+                               skip_own);
     });
   // Profiled as two families, so the tensor-pipe contraction's time is its own.
   const cudaError_t e = timed("mod_up_contract_tc", [&] {
     return launch_mod_up_contract_tc(tables_, dp, *tc, params.n, moduli_id, digits, ext,
-                                     tc_status(), stream_);
+                                     tc_status(), stream_, skip_own);
   });
   if (e != cudaSuccess) return e;
   return timed("mod_up_ntt_tc", [&] {
     if (use_tc_ntt())  // the extended limbs only matter modulo q: the tensor-core NTT
       return launch_tc_ntt(tc_ntt_, tables_, false, dp.count, dp.extended, moduli_id, ext,
                            static_cast<long long>(dp.extended) * params.n, tc_status(), stream_);
-    return launch_extended_ntt(tables_, dp, params.log_n, moduli_id, ext, stream_);
+    return launch_extended_ntt(tables_, dp, params.log_n, moduli_id, ext, stream_, skip_own);
   });
+}
+
+int64_t *Engine::own_limbs_ext(int moduli_id, const Data &rk) {
+  if (use_tc_ntt() || rk.moduli_id > moduli_id) return nullptr;
+  const DevicePartitions &dp = partitions(moduli_id, rk.moduli_id);
+  return alloc_words(static_cast<size_t>(dp.count) * dp.extended * params.n);
 }
 
 cudaError_t Engine::mod_down_transform(int moduli_id, int extended, int64_t *acc, int polys) {
@@ -589,7 +597,7 @@ std::unique_ptr<Data> Engine::multiply(const Data &a, const Data &b) {
 
 void Engine::key_switch_pipeline(const int64_t *c1, int moduli_id, const Data &key,
                                  const int64_t *rotate_c0, const EpilogueOps &ops, int64_t *out,
-                                 const int64_t *decomposed) {
+                                 const int64_t *decomposed, int64_t *own_ext) {
   const int n = params.n;
   const int L = params.chains(moduli_id);
   const int E = params.chains(moduli_id, true);
@@ -602,15 +610,18 @@ void Engine::key_switch_pipeline(const int64_t *c1, int moduli_id, const Data &k
   // A decomposition made earlier (hoisted rotations) replaces the ModUp: its partitions
   // have the same starts and sizes, only the key index depends on the key's level.
   int64_t *digits = alloc_words(static_cast<size_t>(L) * n);
-  int64_t *own_ext = decomposed ? nullptr : alloc_words(static_cast<size_t>(dp.count) * E * n);
-  const int64_t *ext = decomposed ? decomposed : own_ext;
+  const bool skip_own = own_ext != nullptr && !decomposed;
+  int64_t *alloc_ext =
+      decomposed || skip_own ? nullptr : alloc_words(static_cast<size_t>(dp.count) * E * n);
+  int64_t *work_ext = skip_own ? own_ext : alloc_ext;
+  const int64_t *ext = decomposed ? decomposed : work_ext;
   int64_t *acc = alloc_words(static_cast<size_t>(2) * E * n);
   cudaError_t e = cudaSuccess;
   if (!decomposed) {
     e = timed("mixed_radix", [&] {
       return launch_mixed_radix(tables_, dp, n, moduli_id, c1, digits, stream_);
     });
-    if (e == cudaSuccess) e = mod_up(dp, moduli_id, digits, own_ext);
+    if (e == cudaSuccess) e = mod_up(dp, moduli_id, digits, work_ext, skip_own);
   }
   if (e == cudaSuccess)
     e = timed("key_inner_product", [&] {
@@ -626,19 +637,19 @@ void Engine::key_switch_pipeline(const int64_t *c1, int moduli_id, const Data &k
   if (e == cudaSuccess) e = mod_down_transform(moduli_id, E, acc, 2);
   if (e == cudaSuccess) e = mod_down_epilogue(moduli_id, L, acc, ops, out);
   free_words(digits);
-  free_words(own_ext);
+  free_words(alloc_ext);
   free_words(acc);
   check(e, "key switch");
 }
 
 void Engine::relinearize_tail(const int64_t *t3, int moduli_id, const Data &rk, int mode,
-                              int64_t *out) {
+                              int64_t *out, int64_t *own_ext) {
   EpilogueOps ops;
   ops.base = t3;
   ops.base_polys = mode == 0 ? 0 : 2;
   ops.rescale = mode == 2;
   const long long L = params.chains(moduli_id);
-  key_switch_pipeline(t3 + 2 * L * params.n, moduli_id, rk, nullptr, ops, out);
+  key_switch_pipeline(t3 + 2 * L * params.n, moduli_id, rk, nullptr, ops, out, nullptr, own_ext);
 }
 
 std::unique_ptr<Data> Engine::relinearize(const Data &ct, const Data &rk) {
@@ -665,13 +676,28 @@ std::unique_ptr<Data> Engine::relinearize(const Data &ct, const Data &rk) {
     check(e, "relinearize");
   }
   auto out = make_data(kUnitCiphertext, x->flag & ~kFlagNtt, m, 2, x->scale);
+  // The NTT-form third polynomial is at hand: its limbs are ModUp's own limbs.
+  int64_t *own_ext = own_limbs_ext(m, rk);
   try {
-    relinearize_tail(t3, m, rk, 1, out->d);
+    if (own_ext) {
+      const long long n = params.n;
+      const int E = params.chains(m, true);
+      const auto parts = params.partitions(m, rk.moduli_id);
+      for (size_t p = 0; p < parts.size(); p++)
+        check(cudaMemcpyAsync(own_ext + (static_cast<long long>(p) * E + parts[p].start) * n,
+                              x->d + 2 * x->poly_stride() + parts[p].start * n,
+                              static_cast<size_t>(parts[p].size) * n * sizeof(int64_t),
+                              cudaMemcpyDeviceToDevice, stream_),
+              "copy own limbs");
+    }
+    relinearize_tail(t3, m, rk, 1, out->d, own_ext);
   } catch (...) {
     free_words(t3);
+    free_words(own_ext);
     throw;
   }
   free_words(t3);
+  free_words(own_ext);
   return out;
 }
 
@@ -694,22 +720,28 @@ std::unique_ptr<Data> Engine::relinearized_product(const Data &pa, const Data &p
   const int m = pa.moduli_id;
   const int L = pa.chains;
   int64_t *t3 = alloc_words(static_cast<size_t>(3) * L * params.n);
+  // The tensor's NTT-form third polynomial also lands in ModUp's own limbs.
+  int64_t *own_ext = own_limbs_ext(m, rk);
+  const DevicePartitions *dp = own_ext ? &partitions(m, rk.moduli_id) : nullptr;
   cudaError_t e = timed("tensor_to_intt", [&] {
-    return launch_tensor_to_intt(tables_, params.log_n, L, m, pa.d, pb.d, t3, stream_);
+    return launch_tensor_to_intt(tables_, params.log_n, L, m, pa.d, pb.d, t3, stream_, own_ext, dp);
   });
   if (e != cudaSuccess) {
     free_words(t3);
+    free_words(own_ext);
     check(e, "tensor");
   }
   const int flag = (pa.flag | pb.flag) & ~kFlagRescaled & ~kFlagNtt;
   auto out = make_data(kUnitCiphertext, flag, m, 2, pa.scale * pb.scale);
   try {
-    relinearize_tail(t3, m, rk, 1, out->d);
+    relinearize_tail(t3, m, rk, 1, out->d, own_ext);
   } catch (...) {
     free_words(t3);
+    free_words(own_ext);
     throw;
   }
   free_words(t3);
+  free_words(own_ext);
   return out;
 }
 
@@ -734,23 +766,30 @@ std::unique_ptr<Data> Engine::multiply_relinearize_rescale(const Data &a, const 
           "Rescale Unit Ciphertext: the input unit ciphertext should have a positive level.");
   }
   int64_t *t3 = alloc_words(static_cast<size_t>(3) * L * params.n);
+  // The tensor's NTT-form third polynomial also lands in ModUp's own limbs.
+  int64_t *own_ext = own_limbs_ext(m, rk);
+  const DevicePartitions *dp = own_ext ? &partitions(m, rk.moduli_id) : nullptr;
   cudaError_t e = timed("tensor_to_intt", [&] {
-    return launch_tensor_to_intt(tables_, params.log_n, L, m, pa->d, pb->d, t3, stream_);
+    return launch_tensor_to_intt(tables_, params.log_n, L, m, pa->d, pb->d, t3, stream_, own_ext,
+                                 dp);
   });
   if (e != cudaSuccess) {
     free_words(t3);
+    free_words(own_ext);
     check(e, "tensor");
   }
   const int flag = ((pa->flag | pb->flag) & ~kFlagRescaled & ~kFlagNtt) | kFlagRescaled;
   const long double scale = params.rescaled_scale(pa->scale * pb->scale, m);
   auto out = make_data(kUnitCiphertext, flag, m + 1, 2, scale);
   try {
-    relinearize_tail(t3, m, rk, 2, out->d);
+    relinearize_tail(t3, m, rk, 2, out->d, own_ext);
   } catch (...) {
     free_words(t3);
+    free_words(own_ext);
     throw;
   }
   free_words(t3);
+  free_words(own_ext);
   return out;
 }
 

@@ -379,7 +379,7 @@ class Engine {
   bool use_tensor_cores(int min_special) const;
   // ModUp of every partition's digits into NTT-form extended limbs, in the selected form.
   cudaError_t mod_up(const DevicePartitions &dp, int moduli_id, const int64_t *digits,
-                     int64_t *ext);
+                     int64_t *ext, bool skip_own = false);
   int *device_error_ = nullptr;  // set by a kernel whose bounded wait ran out
   uint32_t tc_wait_limit_ = kTcDefaultWaitLimit;
   TcNttTables tc_ntt_{};  // set when the ring degree has a tensor-core NTT
@@ -530,12 +530,20 @@ class Engine {
   // Hybrid key switch of the coefficient-form polynomial c1 at moduli_id (L limbs):
   // decompose, ModUp, key product, optional rotation term b * P (rotate_c0 = the
   // coefficient-form c0), ModDown and the epilogue operations `ops` into `out`.
+  // own_ext: a caller-owned extended buffer [count][E][N] whose partitions' own limbs
+  // already hold NTT-form words of c1 (see own_limbs_ext); ModUp then skips them.
   void key_switch_pipeline(const int64_t *c1, int moduli_id, const Data &key,
                            const int64_t *rotate_c0, const EpilogueOps &ops, int64_t *out,
-                           const int64_t *decomposed = nullptr);
+                           const int64_t *decomposed = nullptr, int64_t *own_ext = nullptr);
   // Key switch tail shared by relinearize variants; t3 is [3][L][N] coefficient
   // form at moduli_id (poly 2 is switched).
-  void relinearize_tail(const int64_t *t3, int moduli_id, const Data &rk, int mode, int64_t *out);
+  void relinearize_tail(const int64_t *t3, int moduli_id, const Data &rk, int mode, int64_t *out,
+                        int64_t *own_ext = nullptr);
+  // ModUp's extended limbs of a partition's own primes are the input limbs' values,
+  // so when the input's NTT form exists their NTT needs no work: an extended buffer
+  // for relinearizing at moduli_id with rk, to be filled with those NTT-form words,
+  // or null when ModUp's transform runs on the tensor pipe (which covers every limb).
+  int64_t *own_limbs_ext(int moduli_id, const Data &rk);
   void require_key_level(const std::string &fn, const Data &text, const Data &key,
                          bool for_multiply, const char *key_name = "relinearization key");
   std::unique_ptr<Data> core_level_down(const Data &text, int level);  // coefficient form

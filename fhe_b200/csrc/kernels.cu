@@ -198,7 +198,7 @@ constexpr int kContractChunk = 8;  // extended limbs per thread
 template <int A>
 __global__ void __launch_bounds__(256)
     mod_up_contract_kernel(PrimeTables t, DevicePartitions dp, int n, int moduli_id,
-                           const int64_t *digits, int64_t *ext) {
+                           const int64_t *digits, int64_t *ext, bool skip_own) {
   const int p = blockIdx.y;
   if (dp.size[p] != A) return;
   const int coeff = blockIdx.x * blockDim.x + threadIdx.x;
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(256)
       }
 #pragma unroll
       for (int l = 0; l < kLanes; l++) {
-        if (j0 + l < E) {
+        if (j0 + l < E && !(skip_own && jl[l] >= start && jl[l] < start + A)) {
           const int prime = moduli_id + jl[l];
           const uint64_t q = t.q[prime];
           out[static_cast<long long>(jl[l]) * n] = sum[l].reduce(q, t.k[prime], q << 1, t.inv_2q[prime]);
@@ -247,6 +247,7 @@ __global__ void __launch_bounds__(256)
     return;
   }
   for (int j = j_begin; j < j_begin + kContractChunk && j < E; j++) {
+    if (skip_own && j >= start && j < start + A) continue;
     const int prime = moduli_id + j;
     const uint64_t q = t.q[prime], k = t.k[prime];
     const int64_t q2 = static_cast<int64_t>(q << 1);
@@ -397,11 +398,26 @@ struct TensorLoad {
   long long poly_stride;  // limbs * n
   const uint64_t *q;
   const uint64_t *k;
+  // Optional sink of the third polynomial's NTT-form words into each partition's own
+  // limbs of ModUp's extended buffer [count][extended][N].
+  int64_t *own_ext = nullptr;
+  const int *part_start = nullptr;
+  const int *part_size = nullptr;
+  int part_count = 0;
+  int extended = 0;
   __device__ __forceinline__ int64_t operator()(int poly, int limb, int prime, int gi, int n) const {
     const long long i = static_cast<long long>(limb) * n + gi;
     const uint64_t qq = q[prime], kk = k[prime];
     if (poly == 0) return mont_mult_lazy(a[i], b[i], qq, kk);
-    if (poly == 2) return mont_mult_lazy(a[poly_stride + i], b[poly_stride + i], qq, kk);
+    if (poly == 2) {
+      const int64_t v = mont_mult_lazy(a[poly_stride + i], b[poly_stride + i], qq, kk);
+      if (own_ext != nullptr) {
+        int p = 0;
+        while (p + 1 < part_count && limb >= part_start[p] + part_size[p]) p++;
+        own_ext[(static_cast<long long>(p) * extended + limb) * n + gi] = v;
+      }
+      return v;
+    }
     const int64_t qs = static_cast<int64_t>(qq);
     return guard(guard(mont_mult_lazy(a[i], b[poly_stride + i], qq, kk) +
                            mont_mult_lazy(a[poly_stride + i], b[i], qq, kk),
@@ -474,7 +490,8 @@ cudaError_t launch_mixed_radix(const PrimeTables &t, const DevicePartitions &dp,
 }
 
 cudaError_t launch_mod_up_ntt(const PrimeTables &t, const DevicePartitions &dp, int log_n,
-                              int moduli_id, const int64_t *digits, int64_t *ext, cudaStream_t s) {
+                              int moduli_id, const int64_t *digits, int64_t *ext, cudaStream_t s,
+                              bool skip_own) {
   const int n = 1 << log_n;
   const dim3 grid(blocks_for(n), dp.count, (dp.extended + kContractChunk - 1) / kContractChunk);
   for (int size = 1; size <= 16; size++) {
@@ -483,7 +500,7 @@ cudaError_t launch_mod_up_ntt(const PrimeTables &t, const DevicePartitions &dp, 
 #define FHE_MU_CASE(A)                                                                    \
   case A:                                                                                 \
     note_launch();                                                                        \
-    mod_up_contract_kernel<A><<<grid, kThreads, 0, s>>>(t, dp, n, moduli_id, digits, ext); \
+    mod_up_contract_kernel<A><<<grid, kThreads, 0, s>>>(t, dp, n, moduli_id, digits, ext, skip_own); \
     break;
       FHE_MU_CASE(1) FHE_MU_CASE(2) FHE_MU_CASE(3) FHE_MU_CASE(4) FHE_MU_CASE(5)
       FHE_MU_CASE(6) FHE_MU_CASE(7) FHE_MU_CASE(8) FHE_MU_CASE(9) FHE_MU_CASE(10)
@@ -495,18 +512,19 @@ cudaError_t launch_mod_up_ntt(const PrimeTables &t, const DevicePartitions &dp, 
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  return launch_extended_ntt(t, dp, log_n, moduli_id, ext, s);
+  return launch_extended_ntt(t, dp, log_n, moduli_id, ext, s, skip_own);
 }
 
 cudaError_t launch_extended_ntt(const PrimeTables &t, const DevicePartitions &dp, int log_n,
-                                int moduli_id, int64_t *ext, cudaStream_t s) {
+                                int moduli_id, int64_t *ext, cudaStream_t s, bool skip_own) {
   const long long stride = static_cast<long long>(dp.extended) << log_n;
   PlainLoad ld{ext, stride};
   PlainStore st{ext, stride};
   // Value-only: the extended polynomial reaches the output only through the key
   // inner product's reduction to [0, q) and ModDown's reduced inverse transform.
   return forward_ntt<PlainLoad, PlainStore, true>(log_n, dp.count, dp.extended, moduli_id, t, ld, st,
-                                                  ext, stride, s);
+                                                  ext, stride, s, skip_own ? dp.start : nullptr,
+                                                  skip_own ? dp.size : nullptr);
 }
 
 cudaError_t launch_key_inner_product(const PrimeTables &t, const DevicePartitions &dp, int n,
@@ -615,9 +633,18 @@ cudaError_t launch_ntt_plain(const PrimeTables &t, int log_n, int polys, int lim
 }
 
 cudaError_t launch_tensor_to_intt(const PrimeTables &t, int log_n, int limbs, int prime_base,
-                                  const int64_t *a, const int64_t *b, int64_t *y, cudaStream_t s) {
+                                  const int64_t *a, const int64_t *b, int64_t *y, cudaStream_t s,
+                                  int64_t *own_ext, const DevicePartitions *dp) {
   const long long stride = static_cast<long long>(limbs) << log_n;
   TensorLoad ld{a, b, stride, t.q, t.k};
+  if (own_ext != nullptr) {
+    if (dp == nullptr) return cudaErrorInvalidValue;
+    ld.own_ext = own_ext;
+    ld.part_start = dp->start;
+    ld.part_size = dp->size;
+    ld.part_count = dp->count;
+    ld.extended = dp->extended;
+  }
   EnterExitStore<false> st{y, stride, t.n_inverse, t.q, t.k};
   return inverse_ntt(log_n, 3, limbs, prime_base, t, ld, st, y, stride, s);
 }

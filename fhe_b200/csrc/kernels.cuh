@@ -78,9 +78,12 @@ cudaError_t launch_mixed_radix(const PrimeTables &t, const DevicePartitions &dp,
                                int moduli_id, const int64_t *x, int64_t *digits, cudaStream_t s);
 
 // ModUp + NTT of every partition (core_key_switch.cpp:92-108): ext [count][E][N].
+// With skip_own, each partition's own limbs [start_p, start_p + alpha_p) of ext
+// already hold NTT-form words of the same values (the caller had the input in NTT
+// form) and are neither contracted nor transformed.
 cudaError_t launch_mod_up_ntt(const PrimeTables &t, const DevicePartitions &dp, int log_n,
                               int moduli_id, const int64_t *digits, int64_t *ext,
-                              cudaStream_t s);
+                              cudaStream_t s, bool skip_own = false);
 
 // Key inner product (core_key_switch.cpp:320-349): acc[2][E][N] = sum over
 // partitions of ext_p * (key_{2i}, key_{2i+1}), reference reduction pattern.
@@ -181,7 +184,7 @@ ModUpTcHost make_mod_up_tc_tables(const std::vector<uint64_t> &q,
 cudaError_t launch_mod_up_contract_tc(const PrimeTables &t, const DevicePartitions &dp,
                                       const ModUpTcTables &tc, int n, int moduli_id,
                                       const int64_t *digits, int64_t *ext, const TcStatus &status,
-                                      cudaStream_t s);
+                                      cudaStream_t s, bool skip_own = false);
 // Tensor-core NTT of the value-only transforms (ntt_tc.cu, N = 2^16): per prime, the
 // four byte-split 16 x 16 transform matrices as UMMA B operands and the powers
 // psi^e R mod q for e < N in natural order.
@@ -204,9 +207,11 @@ cudaError_t launch_tc_ntt(const TcNttTables &tt, const PrimeTables &t, bool inve
                           int limbs, int prime_base, int64_t *data, long long poly_stride,
                           const TcStatus &status, cudaStream_t s);
 
-// The forward NTT that completes ModUp, over every partition's extended limbs.
+// The forward NTT that completes ModUp, over every partition's extended limbs (with
+// skip_own, not over each partition's own limbs).
 cudaError_t launch_extended_ntt(const PrimeTables &t, const DevicePartitions &dp, int log_n,
-                                int moduli_id, int64_t *ext, cudaStream_t s);
+                                int moduli_id, int64_t *ext, cudaStream_t s,
+                                bool skip_own = false);
 
 // Rotation's b * P term (create_key_switcher_for_rotate, core_key_switch.cpp:550-576):
 // acc0[j] = reduce(acc0[j] + NTT(mont(mont(c0[j], P mod q * R), R^2))) for the L
@@ -309,9 +314,12 @@ cudaError_t launch_ntt_plain(const PrimeTables &t, int log_n, int polys, int lim
                              int prime_base, int64_t *x, long long stride, bool inverse,
                              cudaStream_t s);
 // Inverse NTT (to_intt_) of the tensor of two NTT-form 2-poly ciphertexts a, b
-// without materialising the tensor: y [3][L][N] coefficient form.
+// without materialising the tensor: y [3][L][N] coefficient form.  With own_ext, the
+// NTT-form words of the third polynomial are also written to each partition's own
+// limbs of the extended buffer own_ext [count][E][N] (ModUp with skip_own).
 cudaError_t launch_tensor_to_intt(const PrimeTables &t, int log_n, int limbs, int prime_base,
                                   const int64_t *a, const int64_t *b, int64_t *y,
-                                  cudaStream_t s);
+                                  cudaStream_t s, int64_t *own_ext = nullptr,
+                                  const DevicePartitions *dp = nullptr);
 
 }  // namespace fhe_b200

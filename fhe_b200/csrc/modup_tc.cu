@@ -31,7 +31,7 @@ constexpr int digit_row_bytes(int A) { return (8 * A + 31) / 32 * 32; }
 template <int A>
 __global__ void __launch_bounds__(kTcThreads, 4)
     mod_up_tc_kernel(PrimeTables t, DevicePartitions dp, ModUpTcTables tc, int n, int moduli_id,
-                     const int64_t *digits, int64_t *ext, TcStatus status) {
+                     const int64_t *digits, int64_t *ext, TcStatus status, bool skip_own) {
   constexpr int KB = digit_row_bytes(A);
   const int p = blockIdx.y;
   if (dp.size[p] != A) return;  // uniform per CTA, before any barrier
@@ -113,6 +113,7 @@ __global__ void __launch_bounds__(kTcThreads, 4)
       for (int h = 0; h < 2; h++) {
         const int j = j0 + h;
         if (j >= E) break;  // uniform across the warp
+        if (skip_own && j >= start && j < start + A) continue;  // uniform across the warp
         const int prime = moduli_id + j;
         const uint64_t q = t.q[prime], kq = t.k[prime];
         if (fast[row]) {
@@ -192,7 +193,7 @@ ModUpTcHost make_mod_up_tc_tables(const std::vector<uint64_t> &q,
 cudaError_t launch_mod_up_contract_tc(const PrimeTables &t, const DevicePartitions &dp,
                                       const ModUpTcTables &tc, int n, int moduli_id,
                                       const int64_t *digits, int64_t *ext, const TcStatus &status,
-                                      cudaStream_t s) {
+                                      cudaStream_t s, bool skip_own) {
   if (!mod_up_tc_supported(dp.max_size, n) || tc.b == nullptr || status.error == nullptr ||
       tc.rounds != (dp.extended + kTcTargets - 1) / kTcTargets)
     return cudaErrorInvalidValue;
@@ -215,7 +216,7 @@ cudaError_t launch_mod_up_contract_tc(const PrimeTables &t, const DevicePartitio
     }                                                                                             \
     note_launch();                                                                                \
     mod_up_tc_kernel<AA><<<grid, kTcThreads, mod_up_tc_smem(AA), s>>>(t, dp, tc, n, moduli_id,    \
-                                                                      digits, ext, status);        \
+                                                                      digits, ext, status, skip_own); \
     break;
       FHE_UP_CASE(1) FHE_UP_CASE(2) FHE_UP_CASE(3) FHE_UP_CASE(4) FHE_UP_CASE(5) FHE_UP_CASE(6)
       FHE_UP_CASE(7) FHE_UP_CASE(8) FHE_UP_CASE(9) FHE_UP_CASE(10) FHE_UP_CASE(11) FHE_UP_CASE(12)

@@ -36,6 +36,10 @@ struct NttPass {
   int polys;       // batch: polys x limbs, grid.y = limbs * polys (poly fastest)
   int limbs;
   int prime_base;  // prime index of limb 0
+  // Optional: polynomial p's limbs [skip_start[p], skip_start[p] + skip_size[p]) are
+  // left untouched (ModUp's partitions' own limbs, already in NTT form).
+  const int *skip_start = nullptr;
+  const int *skip_size = nullptr;
 };
 
 // Reads word gi of (poly, limb) from a [poly][limb][N] buffer.
@@ -169,6 +173,9 @@ __global__ void __launch_bounds__(256, 4)
   const int pl = blockIdx.y;
   const int poly = pl % a.polys;
   const int limb = pl / a.polys;
+  if (a.skip_start != nullptr && limb >= a.skip_start[poly] &&
+      limb < a.skip_start[poly] + a.skip_size[poly])
+    return;  // uniform per CTA, before any barrier
   const int prime = a.prime_base + limb;
   const uint64_t q = t.q[prime];
   const uint64_t k = t.k[prime];
@@ -416,9 +423,10 @@ cudaError_t dispatch_ntt_pass(int S, const NttPass &a, const PrimeTables &t, con
 template <class Loader, class Storer, bool VALUE_ONLY = false>
 cudaError_t forward_ntt(int log_n, int polys, int limbs, int prime_base, const PrimeTables &t,
                         const Loader &ld, const Storer &st, int64_t *work, long long work_stride,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, const int *skip_start = nullptr,
+                        const int *skip_size = nullptr) {
   const NttPlan plan = ntt_plan(log_n);
-  NttPass a{log_n, 0, 0, 1, polys, limbs, prime_base};
+  NttPass a{log_n, 0, 0, 1, polys, limbs, prime_base, skip_start, skip_size};
   if (plan.passes == 1) {
     a.stride_log = 0;
     a.first = 0;
