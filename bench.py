@@ -178,7 +178,9 @@ def pipe_figures(prof: dict, steps: int, pairs: int, n: int, L: int, K: int, sm_
     hz = (sm_mhz or 1965.0) * 1e6
     log_n = n.bit_length() - 1
     bfly_per_limb = (n // 2) * log_n
-    transforms = {"rescale_to_ntt": 4 * L, "tensor_to_intt": 3 * L, "mod_up_ntt_tc": dnum * E,
+    # ModUp transforms every extended limb but each partition's own (L in all), whose
+    # NTT-form words the tensor's loader provides.
+    transforms = {"rescale_to_ntt": 4 * L, "tensor_to_intt": 3 * L, "mod_up_ntt_tc": dnum * E - L,
                   "mod_down_intt": 2 * E}
     integer = {}
     for fam, limbs in transforms.items():

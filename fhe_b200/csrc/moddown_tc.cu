@@ -165,8 +165,8 @@ __global__ void __launch_bounds__(kTcThreads, K <= 10 && K != 7 ? 4 : (K <= 13 ?
   if (!ok) return;
 
   // 4. The caller's operations on the divided limbs.
-  mod_down_store(t, ks, n, moduli_id, L, poly, coeff0, kTcCoeffs, ops, out, first_limb,
-                 [&](int j, int c) -> int64_t { return divided[j * kTcCoeffs + c]; });
+  mod_down_store<true>(t, ks, n, moduli_id, L, poly, coeff0, kTcCoeffs, ops, out, first_limb,
+                       [&](int j, int c) -> int64_t { return divided[j * kTcCoeffs + c]; });
 }
 
 size_t tc_smem_bytes(int K, int L) {

@@ -162,13 +162,31 @@ __host__ __device__ constexpr int ntt_round_first(int S, int round) {
   return round * (S / ntt_rounds(S)) + (round < S % ntt_rounds(S) ? round : S % ntt_rounds(S));
 }
 
-template <int S, bool INVERSE, class Loader, class Storer, bool VALUE_ONLY = false>
+// A pass shape known at compile time: the default two-pass plan of N = 2^16
+// (8 + 8 stages, 16 sub-transforms per CTA in both passes), whose index arithmetic
+// then folds to constants.  kShapeStrided is the pass over sub-transforms of stride
+// 256, kShapeContiguous the one over 256 adjacent words.
+enum NttShape { kShapeRuntime = 0, kShapeStrided = 1, kShapeContiguous = 2 };
+constexpr int kFixedLogN = 16;
+constexpr int kFixedStages = 8;
+constexpr int kFixedColumnsLog = 4;
+
+template <int S, bool INVERSE, class Loader, class Storer, bool VALUE_ONLY = false,
+          int SHAPE = kShapeRuntime>
 __global__ void __launch_bounds__(256, 4)
     ntt_pass_kernel(NttPass a, PrimeTables t, Loader load, Storer store) {
   constexpr int M = 1 << S;
   constexpr int R = ntt_rounds(S);
   constexpr int kMaxE = 1 << kNttMaxRoundLog;
   extern __shared__ int64_t tile_smem[];
+  static_assert(SHAPE == kShapeRuntime || S == kFixedStages, "fixed shapes are 8-stage passes");
+  if (SHAPE != kShapeRuntime) {
+    // The runtime fields hold the same values; the constants let them fold.
+    a.log_n = kFixedLogN;
+    a.stride_log = SHAPE == kShapeStrided ? kFixedLogN - kFixedStages : 0;
+    a.first = (SHAPE == kShapeStrided) == INVERSE ? kFixedLogN - kFixedStages : 0;
+    a.columns_log = kFixedColumnsLog;
+  }
 
   const int pl = blockIdx.y;
   const int poly = pl % a.polys;
@@ -376,13 +394,14 @@ inline NttPlan ntt_plan(int log_n) {
 
 constexpr int kNttThreads = 256;
 
-template <int S, bool INVERSE, class Loader, class Storer, bool VALUE_ONLY = false>
+template <int S, bool INVERSE, class Loader, class Storer, bool VALUE_ONLY = false,
+          int SHAPE = kShapeRuntime>
 cudaError_t launch_ntt_pass(const NttPass &a, const PrimeTables &t, const Loader &ld,
                             const Storer &st, cudaStream_t stream) {
   const int subs = (1 << a.log_n) >> S;
   const dim3 grid(subs >> a.columns_log, a.polys * a.limbs);
   const size_t smem = sizeof(int64_t) << (a.columns_log + S);
-  auto kernel = ntt_pass_kernel<S, INVERSE, Loader, Storer, VALUE_ONLY>;
+  auto kernel = ntt_pass_kernel<S, INVERSE, Loader, Storer, VALUE_ONLY, SHAPE>;
   // Raised once per instantiation to the most any valid plan uses, so no attribute
   // call lands inside a graph capture.
   static bool raised = false;
@@ -401,6 +420,15 @@ cudaError_t launch_ntt_pass(const NttPass &a, const PrimeTables &t, const Loader
 template <bool INVERSE, class Loader, class Storer, bool VALUE_ONLY = false>
 cudaError_t dispatch_ntt_pass(int S, const NttPass &a, const PrimeTables &t, const Loader &ld,
                               const Storer &st, cudaStream_t stream) {
+  if (S == kFixedStages && a.log_n == kFixedLogN && a.columns_log == kFixedColumnsLog) {
+    const int strided_first = INVERSE ? kFixedLogN - kFixedStages : 0;
+    if (a.stride_log == kFixedLogN - kFixedStages && a.first == strided_first)
+      return launch_ntt_pass<kFixedStages, INVERSE, Loader, Storer, VALUE_ONLY, kShapeStrided>(
+          a, t, ld, st, stream);
+    if (a.stride_log == 0 && a.first == kFixedLogN - kFixedStages - strided_first)
+      return launch_ntt_pass<kFixedStages, INVERSE, Loader, Storer, VALUE_ONLY, kShapeContiguous>(
+          a, t, ld, st, stream);
+  }
   switch (S) {
     case 1: return launch_ntt_pass<1, INVERSE, Loader, Storer, VALUE_ONLY>(a, t, ld, st, stream);
     case 2: return launch_ntt_pass<2, INVERSE, Loader, Storer, VALUE_ONLY>(a, t, ld, st, stream);
