@@ -162,6 +162,8 @@ __host__ __device__ constexpr int ntt_round_first(int S, int round) {
   return round * (S / ntt_rounds(S)) + (round < S % ntt_rounds(S) ? round : S % ntt_rounds(S));
 }
 
+constexpr int kNttThreads = 256;  // threads of every pass kernel
+
 // A pass shape known at compile time: the default two-pass plan of N = 2^16
 // (8 + 8 stages, 16 sub-transforms per CTA in both passes), whose index arithmetic
 // then folds to constants.  kShapeStrided is the pass over sub-transforms of stride
@@ -173,7 +175,7 @@ constexpr int kFixedColumnsLog = 4;
 
 template <int S, bool INVERSE, class Loader, class Storer, bool VALUE_ONLY = false,
           int SHAPE = kShapeRuntime>
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(kNttThreads, 4)
     ntt_pass_kernel(NttPass a, PrimeTables t, Loader load, Storer store) {
   constexpr int M = 1 << S;
   constexpr int R = ntt_rounds(S);
@@ -223,7 +225,8 @@ __global__ void __launch_bounds__(256, 4)
     const int D = 1 << dlog;
     const int groups_per_col = M >> r;
     const int total = C * groups_per_col;
-    for (int gid = threadIdx.x; gid < total; gid += blockDim.x) {
+#pragma unroll 1
+    for (int gid = threadIdx.x; gid < total; gid += kNttThreads) {
       int c, g;
       if (strided) {
         c = gid & (C - 1);
@@ -392,7 +395,6 @@ inline NttPlan ntt_plan(int log_n) {
           tu.second_tile_log - tu.s_second};
 }
 
-constexpr int kNttThreads = 256;
 
 template <int S, bool INVERSE, class Loader, class Storer, bool VALUE_ONLY = false,
           int SHAPE = kShapeRuntime>
