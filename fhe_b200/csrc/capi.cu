@@ -32,8 +32,11 @@ void set_last_error(const std::string &message) { g_last_error = message; }
 
 namespace {
 
+// Every call runs inside an NVTX range named after the C-ABI function, so Nsight
+// tools show the reference-level operations around their kernels.
 template <class F>
-int guarded(F &&f) {
+int guarded(const char *name, F &&f) {
+  const fhe_b200::NvtxRange range(name);
   try {
     f();
     fhe_b200::set_last_error("");
@@ -130,7 +133,7 @@ static void fill_info(const fhe_b200::Parameters &p, fhe_engine_info *info) {
 int fhe_parameters_query(const fhe_config *config, fhe_engine_info *info, uint64_t *moduli,
                          int capacity) {
   REQUIRE_OUT(config);
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fhe_b200::Parameters p(to_config(config));
     if (info) fill_info(p, info);
     if (moduli)
@@ -141,7 +144,7 @@ int fhe_parameters_query(const fhe_config *config, fhe_engine_info *info, uint64
 int fhe_parameters_tables(const fhe_config *config, uint64_t *k, int64_t *r_squared,
                           int64_t *n_inverse, int64_t *root, int64_t *root_inverse) {
   REQUIRE_OUT(config);
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fhe_b200::Parameters p(to_config(config));
     if (k) std::memcpy(k, p.k.data(), sizeof(uint64_t) * p.k.size());
     if (r_squared) std::memcpy(r_squared, p.r_squared.data(), sizeof(int64_t) * p.r_squared.size());
@@ -156,7 +159,7 @@ int fhe_engine_create(const fhe_config *config, fhe_engine **engine) {
   REQUIRE_OUT(config);
   REQUIRE_OUT(engine);
   *engine = nullptr;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     auto e = new Engine(to_config(config));
     *engine = new fhe_engine{e};
   });
@@ -164,7 +167,7 @@ int fhe_engine_create(const fhe_config *config, fhe_engine **engine) {
 
 int fhe_engine_destroy(fhe_engine *engine) {
   if (!engine) return FHE_OK;
-  int rc = guarded([&] { delete engine->impl; });
+  int rc = guarded(__func__, [&] { delete engine->impl; });
   delete engine;
   return rc;
 }
@@ -172,7 +175,7 @@ int fhe_engine_destroy(fhe_engine *engine) {
 int fhe_engine_info_get(const fhe_engine *engine, fhe_engine_info *info) {
   REQUIRE_HANDLE(engine);
   REQUIRE_OUT(info);
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fill_info(engine->impl->params, info);
   });
 }
@@ -180,7 +183,7 @@ int fhe_engine_info_get(const fhe_engine *engine, fhe_engine_info *info) {
 int fhe_engine_moduli(const fhe_engine *engine, uint64_t *moduli, int capacity) {
   REQUIRE_HANDLE(engine);
   REQUIRE_OUT(moduli);
-  return guarded([&] {
+  return guarded(__func__, [&] {
     const auto &q = engine->impl->params.q;
     for (int i = 0; i < capacity && i < static_cast<int>(q.size()); i++) moduli[i] = q[i];
   });
@@ -189,28 +192,28 @@ int fhe_engine_moduli(const fhe_engine *engine, uint64_t *moduli, int capacity) 
 int fhe_engine_moduli_id(const fhe_engine *engine, int level, int *moduli_id) {
   REQUIRE_HANDLE(engine);
   REQUIRE_OUT(moduli_id);
-  return guarded([&] { *moduli_id = engine->impl->params.moduli_id(level); });
+  return guarded(__func__, [&] { *moduli_id = engine->impl->params.moduli_id(level); });
 }
 
 int fhe_engine_synchronize(fhe_engine *engine) {
   REQUIRE_HANDLE(engine);
-  return guarded([&] { engine->impl->synchronize(); });
+  return guarded(__func__, [&] { engine->impl->synchronize(); });
 }
 
 int fhe_engine_set_stream(fhe_engine *engine, void *cuda_stream) {
   REQUIRE_HANDLE(engine);
-  return guarded([&] { engine->impl->set_stream(static_cast<cudaStream_t>(cuda_stream)); });
+  return guarded(__func__, [&] { engine->impl->set_stream(static_cast<cudaStream_t>(cuda_stream)); });
 }
 
 int fhe_engine_set_profiling(fhe_engine *engine, int enable) {
   REQUIRE_HANDLE(engine);
-  return guarded([&] { engine->impl->set_profiling(enable != 0); });
+  return guarded(__func__, [&] { engine->impl->set_profiling(enable != 0); });
 }
 
 int fhe_engine_profile_report(fhe_engine *engine, char *buffer, int capacity) {
   REQUIRE_HANDLE(engine);
   REQUIRE_OUT(buffer);
-  return guarded([&] {
+  return guarded(__func__, [&] {
     const std::string r = engine->impl->profile_report();
     if (capacity <= 0) throw std::invalid_argument("the report buffer is empty.");
     const size_t n = std::min(r.size(), static_cast<size_t>(capacity - 1));
@@ -221,7 +224,7 @@ int fhe_engine_profile_report(fhe_engine *engine, char *buffer, int capacity) {
 
 int fhe_engine_profile_reset(fhe_engine *engine) {
   REQUIRE_HANDLE(engine);
-  return guarded([&] { engine->impl->profile_reset(); });
+  return guarded(__func__, [&] { engine->impl->profile_reset(); });
 }
 
 unsigned long long fhe_kernel_launch_count(void) { return fhe_b200::kernel_launch_count(); }
@@ -231,31 +234,31 @@ int fhe_data_upload(fhe_engine *engine, int type, int flag, int moduli_id, int p
   REQUIRE_HANDLE(engine);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     *out = wrap(engine->impl->upload(type, flag, moduli_id, polys, ckks_scale, host_limbs));
   });
 }
 
 int fhe_data_download(const fhe_data *data, int64_t *host_limbs) {
   REQUIRE_HANDLE(data);
-  return guarded([&] { live(nullptr, data).engine->download(*data->impl, host_limbs); });
+  return guarded(__func__, [&] { live(nullptr, data).engine->download(*data->impl, host_limbs); });
 }
 
 int fhe_data_download_async(const fhe_data *data, int64_t *host_limbs) {
   REQUIRE_HANDLE(data);
-  return guarded([&] { live(nullptr, data).engine->download_async(*data->impl, host_limbs); });
+  return guarded(__func__, [&] { live(nullptr, data).engine->download_async(*data->impl, host_limbs); });
 }
 
 int fhe_data_serialized_size(const fhe_data *data, uint64_t *size) {
   REQUIRE_HANDLE(data);
   REQUIRE_OUT(size);
-  return guarded([&] { *size = live(nullptr, data).engine->serialized_size(*data->impl); });
+  return guarded(__func__, [&] { *size = live(nullptr, data).engine->serialized_size(*data->impl); });
 }
 
 int fhe_data_serialize(const fhe_data *data, void *buffer, uint64_t capacity) {
   REQUIRE_HANDLE(data);
   REQUIRE_OUT(buffer);
-  return guarded([&] {
+  return guarded(__func__, [&] {
     live(nullptr, data).engine->serialize(*data->impl, buffer, static_cast<size_t>(capacity));
   });
 }
@@ -265,13 +268,13 @@ int fhe_data_deserialize(fhe_engine *engine, const void *buffer, uint64_t size, 
   REQUIRE_OUT(buffer);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] { *out = wrap(engine->impl->deserialize(buffer, static_cast<size_t>(size))); });
+  return guarded(__func__, [&] { *out = wrap(engine->impl->deserialize(buffer, static_cast<size_t>(size))); });
 }
 
 int fhe_data_info_get(const fhe_data *data, fhe_data_info *info) {
   REQUIRE_HANDLE(data);
   REQUIRE_OUT(info);
-  return guarded([&] {
+  return guarded(__func__, [&] {
     const Data &d = live(nullptr, data);
     info->type = d.type;
     info->flag = d.flag;
@@ -299,7 +302,7 @@ int fhe_data_device_pointer(const fhe_data *data, int64_t **device_limbs) {
 
 int fhe_data_destroy(fhe_data *data) {
   if (!data) return FHE_OK;
-  int rc = guarded([&] { delete data->impl; });
+  int rc = guarded(__func__, [&] { delete data->impl; });
   delete data;
   return rc;
 }
@@ -310,7 +313,7 @@ int fhe_data_destroy(fhe_data *data) {
     REQUIRE_HANDLE(x);                                                        \
     REQUIRE_OUT(out);                                                         \
     *out = nullptr;                                                           \
-    return guarded([&] { *out = wrap(engine->impl->call(live(engine, x))); }); \
+    return guarded(__func__, [&] { *out = wrap(engine->impl->call(live(engine, x))); }); \
   }
 
 UNARY_OP(fhe_rescale, rescale)
@@ -323,7 +326,7 @@ int fhe_multiply(fhe_engine *engine, const fhe_data *a, const fhe_data *b, fhe_d
   REQUIRE_HANDLE(b);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] { *out = wrap(engine->impl->multiply(live(engine, a), live(engine, b))); });
+  return guarded(__func__, [&] { *out = wrap(engine->impl->multiply(live(engine, a), live(engine, b))); });
 }
 
 int fhe_multiply_relinearize(fhe_engine *engine, const fhe_data *a, const fhe_data *b,
@@ -334,8 +337,8 @@ int fhe_multiply_relinearize(fhe_engine *engine, const fhe_data *a, const fhe_da
   REQUIRE_HANDLE(rk);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded(
-      [&] { *out = wrap(engine->impl->multiply_relinearize(live(engine, a), live(engine, b), live(engine, rk))); });
+  return guarded(__func__,
+                 [&] { *out = wrap(engine->impl->multiply_relinearize(live(engine, a), live(engine, b), live(engine, rk))); });
 }
 
 int fhe_multiply_relinearize_rescale(fhe_engine *engine, const fhe_data *a, const fhe_data *b,
@@ -346,7 +349,7 @@ int fhe_multiply_relinearize_rescale(fhe_engine *engine, const fhe_data *a, cons
   REQUIRE_HANDLE(rk);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     *out = wrap(engine->impl->multiply_relinearize_rescale(live(engine, a), live(engine, b), live(engine, rk)));
   });
 }
@@ -357,13 +360,13 @@ int fhe_relinearize(fhe_engine *engine, const fhe_data *ct, const fhe_data *rk, 
   REQUIRE_HANDLE(rk);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] { *out = wrap(engine->impl->relinearize(live(engine, ct), live(engine, rk))); });
+  return guarded(__func__, [&] { *out = wrap(engine->impl->relinearize(live(engine, ct), live(engine, rk))); });
 }
 
 int fhe_ntt_limbs(fhe_engine *engine, int64_t *device_limbs, int moduli_id, int chains, int polys,
                   long long poly_stride, int inverse) {
   REQUIRE_HANDLE(engine);
-  return guarded([&] {
+  return guarded(__func__, [&] {
     engine->impl->ntt_limbs(device_limbs, moduli_id, chains, polys, poly_stride, inverse != 0);
   });
 }
@@ -371,7 +374,7 @@ int fhe_ntt_limbs(fhe_engine *engine, int64_t *device_limbs, int moduli_id, int 
 int fhe_mont_mult_limbs(fhe_engine *engine, const int64_t *a, const int64_t *b, int64_t *y,
                         int moduli_id, int chains, int polys, long long poly_stride) {
   REQUIRE_HANDLE(engine);
-  return guarded([&] {
+  return guarded(__func__, [&] {
     engine->impl->mont_mult_limbs(a, b, y, moduli_id, chains, polys, poly_stride);
   });
 }
@@ -385,7 +388,7 @@ int fhe_level_down(fhe_engine *engine, const fhe_data *text, int level, fhe_data
   REQUIRE_HANDLE(text);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] { *out = wrap(engine->impl->level_down(live(engine, text), level)); });
+  return guarded(__func__, [&] { *out = wrap(engine->impl->level_down(live(engine, text), level)); });
 }
 
 int fhe_rotate(fhe_engine *engine, const fhe_data *ct, const fhe_data *key, fhe_data **out) {
@@ -394,7 +397,7 @@ int fhe_rotate(fhe_engine *engine, const fhe_data *ct, const fhe_data *key, fhe_
   REQUIRE_HANDLE(key);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] { *out = wrap(engine->impl->rotate(live(engine, ct), live(engine, key))); });
+  return guarded(__func__, [&] { *out = wrap(engine->impl->rotate(live(engine, ct), live(engine, key))); });
 }
 
 int fhe_rotate_with_keys(fhe_engine *engine, const fhe_data *ct, const fhe_data *const *keys,
@@ -409,7 +412,7 @@ int fhe_rotate_with_keys(fhe_engine *engine, const fhe_data *ct, const fhe_data 
     return FHE_ERR_INVALID_ARGUMENT;
   }
   for (int i = 0; i < key_count; i++) REQUIRE_HANDLE(keys[i]);
-  return guarded([&] {
+  return guarded(__func__, [&] {
     std::vector<const fhe_b200::Data *> list;
     for (int i = 0; i < key_count; i++) list.push_back(&live(engine, keys[i]));
     *out = wrap(engine->impl->rotate(live(engine, ct), list, delta, normalize_by_slot_count != 0));
@@ -421,7 +424,7 @@ int fhe_rotate_plaintext(fhe_engine *engine, const fhe_data *pt, int delta, fhe_
   REQUIRE_HANDLE(pt);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] { *out = wrap(engine->impl->rotate_plain(live(engine, pt), delta)); });
+  return guarded(__func__, [&] { *out = wrap(engine->impl->rotate_plain(live(engine, pt), delta)); });
 }
 
 int fhe_conjugate(fhe_engine *engine, const fhe_data *ct, const fhe_data *key, fhe_data **out) {
@@ -430,7 +433,7 @@ int fhe_conjugate(fhe_engine *engine, const fhe_data *ct, const fhe_data *key, f
   REQUIRE_HANDLE(key);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] { *out = wrap(engine->impl->conjugate(live(engine, ct), live(engine, key))); });
+  return guarded(__func__, [&] { *out = wrap(engine->impl->conjugate(live(engine, ct), live(engine, key))); });
 }
 
 int fhe_conjugate_plaintext(fhe_engine *engine, const fhe_data *pt, fhe_data **out) {
@@ -438,7 +441,7 @@ int fhe_conjugate_plaintext(fhe_engine *engine, const fhe_data *pt, fhe_data **o
   REQUIRE_HANDLE(pt);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] { *out = wrap(engine->impl->conjugate_plain(live(engine, pt))); });
+  return guarded(__func__, [&] { *out = wrap(engine->impl->conjugate_plain(live(engine, pt))); });
 }
 
 int fhe_switch_key(fhe_engine *engine, const fhe_data *ct, const fhe_data *key, fhe_data **out) {
@@ -447,7 +450,7 @@ int fhe_switch_key(fhe_engine *engine, const fhe_data *ct, const fhe_data *key, 
   REQUIRE_HANDLE(key);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] { *out = wrap(engine->impl->switch_key(live(engine, ct), live(engine, key))); });
+  return guarded(__func__, [&] { *out = wrap(engine->impl->switch_key(live(engine, ct), live(engine, key))); });
 }
 
 }  // extern "C"
@@ -459,14 +462,14 @@ int fhe_encode(fhe_engine *engine, const double *re, const double *im, int count
   REQUIRE_HANDLE(engine);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded(
-      [&] { *out = wrap(engine->impl->encode(re, im, count, level, include_special != 0)); });
+  return guarded(__func__,
+                 [&] { *out = wrap(engine->impl->encode(re, im, count, level, include_special != 0)); });
 }
 
 int fhe_decode(fhe_engine *engine, const fhe_data *pt, double *re, double *im) {
   REQUIRE_HANDLE(engine);
   REQUIRE_HANDLE(pt);
-  return guarded([&] { engine->impl->decode(live(engine, pt), re, im); });
+  return guarded(__func__, [&] { engine->impl->decode(live(engine, pt), re, im); });
 }
 
 }  // extern "C"
@@ -475,14 +478,14 @@ extern "C" {
 
 int fhe_engine_seed(fhe_engine *engine, const uint32_t *seed, const uint8_t *nonce) {
   REQUIRE_HANDLE(engine);
-  return guarded([&] { engine->impl->seed(seed, nonce); });
+  return guarded(__func__, [&] { engine->impl->seed(seed, nonce); });
 }
 
 int fhe_create_secret_key(fhe_engine *engine, int level, fhe_data **out) {
   REQUIRE_HANDLE(engine);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     auto &e = *engine->impl;
     *out = wrap(e.create_secret_key(level < 0 ? e.params.max_level() : level));
   });
@@ -493,7 +496,7 @@ int fhe_create_secret_key_from(fhe_engine *engine, const int64_t *secret, int co
   REQUIRE_HANDLE(engine);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     auto &e = *engine->impl;
     *out = wrap(e.create_secret_key(secret, count, level < 0 ? e.params.max_level() : level));
   });
@@ -504,7 +507,7 @@ int fhe_create_sparse_secret_key(fhe_engine *engine, int hamming_weight, int lev
   REQUIRE_HANDLE(engine);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     auto &e = *engine->impl;
     *out = wrap(e.create_sparse_secret_key(hamming_weight, level < 0 ? e.params.max_level() : level));
   });
@@ -515,7 +518,7 @@ int fhe_create_public_key(fhe_engine *engine, const fhe_data *sk, int level, fhe
   REQUIRE_HANDLE(sk);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     auto &e = *engine->impl;
     *out = wrap(e.create_public_key(live(engine, sk), level < 0 ? e.params.max_level() : level));
   });
@@ -527,7 +530,7 @@ int fhe_create_relinearization_key(fhe_engine *engine, const fhe_data *sk, int l
   REQUIRE_HANDLE(sk);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     auto &e = *engine->impl;
     *out = wrap(e.create_relinearization_key(
         live(engine, sk), level < 0 ? e.params.max_key_switching_level() : level));
@@ -540,7 +543,7 @@ int fhe_create_fixed_rotation_key(fhe_engine *engine, const fhe_data *sk, int de
   REQUIRE_HANDLE(sk);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     auto &e = *engine->impl;
     const int nd = e.normalized_delta(delta, normalize_by_slot_count != 0);
     *out = wrap(e.create_fixed_rotation_key(
@@ -555,7 +558,7 @@ int fhe_create_rotation_keys(fhe_engine *engine, const fhe_data *sk, int level, 
   REQUIRE_OUT(keys);
   REQUIRE_OUT(count);
   *count = 0;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     auto &e = *engine->impl;
     int needed = 0;
     for (int d = 1; d < e.params.n / 2; d <<= 1) needed++;
@@ -573,7 +576,7 @@ int fhe_create_conjugation_key(fhe_engine *engine, const fhe_data *sk, int level
   REQUIRE_HANDLE(sk);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     auto &e = *engine->impl;
     *out = wrap(e.create_conjugation_key(live(engine, sk),
                                          level < 0 ? e.params.max_key_switching_level() : level));
@@ -586,7 +589,7 @@ int fhe_encrypt(fhe_engine *engine, const fhe_data *pt, const fhe_data *key, fhe
   REQUIRE_HANDLE(key);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] { *out = wrap(engine->impl->encrypt(live(engine, pt), live(engine, key))); });
+  return guarded(__func__, [&] { *out = wrap(engine->impl->encrypt(live(engine, pt), live(engine, key))); });
 }
 
 int fhe_decrypt(fhe_engine *engine, const fhe_data *ct, const fhe_data *sk, fhe_data **out) {
@@ -595,7 +598,7 @@ int fhe_decrypt(fhe_engine *engine, const fhe_data *ct, const fhe_data *sk, fhe_
   REQUIRE_HANDLE(sk);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] { *out = wrap(engine->impl->decrypt(live(engine, ct), live(engine, sk))); });
+  return guarded(__func__, [&] { *out = wrap(engine->impl->decrypt(live(engine, ct), live(engine, sk))); });
 }
 
 }  // extern "C"
@@ -609,7 +612,7 @@ extern "C" {
     REQUIRE_HANDLE(b);                                                                 \
     REQUIRE_OUT(out);                                                                  \
     *out = nullptr;                                                                    \
-    return guarded([&] {                                                               \
+    return guarded(__func__, [&] {                                                               \
       auto &e = *engine->impl;                                                         \
       const Data &x = live(engine, a);                                                 \
       const Data &y = live(engine, b);                                                 \
@@ -630,7 +633,7 @@ FHE_BINARY_OP(fhe_multiply_plaintext, e.multiply_plain(x, y))
     REQUIRE_HANDLE(a);                                                             \
     REQUIRE_OUT(out);                                                              \
     *out = nullptr;                                                                \
-    return guarded([&] {                                                           \
+    return guarded(__func__, [&] {                                                           \
       auto &e = *engine->impl;                                                     \
       const Data &x = live(engine, a);                                             \
       *out = wrap(call);                                                           \
@@ -647,7 +650,7 @@ int fhe_negate(fhe_engine *engine, const fhe_data *ct, fhe_data **out) {
   REQUIRE_HANDLE(ct);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] { *out = wrap(engine->impl->negate(live(engine, ct))); });
+  return guarded(__func__, [&] { *out = wrap(engine->impl->negate(live(engine, ct))); });
 }
 
 int fhe_square(fhe_engine *engine, const fhe_data *ct, const fhe_data *rk, fhe_data **out) {
@@ -655,7 +658,7 @@ int fhe_square(fhe_engine *engine, const fhe_data *ct, const fhe_data *rk, fhe_d
   REQUIRE_HANDLE(ct);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     const Data *key = rk ? &live(engine, rk) : nullptr;
     *out = wrap(engine->impl->square(live(engine, ct), key));
   });
@@ -673,7 +676,7 @@ int fhe_create_small_bootstrap_key(fhe_engine *engine, const fhe_data *sk, fhe_d
   REQUIRE_OUT(to_dense);
   *to_sparse = nullptr;
   *to_dense = nullptr;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     auto keys = engine->impl->create_small_bootstrap_key(live(engine, sk));
     *to_sparse = wrap(std::move(keys.first));
     *to_dense = wrap(std::move(keys.second));
@@ -697,7 +700,7 @@ int fhe_bootstrap(fhe_engine *engine, const fhe_data *ct, const fhe_data *rk, co
     return FHE_ERR_INVALID_ARGUMENT;
   }
   for (int i = 0; i < rotation_key_count; i++) REQUIRE_HANDLE(rotation_keys[i]);
-  return guarded([&] {
+  return guarded(__func__, [&] {
     std::vector<const Data *> keys;
     for (int i = 0; i < rotation_key_count; i++) keys.push_back(&live(engine, rotation_keys[i]));
     *out = wrap(engine->impl->bootstrap(live(engine, ct), live(engine, rk), live(engine, ck), keys,
@@ -730,7 +733,7 @@ int fhe_rotate_batch(fhe_engine *engine, const fhe_data *ct, const fhe_data *con
     REQUIRE_HANDLE(keys[i]);
     out[i] = nullptr;
   }
-  return guarded([&] {
+  return guarded(__func__, [&] {
     std::vector<const Data *> ks;
     for (int i = 0; i < key_count; i++) ks.push_back(&live(engine, keys[i]));
     auto r = engine->impl->rotate_batch(live(engine, ct), ks);
@@ -764,17 +767,17 @@ int fhe_ntt_tuning_get(int log_n, int *s_second, int *first_columns_log, int *se
 
 int fhe_engine_set_tensor_cores(fhe_engine *engine, int mode) {
   REQUIRE_HANDLE(engine);
-  return guarded([&] { engine->impl->set_tensor_cores(mode); });
+  return guarded(__func__, [&] { engine->impl->set_tensor_cores(mode); });
 }
 
 int fhe_engine_set_tensor_core_wait_limit(fhe_engine *engine, long long limit) {
   REQUIRE_HANDLE(engine);
-  return guarded([&] { engine->impl->set_tensor_core_wait_limit(limit); });
+  return guarded(__func__, [&] { engine->impl->set_tensor_core_wait_limit(limit); });
 }
 
 int fhe_engine_set_graphs(fhe_engine *engine, int enable) {
   REQUIRE_HANDLE(engine);
-  return guarded([&] { engine->impl->set_graphs(enable != 0); });
+  return guarded(__func__, [&] { engine->impl->set_graphs(enable != 0); });
 }
 
 int fhe_multiply_rotate_batch(fhe_engine *engine, int count, const fhe_data *const *a,
@@ -796,7 +799,7 @@ int fhe_multiply_rotate_batch(fhe_engine *engine, int count, const fhe_data *con
     REQUIRE_HANDLE(rotation_keys[i]);
     out[i] = nullptr;
   }
-  return guarded([&] {
+  return guarded(__func__, [&] {
     std::vector<const Data *> va, vb, vk;
     for (int i = 0; i < count; i++) {
       va.push_back(&live(engine, a[i]));
@@ -825,7 +828,7 @@ int fhe_multiply_relinearize_rescale_batch(fhe_engine *engine, int count,
     REQUIRE_HANDLE(b[i]);
     out[i] = nullptr;
   }
-  return guarded([&] {
+  return guarded(__func__, [&] {
     std::vector<const Data *> va, vb;
     for (int i = 0; i < count; i++) {
       va.push_back(&live(engine, a[i]));
@@ -854,7 +857,7 @@ int fhe_bootstrap_batch(fhe_engine *engine, int count, const fhe_data *const *ct
     REQUIRE_HANDLE(cts[i]);
     out[i] = nullptr;
   }
-  return guarded([&] {
+  return guarded(__func__, [&] {
     std::vector<const Data *> v;
     for (int i = 0; i < count; i++) v.push_back(&live(engine, cts[i]));
     auto r = engine->impl->bootstrap_batch(v, live(engine, relinearization_key),
@@ -866,14 +869,14 @@ int fhe_bootstrap_batch(fhe_engine *engine, int count, const fhe_data *const *ct
 
 int fhe_engine_set_concurrency(fhe_engine *engine, int streams) {
   REQUIRE_HANDLE(engine);
-  return guarded([&] { engine->impl->set_concurrency(streams); });
+  return guarded(__func__, [&] { engine->impl->set_concurrency(streams); });
 }
 
 int fhe_engine_graph_counts(const fhe_engine *engine, int *captured, int *failed) {
   REQUIRE_HANDLE(engine);
   REQUIRE_OUT(captured);
   REQUIRE_OUT(failed);
-  return guarded([&] {
+  return guarded(__func__, [&] {
     const auto c = engine->impl->graph_counts();
     *captured = c.first;
     *failed = c.second;
@@ -887,7 +890,7 @@ int fhe_create_bootstrap_key(fhe_engine *engine, const fhe_data *secret_key, int
   REQUIRE_OUT(size);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     auto bk = engine->impl->create_bootstrap_key(live(engine, secret_key), stage_count, size);
     auto h = new fhe_bootstrap_key;
     h->impl = bk.release();
@@ -905,7 +908,7 @@ int fhe_bootstrap_key_destroy(fhe_bootstrap_key *key) {
 int fhe_bootstrap_key_info(const fhe_bootstrap_key *key, int *stage_count, int *inner_loop_shift,
                            int *rotation_key_count, uint64_t *bytes) {
   REQUIRE_HANDLE(key);
-  return guarded([&] {
+  return guarded(__func__, [&] {
     const auto &bk = live_key(nullptr, key);
     if (stage_count) *stage_count = bk.stage_count;
     if (inner_loop_shift) *inner_loop_shift = bk.inner_loop_shift;
@@ -917,7 +920,7 @@ int fhe_bootstrap_key_info(const fhe_bootstrap_key *key, int *stage_count, int *
 int fhe_bootstrap_key_deltas(const fhe_bootstrap_key *key, int *deltas, int capacity, int *count) {
   REQUIRE_HANDLE(key);
   REQUIRE_OUT(count);
-  return guarded([&] {
+  return guarded(__func__, [&] {
     const auto &bk = live_key(nullptr, key);
     int i = 0;
     for (const auto &kv : bk.rotation_keys) {
@@ -934,7 +937,7 @@ int fhe_bootstrap_key_rotation_key(fhe_engine *engine, const fhe_bootstrap_key *
   REQUIRE_HANDLE(key);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     const auto &bk = live_key(engine, key);
     auto it = bk.rotation_keys.find(delta);
     if (it == bk.rotation_keys.end())
@@ -955,7 +958,7 @@ static const fhe_b200::BootstrapStage &key_stage(const fhe_b200::BootstrapKey &b
 int fhe_bootstrap_key_stage(const fhe_bootstrap_key *key, int to_slot, int stage, int *level,
                             int *inner_loop_count, int *outer_loop_count) {
   REQUIRE_HANDLE(key);
-  return guarded([&] {
+  return guarded(__func__, [&] {
     const auto &st = key_stage(live_key(nullptr, key), to_slot, stage);
     if (level) *level = st.level;
     if (inner_loop_count) *inner_loop_count = st.inner;
@@ -969,7 +972,7 @@ int fhe_bootstrap_key_diagonal(fhe_engine *engine, const fhe_bootstrap_key *key,
   REQUIRE_HANDLE(key);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     const auto &st = key_stage(live_key(engine, key), to_slot, stage);
     auto row = st.diagonals.find(outer);
     if (row == st.diagonals.end()) return;
@@ -987,7 +990,7 @@ int fhe_bootstrap_key_small(fhe_engine *engine, const fhe_bootstrap_key *key,
   REQUIRE_OUT(to_dense);
   *to_sparse = nullptr;
   *to_dense = nullptr;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     const auto &bk = live_key(engine, key);
     auto a = engine->impl->clone(*bk.to_sparse);
     auto b = engine->impl->clone(*bk.to_dense);
@@ -1006,7 +1009,7 @@ int fhe_bootstrap_with_key(fhe_engine *engine, const fhe_data *ct,
   REQUIRE_HANDLE(bootstrap_key);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     *out = wrap(engine->impl->bootstrap(live(engine, ct), live(engine, relinearization_key),
                                         live(engine, conjugation_key),
                                         live_key(engine, bootstrap_key)));
@@ -1021,7 +1024,7 @@ int fhe_rotate_with_bootstrap_key(fhe_engine *engine, const fhe_data *ct,
   REQUIRE_HANDLE(bootstrap_key);
   REQUIRE_OUT(out);
   *out = nullptr;
-  return guarded([&] {
+  return guarded(__func__, [&] {
     *out = wrap(engine->impl->rotate(live(engine, ct), live_key(engine, bootstrap_key), delta));
   });
 }

@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <complex>
 #include <functional>
@@ -20,6 +21,15 @@
 #include "params.hpp"
 
 namespace fhe_b200 {
+
+// An NVTX range for the lifetime of the object (a no-op unless an Nsight tool is
+// attached): C-ABI calls and kernel families show up by name on profiler timelines.
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 enum DataFlag : int {
   kFlagNone = 0,
@@ -481,6 +491,7 @@ class Engine {
   void collect_timings();
   template <class F>
   cudaError_t timed(const char *name, F &&launch) {
+    const NvtxRange range(name);
     if (!profiling_) return launch();
     PendingTiming p{name, take_event(), take_event()};
     cudaEventRecord(p.start, stream_);
