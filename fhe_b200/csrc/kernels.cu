@@ -148,8 +148,10 @@ __global__ void scalar_rescale_kernel(PrimeTables t, KeySwitchTables ks, int log
 
 // One partition of alpha = A limbs per thread-coefficient (rns_to_mrs,
 // core_key_switch.cpp:21-56, Garner's algorithm with the reference's lazy ranges).
+// Three CTAs per SM where the digits fit the registers that leaves (A <= 10).
 template <int A>
-__global__ void mixed_radix_kernel(PrimeTables t, DevicePartitions dp, int n, int moduli_id,
+__global__ void __launch_bounds__(256, A <= 10 ? 3 : 2)
+    mixed_radix_kernel(PrimeTables t, DevicePartitions dp, int n, int moduli_id,
                                    const int64_t *x, int64_t *digits) {
   const int p = blockIdx.y;
   if (dp.size[p] != A) return;
