@@ -139,17 +139,20 @@ class ClockSampler:
 def kernel_bytes(L: int, E: int, dnum: int, n: int) -> dict:
     """Algorithmic HBM bytes per timed launch of each kernel family at the
     relinearize level (L limbs, E = L + K extended limbs): each limb operand read or
-    written once, twiddle tables excluded."""
+    written once, twiddle tables excluded.  Each partition's own L limbs of the
+    extended polynomials are written by the tensor-product pass from the input's NTT
+    form, so ModUp writes and transforms the other dnum * E - L."""
     limb = 8 * n
+    up = dnum * E - L
     return {
         "rescale": (2 * (L + 1) + 2 * L) * limb,          # 2 polys, L+1 -> L limbs
         "to_ntt": 2 * 4 * L * limb,                         # 4 polys in and out
         "rescale_to_ntt": (2 * (L + 1) + 2 * L) * limb,     # one input: rescaled, NTT
         "tensor_to_intt": (4 * L + 3 * L) * limb,           # 4 NTT polys in, 3 out
         "mixed_radix": 2 * L * limb,                        # digits of poly 2
-        "mod_up_ntt": (L + dnum * E) * limb,                # digits in, extended out
-        "mod_up_contract_tc": (L + dnum * E) * limb,        # digits in, extended out
-        "mod_up_ntt_tc": 2 * dnum * E * limb,               # extended limbs in and out
+        "mod_up_ntt": (L + up) * limb,                      # digits in, extended out
+        "mod_up_contract_tc": (L + up) * limb,              # digits in, extended out
+        "mod_up_ntt_tc": 2 * up * limb,                     # extended limbs in and out
         "key_inner_product": (3 * dnum * E + 2 * E) * limb, # ext + 2 key polys, 2 out
         "mod_down_intt": 2 * 2 * E * limb,                  # 2 polys in and out
         "mod_down_epilogue": (2 * E + 2 * L + 2 * (L - 1)) * limb,
