@@ -832,32 +832,105 @@ std::unique_ptr<Data> Engine::rotate(const Data &ct, const BootstrapKey &bk, int
   return rotate(ct, rotation_context(fn, bk, nd));
 }
 
+std::vector<Owned> Engine::bsgs_inner_sums(const Data &x, const Data &decomposed,
+                                           const BootstrapKey &bk, const BootstrapStage &stage) {
+  // The limits of bsgs.cu (up to 16 inner texts, 8 outer indices, 8 partitions);
+  // outside them, or with a rotation the unfused path would refuse, the caller runs
+  // the unfused path, which also raises its errors.  One sum per process-order
+  // entry; the outer indices of an entry are consecutive kernel groups.
+  const int m = x.moduli_id, n = params.n;
+  if (!fused_bsgs_ || stage.inner < 1 || stage.inner > kBsgsMaxInner ||
+      stage.process_order.empty() || x.polys != 2 || decomposed.moduli_id != m ||
+      decomposed.chains != x.chains || decomposed.polys > kBsgsMaxPartitions ||
+      static_cast<int>(stage.inner_deltas.size()) != stage.inner)
+    return {};
+  BsgsInner b;
+  b.inner = stage.inner;
+  for (int i = 1; i < stage.inner; i++) {
+    const int nd = normalized_delta(stage.inner_deltas[i]);
+    auto it = bk.rotation_keys.find(nd);
+    if (nd == 0 || it == bk.rotation_keys.end()) return {};
+    const Data &key = *it->second;
+    if (key.moduli_id > m) return {};
+    const DevicePartitions &dp = partitions(m, key.moduli_id);
+    if (dp.count != decomposed.polys || key.polys < 2 * (dp.max_key_index + 1)) return {};
+    const auto parts = params.partitions(m, key.moduli_id);
+    const long long kp = key.chains, vo = m - key.moduli_id;
+    for (int p = 0; p < dp.count; p++) {
+      const long long off = (2LL * parts[p].partition_index * kp + vo) * n;
+      if (off + kp * n > INT32_MAX) return {};
+      b.key_off[i][p] = static_cast<int32_t>(off);
+    }
+    b.key_poly[i] = static_cast<int32_t>(kp * n);
+    b.perm[i] = device_ntt_permutation(nd);
+    b.key[i] = key.d;
+  }
+  std::vector<Owned> sums;
+  int g = 0;  // kernel group: one outer index
+  for (size_t e = 0; e < stage.process_order.size(); e++) {
+    b.lead |= 1u << g;
+    for (int o : stage.process_order[e].second) {
+      if (g == kBsgsMaxGroups) return {};
+      const auto row = stage.diagonals.find(o);
+      if (row == stage.diagonals.end()) return {};
+      for (int i = (o == 0 ? 1 : 0); i < stage.inner; i++) {
+        const auto cell = row->second.find(i);
+        if (cell == row->second.end()) return {};
+        const Data &diagonal = *cell->second;
+        if (diagonal.moduli_id != m || diagonal.chains != x.chains) return {};
+        b.diag[i][g] = diagonal.d;
+        b.mask[i] |= 1u << g;
+        if (sums.size() == e)  // the unfused path's inner_sum, made at the entry's first term
+          sums.push_back(make_data(kUnitCiphertext, (x.flag | diagonal.flag) & ~kFlagRescaled, m,
+                                   2, x.scale * diagonal.scale));
+      }
+      if (sums.size() != e + 1) return {};
+      b.out[g] = sums.back()->d;
+      g++;
+    }
+  }
+  b.groups = g;
+  check(timed("bsgs_inner", [&] {
+          return launch_bsgs_inner(tables_, params.log_n, m, x.chains, decomposed.polys, x.d,
+                                   x.poly_stride(), decomposed.d, b, stream_);
+        }),
+        "apply butterfly");
+  return sums;
+}
+
 std::unique_ptr<Data> Engine::apply_butterfly(const Data &ct, const BootstrapKey &bk,
                                               const BootstrapStage &stage) {
   // CKKSEngine::apply_butterfly(ct, bootstrap key, stage) (engine_bootstrap.cpp:216-291):
   // one decomposition serves every inner rotation; the diagonal products of each
-  // outer group are summed in the extended domain and rotated once.
+  // outer group are summed in the extended domain and rotated once.  The inner loop
+  // runs as one fused kernel where bsgs_inner_sums covers the stage.
   if (ct.level() <= 0)
     throw std::runtime_error(
         "Rescale Unit Ciphertext: the input unit ciphertext should have a positive level.");
   Owned inner0;
   std::vector<Owned> rotated;
+  std::vector<Owned> fused;
   {
     auto rescaled = rescale_any(ct);
     auto decomposed = decompose(*rescaled);
     inner0 = attach_special_primes(*rescaled);
-    for (int delta : stage.inner_deltas) {
-      if (delta == 0) continue;
-      rotated.push_back(ntt_rotate(*inner0, *decomposed, bk, delta));
+    fused = bsgs_inner_sums(*inner0, *decomposed, bk, stage);
+    if (fused.empty()) {
+      for (int delta : stage.inner_deltas) {
+        if (delta == 0) continue;
+        rotated.push_back(ntt_rotate(*inner0, *decomposed, bk, delta));
+      }
     }
   }
   auto inner_text = [&](int i) -> const Data & { return i == 0 ? *inner0 : *rotated[i - 1]; };
   Owned outer_sum;
-  for (const auto &[delta, outer_indices] : stage.process_order) {
+  for (size_t gi = 0; gi < stage.process_order.size(); gi++) {
+    const auto &[delta, outer_indices] = stage.process_order[gi];
     // multiply_for_butterfly (CKKSCore::multiply(ct, pt), core.cpp:257-282) of every
     // (text, diagonal) pair of the group, summed with add_inplace: one fused pass per
     // kMaxMacTerms pairs.
     Owned inner_sum;
+    if (!fused.empty()) inner_sum = std::move(fused[gi]);
     MacTerms terms;
     bool continued = false;  // a previous pass already started the chain in inner_sum
     auto flush = [&]() {
@@ -872,7 +945,7 @@ std::unique_ptr<Data> Engine::apply_butterfly(const Data &ct, const BootstrapKey
       terms.count = 0;
       continued = true;
     };
-    for (int o : outer_indices) {
+    for (int o : fused.empty() ? outer_indices : std::vector<int>{}) {
       const auto &row = stage.diagonals.at(o);
       for (int i = (o == 0 ? 1 : 0); i < stage.inner; i++) {
         const Data &x = inner_text(i);

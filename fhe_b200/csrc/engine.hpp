@@ -259,6 +259,10 @@ class Engine {
   // captured once as a CUDA graph and replayed (one launch instead of ~10^4); on by
   // default, off while profiling.  Same words either way.
   void set_graphs(bool on) { graphs_ = on; }
+  // The inner loop of a bootstrap key's linear transforms as one fused kernel (on by
+  // default) or as the per-rotation key products, gathers and diagonal sums; same
+  // words either way.
+  void set_fused_bsgs(bool on) { fused_bsgs_ = on; }
   // Runs a batch of independent multiply-relinearize-rescale operations, each followed
   // by a rotation with its own fixed key (the batched serving step; no reference
   // counterpart), replayed as one CUDA graph after its first run.
@@ -351,7 +355,8 @@ class Engine {
   int tensor_cores_ = kTensorCoresAuto;
   uint64_t serial_ = 0;
   // CUDA graphs of multi-kernel operations (graphs.cu): key = the operation, the
-  // serial numbers of its constant operands, the shapes of its inputs and the stream.
+  // serial numbers of its constant operands, the kernel-form switches, the shapes of
+  // its inputs and the stream.
   struct GraphShape {
     int type, flag, moduli_id, polys;
     long double scale;
@@ -362,6 +367,7 @@ class Engine {
     unsigned long long launches = 0;
   };
   bool graphs_ = true;
+  bool fused_bsgs_ = true;
   // Streams of batch items (graphs.cu): item i of a batch runs on worker i % count,
   // forked from and joined back into the engine's stream by events.
   int concurrency_ = 4;
@@ -461,6 +467,11 @@ class Engine {
                                         int delta);
   std::unique_ptr<Data> apply_butterfly(const Data &ct, const BootstrapKey &bk,
                                         const BootstrapStage &stage);
+  // Every outer group's sum of the stage's inner loop (bsgs.cu), in process order;
+  // empty when the stage falls outside the fused kernel's limits.
+  std::vector<std::unique_ptr<Data>> bsgs_inner_sums(const Data &x, const Data &decomposed,
+                                                     const BootstrapKey &bk,
+                                                     const BootstrapStage &stage);
   // ModUp of every partition of one coefficient-form polynomial (L limbs at
   // moduli_id) into `out` ([partitions][L+K][N]).
   void decompose_into(const int64_t *x, int moduli_id, int64_t *out);

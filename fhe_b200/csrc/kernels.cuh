@@ -253,6 +253,37 @@ cudaError_t launch_diagonal_mac(const PrimeTables &t, int log_n, int limbs, int 
                                 const MacTerms &terms, long long x_stride, bool accumulate,
                                 int64_t *y, long long y_stride, cudaStream_t s);
 
+// The whole inner loop of the hoisted linear transform (apply_butterfly with a
+// bootstrap key, engine_bootstrap.cpp:218-262) in one pass over the extended chain:
+// inner text 0 is x itself, inner text i >= 1 is x rotated by inner delta i through
+// the decomposition (ntt_rotate: the key inner product with rotation key i, x's
+// polynomial 0 added, gathered by perm i), and every outer index g sums its
+// diagonal products over the inner texts, i ascending.  Consecutive outer indices
+// that share a giant-step delta share an output (their sums added): bit g of
+// `lead` marks the first of a run, and out[g] is the run's output.
+constexpr int kBsgsMaxInner = 16;
+constexpr int kBsgsMaxGroups = 8;
+constexpr int kBsgsMaxPartitions = 8;
+struct BsgsInner {
+  int inner = 0;
+  int groups = 0;
+  const int32_t *perm[kBsgsMaxInner] = {};  // [N] source position per output position
+  const int64_t *key[kBsgsMaxInner] = {};   // rotation key i
+  // Words from the key to partition p's polynomial-0 row at the text's first limb,
+  // ((2 key partition) key_primes + moduli_id - key_moduli_id) N, and from a
+  // polynomial-0 row to its polynomial-1 row, key_primes N.
+  int32_t key_off[kBsgsMaxInner][kBsgsMaxPartitions] = {};
+  int32_t key_poly[kBsgsMaxInner] = {};
+  const int64_t *diag[kBsgsMaxInner][kBsgsMaxGroups] = {};  // [extended][N], or none
+  uint32_t mask[kBsgsMaxInner] = {};  // bit g: diag[i][g] present
+  uint32_t lead = 0;                  // bit g: outer index g starts an output
+  int64_t *out[kBsgsMaxGroups] = {};  // [2][extended][N]
+};
+// x: [2][extended][N] at poly stride x_stride; decomposed: [partitions][extended][N].
+cudaError_t launch_bsgs_inner(const PrimeTables &t, int log_n, int moduli_id, int extended,
+                              int partitions, const int64_t *x, long long x_stride,
+                              const int64_t *decomposed, const BsgsInner &b, cudaStream_t s);
+
 // Shapes of the two-pass NTT of 2^log_n words (12 <= log_n <= 17): the inner pass
 // covers s_second stages, the outer (strided) pass the others; first_columns_log
 // sub-transforms share a CTA in the outer pass, 2^second_tile_log words make a CTA

@@ -158,12 +158,39 @@ struct RedcSum {
 // 16 terms: the sum is below 2^126 and its REDC below (terms / 2 + 1) q.
 struct WideSum {
   uint64_t lo = 0, hi = 0;
+  // sum += a b (the caller keeps the sum below 2^128).  On the device the four
+  // 32 x 32 partial products go straight into the 128-bit sum through the carry
+  // flag, column by column.
   FHE_HD void add(uint64_t a, uint64_t b) {
+#ifdef __CUDA_ARCH__
+    asm("{\n\t"
+        ".reg .u32 a0, a1, b0, b1, s0, s1, s2, s3;\n\t"
+        "mov.b64 {a0, a1}, %2;\n\t"
+        "mov.b64 {b0, b1}, %3;\n\t"
+        "mov.b64 {s0, s1}, %0;\n\t"
+        "mov.b64 {s2, s3}, %1;\n\t"
+        "mad.lo.cc.u32 s0, a0, b0, s0;\n\t"
+        "madc.hi.cc.u32 s1, a0, b0, s1;\n\t"
+        "madc.lo.cc.u32 s2, a1, b1, s2;\n\t"
+        "madc.hi.u32 s3, a1, b1, s3;\n\t"
+        "mad.lo.cc.u32 s1, a0, b1, s1;\n\t"
+        "madc.hi.cc.u32 s2, a0, b1, s2;\n\t"
+        "addc.u32 s3, s3, 0;\n\t"
+        "mad.lo.cc.u32 s1, a1, b0, s1;\n\t"
+        "madc.hi.cc.u32 s2, a1, b0, s2;\n\t"
+        "addc.u32 s3, s3, 0;\n\t"
+        "mov.b64 %0, {s0, s1};\n\t"
+        "mov.b64 %1, {s2, s3};\n\t"
+        "}"
+        : "+l"(lo), "+l"(hi)
+        : "l"(a), "l"(b));
+#else
     uint64_t l, h;
     mul_wide(a, b, l, h);
     const uint64_t nl = lo + l;
     hi += h + (nl < lo ? 1 : 0);
     lo = nl;
+#endif
   }
   // REDC(sum) reduced modulo m (q or 2q); inv_m ~ 1/m.
   FHE_HD int64_t reduce(uint64_t q, uint64_t k, uint64_t m, double inv_m) const {

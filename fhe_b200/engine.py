@@ -475,6 +475,11 @@ class Engine:
         """CUDA-graph replay of bootstrap(ct, rk, ck, bootstrap_key) (default on)."""
         check(_lib.load().fhe_engine_set_graphs(self._h, int(enable)))
 
+    def set_fused_bsgs(self, enable: bool) -> None:
+        """The inner loop of a bootstrap key's linear transforms as one fused kernel
+        (default on) or as per-rotation kernels; same words either way."""
+        check(_lib.load().fhe_engine_set_fused_bsgs(self._h, int(enable)))
+
     def multiply_rotate_batch(self, a: list, b: list, relinearization_key: Data,
                               rotation_keys: list) -> list:
         """[rotate(multiply_relinearize_rescale(a[i], b[i], rk), rotation_keys[i])]: one

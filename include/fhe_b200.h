@@ -472,6 +472,11 @@ int fhe_engine_set_concurrency(fhe_engine *engine, int streams);
  * fhe_bootstrap_with_key and fhe_multiply_rotate_batch capture the whole operation
  * once and replay it.  Graphs are not used while profiling.  Same words either way. */
 int fhe_engine_set_graphs(fhe_engine *engine, int enable);
+/* The inner loop of a bootstrap key's linear transforms (engine_bootstrap.cpp:218-262:
+ * the inner rotations through one decomposition and every outer group's diagonal
+ * sums) as one fused kernel (default on) or as per-rotation kernels.  Same words
+ * either way. */
+int fhe_engine_set_fused_bsgs(fhe_engine *engine, int enable);
 /* The number of captured bootstrap graphs the engine holds, and of input shapes
  * whose capture failed and which therefore run directly. */
 int fhe_engine_graph_counts(const fhe_engine *engine, int *captured, int *failed);

@@ -71,7 +71,12 @@ def test_bootstrap_key_matches_recorded_reference(engines, case):
     e.set_graphs(False)
     try:
         assert digest(e.bootstrap(ct, rk, ck, bk).download()) == d["bootstrapped"]
+        # The linear transforms' inner loops as per-rotation kernels instead of the
+        # fused kernel: the same words.
+        e.set_fused_bsgs(False)
+        assert digest(e.bootstrap(ct, rk, ck, bk).download()) == d["bootstrapped"]
     finally:
+        e.set_fused_bsgs(True)
         e.set_graphs(True)
 
     # A batch runs its bootstraps on several streams (each stream with graphs of its
