@@ -409,6 +409,7 @@ const DevicePartitions &Engine::partitions(int moduli_id, int key_moduli_id) {
     ints[p] = pt.start;
     ints[count + p] = pt.size;
     ints[2 * count + p] = pt.partition_index;
+    if (p < 8) dp.key_index_first[p] = pt.partition_index;
     dp.max_key_index = std::max(dp.max_key_index, pt.partition_index);
     if (pt.partition_index < 0)
       throw std::invalid_argument("the key was created at a lower level than the text.");

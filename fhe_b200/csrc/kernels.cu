@@ -329,6 +329,61 @@ __global__ void key_inner_product_kernel(PrimeTables t, DevicePartitions dp, int
   }
 }
 
+// The same for P <= 8 partitions known at compile time: every partition's three
+// words are loaded before any is used (the key rows' offsets come with the launch),
+// and one OR of the operands' high words decides between the exact sum and the
+// chain, so the loads of all partitions are in flight together.
+template <int P>
+__global__ void __launch_bounds__(256, P == 3 ? 4 : 0)  // three partitions: 4 CTAs/SM without spills
+key_inner_product_fixed_kernel(PrimeTables t, DevicePartitions dp, int log_n, int moduli_id,
+                               const int64_t *ext, const int64_t *key, long long poly_row,
+                               KeyRowOffsets rows, int64_t *acc) {
+  const long long total = static_cast<long long>(dp.extended) << log_n;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int prime = moduli_id + static_cast<int>(i >> log_n);
+    const uint64_t q = t.q[prime], k = t.k[prime];
+    int64_t e[P], k0[P], k1[P];
+#pragma unroll
+    for (int p = 0; p < P; p++) {
+      e[p] = ext[p * total + i];
+      k0[p] = key[rows.off[p] + i];
+      k1[p] = key[rows.off[p] + poly_row + i];
+    }
+    uint32_t high = 0;
+    WideSum w0, w1;
+#pragma unroll
+    for (int p = 0; p < P; p++) {
+      high |= static_cast<uint32_t>(static_cast<uint64_t>(e[p]) >> 32) |
+              static_cast<uint32_t>(static_cast<uint64_t>(k0[p]) >> 32) |
+              static_cast<uint32_t>(static_cast<uint64_t>(k1[p]) >> 32);
+      w0.add(static_cast<uint64_t>(e[p]), static_cast<uint64_t>(k0[p]));
+      w1.add(static_cast<uint64_t>(e[p]), static_cast<uint64_t>(k1[p]));
+    }
+    if ((high >> 29) == 0) {  // every operand below 2^61
+      acc[i] = w0.reduce(q, k, q, t.inv_q[prime]);
+      acc[total + i] = w1.reduce(q, k, q, t.inv_q[prime]);
+      continue;
+    }
+    const int64_t qs = static_cast<int64_t>(q), q2 = qs << 1;
+    int64_t x0 = 0, x1 = 0;
+#pragma unroll
+    for (int p = 0; p < P; p++) {
+      const int64_t a0 = mont_mult(e[p], k0[p], q, k);
+      const int64_t a1 = mont_mult(e[p], k1[p], q, k);
+      if (p == 0) {
+        x0 = a0;
+        x1 = a1;
+      } else {  // mont_mult_add then reduce_2q_to_q
+        x0 = guard(guard(a0 + x0, q2), qs);
+        x1 = guard(guard(a1 + x1, q2), qs);
+      }
+    }
+    acc[i] = x0;
+    acc[total + i] = x1;
+  }
+}
+
 // ------------------------------------------------------ mod down epilogue --
 
 // Sequential exact division by the K special primes, last first
@@ -532,6 +587,26 @@ cudaError_t launch_extended_ntt(const PrimeTables &t, const DevicePartitions &dp
 cudaError_t launch_key_inner_product(const PrimeTables &t, const DevicePartitions &dp, int n,
                                      int moduli_id, const int64_t *ext, const int64_t *key,
                                      int key_primes, int view_offset, int64_t *acc, cudaStream_t s) {
+  if (dp.count >= 1 && dp.count <= 8) {
+    KeyRowOffsets rows;
+    for (int p = 0; p < dp.count; p++)
+      rows.off[p] = (2LL * dp.key_index_first[p] * key_primes + view_offset) * n;
+    const int log_n = __builtin_ctz(static_cast<unsigned>(n));
+    const long long poly_row = static_cast<long long>(key_primes) * n;
+    const unsigned grid = blocks_for(static_cast<long long>(dp.extended) * n);
+    note_launch();
+    switch (dp.count) {
+#define FHE_KIP_CASE(P)                                                                           \
+  case P:                                                                                         \
+    key_inner_product_fixed_kernel<P><<<grid, kThreads, 0, s>>>(t, dp, log_n, moduli_id, ext, key, \
+                                                                poly_row, rows, acc);            \
+    break;
+      FHE_KIP_CASE(1) FHE_KIP_CASE(2) FHE_KIP_CASE(3) FHE_KIP_CASE(4)
+      FHE_KIP_CASE(5) FHE_KIP_CASE(6) FHE_KIP_CASE(7) FHE_KIP_CASE(8)
+#undef FHE_KIP_CASE
+    }
+    return cudaGetLastError();
+  }
   note_launch();
   key_inner_product_kernel<<<blocks_for(static_cast<long long>(dp.extended) * n), kThreads, 0, s>>>(
       t, dp, n, moduli_id, ext, key, key_primes, view_offset, acc);

@@ -23,6 +23,7 @@ struct DevicePartitions {
   int *start = nullptr;   // [count]
   int *size = nullptr;    // [count]
   int *key_index = nullptr;           // [count] partition_index
+  int key_index_first[8] = {};        // host copy of key_index[0 .. 7]
   int64_t *inverse_r = nullptr;       // [count][16]
   int64_t *product_r = nullptr;       // [count][16][16]
   int64_t *product_r_squared = nullptr;  // [count][16][extended]
@@ -84,6 +85,12 @@ cudaError_t launch_mixed_radix(const PrimeTables &t, const DevicePartitions &dp,
 cudaError_t launch_mod_up_ntt(const PrimeTables &t, const DevicePartitions &dp, int log_n,
                               int moduli_id, const int64_t *digits, int64_t *ext,
                               cudaStream_t s, bool skip_own = false);
+
+// Word offsets of the first 8 key partitions' polynomial-0 rows at the text's
+// first limb, ((2 partition_index) key_primes + view_offset) N.
+struct KeyRowOffsets {
+  long long off[8] = {};
+};
 
 // Key inner product (core_key_switch.cpp:320-349): acc[2][E][N] = sum over
 // partitions of ext_p * (key_{2i}, key_{2i+1}), reference reduction pattern.

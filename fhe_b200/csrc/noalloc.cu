@@ -191,6 +191,7 @@ void plan_partitions(const Parameters &p, int moduli_id, int key_moduli_id, Part
     dp.max_size = dp.max_size > lay.size[part] ? dp.max_size : lay.size[part];
     dp.size_mask |= 1u << lay.size[part];
     dp.max_key_index = dp.max_key_index > lay.key_index[part] ? dp.max_key_index : lay.key_index[part];
+    if (part < 8) dp.key_index_first[part] = lay.key_index[part];
   }
 }
 
