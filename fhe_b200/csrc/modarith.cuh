@@ -81,7 +81,50 @@ FHE_HD int64_t mont_mult_const(int64_t a, int64_t b, uint64_t q, uint64_t k) {
 // c0 / 2^32 = hi(w0 b0) + hi(s0 q0 + lo(w0 b0)); Y = c1 + c0 / 2^32 is below 2^64
 // and a multiple of 2^30, and Z / 2^62 = Y / 2^30 + 4 c2.  Every partial sum below
 // stays under 2^64 for these bounds (w1, b1, s1 < 2^30; q1 < 2^29).
+// On the device the same sums run as 32-bit multiply-adds chained through the
+// carry flag, so no partial product needs a 64-bit register pair of its own.
 FHE_HD int64_t mont_mult_small(uint64_t w, uint64_t b, uint64_t q, uint64_t k) {
+#ifdef __CUDA_ARCH__
+  uint64_t r;
+  asm("{\n\t"
+      ".reg .u32 w0, w1, b0, b1, q0, q1, k0, k1, pl, ph, yl, yh, s0, s1, ul, uh, tl, th, wx, sx, rl, rh;\n\t"
+      "mov.b64 {w0, w1}, %1;\n\t"
+      "mov.b64 {b0, b1}, %2;\n\t"
+      "mov.b64 {q0, q1}, %3;\n\t"
+      "mov.b64 {k0, k1}, %4;\n\t"
+      "mul.lo.u32 pl, w0, b0;\n\t"           // p = w0 b0
+      "mul.hi.u32 ph, w0, b0;\n\t"
+      "mad.lo.cc.u32 yl, w0, b1, ph;\n\t"    // y = w0 b1 + w1 b0 + p / 2^32
+      "madc.hi.u32 yh, w0, b1, 0;\n\t"
+      "mad.lo.cc.u32 yl, w1, b0, yl;\n\t"
+      "madc.hi.u32 yh, w1, b0, yh;\n\t"
+      "mul.lo.u32 s0, pl, k0;\n\t"           // s = ((yl, pl) k) mod 2^62
+      "mul.hi.u32 s1, pl, k0;\n\t"
+      "mad.lo.u32 s1, pl, k1, s1;\n\t"
+      "mad.lo.u32 s1, yl, k0, s1;\n\t"
+      "and.b32 s1, s1, 0x3fffffff;\n\t"
+      "mad.lo.cc.u32 ul, s0, q0, pl;\n\t"    // u = s0 q0 + p mod 2^32
+      "madc.hi.u32 uh, s0, q0, 0;\n\t"
+      "mad.lo.cc.u32 yl, s1, q0, yl;\n\t"    // y += s1 q0 + s0 q1 + u / 2^32
+      "madc.hi.u32 yh, s1, q0, yh;\n\t"
+      "mad.lo.cc.u32 yl, s0, q1, yl;\n\t"
+      "madc.hi.u32 yh, s0, q1, yh;\n\t"
+      "add.cc.u32 yl, yl, uh;\n\t"
+      "addc.u32 yh, yh, 0;\n\t"
+      "shf.r.clamp.b32 tl, yl, yh, 30;\n\t"  // y / 2^30
+      "shr.b32 th, yh, 30;\n\t"
+      "shl.b32 wx, w1, 2;\n\t"
+      "shl.b32 sx, s1, 2;\n\t"
+      "mad.lo.cc.u32 rl, wx, b1, tl;\n\t"    // + 4 w1 b1 + 4 s1 q1
+      "madc.hi.u32 rh, wx, b1, th;\n\t"
+      "mad.lo.cc.u32 rl, sx, q1, rl;\n\t"
+      "madc.hi.u32 rh, sx, q1, rh;\n\t"
+      "mov.b64 %0, {rl, rh};\n\t"
+      "}"
+      : "=l"(r)
+      : "l"(w), "l"(b), "l"(q), "l"(k));
+  return static_cast<int64_t>(r);
+#else
   const uint32_t w0 = static_cast<uint32_t>(w), w1 = static_cast<uint32_t>(w >> 32);
   const uint32_t b0 = static_cast<uint32_t>(b), b1 = static_cast<uint32_t>(b >> 32);
   const uint32_t q0 = static_cast<uint32_t>(q), q1 = static_cast<uint32_t>(q >> 32);
@@ -93,6 +136,7 @@ FHE_HD int64_t mont_mult_small(uint64_t w, uint64_t b, uint64_t q, uint64_t k) {
   const uint64_t u = mad32(s0, q0, static_cast<uint32_t>(p));
   y = mad32(s1, q0, mad32(s0, q1, y)) + (u >> 32);
   return static_cast<int64_t>(mad32(s1 << 2, q1, mad32(w1 << 2, b1, y >> 30)));
+#endif
 }
 
 // mont_mult taking the short form when both words are below 2^62 (lazy [0, 2q)
