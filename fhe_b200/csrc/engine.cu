@@ -97,6 +97,29 @@ Engine::Engine(const Config &config) : params(config) {
     }
     tables_.root_reduced = upload_table(rc);
     tables_.root_inverse_reduced = upload_table(ric);
+    // Plain twiddles and their Shoup quotients for shoup_mult.
+    std::vector<int64_t> rs(2 * rc.size()), ris(2 * ric.size());
+    for (int i = 0; i < P; i++) {
+      const uint64_t qi = p.q[i];
+      using u128 = unsigned __int128;
+      auto mulmod = [&](uint64_t a, uint64_t b) { return static_cast<uint64_t>(static_cast<u128>(a) * b % qi); };
+      uint64_t r_inverse = 1, base = (uint64_t(1) << 62) % qi;  // R^-1 = R^(q-2) mod q
+      for (uint64_t e = qi - 2; e > 0; e >>= 1) {
+        if (e & 1) r_inverse = mulmod(r_inverse, base);
+        base = mulmod(base, base);
+      }
+      auto pair = [&](int64_t mont, int64_t *out) {
+        const uint64_t w = mulmod(static_cast<uint64_t>(mont), r_inverse);
+        out[0] = static_cast<int64_t>(w);
+        out[1] = static_cast<int64_t>((static_cast<u128>(w) << 64) / qi);
+      };
+      for (size_t j = 0; j < per; j++) {
+        pair(rc[i * per + j], &rs[2 * (i * per + j)]);
+        pair(ric[i * per + j], &ris[2 * (i * per + j)]);
+      }
+    }
+    tables_.root_shoup = upload_table(rs);
+    tables_.root_inverse_shoup = upload_table(ris);
   }
   std::vector<double> inv_q(P), inv_2q(P);
   for (int i = 0; i < P; i++) {

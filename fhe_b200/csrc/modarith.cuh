@@ -139,6 +139,48 @@ FHE_HD int64_t mont_mult_small(uint64_t w, uint64_t b, uint64_t q, uint64_t k) {
 #endif
 }
 
+// Shoup's product for words whose value only matters modulo q: W b mod q in
+// [0, 2q), with W < q a plain (not Montgomery) constant and W' = floor(W 2^64 / q),
+// for any b < 2^64.  qt = floor(W' b / 2^64) undershoots W b / q by less than 2, so
+// W b - qt q, computed modulo 2^64, is the product up to one q.
+FHE_HD uint64_t shoup_mult(uint64_t w, uint64_t wp, uint64_t b, uint64_t q) {
+#ifdef __CUDA_ARCH__
+  uint64_t r;
+  asm("{\n\t"
+      ".reg .u32 w0, w1, p0, p1, b0, b1, q0, q1, t0, t1, t2, r0, r1, s0, s1;\n\t"
+      "mov.b64 {w0, w1}, %1;\n\t"
+      "mov.b64 {p0, p1}, %2;\n\t"
+      "mov.b64 {b0, b1}, %3;\n\t"
+      "mov.b64 {q0, q1}, %4;\n\t"
+      "mul.hi.u32 t0, p0, b0;\n\t"          // (t2, t1) = high 64 bits of W' b
+      "mad.lo.cc.u32 t0, p0, b1, t0;\n\t"
+      "madc.hi.u32 t1, p0, b1, 0;\n\t"
+      "mad.lo.cc.u32 t0, p1, b0, t0;\n\t"
+      "madc.hi.cc.u32 t1, p1, b0, t1;\n\t"
+      "addc.u32 t2, 0, 0;\n\t"
+      "mad.lo.cc.u32 t1, p1, b1, t1;\n\t"
+      "madc.hi.u32 t2, p1, b1, t2;\n\t"
+      "mul.lo.u32 r0, w0, b0;\n\t"          // W b mod 2^64
+      "mul.hi.u32 r1, w0, b0;\n\t"
+      "mad.lo.u32 r1, w0, b1, r1;\n\t"
+      "mad.lo.u32 r1, w1, b0, r1;\n\t"
+      "mul.lo.u32 s0, t1, q0;\n\t"          // qt q mod 2^64
+      "mul.hi.u32 s1, t1, q0;\n\t"
+      "mad.lo.u32 s1, t1, q1, s1;\n\t"
+      "mad.lo.u32 s1, t2, q0, s1;\n\t"
+      "sub.cc.u32 r0, r0, s0;\n\t"
+      "subc.u32 r1, r1, s1;\n\t"
+      "mov.b64 %0, {r0, r1};\n\t"
+      "}"
+      : "=l"(r)
+      : "l"(w), "l"(wp), "l"(b), "l"(q));
+  return r;
+#else
+  const uint64_t qt = static_cast<uint64_t>((static_cast<unsigned __int128>(wp) * b) >> 64);
+  return w * b - qt * q;
+#endif
+}
+
 // mont_mult taking the short form when both words are below 2^62 (lazy [0, 2q)
 // words and table constants are); every engine prime is below 2^61.  For the
 // element-wise loaders and storers of the NTT passes, where it measured faster;
@@ -274,6 +316,10 @@ struct PrimeTables {
   const int64_t *root_inverse;  // [prime][N-1]
   const int64_t *root_reduced;          // root, each word reduced to [0, q)
   const int64_t *root_inverse_reduced;  // root_inverse, each word reduced to [0, q)
+  // The same twiddles as (W, W') pairs for shoup_mult: W = root R^-1 mod q, the
+  // plain twiddle, and W' = floor(W 2^64 / q); [prime][N-1][2].
+  const int64_t *root_shoup;
+  const int64_t *root_inverse_shoup;
   const double *inv_q;          // 1 / q
   const double *inv_2q;         // 1 / (2q)
   int log_n;

@@ -204,6 +204,11 @@ __global__ void __launch_bounds__(kNttThreads, 4)
   const int64_t *tw = (VALUE_ONLY ? (INVERSE ? t.root_inverse_reduced : t.root_reduced)
                                   : (INVERSE ? t.root_inverse : t.root)) +
                      static_cast<size_t>(prime) * (n - 1);
+  // Value-only passes on in-range words multiply by Shoup's (W, W') pairs instead.
+  const longlong2 *tws =
+      VALUE_ONLY ? reinterpret_cast<const longlong2 *>(INVERSE ? t.root_inverse_shoup : t.root_shoup) +
+                       static_cast<size_t>(prime) * (n - 1)
+                 : nullptr;
   // A forward value-only pass after the first reads words in [0, 4q).
   const uint64_t in_bound = (VALUE_ONLY && !INVERSE && a.first > 0) ? (q << 2) : (q << 1);
   const bool last_pass = !INVERSE && a.first + S == a.log_n;
@@ -288,6 +293,23 @@ __global__ void __launch_bounds__(kNttThreads, 4)
           if (kLazy) return mont_mult_small(static_cast<uint64_t>(w), static_cast<uint64_t>(v), q, k);
           return mont_mult_const(w, v, q, k);
         };
+        // The twiddle of table entry i: the Montgomery word, or for Harvey's form
+        // on in-range words the Shoup pair (its product is the same value mod q).
+        constexpr bool kShoup = kLazy && VALUE_ONLY;
+        struct Twiddle {
+          int64_t w, wp;
+        };
+        auto twiddle = [&](size_t i) -> Twiddle {
+          if (kShoup) {
+            const longlong2 v = __ldg(tws + i);
+            return {v.x, v.y};
+          }
+          return {__ldg(tw + i), 0};
+        };
+        auto value_product = [&](const Twiddle &w, int64_t v) -> int64_t {
+          return static_cast<int64_t>(shoup_mult(static_cast<uint64_t>(w.w), static_cast<uint64_t>(w.wp),
+                                                 static_cast<uint64_t>(v), q));
+        };
 #pragma unroll
         for (int j = 0; j < kNttMaxRoundLog; j++) {
           if (j < r) {
@@ -296,26 +318,26 @@ __global__ void __launch_bounds__(kNttThreads, 4)
               // element e is e >> (r - j) (ntt.cpp:46-134)
               const int s = a.first + first_local + j;
               const int half = E >> (j + 1);
-              const int64_t *wp = tw + ((1 << s) - 1 + (gi0 >> (a.log_n - s)));
+              const size_t wi = (1 << s) - 1 + (gi0 >> (a.log_n - s));
 #pragma unroll
               for (int h = 0; h < (1 << j); h++) {
-                const int64_t w = __ldg(wp + h);
+                const Twiddle w = twiddle(wi + h);
 #pragma unroll
                 for (int e2 = 0; e2 < kMaxE / 2; e2++) {
                   if (e2 < half) {
                     const int e = h * 2 * half + e2;
-                    if (kLazy && VALUE_ONLY) {
+                    if (kShoup) {
                       // Harvey's form: words in [0, 4q), one guard per butterfly;
-                      // twiddles below q keep the product below 2q (q < 2^60).
+                      // Shoup's product is below 2q.
                       int64_t uu = x[e] - q2;
                       uu = uu < 0 ? uu + q2 : uu;
-                      const int64_t p = product(w, x[e + half]);
+                      const int64_t p = value_product(w, x[e + half]);
                       x[e] = uu + p;
                       x[e + half] = uu - p + q2;
                       continue;
                     }
                     const int64_t uu = x[e];
-                    const int64_t p = product(w, x[e + half]);
+                    const int64_t p = product(w.w, x[e + half]);
                     x[e] = add_guard(uu, p);
                     x[e + half] = sub_guard(uu, p);
                   }
@@ -326,11 +348,11 @@ __global__ void __launch_bounds__(kNttThreads, 4)
               // (ntt.cpp:177-272); the block of element e is e >> (j + 1)
               const int dg = a.first + first_local + j;
               const int half = 1 << j;
-              const int64_t *wp = tw + (n - (n >> dg) + (gi0 >> (dg + 1)));
+              const size_t wi = n - (n >> dg) + (gi0 >> (dg + 1));
 #pragma unroll
               for (int h = 0; h < kMaxE / 2; h++) {
                 if (h < (E >> (j + 1))) {
-                  const int64_t w = __ldg(wp + h);
+                  const Twiddle w = twiddle(wi + h);
 #pragma unroll
                   for (int e2 = 0; e2 < kMaxE / 2; e2++) {
                     if (e2 < half) {
@@ -339,8 +361,8 @@ __global__ void __launch_bounds__(kNttThreads, 4)
                       const int64_t vv = x[e + half];
                       x[e] = add_guard(uu, vv);
                       // Harvey's form: the product's operand in (0, 4q) needs no guard.
-                      x[e + half] = (kLazy && VALUE_ONLY) ? product(w, uu - vv + q2)
-                                                          : product(w, sub_guard(uu, vv));
+                      x[e + half] = kShoup ? value_product(w, uu - vv + q2)
+                                           : product(w.w, sub_guard(uu, vv));
                     }
                   }
                 }

@@ -1,7 +1,9 @@
 // Host check of the device modular arithmetic (fhe_b200/csrc/modarith.cuh compiles
 // as plain C++): the short Montgomery product of the NTT's in-range butterflies
 // must give the same word as the general sign-extended form, for random odd q
-// below 2^61 (k = -q^-1 mod 2^62) and operands below 2^62, edge values included.
+// below 2^61 (k = -q^-1 mod 2^62) and operands below 2^62, edge values included;
+// Shoup's product of the value-only butterflies must give W b mod q up to one q,
+// for any b below 2^64.
 // Usage: modarith_check <iterations> <seed>; prints the mismatch count.
 #include <cstdio>
 #include <cstdlib>
@@ -35,6 +37,11 @@ int main(int argc, char **argv) {
     if (it % 4 == 3) w = rng() % (2 * q);
     const int64_t want = mont_mult_const(static_cast<int64_t>(w), static_cast<int64_t>(b), q, k);
     if (mont_mult_small(w, b, q, k) != want) bad++;
+    const uint64_t plain = w % q, any = (it % 11 == 0) ? ~(rng() & 0xFFFF) : rng();
+    const uint64_t shoup = static_cast<uint64_t>((static_cast<unsigned __int128>(plain) << 64) / q);
+    const uint64_t r = shoup_mult(plain, shoup, any, q);
+    const uint64_t exact = static_cast<uint64_t>(static_cast<unsigned __int128>(plain) * any % q);
+    if (!(r < 2 * q && r % q == exact)) bad++;
   }
   std::printf("%ld\n", bad);
   return 0;
