@@ -954,7 +954,26 @@ def main(argv=None):
     torch.cuda.synchronize()
     h2d_bytes = B * 2 * in_words * 8
     h2d_gbs = 3 * h2d_bytes / (h0.elapsed_time(h1) / 1e3) / 1e9
-    del dev_in
+    # Both directions at once, as the end-to-end step moves them: the step's inputs
+    # to the device and its results back, on two streams.
+    dev_out = torch.empty(pin_out.shape, dtype=torch.int64, device="cuda")
+    up, down = torch.cuda.Stream(), torch.cuda.Stream()
+    torch.cuda.synchronize()
+    d0, d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    d0.record(stream)
+    up.wait_event(d0)
+    down.wait_event(d0)
+    for _ in range(3):
+        with torch.cuda.stream(up):
+            dev_in.copy_(pin_in, non_blocking=True)
+        with torch.cuda.stream(down):
+            pin_out.copy_(dev_out, non_blocking=True)
+    stream.wait_stream(up)
+    stream.wait_stream(down)
+    d1.record(stream)
+    torch.cuda.synchronize()
+    duplex_ms = d0.elapsed_time(d1) / 3
+    del dev_in, dev_out
 
     line = None
     if rank == 0:
@@ -980,7 +999,9 @@ def main(argv=None):
                     "h2d_bytes_per_step": B * 2 * in_words * 8,
                     "d2h_bytes_per_step": B * out_words * 8,
                     "h2d_gbs_measured": h2d_gbs,
-                    "h2d_ceiling_ct_s": B / (h2d_bytes / (h2d_gbs * 1e9))},
+                    "h2d_ceiling_ct_s": B / (h2d_bytes / (h2d_gbs * 1e9)),
+                    "duplex_copy_ms_per_step": duplex_ms,
+                    "duplex_ceiling_ct_s": B / (duplex_ms / 1e3)},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
         }

@@ -70,9 +70,9 @@ __global__ void tensor_kernel(PrimeTables t, int n, int limbs, int prime_base, c
     const uint64_t q = t.q[prime], k = t.k[prime];
     const int64_t qs = static_cast<int64_t>(q), q2 = qs << 1;
     const int64_t a0 = a[i], a1 = a[ps + i], b0 = b[i], b1 = b[ps + i];
-    z[i] = mont_mult(a0, b0, q, k);
-    z[ps + i] = guard(guard(mont_mult(a0, b1, q, k) + mont_mult(a1, b0, q, k), q2), qs);
-    z[2 * ps + i] = mont_mult(a1, b1, q, k);
+    z[i] = mont_mult_lazy(a0, b0, q, k);
+    z[ps + i] = guard(guard(mont_mult_lazy(a0, b1, q, k) + mont_mult_lazy(a1, b0, q, k), q2), qs);
+    z[2 * ps + i] = mont_mult_lazy(a1, b1, q, k);
   }
 }
 

@@ -179,14 +179,14 @@ __device__ __forceinline__ int64_t pointwise_word(int op, long long i, int log_n
   const int64_t qs = static_cast<int64_t>(q), q2 = qs << 1;
   int64_t v = 0;
   switch (op) {
-    case kOpMult: v = mont_mult(ai, bi, q, k); break;
+    case kOpMult: v = mont_mult_lazy(ai, bi, q, k); break;
     case kOpAddReduce: v = guard(guard(ai + bi, q2), qs); break;
     case kOpSubReduce: v = guard(guard(ai + q2 - bi, q2), qs); break;
     case kOpReduce: v = guard(ai, qs); break;
-    case kOpEnter: v = mont_mult(ai, c.v[j], q, k); break;
+    case kOpEnter: v = mont_mult_lazy(ai, c.v[j], q, k); break;
     case kOpNegate: v = qs - ai; break;
     case kOpAddScalarFirst: v = guard(ai + ((i & ((1LL << log_n) - 1)) == 0 ? c.v[j] : 0), qs); break;
-    case kOpEnterReduce: v = guard(mont_mult(ai, c.v[j], q, k), qs); break;
+    case kOpEnterReduce: v = guard(mont_mult_lazy(ai, c.v[j], q, k), qs); break;
     case kOpMonomial: {
       const int64_t m = c.v[j];
       v = (i & ((1LL << log_n) - 1)) == (1LL << (log_n - 1)) ? (m < 0 ? m + qs : guard(m, qs)) : 0;

@@ -55,22 +55,80 @@ FHE_HD int64_t redc_wide(uint64_t lo, uint64_t hi, uint64_t q, uint64_t k) {
 }
 
 // REDC(a * b) with R = 2^62 on sign-extended operands (unit.h:15-23).  The signed
-// high product is the unsigned one minus b when a < 0 and minus a when b < 0.
+// high product is the unsigned one minus b when a < 0 and minus a when b < 0.  On
+// the device the 128-bit product, its sign correction, s q and the sum run as one
+// chain of 32-bit multiply-adds through the carry flag.
 FHE_HD int64_t mont_mult(int64_t a, int64_t b, uint64_t q, uint64_t k) {
+#ifdef __CUDA_ARCH__
+  uint64_t r;
+  asm("{\n\t"
+      ".reg .u32 a0, a1, b0, b1, q0, q1, k0, k1, z0, z1, z2, z3, s0, s1, c0, c1;\n\t"
+      ".reg .pred na, nb;\n\t"
+      "mov.b64 {a0, a1}, %1;\n\t"
+      "mov.b64 {b0, b1}, %2;\n\t"
+      "mov.b64 {q0, q1}, %3;\n\t"
+      "mov.b64 {k0, k1}, %4;\n\t"
+      "mul.lo.u32 z0, a0, b0;\n\t"          // z = a b, unsigned, 128 bits
+      "mul.hi.u32 z1, a0, b0;\n\t"
+      "mad.lo.cc.u32 z1, a0, b1, z1;\n\t"
+      "madc.hi.u32 z2, a0, b1, 0;\n\t"
+      "mad.lo.cc.u32 z1, a1, b0, z1;\n\t"
+      "madc.hi.cc.u32 z2, a1, b0, z2;\n\t"
+      "addc.u32 z3, 0, 0;\n\t"
+      "mad.lo.cc.u32 z2, a1, b1, z2;\n\t"
+      "madc.hi.u32 z3, a1, b1, z3;\n\t"
+      "setp.lt.s32 na, a1, 0;\n\t"          // signed high half
+      "setp.lt.s32 nb, b1, 0;\n\t"
+      "selp.b32 c0, b0, 0, na;\n\t"
+      "selp.b32 c1, b1, 0, na;\n\t"
+      "sub.cc.u32 z2, z2, c0;\n\t"
+      "subc.u32 z3, z3, c1;\n\t"
+      "selp.b32 c0, a0, 0, nb;\n\t"
+      "selp.b32 c1, a1, 0, nb;\n\t"
+      "sub.cc.u32 z2, z2, c0;\n\t"
+      "subc.u32 z3, z3, c1;\n\t"
+      "mul.lo.u32 s0, z0, k0;\n\t"          // s = (z mod 2^64) k mod 2^62
+      "mul.hi.u32 s1, z0, k0;\n\t"
+      "mad.lo.u32 s1, z0, k1, s1;\n\t"
+      "mad.lo.u32 s1, z1, k0, s1;\n\t"
+      "and.b32 s1, s1, 0x3fffffff;\n\t"
+      "mad.lo.cc.u32 z0, s0, q0, z0;\n\t"   // z += s q
+      "madc.hi.cc.u32 z1, s0, q0, z1;\n\t"
+      "madc.lo.cc.u32 z2, s1, q1, z2;\n\t"
+      "madc.hi.u32 z3, s1, q1, z3;\n\t"
+      "mad.lo.cc.u32 z1, s0, q1, z1;\n\t"
+      "madc.hi.cc.u32 z2, s0, q1, z2;\n\t"
+      "addc.u32 z3, z3, 0;\n\t"
+      "mad.lo.cc.u32 z1, s1, q0, z1;\n\t"
+      "madc.hi.cc.u32 z2, s1, q0, z2;\n\t"
+      "addc.u32 z3, z3, 0;\n\t"
+      "shf.r.clamp.b32 z0, z1, z2, 30;\n\t"  // bits [62, 126)
+      "shf.r.clamp.b32 z1, z2, z3, 30;\n\t"
+      "mov.b64 %0, {z0, z1};\n\t"
+      "}"
+      : "=l"(r)
+      : "l"(a), "l"(b), "l"(q), "l"(k));
+  return static_cast<int64_t>(r);
+#else
   const uint64_t ua = static_cast<uint64_t>(a), ub = static_cast<uint64_t>(b);
   uint64_t lo, hi;
   mul_wide(ua, ub, lo, hi);
   hi -= (a < 0 ? ub : 0) + (b < 0 ? ua : 0);
   return redc_wide(lo, hi, q, k);
+#endif
 }
 
 // mont_mult when `a` is known to be non-negative (a twiddle or table constant).
 FHE_HD int64_t mont_mult_const(int64_t a, int64_t b, uint64_t q, uint64_t k) {
+#ifdef __CUDA_ARCH__
+  return mont_mult(a, b, q, k);  // the same word; the device form has no cheaper variant
+#else
   const uint64_t ua = static_cast<uint64_t>(a), ub = static_cast<uint64_t>(b);
   uint64_t lo, hi;
   mul_wide(ua, ub, lo, hi);
   hi -= (b < 0 ? ua : 0);
   return redc_wide(lo, hi, q, k);
+#endif
 }
 
 // mont_mult_const for operands known to lie in range: 0 <= w, b < 2^62 and odd
@@ -182,9 +240,10 @@ FHE_HD uint64_t shoup_mult(uint64_t w, uint64_t wp, uint64_t b, uint64_t q) {
 }
 
 // mont_mult taking the short form when both words are below 2^62 (lazy [0, 2q)
-// words and table constants are); every engine prime is below 2^61.  For the
-// element-wise loaders and storers of the NTT passes, where it measured faster;
-// elsewhere the branch costs more than it saves.
+// words and table constants are); every engine prime is below 2^61.  The same word
+// as mont_mult for every input.  Used in the element-wise kernels and the NTT's
+// loaders and storers; in the serial triangles of the Garner digits and the ModDown
+// divisors the branch measured slower.
 FHE_HD int64_t mont_mult_lazy(int64_t a, int64_t b, uint64_t q, uint64_t k) {
   const uint64_t ua = static_cast<uint64_t>(a), ub = static_cast<uint64_t>(b);
   if (((ua | ub) >> kMontBits) == 0) return mont_mult_small(ua, ub, q, k);

@@ -27,7 +27,7 @@ struct ScaledEnterLoad {
   __device__ __forceinline__ int64_t operator()(int, int limb, int prime, int gi, int n) const {
     const uint64_t qq = q[prime], kk = k[prime];
     const int64_t x = src[static_cast<long long>(limb) * n + gi];
-    return mont_mult(mont_mult(x, p_product_mult_r[prime], qq, kk), r_squared[prime], qq, kk);
+    return mont_mult_lazy(mont_mult_lazy(x, p_product_mult_r[prime], qq, kk), r_squared[prime], qq, kk);
   }
 };
 
@@ -92,7 +92,7 @@ __global__ void scalar_enter_kernel(PrimeTables t, int log_n, int polys, int lim
     const int prime = prime_base + j;
     const uint64_t q = t.q[prime], k = t.k[prime];
     const int64_t v = x[poly * xs + (static_cast<long long>(x_limb_offset) << log_n) + r];
-    y[poly * ys + r] = guard(mont_mult(v, s.v[j], q, k), static_cast<int64_t>(q));
+    y[poly * ys + r] = guard(mont_mult_lazy(v, s.v[j], q, k), static_cast<int64_t>(q));
   }
 }
 
