@@ -34,6 +34,26 @@ FHE_HD uint64_t mad32(uint32_t a, uint32_t b, uint64_t c) {
 
 // Full unsigned product a * b = hi * 2^64 + lo.
 FHE_HD void mul_wide(uint64_t a, uint64_t b, uint64_t &lo, uint64_t &hi) {
+#ifdef __CUDA_ARCH__
+  asm("{\n\t"
+      ".reg .u32 a0, a1, b0, b1, z0, z1, z2, z3;\n\t"
+      "mov.b64 {a0, a1}, %2;\n\t"
+      "mov.b64 {b0, b1}, %3;\n\t"
+      "mul.lo.u32 z0, a0, b0;\n\t"
+      "mul.hi.u32 z1, a0, b0;\n\t"
+      "mad.lo.cc.u32 z1, a0, b1, z1;\n\t"
+      "madc.hi.u32 z2, a0, b1, 0;\n\t"
+      "mad.lo.cc.u32 z1, a1, b0, z1;\n\t"
+      "madc.hi.cc.u32 z2, a1, b0, z2;\n\t"
+      "addc.u32 z3, 0, 0;\n\t"
+      "mad.lo.cc.u32 z2, a1, b1, z2;\n\t"
+      "madc.hi.u32 z3, a1, b1, z3;\n\t"
+      "mov.b64 %0, {z0, z1};\n\t"
+      "mov.b64 %1, {z2, z3};\n\t"
+      "}"
+      : "=l"(lo), "=l"(hi)
+      : "l"(a), "l"(b));
+#else
   const uint32_t a0 = static_cast<uint32_t>(a), a1 = static_cast<uint32_t>(a >> 32);
   const uint32_t b0 = static_cast<uint32_t>(b), b1 = static_cast<uint32_t>(b >> 32);
   const uint64_t t = mad32(a0, b0, 0);
@@ -42,16 +62,50 @@ FHE_HD void mul_wide(uint64_t a, uint64_t b, uint64_t &lo, uint64_t &hi) {
   const uint64_t h = mad32(a1, b1, m >> 32);
   hi = h + (m2 >> 32);                                             // no overflow
   lo = static_cast<uint32_t>(t) | (m2 << 32);
+#endif
 }
 
-// Bits [62, 126) of X + s*q with s = (X mod 2^64) * k mod 2^62, X = hi*2^64 + lo.
+// Bits [62, 126) of X + s*q with s = (X mod 2^64) * k mod 2^62, X = hi*2^64 + lo
+// (every sum modulo 2^128).
 FHE_HD int64_t redc_wide(uint64_t lo, uint64_t hi, uint64_t q, uint64_t k) {
+#ifdef __CUDA_ARCH__
+  uint64_t r;
+  asm("{\n\t"
+      ".reg .u32 z0, z1, z2, z3, q0, q1, k0, k1, s0, s1;\n\t"
+      "mov.b64 {z0, z1}, %1;\n\t"
+      "mov.b64 {z2, z3}, %2;\n\t"
+      "mov.b64 {q0, q1}, %3;\n\t"
+      "mov.b64 {k0, k1}, %4;\n\t"
+      "mul.lo.u32 s0, z0, k0;\n\t"          // s = (X mod 2^64) k mod 2^62
+      "mul.hi.u32 s1, z0, k0;\n\t"
+      "mad.lo.u32 s1, z0, k1, s1;\n\t"
+      "mad.lo.u32 s1, z1, k0, s1;\n\t"
+      "and.b32 s1, s1, 0x3fffffff;\n\t"
+      "mad.lo.cc.u32 z0, s0, q0, z0;\n\t"   // X += s q
+      "madc.hi.cc.u32 z1, s0, q0, z1;\n\t"
+      "madc.lo.cc.u32 z2, s1, q1, z2;\n\t"
+      "madc.hi.u32 z3, s1, q1, z3;\n\t"
+      "mad.lo.cc.u32 z1, s0, q1, z1;\n\t"
+      "madc.hi.cc.u32 z2, s0, q1, z2;\n\t"
+      "addc.u32 z3, z3, 0;\n\t"
+      "mad.lo.cc.u32 z1, s1, q0, z1;\n\t"
+      "madc.hi.cc.u32 z2, s1, q0, z2;\n\t"
+      "addc.u32 z3, z3, 0;\n\t"
+      "shf.r.clamp.b32 z0, z1, z2, 30;\n\t"  // bits [62, 126)
+      "shf.r.clamp.b32 z1, z2, z3, 30;\n\t"
+      "mov.b64 %0, {z0, z1};\n\t"
+      "}"
+      : "=l"(r)
+      : "l"(lo), "l"(hi), "l"(q), "l"(k));
+  return static_cast<int64_t>(r);
+#else
   const uint64_t s = (lo * k) & kMontMask;
   uint64_t sl, sh;
   mul_wide(s, q, sl, sh);
   const uint64_t zl = lo + sl;
   const uint64_t zh = hi + sh + (zl < lo ? 1 : 0);
   return static_cast<int64_t>((zh << 2) | (zl >> kMontBits));
+#endif
 }
 
 // REDC(a * b) with R = 2^62 on sign-extended operands (unit.h:15-23).  The signed
