@@ -121,24 +121,34 @@ __global__ void __launch_bounds__(kTcThreads, K <= 10 && K != 7 ? 4 : (K <= 13 ?
       mma_round(tmem, sA, sB, KB);
       mma_commit(bar);
     }
+    // This thread's words x_j of the round, loaded while the MMAs run.
+    constexpr int kHalfTargets = kTcTargets / 2;
+    int64_t xs[kHalfTargets];
+#pragma unroll
+    for (int u = 0; u < kHalfTargets; u++) {
+      const int j = round * kTcTargets + half * kHalfTargets + u;
+      xs[u] = j < L ? __ldg(x + static_cast<long long>(j) * n + row) : 0;
+    }
     ok = __syncthreads_and(mbar_wait(bar, round & 1, status.wait_limit)) != 0;
     if (!ok) break;
     tc_fence_after();
     // Each warpgroup folds 8 of the round's 16 targets, two per tensor-memory load.
-    for (int jp = half * (kTcTargets / 2); jp < (half + 1) * (kTcTargets / 2); jp += 2) {
+#pragma unroll
+    for (int u2 = 0; u2 < kHalfTargets / 2; u2++) {
+      const int jp = half * kHalfTargets + 2 * u2;
       const int j0 = round * kTcTargets + jp;
-      if (j0 >= L) break;  // uniform across the warp
+      if (j0 >= L) continue;  // uniform across the warp
       uint32_t d[16];
       tmem_load16(tmem + (static_cast<uint32_t>(lane_base) << 16) + jp * 8, d);
 #pragma unroll
       for (int h = 0; h < 2; h++) {
         const int j = j0 + h;
-        if (j >= L) break;  // uniform across the warp
+        if (j >= L) continue;  // uniform across the warp
         const int prime = moduli_id + j;
         const uint64_t q = t.q[prime], kq = t.k[prime];
         uint64_t lo, hi;
         fold8(d + 8 * h, lo, hi);
-        const int64_t xj = x[static_cast<long long>(j) * n + row];
+        const int64_t xj = xs[2 * u2 + h];
         // REDC(X) < q + 2^19; x_j is the reduced inverse transform's word in [0, q).
         const uint64_t v = static_cast<uint64_t>(redc_wide(lo, hi, q, kq)) +
                            static_cast<uint64_t>(mont_mult_small(static_cast<uint64_t>(xj),
