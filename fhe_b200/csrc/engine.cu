@@ -120,6 +120,22 @@ Engine::Engine(const Config &config) : params(config) {
     }
     tables_.root_shoup = upload_table(rs);
     tables_.root_inverse_shoup = upload_table(ris);
+    // The reduced exit's constant N^-1 R^-1 (n_inverse = N^-1 R) and its Shoup quotient.
+    std::vector<int64_t> es(2 * static_cast<size_t>(P));
+    for (int i = 0; i < P; i++) {
+      const uint64_t qi = p.q[i];
+      using u128 = unsigned __int128;
+      auto mulmod = [&](uint64_t a, uint64_t b) { return static_cast<uint64_t>(static_cast<u128>(a) * b % qi); };
+      uint64_t r_inverse = 1, base = (uint64_t(1) << 62) % qi;
+      for (uint64_t e = qi - 2; e > 0; e >>= 1) {
+        if (e & 1) r_inverse = mulmod(r_inverse, base);
+        base = mulmod(base, base);
+      }
+      const uint64_t c = mulmod(mulmod(static_cast<uint64_t>(p.n_inverse[i]) % qi, r_inverse), r_inverse);
+      es[2 * i] = static_cast<int64_t>(c);
+      es[2 * i + 1] = static_cast<int64_t>((static_cast<u128>(c) << 64) / qi);
+    }
+    tables_.exit_shoup = upload_table(es);
   }
   std::vector<double> inv_q(P), inv_2q(P);
   for (int i = 0; i < P; i++) {

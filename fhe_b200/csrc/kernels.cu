@@ -618,7 +618,7 @@ cudaError_t launch_mod_down_intt(const PrimeTables &t, int log_n, int moduli_id,
   if (polys < 1 || polys > 2) return cudaErrorInvalidValue;
   const long long stride = static_cast<long long>(extended) << log_n;
   PlainLoad ld{acc, stride};
-  EnterExitStore<true> st{acc, stride, t.n_inverse, t.q, t.k};
+  EnterExitStore<true> st{acc, stride, t.n_inverse, t.q, t.k, t.exit_shoup};
   // Value-only: the store reduces every word to [0, q).
   return inverse_ntt<PlainLoad, EnterExitStore<true>, true>(log_n, polys, extended, moduli_id, t, ld,
                                                             st, acc, stride, s);

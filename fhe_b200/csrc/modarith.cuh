@@ -6,10 +6,10 @@
 // the REDC product is formed from sign-extended operands, so out-of-range
 // intermediates evaluate to the same words as on the CPU.  R = 2^62.
 //
-// The 64x64 -> 128-bit products are written as four 32x32 -> 64-bit
-// multiply-adds whose accumulations never overflow, which maps each of them onto
-// one wide integer multiply-add on the FMA pipe and keeps carries off the ALU pipe
-// (the NTT butterflies are ALU-bound otherwise).
+// The 64x64 -> 128-bit products are four 32x32 -> 64-bit multiply-adds: on the
+// device they are PTX chains of 32-bit multiply-adds through the carry flag (no
+// 64-bit register pair per partial product, no carry recomputed by compares); the
+// host form of each function computes the same integers in C++.
 #pragma once
 
 #include <cstdint>
@@ -433,6 +433,10 @@ struct PrimeTables {
   // plain twiddle, and W' = floor(W 2^64 / q); [prime][N-1][2].
   const int64_t *root_shoup;
   const int64_t *root_inverse_shoup;
+  // (C, C') per prime for the reduced exit of a value-only inverse transform:
+  // C = N^-1 R^-1 mod q, the value mont_exit(mont_mult(v, n_inverse)) multiplies by,
+  // and C' = floor(C 2^64 / q).
+  const int64_t *exit_shoup;
   const double *inv_q;          // 1 / q
   const double *inv_2q;         // 1 / (2q)
   int log_n;

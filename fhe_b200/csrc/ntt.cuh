@@ -110,7 +110,9 @@ struct ProductEnterLoad {
 };
 
 // mont_enter_exit by N^-1*R on the way out: to_intt_ (core_ntt.cpp:131-148),
-// optionally followed by reduce_2q_to_q (mod_down, core_key_switch.cpp:121).
+// optionally followed by reduce_2q_to_q (mod_down, core_key_switch.cpp:121).  With
+// the reduction the word is the canonical residue of v N^-1 R^-1, so for v in
+// [0, 2^62) one Shoup product by that constant and one subtraction give it.
 template <bool REDUCE>
 struct EnterExitStore {
   int64_t *dst;
@@ -118,8 +120,16 @@ struct EnterExitStore {
   const int64_t *n_inverse;
   const uint64_t *q;
   const uint64_t *k;
+  const int64_t *exit_shoup = nullptr;  // PrimeTables::exit_shoup, used when REDUCE
   __device__ __forceinline__ void operator()(int poly, int limb, int prime, int gi, int n, int64_t v) const {
     const uint64_t qq = q[prime], kk = k[prime];
+    if (REDUCE && (static_cast<uint64_t>(v) >> kMontBits) == 0) {
+      const uint64_t r = shoup_mult(static_cast<uint64_t>(exit_shoup[2 * prime]),
+                                    static_cast<uint64_t>(exit_shoup[2 * prime + 1]),
+                                    static_cast<uint64_t>(v), qq);
+      dst[poly * poly_stride + (long long)limb * n + gi] = static_cast<int64_t>(r >= qq ? r - qq : r);
+      return;
+    }
     int64_t y = mont_exit(mont_mult_lazy(v, n_inverse[prime], qq, kk), qq, kk);
     if (REDUCE) y = guard(y, static_cast<int64_t>(qq));
     dst[poly * poly_stride + (long long)limb * n + gi] = y;

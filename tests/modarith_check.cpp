@@ -3,7 +3,9 @@
 // must give the same word as the general sign-extended form, for random odd q
 // below 2^61 (k = -q^-1 mod 2^62) and operands below 2^62, edge values included;
 // Shoup's product of the value-only butterflies must give W b mod q up to one q,
-// for any b below 2^64.
+// for any b below 2^64; and the reduced exit of ModDown's inverse transform (one
+// Shoup product by N^-1 R^-1) must give the word of mont_exit(mont_mult(v, N^-1 R))
+// reduced to [0, q), for engine primes and v below 2^62.
 // Usage: modarith_check <iterations> <seed>; prints the mismatch count.
 #include <cstdio>
 #include <cstdlib>
@@ -42,6 +44,33 @@ int main(int argc, char **argv) {
     const uint64_t r = shoup_mult(plain, shoup, any, q);
     const uint64_t exact = static_cast<uint64_t>(static_cast<unsigned __int128>(plain) * any % q);
     if (!(r < 2 * q && r % q == exact)) bad++;
+  }
+  const uint64_t primes[] = {1152921504598720513ull, 18014398506729473ull, 18014398514987009ull,
+                             1099511480321ull};
+  for (uint64_t q : primes) {
+    using u128 = unsigned __int128;
+    auto mulmod = [&](uint64_t a, uint64_t b) { return static_cast<uint64_t>(static_cast<u128>(a) * b % q); };
+    auto powmod = [&](uint64_t a, uint64_t e) {
+      uint64_t r = 1;
+      for (a %= q; e; e >>= 1, a = mulmod(a, a))
+        if (e & 1) r = mulmod(r, a);
+      return r;
+    };
+    const uint64_t k = negated_inverse(q);
+    const uint64_t r_inverse = powmod((uint64_t(1) << 62) % q, q - 2);
+    const uint64_t n_inverse_r = mulmod(powmod(uint64_t(1) << 16, q - 2), (uint64_t(1) << 62) % q);
+    const uint64_t c = mulmod(mulmod(n_inverse_r, r_inverse), r_inverse);
+    const uint64_t c_shoup = static_cast<uint64_t>((static_cast<u128>(c) << 64) / q);
+    for (long it = 0; it < iterations / 8; it++) {
+      uint64_t v = rng() & top;
+      if (it % 3 == 0) v = rng() % (2 * q);
+      if (it % 7 == 0) v = rng() & 3;
+      const int64_t want = guard(mont_exit(mont_mult_lazy(static_cast<int64_t>(v), static_cast<int64_t>(n_inverse_r), q, k), q, k),
+                                 static_cast<int64_t>(q));
+      uint64_t r = shoup_mult(c, c_shoup, v, q);
+      r = r >= q ? r - q : r;
+      if (static_cast<int64_t>(r) != want) bad++;
+    }
   }
   std::printf("%ld\n", bad);
   return 0;
