@@ -162,6 +162,27 @@ Engine::Engine(const Config &config) : params(config) {
   for (size_t i = 0; i < p.p_product_mult_r.size(); i++) ppr[i] = p.p_product_mult_r[i];
   ks_.p_inverse_mult_r = upload_table(pinv);
   ks_.rescale_scale = upload_table(rs);
+  {
+    // Shoup pairs of the rescale constants: C = rescale_scale R^-1 mod q_to.
+    using u128 = unsigned __int128;
+    std::vector<int64_t> rsh(2 * rs.size(), 0);
+    for (int to = 1; to < P; to++) {
+      const uint64_t qt = p.q[to];
+      auto mulmod = [&](uint64_t a, uint64_t b) { return static_cast<uint64_t>(static_cast<u128>(a) * b % qt); };
+      uint64_t r_inverse = 1, base = (uint64_t(1) << 62) % qt;
+      for (uint64_t e = qt - 2; e > 0; e >>= 1) {
+        if (e & 1) r_inverse = mulmod(r_inverse, base);
+        base = mulmod(base, base);
+      }
+      for (int from = 0; from < to; from++) {
+        const size_t at = static_cast<size_t>(from) * P + to;
+        const uint64_t c = mulmod(static_cast<uint64_t>(rs[at]) % qt, r_inverse);
+        rsh[2 * at] = static_cast<int64_t>(c);
+        rsh[2 * at + 1] = static_cast<int64_t>((static_cast<u128>(c) << 64) / qt);
+      }
+    }
+    ks_.rescale_shoup = upload_table(rsh);
+  }
   ks_.p_product_mult_r = upload_table(ppr);
   ks_.prime_count = P;
   ks_.special_count = p.special_prime_count;
@@ -230,6 +251,7 @@ const ModDownTcTables *Engine::mod_down_tc(int moduli_id) {
   ModDownTcTables tc;
   tc.b = upload_table(h.b);
   tc.c_r = upload_table(h.c_r);
+  tc.c_shoup = upload_table(h.c_shoup);
   tc.rounds = h.rounds;
   tc.kb = h.kb;
   return &mod_down_tc_cache_.emplace(moduli_id, tc).first->second;

@@ -11,8 +11,9 @@ namespace fhe_b200 {
 
 // A CTA owns coefficients [coeff0, coeff0 + valid) of polynomial `poly`; divide(j, c)
 // gives the divided limb j of coefficient coeff0 + c.  first_limb holds at least
-// `valid` words of shared memory.  Every thread of the CTA calls this.  LAZY: the
-// rescale's product takes the short form when its operands are in range (same word).
+// `valid` words of shared memory.  Every thread of the CTA calls this.  The rescale's
+// product is Shoup's when its operand is in range (rescale_word_shoup, same word);
+// LAZY is kept for the callers' signatures and selects nothing else.
 template <bool LAZY = false, class Divide>
 __device__ __forceinline__ void mod_down_store(const PrimeTables &t, const KeySwitchTables &ks,
                                                int n, int moduli_id, int L, int poly, int coeff0,
@@ -60,8 +61,9 @@ __device__ __forceinline__ void mod_down_store(const PrimeTables &t, const KeySw
     const int prime = moduli_id + j;
     const int64_t y0 = first_limb[c];
     o[static_cast<long long>(j - 1) * n + c] =
-        rescale_word<LAZY>(combined(j, c), y0, static_cast<uint64_t>(y0) > q_half ? 1 : 0, t.q[prime],
-                     t.k[prime], ks.rescale_scale[static_cast<long long>(moduli_id) * P + prime]);
+        rescale_word_shoup(combined(j, c), y0, static_cast<uint64_t>(y0) > q_half ? 1 : 0, t.q[prime],
+                           t.k[prime], ks.rescale_scale[static_cast<long long>(moduli_id) * P + prime],
+                           ks.rescale_shoup + 2 * (static_cast<long long>(moduli_id) * P + prime));
   }
 }
 

@@ -105,8 +105,9 @@ __global__ void rescale_kernel(PrimeTables t, KeySwitchTables ks, int n, int lim
     const int prime = moduli_id + 1 + j;
     const int64_t x0 = xp[c];
     const int64_t rounder = static_cast<uint64_t>(x0) > q_half ? 1 : 0;  // get_rounder
-    yp[i] = rescale_word(xp[static_cast<long long>(j + 1) * n + c], x0, rounder, t.q[prime],
-                         t.k[prime], ks.rescale_scale[static_cast<long long>(moduli_id) * ks.prime_count + prime]);
+    const long long entry = static_cast<long long>(moduli_id) * ks.prime_count + prime;
+    yp[i] = rescale_word_shoup(xp[static_cast<long long>(j + 1) * n + c], x0, rounder, t.q[prime],
+                               t.k[prime], ks.rescale_scale[entry], ks.rescale_shoup + 2 * entry);
   }
 }
 
@@ -138,9 +139,9 @@ __global__ void scalar_rescale_kernel(PrimeTables t, KeySwitchTables ks, int log
     const int64_t ej = guard(mont_mult_lazy(xp[(static_cast<long long>(j + 1) << log_n) + cidx],
                                             c.v[j + 1], q, k),
                              static_cast<int64_t>(q));
+    const long long entry = static_cast<long long>(moduli_id) * ks.prime_count + prime;
     yp[(static_cast<long long>(j) << log_n) + cidx] =
-        rescale_word<true>(ej, e0, rounder, q, k,
-                           ks.rescale_scale[static_cast<long long>(moduli_id) * ks.prime_count + prime]);
+        rescale_word_shoup(ej, e0, rounder, q, k, ks.rescale_scale[entry], ks.rescale_shoup + 2 * entry);
   }
 }
 
@@ -673,6 +674,7 @@ cudaError_t launch_rescale_to_ntt(const PrimeTables &t, const KeySwitchTables &k
                                   cudaStream_t s) {
   RescaleEnterLoad ld{x, x_stride,
                       ks.rescale_scale + static_cast<long long>(src_moduli_id) * ks.prime_count,
+                      ks.rescale_shoup + 2LL * src_moduli_id * ks.prime_count,
                       t.r_squared, t.q, t.k};
   PlainStore st{y, y_stride};
   return forward_ntt(log_n, polys, limbs, src_moduli_id + 1, t, ld, st, y, y_stride, s);

@@ -38,6 +38,9 @@ void unnote_launches(unsigned long long count);
 struct KeySwitchTables {
   const int64_t *p_inverse_mult_r;  // [K][P] (entry for prime i at [s*P + i])
   const int64_t *rescale_scale;     // [P][P] (entry for from,to at [from*P + to])
+  // [P][P][2]: (C, C') per entry of rescale_scale for shoup_mult, C = the plain
+  // q_from^-1 mod q_to (rescale_scale R^-1) and C' = floor(C 2^64 / q_to).
+  const int64_t *rescale_shoup;
   const int64_t *p_product_mult_r;  // [P] P mod q * R (zero for the special primes)
   int prime_count;
   int special_count;
@@ -130,6 +133,7 @@ cudaError_t launch_mod_down_epilogue_ops(const PrimeTables &t, const KeySwitchTa
 struct ModDownTcTables {
   const uint8_t *b = nullptr;   // [rounds][128 columns][kb bytes], UMMA K-major core matrices
   const int64_t *c_r = nullptr; // [L] prod_s pinv_s * R mod q_j (x_j's Montgomery factor)
+  const int64_t *c_shoup = nullptr;  // [L][2] (C, C'): C = prod_s pinv_s mod q_j, C' = floor(C 2^64 / q_j)
   int rounds = 0;               // ceil(L / 16) MMA rounds of 16 target limbs
   int kb = 0;                   // A row bytes: 9 K rounded up to 32
 };
@@ -158,6 +162,7 @@ bool mod_down_tc_supported(int special_count, int limbs, int n);
 struct ModDownTcHost {
   std::vector<uint8_t> b;
   std::vector<int64_t> c_r;
+  std::vector<int64_t> c_shoup;
   int rounds = 0;
   int kb = 0;
 };

@@ -415,6 +415,25 @@ FHE_HD int64_t rescale_word(int64_t xj, int64_t x0, int64_t rounder, uint64_t q,
   return guard(v, qs);
 }
 
+// rescale_word with the product by q_0^-1 taken as Shoup's when the reduced
+// difference is below 2^62: both products lie in [0, 2q) and have the same value,
+// and the two guards after them leave the canonical residue, so the word is the
+// same.  shoup = (C, C') of the constant (KeySwitchTables::rescale_shoup).
+FHE_HD int64_t rescale_word_shoup(int64_t xj, int64_t x0, int64_t rounder, uint64_t q, uint64_t k,
+                                  int64_t constant, const int64_t *shoup) {
+  const int64_t qs = static_cast<int64_t>(q), q2 = qs << 1;
+  int64_t v = xj - x0;  // mont_subtract (unit.cpp:58-64)
+  v = v >= 0 ? v : v + q2;
+  v = guard(v, qs);
+  if ((static_cast<uint64_t>(v) >> kMontBits) == 0)
+    v = static_cast<int64_t>(shoup_mult(static_cast<uint64_t>(shoup[0]), static_cast<uint64_t>(shoup[1]),
+                                        static_cast<uint64_t>(v), q));
+  else
+    v = mont_mult(v, constant, q, k);
+  v = guard(v + rounder, q2);  // add_tiled
+  return guard(v, qs);
+}
+
 FHE_HD bool redc_operand_ok(int64_t x) {
   return static_cast<uint64_t>(x) < (uint64_t(1) << 61);
 }

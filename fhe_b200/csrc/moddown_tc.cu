@@ -149,10 +149,12 @@ __global__ void __launch_bounds__(kTcThreads, K <= 10 && K != 7 ? 4 : (K <= 13 ?
         uint64_t lo, hi;
         fold8(d + 8 * h, lo, hi);
         const int64_t xj = xs[2 * u2 + h];
-        // REDC(X) < q + 2^19; x_j is the reduced inverse transform's word in [0, q).
+        // REDC(X) < q + 2^19, and x_j prod pinv by Shoup's product is below 2q (its
+        // value is all that matters: the total is reduced to [0, q) below).
         const uint64_t v = static_cast<uint64_t>(redc_wide(lo, hi, q, kq)) +
-                           static_cast<uint64_t>(mont_mult_small(static_cast<uint64_t>(xj),
-                                                                 static_cast<uint64_t>(tc.c_r[j]), q, kq));
+                           shoup_mult(static_cast<uint64_t>(tc.c_shoup[2 * j]),
+                                      static_cast<uint64_t>(tc.c_shoup[2 * j + 1]),
+                                      static_cast<uint64_t>(xj), q);
         uint64_t r = v >= (q << 1) ? v - (q << 1) : v;
         r = r >= q ? r - q : r;
         divided[j * kTcCoeffs + row] = static_cast<int64_t>(r);
@@ -215,6 +217,7 @@ ModDownTcHost make_mod_down_tc_tables(const std::vector<uint64_t> &q,
   h.rounds = (L + kTcTargets - 1) / kTcTargets;
   h.b.assign(static_cast<size_t>(h.rounds) * kTcColumns * h.kb, 0);
   h.c_r.resize(L);
+  h.c_shoup.resize(2 * static_cast<size_t>(L));
   for (int j = 0; j < L; j++) {
     const int prime = moduli_id + j;
     const uint64_t m = q[prime];
@@ -228,6 +231,8 @@ ModDownTcHost make_mod_down_tc_tables(const std::vector<uint64_t> &q,
       w[s] = prod;
     }
     h.c_r[j] = static_cast<int64_t>(mul_mod(prod, r, m));
+    h.c_shoup[2 * j] = static_cast<int64_t>(prod);
+    h.c_shoup[2 * j + 1] = static_cast<int64_t>((static_cast<u128>(prod) << 64) / m);
     const uint64_t two64 = static_cast<uint64_t>((static_cast<u128>(1) << 64) % m);
     const int round = j / kTcTargets, jl = j % kTcTargets;
     uint8_t *b = h.b.data() + static_cast<size_t>(round) * kTcColumns * h.kb;

@@ -79,6 +79,7 @@ struct RescaleEnterLoad {
   const int64_t *src;             // [poly][limbs + 1][N]
   long long poly_stride;
   const int64_t *rescale_scale;   // the dropped prime's row, indexed by prime
+  const int64_t *rescale_shoup;   // the same row's (C, C') pairs
   const int64_t *r_squared;
   const uint64_t *q;
   const uint64_t *k;
@@ -87,8 +88,8 @@ struct RescaleEnterLoad {
     const int64_t x0 = s[gi];
     const int64_t rounder = static_cast<uint64_t>(x0) > (q[prime - limb - 1] >> 1) ? 1 : 0;
     const uint64_t qq = q[prime], kk = k[prime];
-    const int64_t v = rescale_word<true>(s[static_cast<long long>(limb + 1) * n + gi], x0, rounder,
-                                         qq, kk, rescale_scale[prime]);
+    const int64_t v = rescale_word_shoup(s[static_cast<long long>(limb + 1) * n + gi], x0, rounder,
+                                         qq, kk, rescale_scale[prime], rescale_shoup + 2 * prime);
     return mont_mult_lazy(v, r_squared[prime], qq, kk);
   }
 };

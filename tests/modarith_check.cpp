@@ -5,7 +5,8 @@
 // Shoup's product of the value-only butterflies must give W b mod q up to one q,
 // for any b below 2^64; and the reduced exit of ModDown's inverse transform (one
 // Shoup product by N^-1 R^-1) must give the word of mont_exit(mont_mult(v, N^-1 R))
-// reduced to [0, q), for engine primes and v below 2^62.
+// reduced to [0, q), for engine primes and v below 2^62; and the rescale word with
+// Shoup's product must equal the reference's form for any words.
 // Usage: modarith_check <iterations> <seed>; prints the mismatch count.
 #include <cstdio>
 #include <cstdlib>
@@ -70,6 +71,33 @@ int main(int argc, char **argv) {
       uint64_t r = shoup_mult(c, c_shoup, v, q);
       r = r >= q ? r - q : r;
       if (static_cast<int64_t>(r) != want) bad++;
+    }
+  }
+  for (size_t a = 0; a < sizeof(primes) / sizeof(primes[0]); a++) {
+    for (size_t b = 0; b < sizeof(primes) / sizeof(primes[0]); b++) {
+      if (a == b) continue;
+      const uint64_t q0 = primes[a], q = primes[b];  // drop q0, rescale limb mod q
+      using u128 = unsigned __int128;
+      auto mulmod = [&](uint64_t x, uint64_t y) { return static_cast<uint64_t>(static_cast<u128>(x) * y % q); };
+      auto powmod = [&](uint64_t x, uint64_t e) {
+        uint64_t r = 1;
+        for (x %= q; e; e >>= 1, x = mulmod(x, x))
+          if (e & 1) r = mulmod(r, x);
+        return r;
+      };
+      const uint64_t k = negated_inverse(q), r_mod = (uint64_t(1) << 62) % q;
+      const uint64_t plain = powmod(q0 % q, q - 2);             // q0^-1 mod q
+      const int64_t mont = static_cast<int64_t>(mulmod(plain, r_mod));  // q0^-1 R mod q
+      const int64_t pair[2] = {static_cast<int64_t>(plain),
+                               static_cast<int64_t>((static_cast<u128>(plain) << 64) / q)};
+      for (long it = 0; it < iterations / 32; it++) {
+        int64_t xj = static_cast<int64_t>(rng() % q), x0 = static_cast<int64_t>(rng() % q0);
+        if (it % 5 == 0) xj = static_cast<int64_t>(rng());  // any word, negative ones included
+        if (it % 7 == 0) x0 = static_cast<int64_t>(rng() % (2 * q0));
+        const int64_t rounder = static_cast<uint64_t>(x0) > (q0 >> 1) ? 1 : 0;
+        if (rescale_word_shoup(xj, x0, rounder, q, k, mont, pair) != rescale_word(xj, x0, rounder, q, k, mont))
+          bad++;
+      }
     }
   }
   std::printf("%ld\n", bad);
