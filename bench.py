@@ -86,31 +86,64 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples the GPU's SM clock and throttle reasons during the timed region: through
+    NVML in this process (initialised before the region starts, so each sample is
+    one light query), else through nvidia-smi.  Rows keep nvidia-smi's CSV fields."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits: hw_slowdown, hw_thermal_slowdown,
+    # sw_thermal_slowdown, sw_power_cap (the order of the rows' fields 5-8).
+    REASON_BITS = (0x8, 0x40, 0x20, 0x4)
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, period_s: float = 0.05):
         self.gpu = gpu_index
+        self.period = period_s
         self.rows = []
         self._stop = threading.Event()
         self._thread = None
+        self._nvml = None
+        self._handle = None
+
+    def _open_nvml(self):
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self._handle = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            self._nvml = pynvml
+        except Exception:
+            self._nvml = None
+
+    def _sample(self):
+        try:
+            if self._nvml is not None:
+                m, h = self._nvml, self._handle
+                sm = m.nvmlDeviceGetClockInfo(h, m.NVML_CLOCK_SM)
+                mx = m.nvmlDeviceGetMaxClockInfo(h, m.NVML_CLOCK_SM)
+                reasons = m.nvmlDeviceGetCurrentClocksEventReasons(h)
+                power = m.nvmlDeviceGetPowerUsage(h) / 1000.0
+                flags = ["Active" if reasons & bit else "Not Active" for bit in self.REASON_BITS]
+                self.rows.append([str(self.gpu), str(sm), str(mx), f"{power:.1f}", hex(reasons)] + flags)
+                return
+            out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                  "--format=csv,noheader,nounits"], capture_output=True,
+                                 text=True, timeout=5).stdout.strip()
+            if out:
+                self.rows.append([c.strip() for c in out.split(",")])
+        except Exception:
+            pass
 
     def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
-                                      "--format=csv,noheader,nounits"], capture_output=True,
-                                     text=True, timeout=5).stdout.strip()
-                if out:
-                    self.rows.append([c.strip() for c in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+        while not self._stop.wait(self.period if self._nvml is not None else 0.2):
+            self._sample()
 
     def __enter__(self):
+        self._open_nvml()
+        if self._nvml is not None:
+            self._sample()  # a first query before the region: NVML is warm when it starts
+            self.rows.clear()
         self._thread = threading.Thread(target=self._run, daemon=True)
         self._thread.start()
         return self
@@ -119,6 +152,12 @@ class ClockSampler:
         self._stop.set()
         if self._thread:
             self._thread.join(timeout=10)
+        self._sample()  # the state at the end of the region
+        if self._nvml is not None:
+            try:
+                self._nvml.nvmlShutdown()
+            except Exception:
+                pass
 
     def summary(self):
         if not self.rows:
