@@ -102,6 +102,7 @@ SIGNATURES = {
     "fhe_engine_set_tensor_core_wait_limit": (_i, [_vp, ctypes.c_longlong]),
     "fhe_engine_set_graphs": (_i, [_vp, _i]),
     "fhe_engine_set_fused_bsgs": (_i, [_vp, _i]),
+    "fhe_engine_set_value_transforms": (_i, [_vp, _i]),
     "fhe_engine_set_concurrency": (_i, [_vp, _i]),
     "fhe_multiply_relinearize_rescale_batch": (_i, [_vp, _i, ctypes.POINTER(_vp),
                                                    ctypes.POINTER(_vp), _vp, ctypes.POINTER(_vp)]),

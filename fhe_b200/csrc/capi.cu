@@ -785,6 +785,11 @@ int fhe_engine_set_fused_bsgs(fhe_engine *engine, int enable) {
   return guarded(__func__, [&] { engine->impl->set_fused_bsgs(enable != 0); });
 }
 
+int fhe_engine_set_value_transforms(fhe_engine *engine, int enable) {
+  REQUIRE_HANDLE(engine);
+  return guarded(__func__, [&] { engine->impl->set_value_transforms(enable != 0); });
+}
+
 int fhe_multiply_rotate_batch(fhe_engine *engine, int count, const fhe_data *const *a,
                               const fhe_data *const *b, const fhe_data *relinearization_key,
                               const fhe_data *const *rotation_keys, fhe_data **out) {

@@ -182,6 +182,21 @@ Engine::Engine(const Config &config) : params(config) {
       }
     }
     ks_.rescale_shoup = upload_table(rsh);
+    // The rescale and the enter as one product: q_from^-1 R mod q_to, the plain value
+    // of rescale_scale; and R mod q for the rounder.
+    std::vector<int64_t> resh(2 * rs.size(), 0), rmod(P, 0);
+    for (int to = 0; to < P; to++) {
+      const uint64_t qt = p.q[to];
+      rmod[to] = static_cast<int64_t>((uint64_t(1) << 62) % qt);
+      for (int from = 0; from < to; from++) {
+        const size_t at = static_cast<size_t>(from) * P + to;
+        const uint64_t c = static_cast<uint64_t>(rs[at]) % qt;
+        resh[2 * at] = static_cast<int64_t>(c);
+        resh[2 * at + 1] = static_cast<int64_t>((static_cast<u128>(c) << 64) / qt);
+      }
+    }
+    ks_.rescale_enter_shoup = upload_table(resh);
+    ks_.r_mod = upload_table(rmod);
   }
   ks_.p_product_mult_r = upload_table(ppr);
   ks_.prime_count = P;
@@ -557,7 +572,7 @@ std::unique_ptr<Data> Engine::core_rescale(const Data &ct) {
   return out;
 }
 
-std::unique_ptr<Data> Engine::rescale_to_ntt(const Data &ct) {
+std::unique_ptr<Data> Engine::rescale_to_ntt(const Data &ct, const ExactLimbs &exact) {
   // to_ntt(core_rescale(ct)) of a coefficient-form text in one pass.
   if (ct.chains < 2) throw std::runtime_error("cannot rescale a single-limb text.");
   if (ct.is_ntt()) throw std::invalid_argument("rescale to NTT: the text is in NTT form.");
@@ -566,7 +581,7 @@ std::unique_ptr<Data> Engine::rescale_to_ntt(const Data &ct) {
   check(timed("rescale_to_ntt", [&] {
           return launch_rescale_to_ntt(tables_, ks_, params.log_n, ct.polys, out->chains,
                                        ct.moduli_id, ct.d, ct.poly_stride(), out->d,
-                                       out->poly_stride(), stream_);
+                                       out->poly_stride(), stream_, exact);
         }),
         "rescale to NTT");
   return out;
@@ -590,7 +605,7 @@ std::unique_ptr<Data> Engine::rescale(const Data &ct) {
 // ----------------------------------------------------------------- multiply --
 
 // prepare_for_multiply, engine_multiply.cpp:13-28.
-std::unique_ptr<Data> Engine::prepare_for_multiply(const Data &text, int level) {
+std::unique_ptr<Data> Engine::prepare_for_multiply(const Data &text, int level, const Data *rk) {
   std::unique_ptr<Data> cur;
   const Data *t = &text;
   if (t->level() > level) {
@@ -602,12 +617,16 @@ std::unique_ptr<Data> Engine::prepare_for_multiply(const Data &text, int level) 
     t = cur.get();
   }
   if (!t->is_rescaled()) {
-    // rescale_, then the NTT form the product needs: one fused pass.
+    // rescale_, then the NTT form the product needs: one fused pass.  Before a
+    // relinearization only the limbs it reads exactly need the reference's words;
+    // they are limbs of the second polynomial (a1 b1 forms the tensor's third).
+    const ExactLimbs exact = rk ? relinearize_exact_limbs(t->moduli_id + 1, *rk, 1)
+                                : ExactLimbs{ExactLimbs::kAllExact, 0};
     if (t->is_ntt()) {
       auto intt = to_intt(*t);
-      cur = rescale_to_ntt(*intt);
+      cur = rescale_to_ntt(*intt, exact);
     } else {
-      cur = rescale_to_ntt(*t);
+      cur = rescale_to_ntt(*t, exact);
     }
     t = cur.get();
   }
@@ -770,9 +789,43 @@ std::unique_ptr<Data> Engine::multiply_relinearize(const Data &a, const Data &b,
   require_key_level(fn, a, rk, true);
   require_key_level(fn, b, rk, true);
   const int level = std::min(a.level(), b.level());
-  auto pa = prepare_for_multiply(a, level);
-  auto pb = prepare_for_multiply(b, level);
+  auto pa = prepare_for_multiply(a, level, &rk);
+  auto pb = prepare_for_multiply(b, level, &rk);
   return relinearized_product(*pa, *pb, rk);
+}
+
+ExactLimbs Engine::relinearize_exact_limbs(int moduli_id, const Data &rk, int poly) {
+  // Relinearization reduces its output to [0, q) (ModDown's store) and reads the
+  // tensor's first two polynomials as addends below 2q, so only their values matter.
+  // Of the third it reads each partition's limbs through Garner's digits (rns_to_mrs,
+  // core_key_switch.cpp:21-56): the first limb as the first digit itself, word for
+  // word; limb j > 0 as guard(x_j + 2q_j - Y, 2q_j) followed by a Montgomery product
+  // and a reduction to [0, q_j), where Y is the first limb's word or a digit already
+  // reduced.  That result depends on x_j only modulo q_j when 0 <= Y <= 2q_j: the
+  // first limb's word is at most q_first (to_intt_'s exit), and the later Y are below
+  // q_j when q_first <= 2q_j (with every prime below 2^60, the Montgomery products
+  // before them are below 1.5 q_j).  So a partition whose first prime is at most
+  // twice each of its others needs its first limb exact; any other partition needs
+  // all of them.
+  ExactLimbs all{ExactLimbs::kAllExact, 0};
+  if (!value_transforms_) return all;
+  const int L = params.chains(moduli_id);
+  for (int i = 0; i < L; i++)
+    if (params.q[moduli_id + i] >= (uint64_t(1) << 60)) return all;
+  uint64_t mask = 0;
+  for (const Partition &pt : params.partitions(moduli_id, rk.moduli_id)) {
+    const uint64_t q_first = params.q[moduli_id + pt.start];
+    bool bounded = true;
+    for (int j = 1; j < pt.size; j++)
+      if (q_first > 2 * params.q[moduli_id + pt.start + j]) bounded = false;
+    const int exact_count = bounded ? 1 : pt.size;
+    for (int j = 0; j < exact_count; j++) {
+      const int limb = pt.start + j;
+      if (limb >= 64) return all;
+      mask |= uint64_t(1) << limb;
+    }
+  }
+  return ExactLimbs{poly, mask};
 }
 
 std::unique_ptr<Data> Engine::relinearized_product(const Data &pa, const Data &pb, const Data &rk) {
@@ -785,8 +838,10 @@ std::unique_ptr<Data> Engine::relinearized_product(const Data &pa, const Data &p
   // The tensor's NTT-form third polynomial also lands in ModUp's own limbs.
   int64_t *own_ext = own_limbs_ext(m, rk);
   const DevicePartitions *dp = own_ext ? &partitions(m, rk.moduli_id) : nullptr;
+  const ExactLimbs exact = relinearize_exact_limbs(m, rk, 2);
   cudaError_t e = timed("tensor_to_intt", [&] {
-    return launch_tensor_to_intt(tables_, params.log_n, L, m, pa.d, pb.d, t3, stream_, own_ext, dp);
+    return launch_tensor_to_intt(tables_, params.log_n, L, m, pa.d, pb.d, t3, stream_, own_ext, dp,
+                                 exact);
   });
   if (e != cudaSuccess) {
     free_words(t3);
@@ -815,8 +870,8 @@ std::unique_ptr<Data> Engine::multiply_relinearize_rescale(const Data &a, const 
   require_key_level(fn, a, rk, true);
   require_key_level(fn, b, rk, true);
   const int level = std::min(a.level(), b.level());
-  auto pa = prepare_for_multiply(a, level);
-  auto pb = prepare_for_multiply(b, level);
+  auto pa = prepare_for_multiply(a, level, &rk);
+  auto pb = prepare_for_multiply(b, level, &rk);
   const int m = pa->moduli_id;
   const int L = pa->chains;
   {
@@ -831,9 +886,10 @@ std::unique_ptr<Data> Engine::multiply_relinearize_rescale(const Data &a, const 
   // The tensor's NTT-form third polynomial also lands in ModUp's own limbs.
   int64_t *own_ext = own_limbs_ext(m, rk);
   const DevicePartitions *dp = own_ext ? &partitions(m, rk.moduli_id) : nullptr;
+  const ExactLimbs exact = relinearize_exact_limbs(m, rk, 2);
   cudaError_t e = timed("tensor_to_intt", [&] {
     return launch_tensor_to_intt(tables_, params.log_n, L, m, pa->d, pb->d, t3, stream_, own_ext,
-                                 dp);
+                                 dp, exact);
   });
   if (e != cudaSuccess) {
     free_words(t3);

@@ -263,6 +263,10 @@ class Engine {
   // default) or as the per-rotation key products, gathers and diagonal sums; same
   // words either way.
   void set_fused_bsgs(bool on) { fused_bsgs_ = on; }
+  // Multiply-then-relinearize transforms its inputs and the tensor value-only except
+  // the limbs whose words relinearization reads exactly (ExactLimbs); on by default,
+  // off for every limb exact.  Same words either way.
+  void set_value_transforms(bool on) { value_transforms_ = on; }
   // Runs a batch of independent multiply-relinearize-rescale operations, each followed
   // by a rotation with its own fixed key (the batched serving step; no reference
   // counterpart), replayed as one CUDA graph after its first run.
@@ -368,6 +372,7 @@ class Engine {
   };
   bool graphs_ = true;
   bool fused_bsgs_ = true;
+  bool value_transforms_ = true;
   // Streams of batch items (graphs.cu): item i of a batch runs on worker i % count,
   // forked from and joined back into the engine's stream by events.
   int concurrency_ = 4;
@@ -546,9 +551,18 @@ class Engine {
 
   // Core steps.
   std::unique_ptr<Data> core_rescale(const Data &ct);          // coefficient form
-  std::unique_ptr<Data> prepare_for_multiply(const Data &text, int level);
-  std::unique_ptr<Data> rescale_to_ntt(const Data &text);  // to_ntt(core_rescale(text))
+  // With rk, the product is relinearized with rk: the prepared text's words then
+  // only matter where relinearize_exact_limbs says so.
+  std::unique_ptr<Data> prepare_for_multiply(const Data &text, int level,
+                                             const Data *rk = nullptr);
+  // to_ntt(core_rescale(text)); limbs outside `exact` value-only.
+  std::unique_ptr<Data> rescale_to_ntt(const Data &text,
+                                       const ExactLimbs &exact = ExactLimbs{ExactLimbs::kAllExact, 0});
   std::unique_ptr<Data> relinearized_product(const Data &pa, const Data &pb, const Data &rk);
+  // The limbs of polynomial `poly` of a product at moduli_id that relinearization
+  // with rk reads word for word (ExactLimbs), or every limb exact when the switch is
+  // off or the bound that makes the others value-only does not hold.
+  ExactLimbs relinearize_exact_limbs(int moduli_id, const Data &rk, int poly);
   // Hybrid key switch of the coefficient-form polynomial c1 at moduli_id (L limbs):
   // decompose, ModUp, key product, optional rotation term b * P (rotate_c0 = the
   // coefficient-form c0), ModDown and the epilogue operations `ops` into `out`.

@@ -28,7 +28,8 @@ std::vector<std::unique_ptr<Data>> Engine::run_captured(std::vector<uint64_t> ke
                                                         const std::vector<const Data *> &inputs,
                                                         const GraphBody &body) {
   if (!graphs_ || profiling_) return body(inputs);
-  key.insert(key.end(), {static_cast<uint64_t>(tensor_cores_), static_cast<uint64_t>(fused_bsgs_)});
+  key.insert(key.end(), {static_cast<uint64_t>(tensor_cores_), static_cast<uint64_t>(fused_bsgs_),
+                         static_cast<uint64_t>(value_transforms_)});
   for (const Data *d : inputs) {
     const double hi = static_cast<double>(d->scale);
     key.insert(key.end(), {static_cast<uint64_t>(d->type), static_cast<uint64_t>(d->flag),

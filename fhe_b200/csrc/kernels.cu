@@ -580,9 +580,10 @@ cudaError_t launch_extended_ntt(const PrimeTables &t, const DevicePartitions &dp
   PlainStore st{ext, stride};
   // Value-only: the extended polynomial reaches the output only through the key
   // inner product's reduction to [0, q) and ModDown's reduced inverse transform.
-  return forward_ntt<PlainLoad, PlainStore, true>(log_n, dp.count, dp.extended, moduli_id, t, ld, st,
-                                                  ext, stride, s, skip_own ? dp.start : nullptr,
-                                                  skip_own ? dp.size : nullptr);
+  return forward_ntt<PlainLoad, PlainStore, kNttValueOnly>(log_n, dp.count, dp.extended, moduli_id, t,
+                                                           ld, st, ext, stride, s,
+                                                           skip_own ? dp.start : nullptr,
+                                                           skip_own ? dp.size : nullptr);
 }
 
 cudaError_t launch_key_inner_product(const PrimeTables &t, const DevicePartitions &dp, int n,
@@ -621,8 +622,9 @@ cudaError_t launch_mod_down_intt(const PrimeTables &t, int log_n, int moduli_id,
   PlainLoad ld{acc, stride};
   EnterExitStore<true> st{acc, stride, t.n_inverse, t.q, t.k, t.exit_shoup};
   // Value-only: the store reduces every word to [0, q).
-  return inverse_ntt<PlainLoad, EnterExitStore<true>, true>(log_n, polys, extended, moduli_id, t, ld,
-                                                            st, acc, stride, s);
+  return inverse_ntt<PlainLoad, EnterExitStore<true>, kNttValueOnly>(log_n, polys, extended,
+                                                                     moduli_id, t, ld, st, acc,
+                                                                     stride, s);
 }
 
 cudaError_t launch_mod_down_epilogue_ops(const PrimeTables &t, const KeySwitchTables &ks, int n,
@@ -671,13 +673,18 @@ cudaError_t launch_to_ntt(const PrimeTables &t, int log_n, int polys, int limbs,
 cudaError_t launch_rescale_to_ntt(const PrimeTables &t, const KeySwitchTables &ks, int log_n,
                                   int polys, int limbs, int src_moduli_id, const int64_t *x,
                                   long long x_stride, int64_t *y, long long y_stride,
-                                  cudaStream_t s) {
-  RescaleEnterLoad ld{x, x_stride,
-                      ks.rescale_scale + static_cast<long long>(src_moduli_id) * ks.prime_count,
-                      ks.rescale_shoup + 2LL * src_moduli_id * ks.prime_count,
-                      t.r_squared, t.q, t.k};
+                                  cudaStream_t s, const ExactLimbs &exact) {
+  const long long row = static_cast<long long>(src_moduli_id) * ks.prime_count;
   PlainStore st{y, y_stride};
-  return forward_ntt(log_n, polys, limbs, src_moduli_id + 1, t, ld, st, y, y_stride, s);
+  if (exact.poly == ExactLimbs::kAllExact) {
+    RescaleEnterLoad<false> ld{x, x_stride, ks.rescale_scale + row, ks.rescale_shoup + 2 * row,
+                               t.r_squared, t.q, t.k};
+    return forward_ntt(log_n, polys, limbs, src_moduli_id + 1, t, ld, st, y, y_stride, s);
+  }
+  RescaleEnterLoad<true> ld{x, x_stride, ks.rescale_scale + row, ks.rescale_shoup + 2 * row,
+                            t.r_squared, t.q, t.k, ks.rescale_enter_shoup + 2 * row, ks.r_mod, exact};
+  return forward_ntt<RescaleEnterLoad<true>, PlainStore, kNttMixed>(
+      log_n, polys, limbs, src_moduli_id + 1, t, ld, st, y, y_stride, s, nullptr, nullptr, exact);
 }
 
 cudaError_t launch_attach_special_ntt(const PrimeTables &t, const KeySwitchTables &ks, int log_n,
@@ -713,7 +720,8 @@ cudaError_t launch_ntt_plain(const PrimeTables &t, int log_n, int polys, int lim
 
 cudaError_t launch_tensor_to_intt(const PrimeTables &t, int log_n, int limbs, int prime_base,
                                   const int64_t *a, const int64_t *b, int64_t *y, cudaStream_t s,
-                                  int64_t *own_ext, const DevicePartitions *dp) {
+                                  int64_t *own_ext, const DevicePartitions *dp,
+                                  const ExactLimbs &exact) {
   const long long stride = static_cast<long long>(limbs) << log_n;
   TensorLoad ld{a, b, stride, t.q, t.k};
   if (own_ext != nullptr) {
@@ -724,8 +732,13 @@ cudaError_t launch_tensor_to_intt(const PrimeTables &t, int log_n, int limbs, in
     ld.part_count = dp->count;
     ld.extended = dp->extended;
   }
-  EnterExitStore<false> st{y, stride, t.n_inverse, t.q, t.k};
-  return inverse_ntt(log_n, 3, limbs, prime_base, t, ld, st, y, stride, s);
+  if (exact.poly == ExactLimbs::kAllExact) {
+    EnterExitStore<false> st{y, stride, t.n_inverse, t.q, t.k};
+    return inverse_ntt(log_n, 3, limbs, prime_base, t, ld, st, y, stride, s);
+  }
+  MixedExitStore st{y, stride, t.n_inverse, t.q, t.k, t.exit_shoup, exact};
+  return inverse_ntt<TensorLoad, MixedExitStore, kNttMixed>(log_n, 3, limbs, prime_base, t, ld, st, y,
+                                                            stride, s, exact);
 }
 
 }  // namespace fhe_b200

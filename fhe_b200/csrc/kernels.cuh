@@ -12,6 +12,22 @@
 
 namespace fhe_b200 {
 
+// The limbs of a mixed transform (ntt.cuh, kNttMixed) whose words must be the
+// reference's: limbs in `mask` of polynomial `poly`.  A multiply followed by
+// relinearization reduces every word it returns to [0, q) and reads most of its
+// intermediate words only modulo q; what it reads word for word is the first limb of
+// each key-switching partition of the tensor's third polynomial (Garner's first
+// digit, rns_to_mrs, core_key_switch.cpp:21-56), and so the same limbs of the
+// second polynomial of both transformed inputs.
+struct ExactLimbs {
+  int poly = -1;      // -1: none; kAllExact: every limb of every polynomial
+  uint64_t mask = 0;  // limbs below 64
+  static constexpr int kAllExact = -2;
+  __host__ __device__ bool exact(int p, int limb) const {
+    return poly == kAllExact || (p == poly && limb < 64 && ((mask >> limb) & 1) != 0);
+  }
+};
+
 // Constants of the partitions of one (ciphertext moduli id, key moduli id) pair,
 // resident on the device.  Host side: Parameters::partition_constants.
 struct DevicePartitions {
@@ -41,6 +57,11 @@ struct KeySwitchTables {
   // [P][P][2]: (C, C') per entry of rescale_scale for shoup_mult, C = the plain
   // q_from^-1 mod q_to (rescale_scale R^-1) and C' = floor(C 2^64 / q_to).
   const int64_t *rescale_shoup;
+  // [P][P][2]: the rescale and to_ntt's enter as one product, for words that only
+  // matter modulo q_to: (C, C') with C = rescale_scale mod q_to (q_from^-1 R, the
+  // product of the two multipliers) and C' = floor(C 2^64 / q_to).
+  const int64_t *rescale_enter_shoup;
+  const int64_t *r_mod;             // [P] R mod q: the rounder's 1 after the enter
   const int64_t *p_product_mult_r;  // [P] P mod q * R (zero for the special primes)
   int prime_count;
   int special_count;
@@ -337,10 +358,13 @@ cudaError_t launch_to_ntt(const PrimeTables &t, int log_n, int polys, int limbs,
                           cudaStream_t s);
 // to_ntt_ of the rescale of a coefficient-form text in one pass: x is [polys][limbs +
 // 1][N] at src_moduli_id, y is [polys][limbs][N] at src_moduli_id + 1 (NTT form).
+// Limbs outside `exact` (all of them exact by default) are transformed value-only: a
+// word of the same value modulo q, in [0, 2q).
 cudaError_t launch_rescale_to_ntt(const PrimeTables &t, const KeySwitchTables &ks, int log_n,
                                   int polys, int limbs, int src_moduli_id, const int64_t *x,
                                   long long x_stride, int64_t *y, long long y_stride,
-                                  cudaStream_t s);
+                                  cudaStream_t s,
+                                  const ExactLimbs &exact = ExactLimbs{ExactLimbs::kAllExact, 0});
 // attach_special_prime_chains_ of a coefficient-form text: y [polys][limbs + K][N]
 // = to_ntt_ of (x * P on the limbs, zero special limbs); the zero limbs are written
 // as zeros (their transform), the others go through one fused NTT.
@@ -359,10 +383,12 @@ cudaError_t launch_ntt_plain(const PrimeTables &t, int log_n, int polys, int lim
 // Inverse NTT (to_intt_) of the tensor of two NTT-form 2-poly ciphertexts a, b
 // without materialising the tensor: y [3][L][N] coefficient form.  With own_ext, the
 // NTT-form words of the third polynomial are also written to each partition's own
-// limbs of the extended buffer own_ext [count][E][N] (ModUp with skip_own).
+// limbs of the extended buffer own_ext [count][E][N] (ModUp with skip_own).  Limbs
+// outside `exact` are transformed value-only, as in launch_rescale_to_ntt.
 cudaError_t launch_tensor_to_intt(const PrimeTables &t, int log_n, int limbs, int prime_base,
                                   const int64_t *a, const int64_t *b, int64_t *y,
                                   cudaStream_t s, int64_t *own_ext = nullptr,
-                                  const DevicePartitions *dp = nullptr);
+                                  const DevicePartitions *dp = nullptr,
+                                  const ExactLimbs &exact = ExactLimbs{ExactLimbs::kAllExact, 0});
 
 }  // namespace fhe_b200

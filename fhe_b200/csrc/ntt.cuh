@@ -28,6 +28,17 @@ namespace fhe_b200 {
 
 void note_launch(unsigned count);
 
+// Which words a transform must reproduce (template parameter VALUE_ONLY):
+//   kNttExact      every butterfly is the reference's, every word identical;
+//   kNttValueOnly  only each result's value modulo q matters (Harvey's butterflies
+//                  on Shoup twiddles where the words are in range);
+//   kNttMixed      value-only except the limbs that NttPass::exact names, which take
+//                  the exact butterflies (a CTA transforms one limb, so the choice is
+//                  uniform per CTA).
+constexpr int kNttExact = 0;
+constexpr int kNttValueOnly = 1;
+constexpr int kNttMixed = 2;
+
 struct NttPass {
   int log_n;
   int stride_log;  // log2(T); 0 for contiguous passes
@@ -40,6 +51,8 @@ struct NttPass {
   // left untouched (ModUp's partitions' own limbs, already in NTT form).
   const int *skip_start = nullptr;
   const int *skip_size = nullptr;
+  // A kNttMixed transform keeps the exact butterflies on these limbs only.
+  ExactLimbs exact;
 };
 
 // Reads word gi of (poly, limb) from a [poly][limb][N] buffer.
@@ -75,6 +88,13 @@ struct EnterLoad {
 // rescale_once_ (core_rescale.cpp:5-25) and to_ntt_'s enter on the way in: limb
 // `limb` of the rescaled text is made from limbs limb + 1 and 0 of the source, whose
 // first prime is prime - limb - 1 (the rounder compares unsigned, as get_rounder).
+//
+// MIXED: the limbs outside `exact` only matter modulo q.  Their word is
+// ((x_j - x_0) q_0^-1 + rounder) R mod q, the value of the two steps, formed as one
+// Shoup product of the difference by q_0^-1 R plus the rounder's R, in [0, 2q); a
+// difference still negative after adding 2q (words far out of range) takes the
+// exact steps, whose value is the same.
+template <bool MIXED = false>
 struct RescaleEnterLoad {
   const int64_t *src;             // [poly][limbs + 1][N]
   long long poly_stride;
@@ -83,13 +103,29 @@ struct RescaleEnterLoad {
   const int64_t *r_squared;
   const uint64_t *q;
   const uint64_t *k;
+  const int64_t *enter_shoup = nullptr;  // MIXED: the row's rescale_enter_shoup pairs
+  const int64_t *r_mod = nullptr;        // MIXED: R mod q, indexed by prime
+  ExactLimbs exact;
   __device__ __forceinline__ int64_t operator()(int poly, int limb, int prime, int gi, int n) const {
     const int64_t *s = src + poly * poly_stride;
     const int64_t x0 = s[gi];
     const int64_t rounder = static_cast<uint64_t>(x0) > (q[prime - limb - 1] >> 1) ? 1 : 0;
     const uint64_t qq = q[prime], kk = k[prime];
-    const int64_t v = rescale_word_shoup(s[static_cast<long long>(limb + 1) * n + gi], x0, rounder,
-                                         qq, kk, rescale_scale[prime], rescale_shoup + 2 * prime);
+    const int64_t xj = s[static_cast<long long>(limb + 1) * n + gi];
+    if (MIXED && !exact.exact(poly, limb)) {
+      const int64_t q2 = static_cast<int64_t>(qq << 1);
+      int64_t d = xj - x0;
+      d = d >= 0 ? d : d + q2;
+      if (d >= 0) {
+        const uint64_t y = shoup_mult(static_cast<uint64_t>(enter_shoup[2 * prime]),
+                                      static_cast<uint64_t>(enter_shoup[2 * prime + 1]),
+                                      static_cast<uint64_t>(d), qq) +
+                           (rounder ? static_cast<uint64_t>(r_mod[prime]) : 0);  // [0, 3q)
+        return static_cast<int64_t>(y) >= q2 ? static_cast<int64_t>(y) - q2 : static_cast<int64_t>(y);
+      }
+    }
+    const int64_t v = rescale_word_shoup(xj, x0, rounder, qq, kk, rescale_scale[prime],
+                                         rescale_shoup + 2 * prime);
     return mont_mult_lazy(v, r_squared[prime], qq, kk);
   }
 };
@@ -134,6 +170,30 @@ struct EnterExitStore {
     int64_t y = mont_exit(mont_mult_lazy(v, n_inverse[prime], qq, kk), qq, kk);
     if (REDUCE) y = guard(y, static_cast<int64_t>(qq));
     dst[poly * poly_stride + (long long)limb * n + gi] = y;
+  }
+};
+
+// to_intt_'s exit (EnterExitStore<false>) after a mixed inverse transform: the exact
+// limbs keep mont_exit(mont_mult(v, N^-1 R)); the others, whose words only matter
+// modulo q, take one Shoup product by N^-1 R^-1, a word in [0, 2q) of the same value.
+struct MixedExitStore {
+  int64_t *dst;
+  long long poly_stride;
+  const int64_t *n_inverse;
+  const uint64_t *q;
+  const uint64_t *k;
+  const int64_t *exit_shoup;  // PrimeTables::exit_shoup
+  ExactLimbs exact;
+  __device__ __forceinline__ void operator()(int poly, int limb, int prime, int gi, int n, int64_t v) const {
+    const uint64_t qq = q[prime], kk = k[prime];
+    int64_t *d = dst + poly * poly_stride + (long long)limb * n + gi;
+    if (!exact.exact(poly, limb) && (static_cast<uint64_t>(v) >> kMontBits) == 0) {
+      *d = static_cast<int64_t>(shoup_mult(static_cast<uint64_t>(exit_shoup[2 * prime]),
+                                           static_cast<uint64_t>(exit_shoup[2 * prime + 1]),
+                                           static_cast<uint64_t>(v), qq));
+      return;
+    }
+    *d = mont_exit(mont_mult_lazy(v, n_inverse[prime], qq, kk), qq, kk);
   }
 };
 
@@ -184,7 +244,7 @@ constexpr int kFixedLogN = 16;
 constexpr int kFixedStages = 8;
 constexpr int kFixedColumnsLog = 4;
 
-template <int S, bool INVERSE, class Loader, class Storer, bool VALUE_ONLY = false,
+template <int S, bool INVERSE, class Loader, class Storer, int VALUE_ONLY = kNttExact,
           int SHAPE = kShapeRuntime>
 __global__ void __launch_bounds__(kNttThreads, 4)
     ntt_pass_kernel(NttPass a, PrimeTables t, Loader load, Storer store) {
@@ -212,16 +272,21 @@ __global__ void __launch_bounds__(kNttThreads, 4)
   const uint64_t k = t.k[prime];
   const int64_t q2 = static_cast<int64_t>(q << 1);
   const int n = 1 << a.log_n;
-  const int64_t *tw = (VALUE_ONLY ? (INVERSE ? t.root_inverse_reduced : t.root_reduced)
-                                  : (INVERSE ? t.root_inverse : t.root)) +
+  // This CTA's limb only matters modulo q (uniform per CTA).
+  const bool value_limb =
+      VALUE_ONLY == kNttValueOnly || (VALUE_ONLY == kNttMixed && !a.exact.exact(poly, limb));
+  // Twiddles of the general product: a mixed pass has exact limbs, which need the
+  // reference's words; the same values serve its value-only limbs out of range.
+  const int64_t *tw = (VALUE_ONLY == kNttValueOnly ? (INVERSE ? t.root_inverse_reduced : t.root_reduced)
+                                                   : (INVERSE ? t.root_inverse : t.root)) +
                      static_cast<size_t>(prime) * (n - 1);
-  // Value-only passes on in-range words multiply by Shoup's (W, W') pairs instead.
+  // Value-only limbs' in-range words multiply by Shoup's (W, W') pairs instead.
   const longlong2 *tws =
       VALUE_ONLY ? reinterpret_cast<const longlong2 *>(INVERSE ? t.root_inverse_shoup : t.root_shoup) +
                        static_cast<size_t>(prime) * (n - 1)
                  : nullptr;
   // A forward value-only pass after the first reads words in [0, 4q).
-  const uint64_t in_bound = (VALUE_ONLY && !INVERSE && a.first > 0) ? (q << 2) : (q << 1);
+  const uint64_t in_bound = (value_limb && !INVERSE && a.first > 0) ? (q << 2) : (q << 1);
   const bool last_pass = !INVERSE && a.first + S == a.log_n;
   const int T = 1 << a.stride_log;
   const bool strided = T > 1;
@@ -283,7 +348,7 @@ __global__ void __launch_bounds__(kNttThreads, 4)
           if (e < E) in_range = in_range && static_cast<uint64_t>(x[e]) < in_bound;
         slow = slow || !in_range;
       }
-      auto stages = [&](auto lazy) {
+      auto stages = [&](auto lazy, auto shoup) {
         constexpr bool kLazy = decltype(lazy)::value;
         // guard(a + b, q2) and guard(a + q2 - b, q2) (unit.h:13)
         auto add_guard = [&](int64_t a1, int64_t b1) -> int64_t {
@@ -306,7 +371,7 @@ __global__ void __launch_bounds__(kNttThreads, 4)
         };
         // The twiddle of table entry i: the Montgomery word, or for Harvey's form
         // on in-range words the Shoup pair (its product is the same value mod q).
-        constexpr bool kShoup = kLazy && VALUE_ONLY;
+        constexpr bool kShoup = kLazy && decltype(shoup)::value;
         struct Twiddle {
           int64_t w, wp;
         };
@@ -383,15 +448,25 @@ __global__ void __launch_bounds__(kNttThreads, 4)
         }
       };
       if (in_range) {
-        stages(std::true_type{});
+        if constexpr (VALUE_ONLY == kNttValueOnly) {
+          stages(std::true_type{}, std::true_type{});
+        } else if constexpr (VALUE_ONLY == kNttMixed) {
+          if (value_limb) {
+            stages(std::true_type{}, std::true_type{});
+          } else {
+            stages(std::true_type{}, std::false_type{});
+          }
+        } else {
+          stages(std::true_type{}, std::false_type{});
+        }
       } else {
-        stages(std::false_type{});
+        stages(std::false_type{}, std::false_type{});
       }
 #pragma unroll
       for (int e = 0; e < kMaxE; e++) {
         if (e < E) {
           if (round == R - 1) {
-            if (VALUE_ONLY && !INVERSE && last_pass && in_range) {
+            if (VALUE_ONLY && value_limb && !INVERSE && last_pass && in_range) {
               const int64_t y = x[e] - q2;  // [0, 4q) -> [0, 2q)
               x[e] = y < 0 ? x[e] : y;
             }
@@ -429,7 +504,7 @@ inline NttPlan ntt_plan(int log_n) {
 }
 
 
-template <int S, bool INVERSE, class Loader, class Storer, bool VALUE_ONLY = false,
+template <int S, bool INVERSE, class Loader, class Storer, int VALUE_ONLY = kNttExact,
           int SHAPE = kShapeRuntime>
 cudaError_t launch_ntt_pass(const NttPass &a, const PrimeTables &t, const Loader &ld,
                             const Storer &st, cudaStream_t stream) {
@@ -452,7 +527,7 @@ cudaError_t launch_ntt_pass(const NttPass &a, const PrimeTables &t, const Loader
   return cudaGetLastError();
 }
 
-template <bool INVERSE, class Loader, class Storer, bool VALUE_ONLY = false>
+template <bool INVERSE, class Loader, class Storer, int VALUE_ONLY = kNttExact>
 cudaError_t dispatch_ntt_pass(int S, const NttPass &a, const PrimeTables &t, const Loader &ld,
                               const Storer &st, cudaStream_t stream) {
   if (S == kFixedStages && a.log_n == kFixedLogN && a.columns_log == kFixedColumnsLog) {
@@ -483,13 +558,13 @@ cudaError_t dispatch_ntt_pass(int S, const NttPass &a, const PrimeTables &t, con
 // Batched forward NTT of `polys` x `limbs` limbs.  The first pass reads through
 // `ld`, the last pass writes through `st`; intermediate data lives in `work`
 // ([poly][limb][N], stride work_stride), which may alias the final destination.
-template <class Loader, class Storer, bool VALUE_ONLY = false>
+template <class Loader, class Storer, int VALUE_ONLY = kNttExact>
 cudaError_t forward_ntt(int log_n, int polys, int limbs, int prime_base, const PrimeTables &t,
                         const Loader &ld, const Storer &st, int64_t *work, long long work_stride,
                         cudaStream_t stream, const int *skip_start = nullptr,
-                        const int *skip_size = nullptr) {
+                        const int *skip_size = nullptr, const ExactLimbs &exact = ExactLimbs{}) {
   const NttPlan plan = ntt_plan(log_n);
-  NttPass a{log_n, 0, 0, 1, polys, limbs, prime_base, skip_start, skip_size};
+  NttPass a{log_n, 0, 0, 1, polys, limbs, prime_base, skip_start, skip_size, exact};
   if (plan.passes == 1) {
     a.stride_log = 0;
     a.first = 0;
@@ -511,12 +586,13 @@ cudaError_t forward_ntt(int log_n, int polys, int limbs, int prime_base, const P
                                                                  stream);
 }
 
-template <class Loader, class Storer, bool VALUE_ONLY = false>
+template <class Loader, class Storer, int VALUE_ONLY = kNttExact>
 cudaError_t inverse_ntt(int log_n, int polys, int limbs, int prime_base, const PrimeTables &t,
                         const Loader &ld, const Storer &st, int64_t *work, long long work_stride,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, const ExactLimbs &exact = ExactLimbs{}) {
   const NttPlan plan = ntt_plan(log_n);
   NttPass a{log_n, 0, 0, 1, polys, limbs, prime_base};
+  a.exact = exact;
   if (plan.passes == 1) {
     a.stride_log = 0;
     a.first = 0;

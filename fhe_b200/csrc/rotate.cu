@@ -181,9 +181,8 @@ cudaError_t launch_rotate_base(const PrimeTables &t, const KeySwitchTables &ks, 
   ScaledEnterLoad ld{c0, ks.p_product_mult_r, t.r_squared, t.q, t.k};
   AccumulateStore st{acc0, t.q};
   // Value-only: the accumulated key product reaches the output through ModDown.
-  return forward_ntt<ScaledEnterLoad, AccumulateStore, true>(log_n, 1, limbs, moduli_id, t, ld, st,
-                                                             work,
-                                                             static_cast<long long>(limbs) << log_n, s);
+  return forward_ntt<ScaledEnterLoad, AccumulateStore, kNttValueOnly>(
+      log_n, 1, limbs, moduli_id, t, ld, st, work, static_cast<long long>(limbs) << log_n, s);
 }
 
 cudaError_t launch_permute_signed(const PrimeTables &t, int n, int polys, int limbs,

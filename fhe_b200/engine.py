@@ -480,6 +480,12 @@ class Engine:
         (default on) or as per-rotation kernels; same words either way."""
         check(_lib.load().fhe_engine_set_fused_bsgs(self._h, int(enable)))
 
+    def set_value_transforms(self, enable: bool) -> None:
+        """Multiply-then-relinearize transforms its inputs and tensor value-only on the
+        limbs that relinearization reads only modulo q (default on), or every limb with
+        the reference's butterflies; same words either way."""
+        check(_lib.load().fhe_engine_set_value_transforms(self._h, int(enable)))
+
     def multiply_rotate_batch(self, a: list, b: list, relinearization_key: Data,
                               rotation_keys: list) -> list:
         """[rotate(multiply_relinearize_rescale(a[i], b[i], rk), rotation_keys[i])]: one

@@ -477,6 +477,11 @@ int fhe_engine_set_graphs(fhe_engine *engine, int enable);
  * sums) as one fused kernel (default on) or as per-rotation kernels.  Same words
  * either way. */
 int fhe_engine_set_fused_bsgs(fhe_engine *engine, int enable);
+/* Multiply-then-relinearize (fhe_multiply_relinearize[_rescale] and the batches over
+ * them) transforms its rescaled inputs and its tensor value-only on the limbs whose
+ * words relinearization reads only modulo q (default on), or every limb with the
+ * reference's butterflies.  Same words either way; no reference counterpart. */
+int fhe_engine_set_value_transforms(fhe_engine *engine, int enable);
 /* The number of captured bootstrap graphs the engine holds, and of input shapes
  * whose capture failed and which therefore run directly. */
 int fhe_engine_graph_counts(const fhe_engine *engine, int *captured, int *failed);
