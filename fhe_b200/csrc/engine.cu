@@ -197,6 +197,22 @@ Engine::Engine(const Config &config) : params(config) {
     }
     ks_.rescale_enter_shoup = upload_table(resh);
     ks_.r_mod = upload_table(rmod);
+    // P mod q and its Shoup quotient (the tensor addend of the key inner product):
+    // p_product_mult_r R^-1.
+    std::vector<int64_t> psh(2 * static_cast<size_t>(P), 0);
+    for (int i = 0; i < P; i++) {
+      const uint64_t qi = p.q[i];
+      auto mulmod = [&](uint64_t a, uint64_t b) { return static_cast<uint64_t>(static_cast<u128>(a) * b % qi); };
+      uint64_t r_inverse = 1, base = (uint64_t(1) << 62) % qi;
+      for (uint64_t e = qi - 2; e > 0; e >>= 1) {
+        if (e & 1) r_inverse = mulmod(r_inverse, base);
+        base = mulmod(base, base);
+      }
+      const uint64_t c = mulmod(static_cast<uint64_t>(ppr[i]) % qi, r_inverse);
+      psh[2 * i] = static_cast<int64_t>(c);
+      psh[2 * i + 1] = static_cast<int64_t>((static_cast<u128>(c) << 64) / qi);
+    }
+    ks_.p_shoup = upload_table(psh);
   }
   ks_.p_product_mult_r = upload_table(ppr);
   ks_.prime_count = P;
@@ -678,7 +694,8 @@ std::unique_ptr<Data> Engine::multiply(const Data &a, const Data &b) {
 
 void Engine::key_switch_pipeline(const int64_t *c1, int moduli_id, const Data &key,
                                  const int64_t *rotate_c0, const EpilogueOps &ops, int64_t *out,
-                                 const int64_t *decomposed, int64_t *own_ext) {
+                                 const int64_t *decomposed, int64_t *own_ext,
+                                 const TensorAddend *addend) {
   const int n = params.n;
   const int L = params.chains(moduli_id);
   const int E = params.chains(moduli_id, true);
@@ -707,7 +724,8 @@ void Engine::key_switch_pipeline(const int64_t *c1, int moduli_id, const Data &k
   if (e == cudaSuccess)
     e = timed("key_inner_product", [&] {
       return launch_key_inner_product(tables_, dp, n, moduli_id, ext, key.d, key.chains,
-                                      moduli_id - key.moduli_id, acc, stream_);
+                                      moduli_id - key.moduli_id, acc, stream_,
+                                      addend ? *addend : TensorAddend{});
     });
   if (e == cudaSuccess && rotate_c0 != nullptr)
     e = timed("rotate_base", [&] {
@@ -724,13 +742,46 @@ void Engine::key_switch_pipeline(const int64_t *c1, int moduli_id, const Data &k
 }
 
 void Engine::relinearize_tail(const int64_t *t3, int moduli_id, const Data &rk, int mode,
-                              int64_t *out, int64_t *own_ext) {
+                              int64_t *out, int64_t *own_ext, const TensorAddend *addend) {
   EpilogueOps ops;
-  ops.base = t3;
-  ops.base_polys = mode == 0 ? 0 : 2;
   ops.rescale = mode == 2;
   const long long L = params.chains(moduli_id);
+  if (addend) {
+    // The first two polynomials enter through the key inner product; t3 holds the
+    // third alone.
+    key_switch_pipeline(t3, moduli_id, rk, nullptr, ops, out, nullptr, own_ext, addend);
+    return;
+  }
+  ops.base = t3;
+  ops.base_polys = mode == 0 ? 0 : 2;
   key_switch_pipeline(t3 + 2 * L * params.n, moduli_id, rk, nullptr, ops, out, nullptr, own_ext);
+}
+
+bool Engine::fold_tensor(int moduli_id, const Data &rk) {
+  if (!value_transforms_) return false;
+  if (partitions(moduli_id, rk.moduli_id).count > 8) return false;
+  // The exact sum takes operands below 2^61: words in [0, 2q) for q below 2^60.  And
+  // P d carries d only where P is invertible: a chain whose first prime is also a
+  // special prime (P = 0 modulo it, at the top level) keeps the addend in ModDown's
+  // store, where the reference adds it.
+  const int L = params.chains(moduli_id);
+  for (int i = 0; i < L; i++)
+    if (params.q[moduli_id + i] >= (uint64_t(1) << 60) ||
+        params.p_product_mult_r[moduli_id + i] == 0)
+      return false;
+  return true;
+}
+
+TensorAddend Engine::tensor_addend(const Data &pa, const Data &pb) const {
+  TensorAddend add;
+  add.a = pa.d;
+  add.b = pb.d;
+  add.a_stride = pa.poly_stride();
+  add.b_stride = pb.poly_stride();
+  add.p_shoup = ks_.p_shoup;
+  add.p_mont = ks_.p_product_mult_r;
+  add.limbs = pa.chains;
+  return add;
 }
 
 std::unique_ptr<Data> Engine::relinearize(const Data &ct, const Data &rk) {
@@ -834,14 +885,17 @@ std::unique_ptr<Data> Engine::relinearized_product(const Data &pa, const Data &p
   // NTT-form polynomials are never written.
   const int m = pa.moduli_id;
   const int L = pa.chains;
-  int64_t *t3 = alloc_words(static_cast<size_t>(3) * L * params.n);
+  // With the fold, only the third polynomial is transformed; the first two go to the
+  // key inner product.
+  const bool fold = fold_tensor(m, rk);
+  int64_t *t3 = alloc_words(static_cast<size_t>(fold ? 1 : 3) * L * params.n);
   // The tensor's NTT-form third polynomial also lands in ModUp's own limbs.
   int64_t *own_ext = own_limbs_ext(m, rk);
   const DevicePartitions *dp = own_ext ? &partitions(m, rk.moduli_id) : nullptr;
-  const ExactLimbs exact = relinearize_exact_limbs(m, rk, 2);
+  const ExactLimbs exact = relinearize_exact_limbs(m, rk, fold ? 0 : 2);
   cudaError_t e = timed("tensor_to_intt", [&] {
     return launch_tensor_to_intt(tables_, params.log_n, L, m, pa.d, pb.d, t3, stream_, own_ext, dp,
-                                 exact);
+                                 exact, fold);
   });
   if (e != cudaSuccess) {
     free_words(t3);
@@ -851,7 +905,8 @@ std::unique_ptr<Data> Engine::relinearized_product(const Data &pa, const Data &p
   const int flag = (pa.flag | pb.flag) & ~kFlagRescaled & ~kFlagNtt;
   auto out = make_data(kUnitCiphertext, flag, m, 2, pa.scale * pb.scale);
   try {
-    relinearize_tail(t3, m, rk, 1, out->d, own_ext);
+    const TensorAddend add = tensor_addend(pa, pb);
+    relinearize_tail(t3, m, rk, 1, out->d, own_ext, fold ? &add : nullptr);
   } catch (...) {
     free_words(t3);
     free_words(own_ext);
@@ -882,14 +937,15 @@ std::unique_ptr<Data> Engine::multiply_relinearize_rescale(const Data &a, const 
       throw std::runtime_error(
           "Rescale Unit Ciphertext: the input unit ciphertext should have a positive level.");
   }
-  int64_t *t3 = alloc_words(static_cast<size_t>(3) * L * params.n);
+  const bool fold = fold_tensor(m, rk);
+  int64_t *t3 = alloc_words(static_cast<size_t>(fold ? 1 : 3) * L * params.n);
   // The tensor's NTT-form third polynomial also lands in ModUp's own limbs.
   int64_t *own_ext = own_limbs_ext(m, rk);
   const DevicePartitions *dp = own_ext ? &partitions(m, rk.moduli_id) : nullptr;
-  const ExactLimbs exact = relinearize_exact_limbs(m, rk, 2);
+  const ExactLimbs exact = relinearize_exact_limbs(m, rk, fold ? 0 : 2);
   cudaError_t e = timed("tensor_to_intt", [&] {
     return launch_tensor_to_intt(tables_, params.log_n, L, m, pa->d, pb->d, t3, stream_, own_ext,
-                                 dp, exact);
+                                 dp, exact, fold);
   });
   if (e != cudaSuccess) {
     free_words(t3);
@@ -900,7 +956,8 @@ std::unique_ptr<Data> Engine::multiply_relinearize_rescale(const Data &a, const 
   const long double scale = params.rescaled_scale(pa->scale * pb->scale, m);
   auto out = make_data(kUnitCiphertext, flag, m + 1, 2, scale);
   try {
-    relinearize_tail(t3, m, rk, 2, out->d, own_ext);
+    const TensorAddend add = tensor_addend(*pa, *pb);
+    relinearize_tail(t3, m, rk, 2, out->d, own_ext, fold ? &add : nullptr);
   } catch (...) {
     free_words(t3);
     free_words(own_ext);

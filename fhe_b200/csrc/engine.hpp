@@ -570,11 +570,18 @@ class Engine {
   // already hold NTT-form words of c1 (see own_limbs_ext); ModUp then skips them.
   void key_switch_pipeline(const int64_t *c1, int moduli_id, const Data &key,
                            const int64_t *rotate_c0, const EpilogueOps &ops, int64_t *out,
-                           const int64_t *decomposed = nullptr, int64_t *own_ext = nullptr);
+                           const int64_t *decomposed = nullptr, int64_t *own_ext = nullptr,
+                           const TensorAddend *addend = nullptr);
   // Key switch tail shared by relinearize variants; t3 is [3][L][N] coefficient
-  // form at moduli_id (poly 2 is switched).
+  // form at moduli_id (poly 2 is switched), or with an addend the switched polynomial
+  // alone, the first two entering through the key inner product (TensorAddend).
   void relinearize_tail(const int64_t *t3, int moduli_id, const Data &rk, int mode, int64_t *out,
-                        int64_t *own_ext = nullptr);
+                        int64_t *own_ext = nullptr, const TensorAddend *addend = nullptr);
+  // Whether a product at moduli_id relinearized with rk folds its first two tensor
+  // polynomials into the key inner product (value transforms on, at most 8
+  // partitions, every prime below 2^60 and none of them special).
+  bool fold_tensor(int moduli_id, const Data &rk);
+  TensorAddend tensor_addend(const Data &pa, const Data &pb) const;
   // ModUp's extended limbs of a partition's own primes are the input limbs' values,
   // so when the input's NTT form exists their NTT needs no work: an extended buffer
   // for relinearizing at moduli_id with rk, to be filled with those NTT-form words,

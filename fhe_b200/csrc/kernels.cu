@@ -338,12 +338,22 @@ template <int P>
 __global__ void __launch_bounds__(256, P == 3 ? 4 : 0)  // three partitions: 4 CTAs/SM without spills
 key_inner_product_fixed_kernel(PrimeTables t, DevicePartitions dp, int log_n, int moduli_id,
                                const int64_t *ext, const int64_t *key, long long poly_row,
-                               KeyRowOffsets rows, int64_t *acc) {
+                               KeyRowOffsets rows, int64_t *acc, TensorAddend add) {
   const long long total = static_cast<long long>(dp.extended) << log_n;
   for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
        i += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const int prime = moduli_id + static_cast<int>(i >> log_n);
+    const int limb = static_cast<int>(i >> log_n);
+    const int prime = moduli_id + limb;
     const uint64_t q = t.q[prime], k = t.k[prime];
+    // The tensor's factors at this word (a normal limb: index i in [poly][limbs][N]).
+    const bool tensor = limb < add.limbs;  // uniform per warp (N >= 32)
+    int64_t ta0 = 0, ta1 = 0, tb0 = 0, tb1 = 0;
+    if (tensor) {
+      ta0 = add.a[i];
+      ta1 = add.a[add.a_stride + i];
+      tb0 = add.b[i];
+      tb1 = add.b[add.b_stride + i];
+    }
     int64_t e[P], k0[P], k1[P];
 #pragma unroll
     for (int p = 0; p < P; p++) {
@@ -360,6 +370,18 @@ key_inner_product_fixed_kernel(PrimeTables t, DevicePartitions dp, int log_n, in
               static_cast<uint32_t>(static_cast<uint64_t>(k1[p]) >> 32);
       w0.add(static_cast<uint64_t>(e[p]), static_cast<uint64_t>(k0[p]));
       w1.add(static_cast<uint64_t>(e[p]), static_cast<uint64_t>(k1[p]));
+    }
+    if (tensor) {
+      high |= static_cast<uint32_t>((static_cast<uint64_t>(ta0) | static_cast<uint64_t>(ta1) |
+                                     static_cast<uint64_t>(tb0) | static_cast<uint64_t>(tb1)) >> 32);
+      // b P as Shoup products (in [0, 2q)), then a0 (b0 P), a0 (b1 P) + a1 (b0 P).
+      const uint64_t pw = static_cast<uint64_t>(add.p_shoup[2 * prime]);
+      const uint64_t pwp = static_cast<uint64_t>(add.p_shoup[2 * prime + 1]);
+      const uint64_t bp0 = shoup_mult(pw, pwp, static_cast<uint64_t>(tb0), q);
+      const uint64_t bp1 = shoup_mult(pw, pwp, static_cast<uint64_t>(tb1), q);
+      w0.add(static_cast<uint64_t>(ta0), bp0);
+      w1.add(static_cast<uint64_t>(ta0), bp1);
+      w1.add(static_cast<uint64_t>(ta1), bp0);
     }
     if ((high >> 29) == 0) {  // every operand below 2^61
       acc[i] = w0.reduce(q, k, q, t.inv_q[prime]);
@@ -379,6 +401,14 @@ key_inner_product_fixed_kernel(PrimeTables t, DevicePartitions dp, int log_n, in
         x0 = guard(guard(a0 + x0, q2), qs);
         x1 = guard(guard(a1 + x1, q2), qs);
       }
+    }
+    if (tensor) {
+      // The same values term by term, for words outside the exact sum's range.
+      const int64_t pr = add.p_mont[prime];
+      const int64_t bp0 = mont_mult(tb0, pr, q, k), bp1 = mont_mult(tb1, pr, q, k);
+      x0 = guard(guard(mont_mult(ta0, bp0, q, k) + x0, q2), qs);
+      x1 = guard(guard(mont_mult(ta0, bp1, q, k) + x1, q2), qs);
+      x1 = guard(guard(mont_mult(ta1, bp0, q, k) + x1, q2), qs);
     }
     acc[i] = x0;
     acc[total + i] = x1;
@@ -463,9 +493,11 @@ struct TensorLoad {
   const int *part_size = nullptr;
   int part_count = 0;
   int extended = 0;
+  bool third_only = false;  // a one-polynomial launch of the third polynomial
   __device__ __forceinline__ int64_t operator()(int poly, int limb, int prime, int gi, int n) const {
     const long long i = static_cast<long long>(limb) * n + gi;
     const uint64_t qq = q[prime], kk = k[prime];
+    if (third_only) poly = 2;
     if (poly == 0) return mont_mult_lazy(a[i], b[i], qq, kk);
     if (poly == 2) {
       const int64_t v = mont_mult_lazy(a[poly_stride + i], b[poly_stride + i], qq, kk);
@@ -588,7 +620,12 @@ cudaError_t launch_extended_ntt(const PrimeTables &t, const DevicePartitions &dp
 
 cudaError_t launch_key_inner_product(const PrimeTables &t, const DevicePartitions &dp, int n,
                                      int moduli_id, const int64_t *ext, const int64_t *key,
-                                     int key_primes, int view_offset, int64_t *acc, cudaStream_t s) {
+                                     int key_primes, int view_offset, int64_t *acc, cudaStream_t s,
+                                     const TensorAddend &addend) {
+  if (addend.limbs > 0 &&
+      (dp.count > 8 || addend.limbs > dp.extended || addend.a == nullptr || addend.b == nullptr ||
+       addend.p_shoup == nullptr || addend.p_mont == nullptr))
+    return cudaErrorInvalidValue;
   if (dp.count >= 1 && dp.count <= 8) {
     KeyRowOffsets rows;
     for (int p = 0; p < dp.count; p++)
@@ -601,7 +638,7 @@ cudaError_t launch_key_inner_product(const PrimeTables &t, const DevicePartition
 #define FHE_KIP_CASE(P)                                                                           \
   case P:                                                                                         \
     key_inner_product_fixed_kernel<P><<<grid, kThreads, 0, s>>>(t, dp, log_n, moduli_id, ext, key, \
-                                                                poly_row, rows, acc);            \
+                                                                poly_row, rows, acc, addend);    \
     break;
       FHE_KIP_CASE(1) FHE_KIP_CASE(2) FHE_KIP_CASE(3) FHE_KIP_CASE(4)
       FHE_KIP_CASE(5) FHE_KIP_CASE(6) FHE_KIP_CASE(7) FHE_KIP_CASE(8)
@@ -721,9 +758,11 @@ cudaError_t launch_ntt_plain(const PrimeTables &t, int log_n, int polys, int lim
 cudaError_t launch_tensor_to_intt(const PrimeTables &t, int log_n, int limbs, int prime_base,
                                   const int64_t *a, const int64_t *b, int64_t *y, cudaStream_t s,
                                   int64_t *own_ext, const DevicePartitions *dp,
-                                  const ExactLimbs &exact) {
+                                  const ExactLimbs &exact, bool third_only) {
   const long long stride = static_cast<long long>(limbs) << log_n;
+  const int polys = third_only ? 1 : 3;
   TensorLoad ld{a, b, stride, t.q, t.k};
+  ld.third_only = third_only;
   if (own_ext != nullptr) {
     if (dp == nullptr) return cudaErrorInvalidValue;
     ld.own_ext = own_ext;
@@ -734,11 +773,11 @@ cudaError_t launch_tensor_to_intt(const PrimeTables &t, int log_n, int limbs, in
   }
   if (exact.poly == ExactLimbs::kAllExact) {
     EnterExitStore<false> st{y, stride, t.n_inverse, t.q, t.k};
-    return inverse_ntt(log_n, 3, limbs, prime_base, t, ld, st, y, stride, s);
+    return inverse_ntt(log_n, polys, limbs, prime_base, t, ld, st, y, stride, s);
   }
   MixedExitStore st{y, stride, t.n_inverse, t.q, t.k, t.exit_shoup, exact};
-  return inverse_ntt<TensorLoad, MixedExitStore, kNttMixed>(log_n, 3, limbs, prime_base, t, ld, st, y,
-                                                            stride, s, exact);
+  return inverse_ntt<TensorLoad, MixedExitStore, kNttMixed>(log_n, polys, limbs, prime_base, t, ld,
+                                                            st, y, stride, s, exact);
 }
 
 }  // namespace fhe_b200

@@ -63,6 +63,7 @@ struct KeySwitchTables {
   const int64_t *rescale_enter_shoup;
   const int64_t *r_mod;             // [P] R mod q: the rounder's 1 after the enter
   const int64_t *p_product_mult_r;  // [P] P mod q * R (zero for the special primes)
+  const int64_t *p_shoup;           // [P][2] (P mod q, floor((P mod q) 2^64 / q))
   int prime_count;
   int special_count;
 };
@@ -116,13 +117,31 @@ struct KeyRowOffsets {
   long long off[8] = {};
 };
 
+// The first two polynomials of a tensor, folded into a relinearization's key inner
+// product instead of being added after ModDown: ModDown is linear and P = prod p_s is
+// zero modulo every special prime, so ModDown(acc + P d) = ModDown(acc) + d, and a
+// relinearization reads its addends (and returns its words) only modulo q.  With
+// the NTT-form factors a, b of the product, d0 = a0 b0 and d1 = a0 b1 + a1 b0
+// (Montgomery products); acc0 gains a0 (b0 P) and acc1 a0 (b1 P) + a1 (b0 P) inside
+// the exact sum before its one REDC, which makes them P d0 and P d1.
+struct TensorAddend {
+  const int64_t *a = nullptr;  // [2][limbs][N] NTT form, poly stride a_stride
+  const int64_t *b = nullptr;  // [2][limbs][N] NTT form, poly stride b_stride
+  long long a_stride = 0;
+  long long b_stride = 0;
+  const int64_t *p_shoup = nullptr;  // [P][2]: (P mod q, floor((P mod q) 2^64 / q)) by prime
+  const int64_t *p_mont = nullptr;   // [P]: P R mod q by prime (KeySwitchTables::p_product_mult_r)
+  int limbs = 0;                     // the normal limbs; 0: no addend
+};
+
 // Key inner product (core_key_switch.cpp:320-349): acc[2][E][N] = sum over
 // partitions of ext_p * (key_{2i}, key_{2i+1}), reference reduction pattern.
 // key is [2*dnum_key][key_primes][N]; view_offset = moduli_id - key_moduli_id.
+// An addend (up to 8 partitions) adds the tensor's P d0, P d1 on the normal limbs.
 cudaError_t launch_key_inner_product(const PrimeTables &t, const DevicePartitions &dp, int n,
                                      int moduli_id, const int64_t *ext, const int64_t *key,
                                      int key_primes, int view_offset, int64_t *acc,
-                                     cudaStream_t s);
+                                     cudaStream_t s, const TensorAddend &addend = TensorAddend{});
 
 // Inverse NTT of both accumulators, then to_intt_ scaling and reduce_2q_to_q
 // (mod_down, core_key_switch.cpp:110-121), in place.
@@ -385,10 +404,14 @@ cudaError_t launch_ntt_plain(const PrimeTables &t, int log_n, int polys, int lim
 // NTT-form words of the third polynomial are also written to each partition's own
 // limbs of the extended buffer own_ext [count][E][N] (ModUp with skip_own).  Limbs
 // outside `exact` are transformed value-only, as in launch_rescale_to_ntt.
+// With third_only, y is [1][L][N] and receives the third polynomial alone (its first
+// two then go to the key inner product as a TensorAddend); `exact` names its
+// polynomial as 0.
 cudaError_t launch_tensor_to_intt(const PrimeTables &t, int log_n, int limbs, int prime_base,
                                   const int64_t *a, const int64_t *b, int64_t *y,
                                   cudaStream_t s, int64_t *own_ext = nullptr,
                                   const DevicePartitions *dp = nullptr,
-                                  const ExactLimbs &exact = ExactLimbs{ExactLimbs::kAllExact, 0});
+                                  const ExactLimbs &exact = ExactLimbs{ExactLimbs::kAllExact, 0},
+                                  bool third_only = false);
 
 }  // namespace fhe_b200

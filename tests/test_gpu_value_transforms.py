@@ -7,8 +7,12 @@ first limb of the tensor's third polynomial (Garner's first digit), or all of a
 partition's limbs where its first prime exceeds twice another of its primes (the
 60-bit first prime of the top level).  With the switch on (the default) the inputs'
 rescale-and-transform and the tensor's inverse transform take Harvey's butterflies
-on Shoup twiddles on the other limbs; off, every limb is exact.  The recorded
-reference digests run with the switch on."""
+on Shoup twiddles on the other limbs, and the tensor's first two polynomials are
+folded into the key inner product as P d0, P d1 (ModDown(acc + P d) = ModDown(acc)
++ d) instead of being transformed and added after ModDown; off, every limb is exact
+and the addend is added in ModDown's store.  At the top level of the 10-special-prime
+chain the first prime is also a special prime, so P vanishes modulo it and the fold
+is not taken there.  The recorded reference digests run with the switch on."""
 import numpy as np
 import pytest
 
