@@ -180,22 +180,26 @@ def kernel_bytes(L: int, E: int, dnum: int, n: int) -> dict:
     relinearize level (L limbs, E = L + K extended limbs): each limb operand read or
     written once, twiddle tables excluded.  Each partition's own L limbs of the
     extended polynomials are written by the tensor-product pass from the input's NTT
-    form, so ModUp writes and transforms the other dnum * E - L."""
+    form, so ModUp writes and transforms the other dnum * E - L.  The tensor's first
+    two polynomials enter the key inner product as P d0, P d1 (the engine's default
+    on this chain), so the tensor pass transforms the third alone and the ModDown
+    epilogue adds nothing."""
     limb = 8 * n
     up = dnum * E - L
     return {
         "rescale": (2 * (L + 1) + 2 * L) * limb,          # 2 polys, L+1 -> L limbs
         "to_ntt": 2 * 4 * L * limb,                         # 4 polys in and out
         "rescale_to_ntt": (2 * (L + 1) + 2 * L) * limb,     # one input: rescaled, NTT
-        "tensor_to_intt": (4 * L + 3 * L) * limb,           # 4 NTT polys in, 3 out
+        "tensor_to_intt": (2 * L + L + L) * limb,           # a1, b1 in; d2 out, its own limbs
         "mixed_radix": 2 * L * limb,                        # digits of poly 2
         "mod_up_ntt": (L + up) * limb,                      # digits in, extended out
         "mod_up_contract_tc": (L + up) * limb,              # digits in, extended out
         "mod_up_ntt_tc": 2 * up * limb,                     # extended limbs in and out
-        "key_inner_product": (3 * dnum * E + 2 * E) * limb, # ext + 2 key polys, 2 out
+        # ext + 2 key polys + the 4 NTT-form factors in, 2 out
+        "key_inner_product": (3 * dnum * E + 4 * L + 2 * E) * limb,
         "mod_down_intt": 2 * 2 * E * limb,                  # 2 polys in and out
-        "mod_down_epilogue": (2 * E + 2 * L + 2 * (L - 1)) * limb,
-        "mod_down_epilogue_tc": (2 * E + 2 * L + 2 * (L - 1)) * limb,
+        "mod_down_epilogue": (2 * E + 2 * (L - 1)) * limb,
+        "mod_down_epilogue_tc": (2 * E + 2 * (L - 1)) * limb,
     }
 
 
@@ -221,8 +225,9 @@ def pipe_figures(prof: dict, steps: int, pairs: int, n: int, L: int, K: int, sm_
     log_n = n.bit_length() - 1
     bfly_per_limb = (n // 2) * log_n
     # ModUp transforms every extended limb but each partition's own (L in all), whose
-    # NTT-form words the tensor's loader provides.
-    transforms = {"rescale_to_ntt": 4 * L, "tensor_to_intt": 3 * L, "mod_up_ntt_tc": dnum * E - L,
+    # NTT-form words the tensor's loader provides; the tensor pass transforms its
+    # third polynomial alone (the first two enter the key inner product).
+    transforms = {"rescale_to_ntt": 4 * L, "tensor_to_intt": L, "mod_up_ntt_tc": dnum * E - L,
                   "mod_down_intt": 2 * E}
     integer = {}
     for fam, limbs in transforms.items():
