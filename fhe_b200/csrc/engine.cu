@@ -798,9 +798,13 @@ std::unique_ptr<Data> Engine::relinearize(const Data &ct, const Data &rk) {
   }
   const int m = x->moduli_id;
   const int L = x->chains;
-  int64_t *t3 = alloc_words(static_cast<size_t>(3) * L * params.n);
+  // With the fold, c0 and c1 enter the key inner product as P c0, P c1 and only c2 is
+  // transformed back.
+  const bool fold = fold_tensor(m, rk);
+  int64_t *t3 = alloc_words(static_cast<size_t>(fold ? 1 : 3) * L * params.n);
   cudaError_t e = timed("to_intt", [&] {
-    return launch_to_intt(tables_, params.log_n, 3, L, m, x->d, x->poly_stride(), t3,
+    return launch_to_intt(tables_, params.log_n, fold ? 1 : 3, L, m,
+                          x->d + (fold ? 2 * x->poly_stride() : 0), x->poly_stride(), t3,
                           static_cast<long long>(L) * params.n, stream_);
   });
   if (e != cudaSuccess) {
@@ -822,7 +826,13 @@ std::unique_ptr<Data> Engine::relinearize(const Data &ct, const Data &rk) {
                               cudaMemcpyDeviceToDevice, stream_),
               "copy own limbs");
     }
-    relinearize_tail(t3, m, rk, 1, out->d, own_ext);
+    TensorAddend add;
+    add.a = x->d;
+    add.a_stride = x->poly_stride();
+    add.p_shoup = ks_.p_shoup;
+    add.p_mont = ks_.p_product_mult_r;
+    add.limbs = L;
+    relinearize_tail(t3, m, rk, 1, out->d, own_ext, fold ? &add : nullptr);
   } catch (...) {
     free_words(t3);
     free_words(own_ext);

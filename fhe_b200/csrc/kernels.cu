@@ -348,11 +348,14 @@ key_inner_product_fixed_kernel(PrimeTables t, DevicePartitions dp, int log_n, in
     // The tensor's factors at this word (a normal limb: index i in [poly][limbs][N]).
     const bool tensor = limb < add.limbs;  // uniform per warp (N >= 32)
     int64_t ta0 = 0, ta1 = 0, tb0 = 0, tb1 = 0;
+    const bool product = add.b != nullptr;
     if (tensor) {
       ta0 = add.a[i];
       ta1 = add.a[add.a_stride + i];
-      tb0 = add.b[i];
-      tb1 = add.b[add.b_stride + i];
+      if (product) {
+        tb0 = add.b[i];
+        tb1 = add.b[add.b_stride + i];
+      }
     }
     int64_t e[P], k0[P], k1[P];
 #pragma unroll
@@ -374,14 +377,20 @@ key_inner_product_fixed_kernel(PrimeTables t, DevicePartitions dp, int log_n, in
     if (tensor) {
       high |= static_cast<uint32_t>((static_cast<uint64_t>(ta0) | static_cast<uint64_t>(ta1) |
                                      static_cast<uint64_t>(tb0) | static_cast<uint64_t>(tb1)) >> 32);
-      // b P as Shoup products (in [0, 2q)), then a0 (b0 P), a0 (b1 P) + a1 (b0 P).
-      const uint64_t pw = static_cast<uint64_t>(add.p_shoup[2 * prime]);
-      const uint64_t pwp = static_cast<uint64_t>(add.p_shoup[2 * prime + 1]);
-      const uint64_t bp0 = shoup_mult(pw, pwp, static_cast<uint64_t>(tb0), q);
-      const uint64_t bp1 = shoup_mult(pw, pwp, static_cast<uint64_t>(tb1), q);
-      w0.add(static_cast<uint64_t>(ta0), bp0);
-      w1.add(static_cast<uint64_t>(ta0), bp1);
-      w1.add(static_cast<uint64_t>(ta1), bp0);
+      if (product) {
+        // b P as Shoup products (in [0, 2q)), then a0 (b0 P), a0 (b1 P) + a1 (b0 P).
+        const uint64_t pw = static_cast<uint64_t>(add.p_shoup[2 * prime]);
+        const uint64_t pwp = static_cast<uint64_t>(add.p_shoup[2 * prime + 1]);
+        const uint64_t bp0 = shoup_mult(pw, pwp, static_cast<uint64_t>(tb0), q);
+        const uint64_t bp1 = shoup_mult(pw, pwp, static_cast<uint64_t>(tb1), q);
+        w0.add(static_cast<uint64_t>(ta0), bp0);
+        w1.add(static_cast<uint64_t>(ta0), bp1);
+        w1.add(static_cast<uint64_t>(ta1), bp0);
+      } else {
+        const uint64_t pr = static_cast<uint64_t>(add.p_mont[prime]);  // P R mod q, below q
+        w0.add(static_cast<uint64_t>(ta0), pr);
+        w1.add(static_cast<uint64_t>(ta1), pr);
+      }
     }
     if ((high >> 29) == 0) {  // every operand below 2^61
       acc[i] = w0.reduce(q, k, q, t.inv_q[prime]);
@@ -405,10 +414,15 @@ key_inner_product_fixed_kernel(PrimeTables t, DevicePartitions dp, int log_n, in
     if (tensor) {
       // The same values term by term, for words outside the exact sum's range.
       const int64_t pr = add.p_mont[prime];
-      const int64_t bp0 = mont_mult(tb0, pr, q, k), bp1 = mont_mult(tb1, pr, q, k);
-      x0 = guard(guard(mont_mult(ta0, bp0, q, k) + x0, q2), qs);
-      x1 = guard(guard(mont_mult(ta0, bp1, q, k) + x1, q2), qs);
-      x1 = guard(guard(mont_mult(ta1, bp0, q, k) + x1, q2), qs);
+      if (product) {
+        const int64_t bp0 = mont_mult(tb0, pr, q, k), bp1 = mont_mult(tb1, pr, q, k);
+        x0 = guard(guard(mont_mult(ta0, bp0, q, k) + x0, q2), qs);
+        x1 = guard(guard(mont_mult(ta0, bp1, q, k) + x1, q2), qs);
+        x1 = guard(guard(mont_mult(ta1, bp0, q, k) + x1, q2), qs);
+      } else {
+        x0 = guard(guard(mont_mult(ta0, pr, q, k) + x0, q2), qs);
+        x1 = guard(guard(mont_mult(ta1, pr, q, k) + x1, q2), qs);
+      }
     }
     acc[i] = x0;
     acc[total + i] = x1;
@@ -623,7 +637,7 @@ cudaError_t launch_key_inner_product(const PrimeTables &t, const DevicePartition
                                      int key_primes, int view_offset, int64_t *acc, cudaStream_t s,
                                      const TensorAddend &addend) {
   if (addend.limbs > 0 &&
-      (dp.count > 8 || addend.limbs > dp.extended || addend.a == nullptr || addend.b == nullptr ||
+      (dp.count > 8 || addend.limbs > dp.extended || addend.a == nullptr ||
        addend.p_shoup == nullptr || addend.p_mont == nullptr))
     return cudaErrorInvalidValue;
   if (dp.count >= 1 && dp.count <= 8) {

@@ -123,10 +123,12 @@ struct KeyRowOffsets {
 // relinearization reads its addends (and returns its words) only modulo q.  With
 // the NTT-form factors a, b of the product, d0 = a0 b0 and d1 = a0 b1 + a1 b0
 // (Montgomery products); acc0 gains a0 (b0 P) and acc1 a0 (b1 P) + a1 (b0 P) inside
-// the exact sum before its one REDC, which makes them P d0 and P d1.
+// the exact sum before its one REDC, which makes them P d0 and P d1.  Without b, a is
+// a three-polynomial text being relinearized and acc gains a0 (P R), a1 (P R), which
+// the REDC makes P a0, P a1.
 struct TensorAddend {
   const int64_t *a = nullptr;  // [2][limbs][N] NTT form, poly stride a_stride
-  const int64_t *b = nullptr;  // [2][limbs][N] NTT form, poly stride b_stride
+  const int64_t *b = nullptr;  // [2][limbs][N] NTT form, poly stride b_stride; or null
   long long a_stride = 0;
   long long b_stride = 0;
   const int64_t *p_shoup = nullptr;  // [P][2]: (P mod q, floor((P mod q) 2^64 / q)) by prime

@@ -10,7 +10,8 @@ rescale-and-transform and the tensor's inverse transform take Harvey's butterfli
 on Shoup twiddles on the other limbs, and the tensor's first two polynomials are
 folded into the key inner product as P d0, P d1 (ModDown(acc + P d) = ModDown(acc)
 + d) instead of being transformed and added after ModDown; off, every limb is exact
-and the addend is added in ModDown's store.  At the top level of the 10-special-prime
+and the addend is added in ModDown's store.  A three-polynomial text being
+relinearized has its c0, c1 folded the same way (P c0, P c1).  At the top level of the 10-special-prime
 chain the first prime is also a special prime, so P vanishes modulo it and the fold
 is not taken there.  The recorded reference digests run with the switch on."""
 import numpy as np
@@ -66,9 +67,15 @@ def test_value_transforms_give_the_same_words(engines, log_n, K, preset, mids):
         key = uniform_limbs(rng, e.moduli[mid:], 2 * e.partition_count(mid), n)
         rk = e.upload(key, mid, NTT | SPECIAL, RELIN)
         la, lb = lazy(rng, a, moduli), lazy(rng, b, moduli)
+        t3 = uniform_limbs(rng, moduli, 3, n)
+        lt3 = lazy(rng, t3, moduli)
 
         def ops():
             out = []
+            for c in (t3, lt3):
+                # A three-polynomial text: its c0, c1 enter the key inner product.
+                out.append(e.relinearize(e.upload(c, mid, NTT), rk).download())
+                out.append(e.relinearize(e.upload(c, mid), rk).download())
             for x, y in ((a, b), (la, lb)):
                 if e.chain_count - mid >= 2:
                     # Rescaled inputs are transformed as they are: the product is at `mid`.
