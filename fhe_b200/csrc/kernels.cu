@@ -530,6 +530,36 @@ struct TensorLoad {
   }
 };
 
+// The tensor's third polynomial d2 = a1 b1 as a streaming pass before a plain mixed
+// inverse transform (TensorLoad's words, with 16-byte accesses by a full grid: the
+// loader pass of d2 alone waits on its loads and fills under one wave), and its
+// NTT-form words into each partition's own limbs of ModUp's extended buffer when one
+// is given.  Same words either way.
+__global__ void __launch_bounds__(256)
+    tensor_third_kernel(PrimeTables t, TensorLoad ld, int log_n, int limbs, int prime_base,
+                        int64_t *y) {
+  const long long pairs = static_cast<long long>(limbs) << (log_n - 1);
+  const long long n = 1LL << log_n;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < pairs;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long w = 2 * i;
+    const int limb = static_cast<int>(w >> log_n);
+    const int prime = prime_base + limb;
+    const uint64_t q = t.q[prime], k = t.k[prime];
+    const longlong2 a = *reinterpret_cast<const longlong2 *>(ld.a + ld.poly_stride + w);
+    const longlong2 b = *reinterpret_cast<const longlong2 *>(ld.b + ld.poly_stride + w);
+    longlong2 v;
+    v.x = mont_mult_lazy(a.x, b.x, q, k);
+    v.y = mont_mult_lazy(a.y, b.y, q, k);
+    *reinterpret_cast<longlong2 *>(y + w) = v;
+    if (ld.own_ext != nullptr) {
+      int p = 0;
+      while (p + 1 < ld.part_count && limb >= ld.part_start[p] + ld.part_size[p]) p++;
+      *reinterpret_cast<longlong2 *>(ld.own_ext + (static_cast<long long>(p) * ld.extended) * n + w) = v;
+    }
+  }
+}
+
 }  // namespace
 
 // ============================================================ launchers ==
@@ -790,6 +820,21 @@ cudaError_t launch_tensor_to_intt(const PrimeTables &t, int log_n, int limbs, in
     return inverse_ntt(log_n, polys, limbs, prime_base, t, ld, st, y, stride, s);
   }
   MixedExitStore st{y, stride, t.n_inverse, t.q, t.k, t.exit_shoup, exact};
+  const bool aligned = (reinterpret_cast<uintptr_t>(a) & 15) == 0 &&
+                       (reinterpret_cast<uintptr_t>(b) & 15) == 0 &&
+                       (reinterpret_cast<uintptr_t>(y) & 15) == 0 &&
+                       (own_ext == nullptr || (reinterpret_cast<uintptr_t>(own_ext) & 15) == 0);
+  if (third_only && log_n >= 9 && aligned) {
+    // d2 first, then a plain mixed inverse transform in place.
+    note_launch();
+    tensor_third_kernel<<<blocks_for(static_cast<long long>(limbs) << (log_n - 1)), kThreads, 0, s>>>(
+        t, ld, log_n, limbs, prime_base, y);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    PlainLoad pl{y, stride};
+    return inverse_ntt<PlainLoad, MixedExitStore, kNttMixed>(log_n, 1, limbs, prime_base, t, pl, st, y,
+                                                             stride, s, exact);
+  }
   return inverse_ntt<TensorLoad, MixedExitStore, kNttMixed>(log_n, polys, limbs, prime_base, t, ld,
                                                             st, y, stride, s, exact);
 }

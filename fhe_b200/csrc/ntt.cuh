@@ -109,9 +109,9 @@ struct RescaleEnterLoad {
   __device__ __forceinline__ int64_t operator()(int poly, int limb, int prime, int gi, int n) const {
     const int64_t *s = src + poly * poly_stride;
     const int64_t x0 = s[gi];
+    const int64_t xj = s[static_cast<long long>(limb + 1) * n + gi];
     const int64_t rounder = static_cast<uint64_t>(x0) > (q[prime - limb - 1] >> 1) ? 1 : 0;
     const uint64_t qq = q[prime], kk = k[prime];
-    const int64_t xj = s[static_cast<long long>(limb + 1) * n + gi];
     if (MIXED && !exact.exact(poly, limb)) {
       const int64_t q2 = static_cast<int64_t>(qq << 1);
       int64_t d = xj - x0;
