@@ -561,6 +561,14 @@ static void mod_down(const oracle_ctx *c, int mid, int64_t *x, int64_t *y) {
   }
 }
 
+void oracle_mod_down(const oracle_ctx *c, int mid, const int64_t *x, int64_t *out) {
+  const size_t words = (size_t)(c->prime_count - mid) * c->n;
+  int64_t *w = malloc(sizeof(int64_t) * words);
+  memcpy(w, x, sizeof(int64_t) * words);
+  mod_down(c, mid, w, out);
+  free(w);
+}
+
 /* create_key_switcher (K > 1, core_key_switch.cpp:293-358) and
  * create_key_switcher_single (K == 1, core_key_switch.cpp:225-291). */
 void oracle_key_switch(const oracle_ctx *c, int mid, const int64_t *x, int key_mid,

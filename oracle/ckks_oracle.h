@@ -69,6 +69,11 @@ void oracle_tensor(const oracle_ctx *ctx, int moduli_id, const int64_t *a,
 void oracle_relinearize(const oracle_ctx *ctx, int moduli_id, const int64_t *ct,
                         int key_moduli_id, const int64_t *key, int64_t *out);
 
+/* mod_down (core_key_switch.cpp:110-160) of one NTT-form polynomial x of
+ * prime_count(moduli_id) limbs (copied, not modified); out is its L canonical
+ * coefficient-form limbs. */
+void oracle_mod_down(const oracle_ctx *ctx, int moduli_id, const int64_t *x, int64_t *out);
+
 /* Key switch of one coefficient-form polynomial x (L limbs at moduli_id) with a
  * key switching key: create_key_switcher_from_intt (core_key_switch.cpp:410);
  * out is [2][L][N]. */

@@ -66,6 +66,8 @@ def lib():
         L.oracle_relinearize.argtypes = [ctypes.c_void_p, ctypes.c_int, _i64p, ctypes.c_int, _i64p, _i64p]
         L.oracle_key_switch.restype = None
         L.oracle_key_switch.argtypes = [ctypes.c_void_p, ctypes.c_int, _i64p, ctypes.c_int, _i64p, _i64p]
+        L.oracle_mod_down.restype = None
+        L.oracle_mod_down.argtypes = [ctypes.c_void_p, ctypes.c_int, _i64p, _i64p]
         L.oracle_rescale.restype = None
         L.oracle_rescale.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _i64p, _i64p]
         L.oracle_mult_relin_rescale.restype = None
@@ -267,6 +269,14 @@ class Context:
         L = self.chains(moduli_id)
         out = np.empty((2, L, self.n), dtype=np.int64)
         lib().oracle_key_switch(self._ctx, moduli_id, _p(x), key_moduli_id, _p(key), _p(out))
+        return out
+
+    def mod_down(self, moduli_id, x):
+        """mod_down (core_key_switch.cpp:110-160) of one NTT-form polynomial of all the
+        primes at moduli_id: its chains(moduli_id) canonical coefficient-form limbs."""
+        x = np.ascontiguousarray(x, dtype=np.int64)
+        out = np.empty((self.chains(moduli_id), self.n), dtype=np.int64)
+        lib().oracle_mod_down(self._ctx, moduli_id, _p(x), _p(out))
         return out
 
     def rescale(self, moduli_id, x):
