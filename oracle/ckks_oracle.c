@@ -561,6 +561,17 @@ static void mod_down(const oracle_ctx *c, int mid, int64_t *x, int64_t *y) {
   }
 }
 
+void oracle_mixed_radix(const oracle_ctx *c, int mid, int key_mid, const int64_t *x, int64_t *out) {
+  partition_t parts[64];
+  const int pcount = make_partitions(c, mid, key_mid, parts);
+  for (int pi = 0; pi < pcount; pi++) {
+    partition_params_t pp;
+    make_partition_params(c, mid, &parts[pi], &pp);
+    rns_to_mrs(c, mid, x, &parts[pi], &pp, out + (size_t)parts[pi].start * c->n);
+    free(pp.prod_r2);
+  }
+}
+
 void oracle_mod_down(const oracle_ctx *c, int mid, const int64_t *x, int64_t *out) {
   const size_t words = (size_t)(c->prime_count - mid) * c->n;
   int64_t *w = malloc(sizeof(int64_t) * words);

@@ -69,6 +69,13 @@ void oracle_tensor(const oracle_ctx *ctx, int moduli_id, const int64_t *a,
 void oracle_relinearize(const oracle_ctx *ctx, int moduli_id, const int64_t *ct,
                         int key_moduli_id, const int64_t *key, int64_t *out);
 
+/* rns_to_mrs (core_key_switch.cpp:21-56) of every key-switching partition of the
+ * coefficient-form polynomial x (L limbs at moduli_id, partitions for a key at
+ * key_moduli_id, K > 1): out[limb] holds the digit of the limb's partition at the
+ * limb's position, [L][N]. */
+void oracle_mixed_radix(const oracle_ctx *ctx, int moduli_id, int key_moduli_id,
+                        const int64_t *x, int64_t *out);
+
 /* mod_down (core_key_switch.cpp:110-160) of one NTT-form polynomial x of
  * prime_count(moduli_id) limbs (copied, not modified); out is its L canonical
  * coefficient-form limbs. */

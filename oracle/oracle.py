@@ -68,6 +68,8 @@ def lib():
         L.oracle_key_switch.argtypes = [ctypes.c_void_p, ctypes.c_int, _i64p, ctypes.c_int, _i64p, _i64p]
         L.oracle_mod_down.restype = None
         L.oracle_mod_down.argtypes = [ctypes.c_void_p, ctypes.c_int, _i64p, _i64p]
+        L.oracle_mixed_radix.restype = None
+        L.oracle_mixed_radix.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _i64p, _i64p]
         L.oracle_rescale.restype = None
         L.oracle_rescale.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _i64p, _i64p]
         L.oracle_mult_relin_rescale.restype = None
@@ -269,6 +271,14 @@ class Context:
         L = self.chains(moduli_id)
         out = np.empty((2, L, self.n), dtype=np.int64)
         lib().oracle_key_switch(self._ctx, moduli_id, _p(x), key_moduli_id, _p(key), _p(out))
+        return out
+
+    def mixed_radix(self, moduli_id, key_moduli_id, x):
+        """rns_to_mrs (core_key_switch.cpp:21-56) of every partition of the
+        coefficient-form polynomial x: each limb's digit at the limb's position (K > 1)."""
+        x = np.ascontiguousarray(x, dtype=np.int64)
+        out = np.empty((self.chains(moduli_id), self.n), dtype=np.int64)
+        lib().oracle_mixed_radix(self._ctx, moduli_id, key_moduli_id, _p(x), _p(out))
         return out
 
     def mod_down(self, moduli_id, x):
