@@ -891,8 +891,9 @@ ExactLimbs Engine::relinearize_exact_limbs(int moduli_id, const Data &rk, int po
 
 std::unique_ptr<Data> Engine::relinearized_product(const Data &pa, const Data &pb, const Data &rk) {
   // multiply (core.cpp:284-314) then relinearize (core.cpp:713-741) of prepared
-  // NTT-form inputs: the tensor is formed inside the inverse NTT's load, so its three
-  // NTT-form polynomials are never written.
+  // NTT-form inputs: the tensor's NTT-form polynomials are formed on the way into
+  // the inverse NTT (all three) or, with the fold, into the key inner product (d0,
+  // d1) and a streaming pass before d2's inverse NTT.
   const int m = pa.moduli_id;
   const int L = pa.chains;
   // With the fold, only the third polynomial is transformed; the first two go to the

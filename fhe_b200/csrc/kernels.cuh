@@ -407,8 +407,8 @@ cudaError_t launch_ntt_plain(const PrimeTables &t, int log_n, int polys, int lim
 // limbs of the extended buffer own_ext [count][E][N] (ModUp with skip_own).  Limbs
 // outside `exact` are transformed value-only, as in launch_rescale_to_ntt.
 // With third_only, y is [1][L][N] and receives the third polynomial alone (its first
-// two then go to the key inner product as a TensorAddend); `exact` names its
-// polynomial as 0.
+// two then go to the key inner product as a TensorAddend), formed by a streaming pass
+// before the transform; `exact` names its polynomial as 0.
 cudaError_t launch_tensor_to_intt(const PrimeTables &t, int log_n, int limbs, int prime_base,
                                   const int64_t *a, const int64_t *b, int64_t *y,
                                   cudaStream_t s, int64_t *own_ext = nullptr,
