@@ -98,3 +98,28 @@ def test_value_transforms_give_the_same_words(engines, log_n, K, preset, mids):
             assert len(fast) == len(exact) > 0
             for i, (got, want) in enumerate(zip(fast, exact)):
                 assert np.array_equal(got, want), (mid, tc, i)
+
+
+@pytest.mark.parametrize("log_n,K,preset,key_mid,mid", [(16, 10, 1, 1, 5), (16, 4, 2, 2, 9)],
+                         ids=lambda v: str(v))
+def test_value_transforms_with_a_key_above_the_text(engines, log_n, K, preset, key_mid, mid):
+    """A relinearization key made at a higher level than the texts: the partitions'
+    key rows are offset, the folded addend and the exact limbs are not."""
+    e = engines(log_n, K, preset)
+    n = e.coeff_count
+    rng = np.random.default_rng(7300 + 100 * log_n + 10 * key_mid + mid)
+    moduli = e.moduli[mid:e.chain_count]
+    a = uniform_limbs(rng, moduli, 2, n)
+    b = uniform_limbs(rng, moduli, 2, n)
+    t3 = uniform_limbs(rng, moduli, 3, n)
+    key = uniform_limbs(rng, e.moduli[key_mid:], 2 * e.partition_count(key_mid), n)
+    rk = e.upload(key, key_mid, NTT | SPECIAL, RELIN)
+
+    def ops():
+        return [e.multiply_relinearize_rescale(e.upload(a, mid), e.upload(b, mid), rk).download(),
+                e.multiply(e.upload(a, mid, RESCALED), e.upload(b, mid, RESCALED), rk).download(),
+                e.relinearize(e.upload(t3, mid, NTT), rk).download()]
+
+    fast, exact = both(e, ops)
+    for i, (got, want) in enumerate(zip(fast, exact)):
+        assert np.array_equal(got, want), i
